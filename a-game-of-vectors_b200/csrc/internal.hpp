@@ -1,0 +1,125 @@
+// internal.hpp — device-resident index, per-call workspace and kernel launchers.
+#pragma once
+
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/sieve_gpu.h"
+
+namespace sg {
+
+// Blocks (32 slots) a scan work item covers at most; the scan CTA holds one chunk's estimates.
+constexpr uint32_t kChunkBlocks = 64;
+// Largest cand / k / r the select kernels sort in shared memory.
+constexpr uint32_t kMaxCand = 4096;
+// Status bits a kernel raises in Workspace::status.
+constexpr uint32_t kStatusOverflow = 1u;   // a candidate buffer filled up (query is retried)
+constexpr uint32_t kStatusWindow = 2u;     // a BF16 routing window exceeded its buffer
+
+// HBM layout of one IVF index (all arrays on the index's device).
+struct DevIndex {
+  int device = 0;
+  uint32_t k = 0;
+  uint64_t n = 0, nblocks = 0, nslots = 0;
+  float* cent = nullptr;             // [k*256] centroids.f32
+  float* cent_t = nullptr;           // [256*k] transposed, for the exact routing kernel
+  __nv_bfloat16* cent_bf16 = nullptr;  // [k*256] BF16 copy for the tensor-core routing GEMM
+  float cent_norm_max = 0.0f;
+  uint32_t* block_off = nullptr;     // [k+1] first block of each cluster
+  uint32_t* clen = nullptr;          // [k] real (non-PAD) slots of each cluster
+  uint8_t* blocks = nullptr;         // [nblocks*1024] nibble-transposed codes (blocks.bin)
+  float* mul = nullptr;              // [nslots] factors.f32 [.., 0]
+  float* err = nullptr;              // [nslots] factors.f32 [.., 1]
+  uint32_t* ids = nullptr;           // [nslots] ids.u32
+  float* rot = nullptr;              // [768] rotation.f32
+  float rot_norm = 0.0f;             // (256 as f32).powf(-1.5)
+  bool has_t2 = false;
+  float* t2_sigma = nullptr;         // [256]
+  uint8_t* t2_codes = nullptr;       // [n*64]
+  float* t2_norm = nullptr;          // [n]
+  int8_t* rerank = nullptr;          // [n*768]
+  float* norm256 = nullptr;          // [n]
+  float* qscale = nullptr;           // [768]
+  std::vector<uint64_t> h_block_off;
+  std::vector<uint32_t> h_clen;
+  std::vector<uint32_t> h_chunks_desc_prefix;  // prefix sums of per-cluster chunk counts, largest first
+  int route_precision = SG_ROUTE_BF16;
+};
+
+// Device buffers of one batched call, grown on demand and reused.
+struct Workspace {
+  uint32_t nq_cap = 0, P_cap = 0, cand_cap = 0, k_cap = 0, r_cap = 0;
+  uint64_t item_cap = 0, cbuf_cap = 0;
+  float* q768 = nullptr;       // [nq*768]
+  float* q256 = nullptr;       // [nq*256]
+  uint8_t* tables = nullptr;   // [nq*1024]
+  float4* qp = nullptr;        // [nq] (scale, bias, a, b)
+  float* qnorm = nullptr;      // [nq]
+  int8_t* wq = nullptr;        // [nq*768]
+  float* winv = nullptr;       // [nq]
+  int8_t* wq256 = nullptr;     // [nq*256]
+  float* winv256 = nullptr;    // [nq]
+  float* scores = nullptr;     // [nq*k] routing scores
+  uint64_t scores_cap = 0;
+  float* probe_sc = nullptr;   // [nq*P]
+  uint32_t* probe_cl = nullptr;  // [nq*P]
+  uint32_t* probe_off = nullptr;  // [nq*P] admission offset of each probe's first slot
+  uint32_t* probe_n = nullptr;   // [nq]
+  uint64_t* scanned = nullptr;   // [nq]
+  uint4* items = nullptr;        // [item_cap] (query, probe rank, first block, end block)
+  uint32_t* counters = nullptr;  // [4]: nitems, next item, status, spare
+  uint32_t* thr = nullptr;       // [nq] running lower bound of the cand-th estimate (ordered)
+  uint32_t* ccount = nullptr;    // [nq] entries appended to a query's candidate buffer
+  uint4* cbuf = nullptr;         // [nq*cbuf_per_q] (est bits, admission key, slot, 0)
+  uint32_t cbuf_per_q = 0;
+  uint8_t* overflow = nullptr;   // [nq]
+  float* cest = nullptr;         // [nq*cand] candidates after cut + dedup, in row order
+  uint32_t* cid = nullptr;
+  float* cerr = nullptr;
+  uint32_t* cn = nullptr;        // [nq]
+  uint32_t* lid = nullptr;       // [nq*cand] rerank list (after pruning / tier-2)
+  float* lsc = nullptr;          // [nq*cand] scores of the rerank list
+  uint32_t* ln = nullptr;        // [nq]
+  float* out_sc = nullptr;       // [nq*k]
+  uint32_t* out_id = nullptr;
+  uint32_t* out_n = nullptr;
+  uint64_t* allow = nullptr;     // [allow_words]
+  uint64_t allow_cap = 0;
+  void* host_pinned = nullptr;   // pinned staging for host<->device copies
+  size_t host_pinned_cap = 0;
+  cudaEvent_t ev[6] = {};
+  bool events = false;
+};
+
+struct Config {
+  uint32_t chunk_blocks = kChunkBlocks;  // autotuned
+  uint32_t scan_ctas_per_sm = 4;
+};
+
+std::string& last_error();
+int fail(int code, const std::string& msg);
+
+// kernel launchers (one per .cu file section)
+void launch_prefix(Workspace& w, uint32_t nq, cudaStream_t st);
+void launch_prep(const DevIndex& ix, Workspace& w, uint32_t nq, cudaStream_t st);
+void launch_route_scores(const DevIndex& ix, Workspace& w, uint32_t nq, int precision,
+                         cudaStream_t st);
+void launch_route_select(const DevIndex& ix, Workspace& w, uint32_t nq, const sg_params& p,
+                         int precision, uint32_t chunk_blocks, cudaStream_t st);
+void launch_scan(const DevIndex& ix, Workspace& w, uint32_t nq, const sg_params& p,
+                 const uint64_t* allow, uint64_t allow_words, int sms, cudaStream_t st);
+void launch_cut(const DevIndex& ix, Workspace& w, uint32_t nq, const sg_params& p,
+                cudaStream_t st);
+void launch_rerank(const DevIndex& ix, Workspace& w, uint32_t nq, const sg_params& p,
+                   cudaStream_t st, cudaEvent_t ev_t2_begin, cudaEvent_t ev_t2_end);
+void launch_lut_scan(uint32_t groups, const uint8_t* tables, const uint8_t* blocks,
+                     uint64_t nblocks, uint16_t* out, cudaStream_t st);
+void launch_dot_i8i8(const int8_t* q, const int8_t* rows, uint64_t nrows, uint32_t dim,
+                     int32_t* out, cudaStream_t st);
+
+}  // namespace sg

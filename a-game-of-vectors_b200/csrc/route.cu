@@ -1,0 +1,365 @@
+// route.cu — centroid routing, ivf::Index::route (src/ivf.rs:589-618).
+//
+// Two ways to score q256 against the K centroids:
+//   FP32: every (query, centroid) dot in the reference's order — a sequential f32 sum from -0.0
+//         of rounded products (blas::gemm_abt portable, src/blas.rs:43-54). Exact by construction.
+//   BF16: a tensor-core GEMM [nq x 256] x [256 x K] with FP32 accumulation, then, per query,
+//         every centroid whose BF16 score lies within 2*delta of the nprobe-th best BF16 score is
+//         rescored with the FP32 sequential dot. delta bounds |BF16 score - FP32 score|:
+//         inputs rounded to bf16 (unit roundoff 2^-8) give a product error <= (2^-7 + 2^-16)|q_i c_i|;
+//         FP32 accumulation of 256 exact bf16 products adds <= 256*2^-23 * sum|q_i c_i|, and the
+//         reference's own sequential sum differs from the real dot by <= 256*2^-24 * sum|q_i c_i|.
+//         With sum|q_i c_i| <= |q||c|, delta = 0.0085 |q| max|c| covers all three. The true top
+//         nprobe is inside the window (its members score >= s_np - 2 delta in BF16), so the probe
+//         set and its scores equal the FP32 path's bit for bit.
+// Then TopK(nprobe) ordering (score desc, id asc), the margin cut v >= best - m, and the slot
+// budget (take while the running slot count stays <= b, keep at least one), and the scan work
+// items of each probe (chunks of at most chunk_blocks blocks).
+#include <float.h>
+
+#include "common.cuh"
+#include "internal.hpp"
+
+namespace sg {
+
+constexpr int kRouteQB = 8;  // queries per thread in the exact kernel
+
+__global__ void __launch_bounds__(256) k_route_fp32(const float* __restrict__ q256,
+                                                    const float* __restrict__ cent_t, uint32_t K,
+                                                    uint32_t nq, float* __restrict__ scores) {
+  __shared__ float qs[kRouteQB][SG_PDIM];
+  const uint32_t q0 = blockIdx.y * kRouteQB;
+  for (int i = threadIdx.x; i < kRouteQB * SG_PDIM; i += blockDim.x) {
+    uint32_t qq = q0 + i / SG_PDIM;
+    qs[i / SG_PDIM][i % SG_PDIM] = qq < nq ? q256[(size_t)qq * SG_PDIM + i % SG_PDIM] : 0.0f;
+  }
+  __syncthreads();
+  const uint32_t c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= K) return;
+  float acc[kRouteQB];
+#pragma unroll
+  for (int j = 0; j < kRouteQB; j++) acc[j] = -0.0f;
+#pragma unroll 4
+  for (int t = 0; t < SG_PDIM; t++) {
+    float cv = __ldg(cent_t + (size_t)t * K + c);
+#pragma unroll
+    for (int j = 0; j < kRouteQB; j++) acc[j] = __fadd_rn(acc[j], __fmul_rn(qs[j][t], cv));
+  }
+#pragma unroll
+  for (int j = 0; j < kRouteQB; j++)
+    if (q0 + j < nq) scores[(size_t)(q0 + j) * K + c] = acc[j];
+}
+
+// ---- BF16 tensor-core GEMM: 64 queries x 128 centroids per CTA, 8 warps of 32x32 -------------
+constexpr int kBM = 64, kBN = 128, kLD = SG_PDIM + 8;  // padded rows: conflict-free fragments
+
+SG_DEV void mma_bf16(float* d, const uint32_t* a, const uint32_t* b) {
+  asm volatile(
+      "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, "
+      "{%8,%9}, {%0,%1,%2,%3};\n"
+      : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
+      : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b[0]), "r"(b[1]));
+}
+
+__global__ void __launch_bounds__(256) k_route_bf16(const float* __restrict__ q256,
+                                                    const __nv_bfloat16* __restrict__ cb,
+                                                    uint32_t K, uint32_t nq,
+                                                    float* __restrict__ scores) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  __nv_bfloat16* As = reinterpret_cast<__nv_bfloat16*>(smem_raw);
+  __nv_bfloat16* Bs = As + kBM * kLD;
+  const uint32_t m0 = blockIdx.y * kBM, n0 = blockIdx.x * kBN;
+  // A: queries f32 -> bf16 (round to nearest even)
+  for (int i = threadIdx.x; i < kBM * SG_PDIM / 4; i += blockDim.x) {
+    int r = i / (SG_PDIM / 4), c4 = i % (SG_PDIM / 4);
+    float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
+    if (m0 + r < nq) v = *reinterpret_cast<const float4*>(q256 + (size_t)(m0 + r) * SG_PDIM + 4 * c4);
+    __nv_bfloat162 lo = __floats2bfloat162_rn(v.x, v.y), hi = __floats2bfloat162_rn(v.z, v.w);
+    *reinterpret_cast<__nv_bfloat162*>(As + r * kLD + 4 * c4) = lo;
+    *reinterpret_cast<__nv_bfloat162*>(As + r * kLD + 4 * c4 + 2) = hi;
+  }
+  // B: centroid rows (k contiguous = the col-major B operand)
+  for (int i = threadIdx.x; i < kBN * SG_PDIM / 8; i += blockDim.x) {
+    int r = i / (SG_PDIM / 8), c8 = i % (SG_PDIM / 8);
+    uint4 v = make_uint4(0, 0, 0, 0);
+    if (n0 + r < K) v = *reinterpret_cast<const uint4*>(cb + (size_t)(n0 + r) * SG_PDIM + 8 * c8);
+    *reinterpret_cast<uint2*>(Bs + r * kLD + 8 * c8) = make_uint2(v.x, v.y);
+    *reinterpret_cast<uint2*>(Bs + r * kLD + 8 * c8 + 4) = make_uint2(v.z, v.w);
+  }
+  __syncthreads();
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int g = lane >> 2, tig = lane & 3;
+  const int wm = (warp >> 2) * 32, wn = (warp & 3) * 32;
+  float acc[2][4][4];
+#pragma unroll
+  for (int i = 0; i < 2; i++)
+#pragma unroll
+    for (int j = 0; j < 4; j++)
+#pragma unroll
+      for (int e = 0; e < 4; e++) acc[i][j][e] = 0.0f;
+#pragma unroll 4
+  for (int k0 = 0; k0 < SG_PDIM; k0 += 16) {
+    uint32_t a[2][4], b[4][2];
+#pragma unroll
+    for (int i = 0; i < 2; i++) {
+      const __nv_bfloat16* base = As + (wm + 16 * i + g) * kLD + k0 + 2 * tig;
+      a[i][0] = *reinterpret_cast<const uint32_t*>(base);
+      a[i][1] = *reinterpret_cast<const uint32_t*>(base + 8 * kLD);
+      a[i][2] = *reinterpret_cast<const uint32_t*>(base + 8);
+      a[i][3] = *reinterpret_cast<const uint32_t*>(base + 8 * kLD + 8);
+    }
+#pragma unroll
+    for (int j = 0; j < 4; j++) {
+      const __nv_bfloat16* base = Bs + (wn + 8 * j + g) * kLD + k0 + 2 * tig;
+      b[j][0] = *reinterpret_cast<const uint32_t*>(base);
+      b[j][1] = *reinterpret_cast<const uint32_t*>(base + 8);
+    }
+#pragma unroll
+    for (int i = 0; i < 2; i++)
+#pragma unroll
+      for (int j = 0; j < 4; j++) mma_bf16(acc[i][j], a[i], b[j]);
+  }
+#pragma unroll
+  for (int i = 0; i < 2; i++)
+#pragma unroll
+    for (int j = 0; j < 4; j++) {
+      uint32_t r = m0 + wm + 16 * i + g, c = n0 + wn + 8 * j + 2 * tig;
+      if (r < nq) {
+        if (c < K) scores[(size_t)r * K + c] = acc[i][j][0];
+        if (c + 1 < K) scores[(size_t)r * K + c + 1] = acc[i][j][1];
+      }
+      if (r + 8 < nq) {
+        if (c < K) scores[(size_t)(r + 8) * K + c] = acc[i][j][2];
+        if (c + 1 < K) scores[(size_t)(r + 8) * K + c + 1] = acc[i][j][3];
+      }
+    }
+}
+
+// The reference's sequential FP32 dot of one query with one centroid row.
+SG_DEV float exact_dot(const float* __restrict__ q, const float* __restrict__ c) {
+  float s = -0.0f;
+  const float4* c4 = reinterpret_cast<const float4*>(c);
+#pragma unroll 8
+  for (int t = 0; t < SG_PDIM / 4; t++) {
+    float4 v = __ldg(c4 + t);
+    s = __fadd_rn(s, __fmul_rn(q[4 * t + 0], v.x));
+    s = __fadd_rn(s, __fmul_rn(q[4 * t + 1], v.y));
+    s = __fadd_rn(s, __fmul_rn(q[4 * t + 2], v.z));
+    s = __fadd_rn(s, __fmul_rn(q[4 * t + 3], v.w));
+  }
+  return s;
+}
+
+constexpr uint32_t kWinCap = 4096;
+
+struct SelectArgs {
+  const float* q256;
+  const float* cent;
+  const float* qnorm;
+  float cent_norm_max;
+  const uint32_t* block_off;
+  uint32_t K;
+  float* scores;
+  uint32_t P;  // min(nprobe, K): stride of the probe arrays
+  int bf16;
+  sg_params p;
+  uint32_t chunk_blocks;
+  float* probe_sc;
+  uint32_t* probe_cl;
+  uint32_t* probe_off;
+  uint32_t* probe_n;
+  uint64_t* scanned;
+  uint4* items;
+  uint64_t item_cap;
+  uint32_t* counters;
+};
+
+__global__ void __launch_bounds__(256) k_route_select(SelectArgs a) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  uint64_t* keys = reinterpret_cast<uint64_t*>(smem_raw);  // [kWinCap]
+  __shared__ float qv[SG_PDIM];
+  __shared__ uint32_t hist[256], tmp[32];
+  __shared__ uint32_t s_nw, s_m, s_keep;
+  const uint32_t q = blockIdx.x, P = a.P, K = a.K;
+  float* row = a.scores + (size_t)q * K;
+  for (int i = threadIdx.x; i < SG_PDIM; i += blockDim.x) qv[i] = a.q256[(size_t)q * SG_PDIM + i];
+  if (threadIdx.x == 0) s_nw = 0;
+  __syncthreads();
+  if (P == 0) {
+    if (threadIdx.x == 0) {
+      a.probe_n[q] = 0;
+      a.scanned[q] = 0;
+    }
+    return;
+  }
+  bool exact = !a.bf16;
+  if (a.bf16) {
+    // the P-th largest BF16 score and the window below it
+    uint64_t kth = block_select_nth_u64(
+        [&](uint32_t i) { return ((uint64_t)ord(row[i]) << 32) | (0xFFFFFFFFu - i); }, K, P, hist,
+        tmp);
+    float sP = unord((uint32_t)(kth >> 32));
+    float delta = 0.0085f * a.qnorm[q] * a.cent_norm_max;
+    float lim = sP - 2.0f * delta;
+    for (uint32_t c = threadIdx.x; c < K; c += blockDim.x)
+      if (row[c] >= lim) {
+        uint32_t slot = atomicAdd(&s_nw, 1u);
+        if (slot < kWinCap) keys[slot] = c;
+      }
+    __syncthreads();
+    uint32_t nw = s_nw;
+    // a window narrower than P means a non-finite score or norm: take the exact path
+    if (nw >= P && nw <= kWinCap) {
+      for (uint32_t i = threadIdx.x; i < nw; i += blockDim.x) {
+        uint32_t c = (uint32_t)keys[i];
+        keys[i] = rank_key(exact_dot(qv, a.cent + (size_t)c * SG_PDIM), c);
+      }
+      __syncthreads();
+      uint64_t T = block_select_nth_u64([&](uint32_t i) { return keys[i]; }, nw, P, hist, tmp);
+      __syncthreads();
+      // compact the P winners to the front
+      if (threadIdx.x == 0) s_m = 0;
+      __syncthreads();
+      uint64_t mine[kWinCap / 256];
+      uint32_t nm = 0;
+      for (uint32_t i = threadIdx.x; i < nw; i += blockDim.x)
+        if (keys[i] >= T) mine[nm++] = keys[i];
+      __syncthreads();
+      for (uint32_t j = 0; j < nm; j++) keys[atomicAdd(&s_m, 1u)] = mine[j];
+      __syncthreads();
+    } else {
+      // window too wide for the buffer (or degenerate): score every centroid exactly
+      if (threadIdx.x == 0) atomicOr(&a.counters[2], kStatusWindow);
+      for (uint32_t c = threadIdx.x; c < K; c += blockDim.x)
+        row[c] = exact_dot(qv, a.cent + (size_t)c * SG_PDIM);
+      __syncthreads();
+      exact = true;
+    }
+  }
+  if (exact) {
+    uint64_t T = block_select_nth_u64([&](uint32_t i) { return rank_key(row[i], i); }, K, P, hist,
+                                      tmp);
+    if (threadIdx.x == 0) s_m = 0;
+    __syncthreads();
+    for (uint32_t c = threadIdx.x; c < K; c += blockDim.x) {
+      uint64_t k = rank_key(row[c], c);
+      if (k >= T) keys[atomicAdd(&s_m, 1u)] = k;
+    }
+    __syncthreads();
+  }
+  // keys[0..P) hold the winners: sort best first
+  uint32_t n2 = next_pow2(P);
+  for (uint32_t i = P + threadIdx.x; i < n2; i += blockDim.x) keys[i] = 0;
+  __syncthreads();
+  block_bitonic_sort_desc(keys, n2);
+  // margin (prefix of the sorted list) and budget
+  if (threadIdx.x == 0) {
+    uint32_t m = P;
+    if (a.p.has_margin) {
+      float lim = __fsub_rn(key_score(keys[0]), a.p.margin);
+      uint32_t w = 0;
+      while (w < m && key_score(keys[w]) >= lim) w++;
+      m = w;
+    }
+    if (a.p.has_budget) {
+      uint64_t used = 0;
+      uint32_t keep = 0;
+      for (uint32_t i = 0; i < m; i++) {
+        uint32_t c = key_id(keys[i]);
+        used += (uint64_t)(a.block_off[c + 1] - a.block_off[c]) * SG_BLOCK;
+        if (used <= a.p.budget) keep++;
+        else break;
+      }
+      if (keep < 1) keep = 1;
+      if (keep < m) m = keep;
+    }
+    s_keep = m;
+  }
+  __syncthreads();
+  const uint32_t m = s_keep;
+  // probe list, admission offsets and chunk counts (block scans over probe ranks)
+  uint32_t nloc = (m + blockDim.x - 1) / blockDim.x;  // probes per thread (contiguous)
+  uint32_t r0 = threadIdx.x * nloc, r1 = min(m, r0 + nloc);
+  uint32_t slots = 0, chunks = 0;
+  for (uint32_t r = r0; r < r1; r++) {
+    uint32_t c = key_id(keys[r]);
+    uint32_t nb = a.block_off[c + 1] - a.block_off[c];
+    slots += nb * SG_BLOCK;
+    chunks += (nb + a.chunk_blocks - 1) / a.chunk_blocks;
+  }
+  uint32_t tot_slots, tot_chunks;
+  uint32_t soff = block_exclusive_scan(slots, tmp, &tot_slots);
+  uint32_t coff = block_exclusive_scan(chunks, tmp, &tot_chunks);
+  __shared__ uint32_t s_base;
+  if (threadIdx.x == 0) {
+    uint32_t base = atomicAdd(&a.counters[0], tot_chunks);
+    if ((uint64_t)base + tot_chunks > a.item_cap) atomicOr(&a.counters[2], kStatusOverflow);
+    s_base = base;
+    a.probe_n[q] = m;
+    a.scanned[q] = tot_slots;
+  }
+  __syncthreads();
+  uint64_t ibase = (uint64_t)s_base + coff;
+  for (uint32_t r = r0; r < r1; r++) {
+    uint32_t c = key_id(keys[r]);
+    a.probe_cl[(size_t)q * P + r] = c;
+    a.probe_sc[(size_t)q * P + r] = key_score(keys[r]);
+    a.probe_off[(size_t)q * P + r] = soff;
+    uint32_t b0 = a.block_off[c], b1 = a.block_off[c + 1];
+    soff += (b1 - b0) * SG_BLOCK;
+    for (uint32_t b = b0; b < b1; b += a.chunk_blocks) {
+      if (ibase < a.item_cap) a.items[ibase] = make_uint4(q, r, b, min(b1, b + a.chunk_blocks));
+      ibase++;
+    }
+  }
+}
+
+void launch_route_scores(const DevIndex& ix, Workspace& w, uint32_t nq, int precision,
+                         cudaStream_t st) {
+  if (precision == SG_ROUTE_BF16) {
+    static bool attr = false;
+    size_t smem = (size_t)(kBM + kBN) * kLD * sizeof(__nv_bfloat16);
+    if (!attr) {
+      cudaFuncSetAttribute(k_route_bf16, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+      attr = true;
+    }
+    dim3 grid((ix.k + kBN - 1) / kBN, (nq + kBM - 1) / kBM);
+    k_route_bf16<<<grid, 256, smem, st>>>(w.q256, ix.cent_bf16, ix.k, nq, w.scores);
+  } else {
+    dim3 grid((ix.k + 255) / 256, (nq + kRouteQB - 1) / kRouteQB);
+    k_route_fp32<<<grid, 256, 0, st>>>(w.q256, ix.cent_t, ix.k, nq, w.scores);
+  }
+}
+
+void launch_route_select(const DevIndex& ix, Workspace& w, uint32_t nq, const sg_params& p,
+                         int precision, uint32_t chunk_blocks, cudaStream_t st) {
+  SelectArgs a;
+  a.q256 = w.q256;
+  a.cent = ix.cent;
+  a.qnorm = w.qnorm;
+  a.cent_norm_max = ix.cent_norm_max;
+  a.block_off = ix.block_off;
+  a.K = ix.k;
+  a.scores = w.scores;
+  a.P = p.nprobe < ix.k ? p.nprobe : ix.k;
+  a.bf16 = precision == SG_ROUTE_BF16;
+  a.p = p;
+  a.chunk_blocks = chunk_blocks;
+  a.probe_sc = w.probe_sc;
+  a.probe_cl = w.probe_cl;
+  a.probe_off = w.probe_off;
+  a.probe_n = w.probe_n;
+  a.scanned = w.scanned;
+  a.items = w.items;
+  a.item_cap = w.item_cap;
+  a.counters = w.counters;
+  static bool attr = false;
+  size_t smem = kWinCap * sizeof(uint64_t);
+  if (!attr) {
+    cudaFuncSetAttribute(k_route_select, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    attr = true;
+  }
+  k_route_select<<<nq, 256, smem, st>>>(a);
+}
+
+}  // namespace sg

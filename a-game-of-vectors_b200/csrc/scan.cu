@@ -1,0 +1,300 @@
+// scan.cu — the LUT scan with the RaBitQ estimator and the candidate admission
+// (ivf::Index::candidates, src/ivf.rs:647-698; lut::scan, src/lut.rs:96-126;
+// rabitq::Query::estimate, src/rabitq.rs:127-130).
+//
+// Work: a persistent grid drains the (query, probe, chunk) work queue the routing kernel wrote.
+// One CTA scores one chunk (<= CHB blocks of 32 slots) of one probed cluster for one query:
+//   - the query's 64 u8 nibble tables sit in shared memory (1 KB);
+//   - four threads share a block: thread t takes groups t, t+4, ..., t+60, so each warp-wide
+//     16-byte load covers 64 contiguous bytes of each of 8 blocks (full 32-byte sectors);
+//   - lookups are register PRMTs (lut4), sums are packed u16 pairs (never above 16320);
+//   - the four partial sums are combined by shuffles; est = cent + mul*(a*score + b) in f32
+//     with the reference's rounding (no FMA).
+// Admission is exact. The reference keeps the best `cand` slots by estimate (TopK<f32>,
+// src/topk.rs), breaking ties by admission order. Here a chunk keeps its own best `cand`
+// eligible slots (est desc, then slot order) at or above the query's running threshold, appends
+// them to the query's candidate buffer and raises the threshold to its cand-th estimate (a valid
+// lower bound of the final cand-th). The cut kernel then takes the global best `cand` of the buffer.
+#include "common.cuh"
+#include "internal.hpp"
+
+namespace sg {
+
+struct ScanArgs {
+  const uint8_t* blocks;
+  const float* mul;
+  const uint32_t* ids;
+  const uint32_t* block_off;
+  const uint32_t* clen;
+  const uint8_t* tables;
+  const float4* qp;
+  const float* probe_sc;
+  const uint32_t* probe_cl;
+  const uint32_t* probe_off;
+  uint32_t P;
+  const uint4* items;
+  uint64_t item_cap;
+  uint32_t* counters;
+  uint32_t* thr;
+  uint32_t* ccount;
+  uint4* cbuf;
+  uint32_t cap;
+  uint8_t* overflow;
+  uint32_t cand;
+  const uint64_t* allow;
+  uint64_t allow_words;
+};
+
+SG_DEV uint4 ldg_nc(const uint4* p) {
+  uint4 v;
+  asm volatile("ld.global.nc.v4.u32 {%0,%1,%2,%3}, [%4];"
+               : "=r"(v.x), "=r"(v.y), "=r"(v.z), "=r"(v.w)
+               : "l"(p));
+  return v;
+}
+
+SG_DEV uint32_t ld_cg(const uint32_t* p) {
+  uint32_t v;
+  asm volatile("ld.global.cg.u32 %0, [%1];" : "=r"(v) : "l"(p));
+  return v;
+}
+
+// Scores one block's 32 slots into 16 packed accumulators (sum over this thread's 16 groups).
+SG_DEV void score_block_quarter(const uint8_t* __restrict__ block, const uint4* s_tab, int t4,
+                                uint32_t* acc) {
+  const uint4* src = reinterpret_cast<const uint4*>(block);
+#pragma unroll
+  for (int e = 0; e < 16; e++) acc[e] = 0;
+#pragma unroll 4
+  for (int i = 0; i < 16; i++) {
+    const int g = 4 * i + t4;
+    uint4 code = ldg_nc(src + g);
+    uint4 tab = s_tab[g];
+    lut_word(code.x, tab, acc + 0);
+    lut_word(code.y, tab, acc + 4);
+    lut_word(code.z, tab, acc + 8);
+    lut_word(code.w, tab, acc + 12);
+  }
+}
+
+template <int CHB>
+__global__ void __launch_bounds__(256, 2) k_scan(ScanArgs a) {
+  constexpr int NS = CHB * 32;
+  constexpr int PER = NS / 256;  // slots per thread in the admission phase (contiguous)
+  __shared__ uint4 s_tab[SG_GROUPS];
+  __shared__ uint32_t s_key[NS];
+  __shared__ uint32_t hist[256], tmp[32];
+  __shared__ uint32_t s_item, s_base;
+  const int tid = threadIdx.x, t4 = tid & 3, lbw = tid >> 2;
+  uint32_t nitems = a.counters[0];
+  if (nitems > a.item_cap) nitems = (uint32_t)a.item_cap;
+  for (;;) {
+    if (tid == 0) s_item = atomicAdd(&a.counters[1], 1u);
+    __syncthreads();
+    const uint32_t item = s_item;
+    if (item >= nitems) break;
+    const uint4 it = a.items[item];
+    const uint32_t q = it.x, r = it.y, b0 = it.z, nb = it.w - it.z;
+    const uint32_t c = a.probe_cl[(size_t)q * a.P + r];
+    const float cent = a.probe_sc[(size_t)q * a.P + r];
+    const float4 qp = a.qp[q];
+    if (tid < SG_GROUPS)
+      s_tab[tid] = reinterpret_cast<const uint4*>(a.tables + (size_t)q * SG_GROUPS * 16)[tid];
+    const uint32_t cb0 = a.block_off[c];
+    const uint32_t cl = a.clen[c];
+    const uint32_t loc0 = (b0 - cb0) * SG_BLOCK;  // slot index of the chunk's first slot
+    const uint32_t kbase = a.probe_off[(size_t)q * a.P + r] + loc0;
+    __syncthreads();
+    // ---- scoring --------------------------------------------------------------------------
+    for (int pb = 0; pb < CHB; pb += 64) {
+      const int lb = pb + lbw;
+      uint32_t acc[16];
+      if (lb < (int)nb) {
+        score_block_quarter(a.blocks + (size_t)(b0 + lb) * SG_BLOCK_BYTES, s_tab, t4, acc);
+      } else {
+#pragma unroll
+        for (int e = 0; e < 16; e++) acc[e] = 0;
+      }
+#pragma unroll
+      for (int e = 0; e < 16; e++) {
+        acc[e] += __shfl_xor_sync(0xFFFFFFFFu, acc[e], 1);
+        acc[e] += __shfl_xor_sync(0xFFFFFFFFu, acc[e], 2);
+      }
+      if (lb < (int)nb) {
+        uint32_t x0 = acc[0], x1 = acc[1], x2 = acc[2], x3 = acc[3];
+        if (t4 == 1) {
+          x0 = acc[4]; x1 = acc[5]; x2 = acc[6]; x3 = acc[7];
+        } else if (t4 == 2) {
+          x0 = acc[8]; x1 = acc[9]; x2 = acc[10]; x3 = acc[11];
+        } else if (t4 == 3) {
+          x0 = acc[12]; x1 = acc[13]; x2 = acc[14]; x3 = acc[15];
+        }
+        const float* mrow = a.mul + (size_t)(b0 + lb) * SG_BLOCK;
+        const float4 mlo = __ldg(reinterpret_cast<const float4*>(mrow + 4 * t4));
+        const float4 mhi = __ldg(reinterpret_cast<const float4*>(mrow + 16 + 4 * t4));
+        const uint32_t sc[8] = {x0 & 0xFFFFu, x0 >> 16, x2 & 0xFFFFu, x2 >> 16,
+                                x1 & 0xFFFFu, x1 >> 16, x3 & 0xFFFFu, x3 >> 16};
+        const float mv[8] = {mlo.x, mlo.y, mlo.z, mlo.w, mhi.x, mhi.y, mhi.z, mhi.w};
+#pragma unroll
+        for (int d = 0; d < 8; d++) {
+          const uint32_t doc = d < 4 ? 4 * t4 + d : 16 + 4 * t4 + (d - 4);
+          const uint32_t loc = lb * SG_BLOCK + doc;
+          const float est =
+              __fadd_rn(cent, __fmul_rn(mv[d], __fadd_rn(__fmul_rn(qp.z, (float)sc[d]), qp.w)));
+          s_key[loc] = (loc0 + loc < cl) ? ord(est) : 0u;
+        }
+      }
+    }
+    __syncthreads();
+    // ---- admission ----------------------------------------------------------------------------
+    const uint32_t thr = ld_cg(a.thr + q);
+    const uint32_t nloc = nb * SG_BLOCK;
+    const uint32_t i0 = tid * PER;
+    uint32_t cnt = 0;
+#pragma unroll
+    for (int j = 0; j < PER; j++) {
+      const uint32_t i = i0 + j;
+      if (i < nloc) {
+        const uint32_t k = s_key[i];
+        bool surv = k != 0u && k >= thr;
+        if (surv && a.allow) surv = allowed(a.allow, a.allow_words, a.ids[(size_t)b0 * SG_BLOCK + i]);
+        if (!surv) s_key[i] = 0u;
+        cnt += surv;
+      }
+    }
+    const uint32_t n_s = block_sum(cnt, tmp);
+    const bool cut = n_s > a.cand;
+    uint32_t T = 0, need = 0;
+    if (cut) {
+      T = block_select_nth_u32([&](uint32_t i) { return s_key[i]; }, nloc, a.cand, hist);
+      uint32_t gt = 0;
+#pragma unroll
+      for (int j = 0; j < PER; j++) {
+        const uint32_t i = i0 + j;
+        if (i < nloc && s_key[i] > T) gt++;
+      }
+      need = a.cand - block_sum(gt, tmp);
+    }
+    uint32_t ties = 0;
+    if (cut) {
+#pragma unroll
+      for (int j = 0; j < PER; j++) {
+        const uint32_t i = i0 + j;
+        if (i < nloc && s_key[i] == T) ties++;
+      }
+    }
+    uint32_t tie_rank = block_exclusive_scan(ties, tmp, nullptr);
+    uint32_t nsel = 0;
+    uint32_t selmask = 0;
+    {
+      uint32_t tr = tie_rank;
+#pragma unroll
+      for (int j = 0; j < PER; j++) {
+        const uint32_t i = i0 + j;
+        bool sel = false;
+        if (i < nloc) {
+          const uint32_t k = s_key[i];
+          if (!cut) sel = k != 0u;
+          else if (k > T) sel = true;
+          else if (k == T) sel = (tr++ < need);
+        }
+        if (sel) {
+          selmask |= 1u << j;
+          nsel++;
+        }
+      }
+    }
+    uint32_t total;
+    uint32_t off = block_exclusive_scan(nsel, tmp, &total);
+    if (tid == 0) {
+      s_base = total ? atomicAdd(a.ccount + q, total) : 0u;
+      if (cut) atomicMax(a.thr + q, T);
+    }
+    __syncthreads();
+    const uint32_t base = s_base;
+    uint4* dst = a.cbuf + (size_t)q * a.cap;
+#pragma unroll
+    for (int j = 0; j < PER; j++) {
+      if (selmask & (1u << j)) {
+        const uint32_t i = i0 + j;
+        const uint32_t pos = base + off++;
+        if (pos < a.cap)
+          dst[pos] = make_uint4(__float_as_uint(unord(s_key[i])), kbase + i,
+                                b0 * SG_BLOCK + i, 0u);
+        else
+          a.overflow[q] = 1;
+      }
+    }
+    __syncthreads();
+  }
+}
+
+void launch_scan(const DevIndex& ix, Workspace& w, uint32_t nq, const sg_params& p,
+                 const uint64_t* allow, uint64_t allow_words, int sms, cudaStream_t st) {
+  ScanArgs a;
+  a.blocks = ix.blocks;
+  a.mul = ix.mul;
+  a.ids = ix.ids;
+  a.block_off = ix.block_off;
+  a.clen = ix.clen;
+  a.tables = w.tables;
+  a.qp = w.qp;
+  a.probe_sc = w.probe_sc;
+  a.probe_cl = w.probe_cl;
+  a.probe_off = w.probe_off;
+  a.P = p.nprobe < ix.k ? p.nprobe : ix.k;
+  a.items = w.items;
+  a.item_cap = w.item_cap;
+  a.counters = w.counters;
+  a.thr = w.thr;
+  a.ccount = w.ccount;
+  a.cbuf = w.cbuf;
+  a.cap = w.cbuf_per_q;
+  a.overflow = w.overflow;
+  a.cand = p.cand;
+  a.allow = allow;
+  a.allow_words = allow_words;
+  k_scan<kChunkBlocks><<<sms * 2, 256, 0, st>>>(a);
+}
+
+// ---- stateless kernels for the parity tests ---------------------------------------------------
+// lut::scan of whole blocks (G = 64 or 32 groups): one thread per block, all groups.
+__global__ void k_lut_scan(uint32_t groups, const uint8_t* __restrict__ tables,
+                           const uint8_t* __restrict__ blocks, uint64_t nblocks,
+                           uint16_t* __restrict__ out) {
+  const uint64_t b = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= nblocks) return;
+  const uint4* src = reinterpret_cast<const uint4*>(blocks + b * groups * 16);
+  const uint4* tab = reinterpret_cast<const uint4*>(tables);
+  uint32_t acc[16];
+#pragma unroll
+  for (int e = 0; e < 16; e++) acc[e] = 0;
+  for (uint32_t g = 0; g < groups; g++) {
+    uint4 code = src[g], t = tab[g];
+    lut_word(code.x, t, acc + 0);
+    lut_word(code.y, t, acc + 4);
+    lut_word(code.z, t, acc + 8);
+    lut_word(code.w, t, acc + 12);
+  }
+  uint16_t* o = out + b * SG_BLOCK;
+#pragma unroll
+  for (int j = 0; j < 4; j++) {
+    o[4 * j + 0] = (uint16_t)(acc[4 * j] & 0xFFFF);
+    o[4 * j + 1] = (uint16_t)(acc[4 * j] >> 16);
+    o[4 * j + 2] = (uint16_t)(acc[4 * j + 2] & 0xFFFF);
+    o[4 * j + 3] = (uint16_t)(acc[4 * j + 2] >> 16);
+    o[16 + 4 * j + 0] = (uint16_t)(acc[4 * j + 1] & 0xFFFF);
+    o[16 + 4 * j + 1] = (uint16_t)(acc[4 * j + 1] >> 16);
+    o[16 + 4 * j + 2] = (uint16_t)(acc[4 * j + 3] & 0xFFFF);
+    o[16 + 4 * j + 3] = (uint16_t)(acc[4 * j + 3] >> 16);
+  }
+}
+
+void launch_lut_scan(uint32_t groups, const uint8_t* tables, const uint8_t* blocks,
+                     uint64_t nblocks, uint16_t* out, cudaStream_t st) {
+  if (nblocks == 0) return;
+  k_lut_scan<<<(unsigned)((nblocks + 127) / 128), 128, 0, st>>>(groups, tables, blocks, nblocks,
+                                                                out);
+}
+
+}  // namespace sg

@@ -1,0 +1,786 @@
+// sieve_gpu.cu — the C ABI (include/sieve_gpu.h): index upload, workspace and the query pipeline.
+//
+// Pipeline of one batched call (every stage one kernel on the index's stream):
+//   prefix (if q256 not given) -> prep -> route scores (BF16 tensor cores or exact FP32)
+//   -> route select (+FP32 rescoring window, margin, budget, work items) -> scan (persistent,
+//   drains the (query, probe, chunk) queue) -> cut + dedup -> prune / tier-2 / int8 rerank -> top-k.
+#include <cuda_bf16.h>
+#include <math.h>
+#include <string.h>
+
+#include <algorithm>
+#include <cstdio>
+#include <fstream>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "internal.hpp"
+
+struct sg_index {
+  sg::DevIndex ix;
+  sg::Workspace ws;
+  sg::Config cfg;
+  std::mutex mu;
+  cudaStream_t stream = nullptr;
+  int sms = 148;
+};
+
+namespace sg {
+
+std::string& last_error() {
+  static thread_local std::string e;
+  return e;
+}
+
+int fail(int code, const std::string& msg) {
+  last_error() = msg;
+  return code;
+}
+
+}  // namespace sg
+
+using sg::fail;
+
+#define CK(call)                                                                       \
+  do {                                                                                 \
+    cudaError_t e_ = (call);                                                           \
+    if (e_ != cudaSuccess)                                                             \
+      return fail(SG_ERR_DEVICE, std::string(#call) + ": " + cudaGetErrorString(e_)); \
+  } while (0)
+
+namespace {
+
+template <typename T>
+int dalloc(T** p, size_t n) {
+  *p = nullptr;
+  if (n == 0) n = 1;
+  cudaError_t e = cudaMalloc((void**)p, n * sizeof(T));
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    return fail(SG_ERR_OOM, std::string("cudaMalloc ") + std::to_string(n * sizeof(T)) +
+                                " bytes: " + cudaGetErrorString(e));
+  }
+  return SG_OK;
+}
+
+template <typename T>
+void dfree(T*& p) {
+  if (p) cudaFree((void*)p);
+  p = nullptr;
+}
+
+template <typename T>
+int upload(T** d, const T* h, size_t n) {
+  int rc = dalloc(d, n);
+  if (rc) return rc;
+  if (n) CK(cudaMemcpy(*d, h, n * sizeof(T), cudaMemcpyHostToDevice));
+  return SG_OK;
+}
+
+void free_index(sg::DevIndex& x) {
+  dfree(x.cent);
+  dfree(x.cent_t);
+  dfree(x.cent_bf16);
+  dfree(x.block_off);
+  dfree(x.clen);
+  dfree(x.blocks);
+  dfree(x.mul);
+  dfree(x.err);
+  dfree(x.ids);
+  dfree(x.rot);
+  dfree(x.t2_sigma);
+  dfree(x.t2_codes);
+  dfree(x.t2_norm);
+  dfree(x.rerank);
+  dfree(x.norm256);
+  dfree(x.qscale);
+}
+
+void free_ws(sg::Workspace& w) {
+  dfree(w.q768);
+  dfree(w.q256);
+  dfree(w.tables);
+  dfree(w.qp);
+  dfree(w.qnorm);
+  dfree(w.wq);
+  dfree(w.winv);
+  dfree(w.wq256);
+  dfree(w.winv256);
+  dfree(w.scores);
+  dfree(w.probe_sc);
+  dfree(w.probe_cl);
+  dfree(w.probe_off);
+  dfree(w.probe_n);
+  dfree(w.scanned);
+  dfree(w.items);
+  dfree(w.counters);
+  dfree(w.thr);
+  dfree(w.ccount);
+  dfree(w.cbuf);
+  dfree(w.overflow);
+  dfree(w.cest);
+  dfree(w.cid);
+  dfree(w.cerr);
+  dfree(w.cn);
+  dfree(w.lid);
+  dfree(w.lsc);
+  dfree(w.ln);
+  dfree(w.out_sc);
+  dfree(w.out_id);
+  dfree(w.out_n);
+  dfree(w.allow);
+  if (w.events)
+    for (auto& e : w.ev) cudaEventDestroy(e);
+  w = sg::Workspace();
+}
+
+int build_index(const sg_ivf_arrays* a, int device, sg_index** out) {
+  if (!a || !out) return fail(SG_ERR_INVALID, "null argument");
+  *out = nullptr;
+  if (a->k == 0 || !a->centroids || !a->block_off)
+    return fail(SG_ERR_INVALID, "index needs centroids and block_off");
+  if (!a->ids || !a->blocks) return fail(SG_ERR_INVALID, "index needs ids.u32 and blocks.bin");
+  if (!a->factors || !a->rotation)
+    return fail(SG_ERR_UNSUPPORTED,
+                "only RaBitQ indexes (rotation.f32 + factors.f32) run on the GPU path");
+  if (!a->rerank || !a->quant_scale)
+    return fail(SG_ERR_INVALID, "corpus needs rerank.i8 and quant.f32");
+  const uint32_t K = a->k;
+  if (a->block_off[0] != 0) return fail(SG_ERR_INVALID, "block_off[0] != 0");
+  for (uint32_t c = 0; c < K; c++)
+    if (a->block_off[c + 1] < a->block_off[c]) return fail(SG_ERR_INVALID, "block_off not monotonic");
+  const uint64_t nblocks = a->block_off[K];
+  if (nblocks * SG_BLOCK >= 0xFFFFFFFFull) return fail(SG_ERR_INVALID, "more than 2^32 slots");
+  int ndev = 0;
+  CK(cudaGetDeviceCount(&ndev));
+  if (device < 0 || device >= ndev) return fail(SG_ERR_DEVICE, "no such CUDA device");
+  CK(cudaSetDevice(device));
+  std::unique_ptr<sg_index> h(new sg_index());
+  sg::DevIndex& x = h->ix;
+  x.device = device;
+  x.k = K;
+  x.n = a->n;
+  x.nblocks = nblocks;
+  x.nslots = nblocks * SG_BLOCK;
+  // cluster lengths: PAD may only fill the tail of a cluster's last block (src/ivf.rs:378-380)
+  x.h_block_off.assign(a->block_off, a->block_off + K + 1);
+  x.h_clen.resize(K);
+  for (uint32_t c = 0; c < K; c++) {
+    uint64_t s0 = a->block_off[c] * SG_BLOCK, s1 = a->block_off[c + 1] * SG_BLOCK;
+    uint64_t len = s0;
+    while (len < s1 && a->ids[len] != SG_PAD) {
+      if (a->ids[len] >= a->n) return fail(SG_ERR_INVALID, "ids.u32 holds a row beyond the corpus");
+      len++;
+    }
+    for (uint64_t s = len; s < s1; s++)
+      if (a->ids[s] != SG_PAD)
+        return fail(SG_ERR_INVALID, "PAD slot inside a cluster (ids.u32 is not in build layout)");
+    if (s1 - len >= SG_BLOCK) return fail(SG_ERR_INVALID, "a cluster holds a whole block of PAD");
+    x.h_clen[c] = (uint32_t)(len - s0);
+  }
+  std::vector<uint32_t> boff32(K + 1);
+  for (uint32_t c = 0; c <= K; c++) boff32[c] = (uint32_t)a->block_off[c];
+  // per-cluster chunk counts, largest first, for the work-queue capacity bound
+  {
+    std::vector<uint32_t> ch(K);
+    for (uint32_t c = 0; c < K; c++)
+      ch[c] = (boff32[c + 1] - boff32[c] + h->cfg.chunk_blocks - 1) / h->cfg.chunk_blocks;
+    std::sort(ch.begin(), ch.end(), std::greater<uint32_t>());
+    x.h_chunks_desc_prefix.assign(K + 1, 0);
+    for (uint32_t c = 0; c < K; c++) x.h_chunks_desc_prefix[c + 1] = x.h_chunks_desc_prefix[c] + ch[c];
+  }
+  // centroids: row-major, transposed, BF16; largest norm for the routing error window
+  std::vector<float> ct((size_t)K * SG_PDIM);
+  std::vector<__nv_bfloat16> cb((size_t)K * SG_PDIM);
+  float nmax = 0.0f;
+  for (uint32_t c = 0; c < K; c++) {
+    double s = 0;
+    for (int t = 0; t < SG_PDIM; t++) {
+      float v = a->centroids[(size_t)c * SG_PDIM + t];
+      ct[(size_t)t * K + c] = v;
+      cb[(size_t)c * SG_PDIM + t] = __float2bfloat16_rn(v);
+      s += (double)v * v;
+    }
+    nmax = std::max(nmax, (float)sqrt(s));
+  }
+  x.cent_norm_max = nmax * 1.0001f;
+  // factors.f32 [mul, err] per slot -> two planes
+  std::vector<float> mul(x.nslots), err(x.nslots);
+  for (uint64_t s = 0; s < x.nslots; s++) {
+    mul[s] = a->factors[2 * s];
+    err[s] = a->factors[2 * s + 1];
+  }
+  x.rot_norm = powf(256.0f, -1.5f);
+  int rc;
+  if ((rc = upload(&x.cent, a->centroids, (size_t)K * SG_PDIM)) ||
+      (rc = upload(&x.cent_t, ct.data(), ct.size())) ||
+      (rc = upload(&x.cent_bf16, cb.data(), cb.size())) ||
+      (rc = upload(&x.block_off, boff32.data(), boff32.size())) ||
+      (rc = upload(&x.clen, x.h_clen.data(), x.h_clen.size())) ||
+      (rc = upload(&x.blocks, a->blocks, (size_t)nblocks * SG_BLOCK_BYTES)) ||
+      (rc = upload(&x.mul, mul.data(), mul.size())) || (rc = upload(&x.err, err.data(), err.size())) ||
+      (rc = upload(&x.ids, a->ids, x.nslots)) || (rc = upload(&x.rot, a->rotation, 3 * SG_PDIM)) ||
+      (rc = upload(&x.rerank, a->rerank, (size_t)a->n * SG_DIM)) ||
+      (rc = upload(&x.qscale, a->quant_scale, SG_DIM))) {
+    free_index(x);
+    return rc;
+  }
+  if (a->norm256 && (rc = upload(&x.norm256, a->norm256, a->n))) {
+    free_index(x);
+    return rc;
+  }
+  if (a->tier2_sigma && a->tier2_codes && a->tier2_norm) {
+    if ((rc = upload(&x.t2_sigma, a->tier2_sigma, SG_PDIM)) ||
+        (rc = upload(&x.t2_codes, a->tier2_codes, (size_t)a->n * SG_TIER2_BYTES)) ||
+        (rc = upload(&x.t2_norm, a->tier2_norm, a->n))) {
+      free_index(x);
+      return rc;
+    }
+    x.has_t2 = true;
+  }
+  cudaDeviceProp prop;
+  CK(cudaGetDeviceProperties(&prop, device));
+  h->sms = prop.multiProcessorCount;
+  CK(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));
+  *out = h.release();
+  return SG_OK;
+}
+
+// Sizes the workspace for nq queries under params p (grows, never shrinks).
+int ensure_ws(sg_index* h, uint32_t nq, const sg_params& p, uint32_t cbuf_per_q) {
+  sg::Workspace& w = h->ws;
+  const sg::DevIndex& x = h->ix;
+  const uint32_t P = std::min<uint32_t>(p.nprobe, x.k);
+  const uint32_t cand = std::max<uint32_t>(p.cand, 1);
+  const uint32_t k = std::max<uint32_t>(p.k, 1);
+  int rc;
+  if (!w.events) {
+    for (auto& e : w.ev) CK(cudaEventCreate(&e));
+    w.events = true;
+  }
+  if (nq > w.nq_cap) {
+    uint32_t n = std::max(nq, w.nq_cap * 2);
+    dfree(w.q768); dfree(w.q256); dfree(w.tables); dfree(w.qp); dfree(w.qnorm); dfree(w.wq);
+    dfree(w.winv); dfree(w.wq256); dfree(w.winv256); dfree(w.probe_n); dfree(w.scanned);
+    dfree(w.thr); dfree(w.ccount); dfree(w.overflow); dfree(w.cn); dfree(w.ln); dfree(w.out_n);
+    if ((rc = dalloc(&w.q768, (size_t)n * SG_DIM)) || (rc = dalloc(&w.q256, (size_t)n * SG_PDIM)) ||
+        (rc = dalloc(&w.tables, (size_t)n * SG_GROUPS * 16)) || (rc = dalloc(&w.qp, n)) ||
+        (rc = dalloc(&w.qnorm, n)) || (rc = dalloc(&w.wq, (size_t)n * SG_DIM)) ||
+        (rc = dalloc(&w.winv, n)) || (rc = dalloc(&w.wq256, (size_t)n * SG_PDIM)) ||
+        (rc = dalloc(&w.winv256, n)) || (rc = dalloc(&w.probe_n, n)) ||
+        (rc = dalloc(&w.scanned, n)) || (rc = dalloc(&w.thr, n)) || (rc = dalloc(&w.ccount, n)) ||
+        (rc = dalloc(&w.overflow, n)) || (rc = dalloc(&w.cn, n)) || (rc = dalloc(&w.ln, n)) ||
+        (rc = dalloc(&w.out_n, n)))
+      return rc;
+    w.nq_cap = n;
+    w.P_cap = w.cand_cap = w.k_cap = 0;
+    w.scores_cap = 0;
+    w.item_cap = 0;
+    w.cbuf_cap = 0;
+  }
+  const uint32_t n = w.nq_cap;
+  if ((uint64_t)n * x.k > w.scores_cap) {
+    dfree(w.scores);
+    if ((rc = dalloc(&w.scores, (size_t)n * x.k))) return rc;
+    w.scores_cap = (uint64_t)n * x.k;
+  }
+  if (P > w.P_cap) {
+    dfree(w.probe_sc); dfree(w.probe_cl); dfree(w.probe_off);
+    if ((rc = dalloc(&w.probe_sc, (size_t)n * P)) || (rc = dalloc(&w.probe_cl, (size_t)n * P)) ||
+        (rc = dalloc(&w.probe_off, (size_t)n * P)))
+      return rc;
+    w.P_cap = P;
+  }
+  if (cand > w.cand_cap) {
+    dfree(w.cest); dfree(w.cid); dfree(w.cerr); dfree(w.lid); dfree(w.lsc);
+    if ((rc = dalloc(&w.cest, (size_t)n * cand)) || (rc = dalloc(&w.cid, (size_t)n * cand)) ||
+        (rc = dalloc(&w.cerr, (size_t)n * cand)) || (rc = dalloc(&w.lid, (size_t)n * cand)) ||
+        (rc = dalloc(&w.lsc, (size_t)n * cand)))
+      return rc;
+    w.cand_cap = cand;
+  }
+  if (k > w.k_cap) {
+    dfree(w.out_sc); dfree(w.out_id);
+    if ((rc = dalloc(&w.out_sc, (size_t)n * k)) || (rc = dalloc(&w.out_id, (size_t)n * k))) return rc;
+    w.k_cap = k;
+  }
+  const uint64_t items = (uint64_t)nq * x.h_chunks_desc_prefix[P];
+  if (items > w.item_cap) {
+    dfree(w.items);
+    uint64_t want = std::max<uint64_t>(items, w.item_cap * 2);
+    if ((rc = dalloc(&w.items, want))) return rc;
+    w.item_cap = want;
+  }
+  if (!w.counters && (rc = dalloc(&w.counters, 4))) return rc;
+  const uint64_t cb = (uint64_t)nq * cbuf_per_q;
+  if (cb > w.cbuf_cap) {
+    dfree(w.cbuf);
+    if ((rc = dalloc(&w.cbuf, cb))) return rc;
+    w.cbuf_cap = cb;
+  }
+  w.cbuf_per_q = cbuf_per_q;
+  return SG_OK;
+}
+
+int check_params(const sg_index* h, const sg_params* p) {
+  if (!p) return fail(SG_ERR_INVALID, "params is null");
+  if (p->cand > sg::kMaxCand || p->k > sg::kMaxCand || p->rerank_r > sg::kMaxCand)
+    return fail(SG_ERR_INVALID, "cand, k and rerank_r must be <= 4096");
+  if (std::min<uint32_t>(p->nprobe, h->ix.k) > 4096)
+    return fail(SG_ERR_INVALID, "nprobe must be <= 4096");
+  if (p->rerank_kind > SG_RERANK_SSD) return fail(SG_ERR_INVALID, "unknown rerank kind");
+  if ((p->rerank_kind == SG_RERANK_PREFIX ||
+       (p->rerank_kind == SG_RERANK_TIERED && !h->ix.has_t2)) &&
+      !h->ix.norm256)
+    return fail(SG_ERR_UNSUPPORTED, "prefix rerank needs norm256.f32");
+  if (p->has_prune && !(p->prune_w == p->prune_w)) return fail(SG_ERR_INVALID, "prune_w is NaN");
+  return SG_OK;
+}
+
+// Per-query candidate buffer: every chunk appends at most `cand`, so chunks x cand is exact.
+uint32_t full_cap(const sg_index* h, const sg_params& p) {
+  const uint32_t P = std::min<uint32_t>(p.nprobe, h->ix.k);
+  uint64_t b = (uint64_t)h->ix.h_chunks_desc_prefix[P] * std::max<uint32_t>(p.cand, 1);
+  return (uint32_t)std::min<uint64_t>(std::max<uint64_t>(b, 1), 0x7FFFFFFFull);
+}
+
+uint32_t batch_cap(const sg_index* h, const sg_params& p, uint32_t nq) {
+  uint32_t full = full_cap(h, p);
+  if (nq <= 8) return full;
+  uint32_t soft = std::max<uint32_t>(16 * std::max<uint32_t>(p.cand, 1), 65536);
+  return std::min(full, soft);
+}
+
+enum Stage { kToCandidates = 1, kToSearch = 2 };
+
+// Runs the pipeline on queries already in ws.q768 / ws.q256 (have_q256 = false: derive it).
+int run_pipeline(sg_index* h, uint32_t nq, const sg_params& p, bool have_q256,
+                 const uint64_t* d_allow, uint64_t allow_words, Stage stage, bool timed) {
+  sg::Workspace& w = h->ws;
+  sg::DevIndex& x = h->ix;
+  cudaStream_t st = h->stream;
+  CK(cudaMemsetAsync(w.counters, 0, 4 * sizeof(uint32_t), st));
+  CK(cudaMemsetAsync(w.thr, 0, nq * sizeof(uint32_t), st));
+  CK(cudaMemsetAsync(w.ccount, 0, nq * sizeof(uint32_t), st));
+  CK(cudaMemsetAsync(w.overflow, 0, nq, st));
+  if (timed) CK(cudaEventRecord(w.ev[0], st));
+  if (!have_q256) sg::launch_prefix(w, nq, st);
+  sg::launch_prep(x, w, nq, st);
+  sg::launch_route_scores(x, w, nq, x.route_precision, st);
+  sg::launch_route_select(x, w, nq, p, x.route_precision, h->cfg.chunk_blocks, st);
+  if (timed) CK(cudaEventRecord(w.ev[1], st));
+  if (p.cand > 0) {
+    sg::launch_scan(x, w, nq, p, d_allow, allow_words, h->sms, st);
+    sg::launch_cut(x, w, nq, p, st);
+  } else {
+    CK(cudaMemsetAsync(w.cn, 0, nq * sizeof(uint32_t), st));
+  }
+  if (timed) CK(cudaEventRecord(w.ev[2], st));
+  if (stage == kToSearch)
+    sg::launch_rerank(x, w, nq, p, st, timed ? w.ev[4] : nullptr, timed ? w.ev[5] : nullptr);
+  if (timed) CK(cudaEventRecord(w.ev[3], st));
+  CK(cudaGetLastError());
+  return SG_OK;
+}
+
+int stage_inputs(sg_index* h, uint32_t nq, const float* q768, const float* q256, bool device) {
+  sg::Workspace& w = h->ws;
+  cudaMemcpyKind kind = device ? cudaMemcpyDeviceToDevice : cudaMemcpyDefault;
+  if (q768) CK(cudaMemcpyAsync(w.q768, q768, (size_t)nq * SG_DIM * 4, kind, h->stream));
+  else CK(cudaMemsetAsync(w.q768, 0, (size_t)nq * SG_DIM * 4, h->stream));
+  if (q256) CK(cudaMemcpyAsync(w.q256, q256, (size_t)nq * SG_PDIM * 4, kind, h->stream));
+  return SG_OK;
+}
+
+int stage_allow(sg_index* h, const uint64_t* allow, uint64_t words, bool device,
+                const uint64_t** d_allow) {
+  *d_allow = nullptr;
+  if (!allow) return SG_OK;
+  if (device) {
+    *d_allow = allow;
+    return SG_OK;
+  }
+  sg::Workspace& w = h->ws;
+  if (words > w.allow_cap) {
+    dfree(w.allow);
+    int rc = dalloc(&w.allow, words);
+    if (rc) return rc;
+    w.allow_cap = words;
+  }
+  CK(cudaMemcpyAsync(w.allow, allow, words * 8, cudaMemcpyDefault, h->stream));
+  *d_allow = w.allow;
+  return SG_OK;
+}
+
+// Full search of nq queries with inputs staged; copies results out (kind: D2H or D2D).
+int search_impl(sg_index* h, uint32_t nq, const float* q768, const float* q256,
+                const sg_params& p, const uint64_t* allow, uint64_t allow_words, float* out_sc,
+                uint32_t* out_id, uint32_t* out_n, sg_timing* t, bool device) {
+  int rc;
+  if ((rc = check_params(h, &p))) return rc;
+  if (nq == 0) return SG_OK;
+  if (!q768) return fail(SG_ERR_INVALID, "q768 is null");
+  CK(cudaSetDevice(h->ix.device));
+  uint32_t cap = batch_cap(h, p, nq);
+  if ((rc = ensure_ws(h, nq, p, cap))) return rc;
+  if ((rc = stage_inputs(h, nq, q768, q256, device))) return rc;
+  const uint64_t* d_allow;
+  if ((rc = stage_allow(h, allow, allow_words, device, &d_allow))) return rc;
+  if ((rc = run_pipeline(h, nq, p, q256 != nullptr, d_allow, allow_words, kToSearch, t != nullptr)))
+    return rc;
+  sg::Workspace& w = h->ws;
+  std::vector<uint8_t> ovf(nq);
+  CK(cudaMemcpyAsync(ovf.data(), w.overflow, nq, cudaMemcpyDeviceToHost, h->stream));
+  uint32_t status = 0;
+  CK(cudaMemcpyAsync(&status, w.counters + 2, 4, cudaMemcpyDeviceToHost, h->stream));
+  const uint32_t k = p.k;
+  cudaMemcpyKind okind = device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost;
+  if (k) {
+    CK(cudaMemcpyAsync(out_sc, w.out_sc, (size_t)nq * k * 4, okind, h->stream));
+    CK(cudaMemcpyAsync(out_id, w.out_id, (size_t)nq * k * 4, okind, h->stream));
+  }
+  CK(cudaMemcpyAsync(out_n, w.out_n, (size_t)nq * 4, okind, h->stream));
+  std::vector<uint64_t> scanned;
+  std::vector<uint32_t> probed, reranked;
+  if (t) {
+    scanned.resize(nq);
+    probed.resize(nq);
+    reranked.resize(nq);
+    CK(cudaMemcpyAsync(scanned.data(), w.scanned, nq * 8, cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaMemcpyAsync(probed.data(), w.probe_n, nq * 4, cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaMemcpyAsync(reranked.data(), w.ln, nq * 4, cudaMemcpyDeviceToHost, h->stream));
+  }
+  CK(cudaStreamSynchronize(h->stream));
+  if (status & sg::kStatusOverflow) return fail(SG_ERR_INVALID, "work queue overflow");
+  if (t) {
+    float ms[4] = {0, 0, 0, 0};
+    cudaEventElapsedTime(&ms[0], w.ev[0], w.ev[1]);
+    cudaEventElapsedTime(&ms[1], w.ev[1], w.ev[2]);
+    cudaEventElapsedTime(&ms[2], w.ev[2], w.ev[3]);
+    if (p.rerank_kind == SG_RERANK_TIERED) cudaEventElapsedTime(&ms[3], w.ev[4], w.ev[5]);
+    t->route += (uint64_t)(ms[0] * 1e6);
+    t->scan += (uint64_t)(ms[1] * 1e6);
+    t->rerank += (uint64_t)(ms[2] * 1e6);
+    t->tier2 += (uint64_t)(ms[3] * 1e6);
+    for (uint32_t i = 0; i < nq; i++) {
+      t->scanned += scanned[i];
+      t->probed += probed[i];
+      t->reranked += reranked[i];
+    }
+  }
+  // queries whose candidate buffer filled up run again alone with the exact bound
+  for (uint32_t i = 0; i < nq; i++) {
+    if (!ovf[i]) continue;
+    const uint64_t* al = allow;
+    const float* q1 = q768 + (size_t)i * SG_DIM;
+    const float* q2 = q256 ? q256 + (size_t)i * SG_PDIM : nullptr;
+    uint32_t fcap = full_cap(h, p);
+    if ((rc = ensure_ws(h, 1, p, fcap))) return rc;
+    if ((rc = stage_inputs(h, 1, q1, q2, device))) return rc;
+    if ((rc = stage_allow(h, al, allow_words, device, &d_allow))) return rc;
+    if ((rc = run_pipeline(h, 1, p, q2 != nullptr, d_allow, allow_words, kToSearch, false)))
+      return rc;
+    uint8_t o1 = 0;
+    CK(cudaMemcpyAsync(&o1, w.overflow, 1, cudaMemcpyDeviceToHost, h->stream));
+    if (k) {
+      CK(cudaMemcpyAsync(out_sc + (size_t)i * k, w.out_sc, k * 4, okind, h->stream));
+      CK(cudaMemcpyAsync(out_id + (size_t)i * k, w.out_id, k * 4, okind, h->stream));
+    }
+    CK(cudaMemcpyAsync(out_n + i, w.out_n, 4, okind, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    if (o1) return fail(SG_ERR_INVALID, "candidate buffer overflow at the exact bound");
+    if ((rc = ensure_ws(h, nq, p, cap))) return rc;
+  }
+  return SG_OK;
+}
+
+bool read_file(const std::string& path, std::vector<char>& out, bool optional, int* rc) {
+  std::ifstream f(path, std::ios::binary | std::ios::ate);
+  if (!f) {
+    if (!optional) *rc = fail(SG_ERR_IO, "cannot open " + path);
+    return false;
+  }
+  std::streamsize n = f.tellg();
+  f.seekg(0);
+  out.resize((size_t)n);
+  if (n && !f.read(out.data(), n)) {
+    *rc = fail(SG_ERR_IO, "cannot read " + path);
+    return false;
+  }
+  return true;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* sg_last_error(void) { return sg::last_error().c_str(); }
+
+const char* sg_version(void) { return "sieve_gpu 0.1 (sm_100a)"; }
+
+int sg_open_ivf_arrays(const sg_ivf_arrays* a, int device, sg_index** out) {
+  try {
+    return build_index(a, device, out);
+  } catch (const std::exception& e) {
+    return fail(SG_ERR_OOM, std::string("host allocation: ") + e.what());
+  }
+}
+
+int sg_open_ivf(const char* ingest_dir, const char* index_dir, int device, sg_index** out) {
+  if (!ingest_dir || !index_dir || !out) return fail(SG_ERR_INVALID, "null argument");
+  try {
+    std::string I(ingest_dir), X(index_dir);
+    std::vector<char> cent, boff, ids, blocks, fac, rot, sig, t2c, t2n, rer, n256, qs;
+    int rc = SG_OK;
+    if (!read_file(X + "/centroids.f32", cent, false, &rc) ||
+        !read_file(X + "/block_off.u64", boff, false, &rc) ||
+        !read_file(X + "/ids.u32", ids, false, &rc) ||
+        !read_file(X + "/blocks.bin", blocks, false, &rc) ||
+        !read_file(I + "/rerank.i8", rer, false, &rc) ||
+        !read_file(I + "/norm256.f32", n256, false, &rc) ||
+        !read_file(I + "/quant.f32", qs, false, &rc))
+      return rc;
+    bool has_rot = read_file(X + "/rotation.f32", rot, true, &rc);
+    bool has_fac = read_file(X + "/factors.f32", fac, true, &rc);
+    bool has_t2 = read_file(X + "/tier2.bin", t2c, true, &rc) &&
+                  read_file(X + "/tier2.sigma", sig, false, &rc) &&
+                  read_file(X + "/tier2.norm", t2n, false, &rc);
+    if (rc) return rc;
+    sg_ivf_arrays a;
+    memset(&a, 0, sizeof a);
+    a.n = n256.size() / 4;
+    a.k = (uint32_t)(cent.size() / (4 * SG_PDIM));
+    if (boff.size() != 8 * ((size_t)a.k + 1))
+      return fail(SG_ERR_INVALID, "block_off.u64 does not match centroids");
+    if (rer.size() != a.n * SG_DIM) return fail(SG_ERR_INVALID, "rerank.i8 size");
+    if (qs.size() != 4 * SG_DIM) return fail(SG_ERR_INVALID, "quant.f32 size");
+    a.centroids = (const float*)cent.data();
+    a.block_off = (const uint64_t*)boff.data();
+    uint64_t nb = a.block_off[a.k];
+    if (ids.size() != nb * SG_BLOCK * 4 || blocks.size() != nb * SG_BLOCK_BYTES)
+      return fail(SG_ERR_INVALID, "ids.u32 / blocks.bin do not match block_off.u64");
+    a.ids = (const uint32_t*)ids.data();
+    a.blocks = (const uint8_t*)blocks.data();
+    if (has_fac) {
+      if (fac.size() != nb * SG_BLOCK * 8) return fail(SG_ERR_INVALID, "factors.f32 size");
+      a.factors = (const float*)fac.data();
+    }
+    if (has_rot) {
+      if (rot.size() != 3 * SG_PDIM * 4) return fail(SG_ERR_INVALID, "rotation.f32 is not 3 x 256");
+      a.rotation = (const float*)rot.data();
+    }
+    if (has_t2) {
+      if (t2c.size() != a.n * SG_TIER2_BYTES || t2n.size() != a.n * 4 || sig.size() != SG_PDIM * 4)
+        return fail(SG_ERR_INVALID, "tier2 file sizes");
+      a.tier2_codes = (const uint8_t*)t2c.data();
+      a.tier2_norm = (const float*)t2n.data();
+      a.tier2_sigma = (const float*)sig.data();
+    }
+    a.rerank = (const int8_t*)rer.data();
+    a.norm256 = (const float*)n256.data();
+    a.quant_scale = (const float*)qs.data();
+    return build_index(&a, device, out);
+  } catch (const std::exception& e) {
+    return fail(SG_ERR_OOM, std::string("host allocation: ") + e.what());
+  }
+}
+
+int sg_close(sg_index* h) {
+  if (!h) return SG_OK;
+  cudaSetDevice(h->ix.device);
+  if (h->stream) cudaStreamSynchronize(h->stream);
+  free_ws(h->ws);
+  free_index(h->ix);
+  if (h->stream) cudaStreamDestroy(h->stream);
+  delete h;
+  return SG_OK;
+}
+
+int sg_index_info(const sg_index* h, uint32_t* k, uint64_t* n, uint64_t* nblocks,
+                  uint32_t* has_tier2) {
+  if (!h) return fail(SG_ERR_INVALID, "null index");
+  if (k) *k = h->ix.k;
+  if (n) *n = h->ix.n;
+  if (nblocks) *nblocks = h->ix.nblocks;
+  if (has_tier2) *has_tier2 = h->ix.has_t2;
+  return SG_OK;
+}
+
+int sg_set_route_precision(sg_index* h, int precision) {
+  if (!h) return fail(SG_ERR_INVALID, "null index");
+  if (precision != SG_ROUTE_FP32 && precision != SG_ROUTE_BF16)
+    return fail(SG_ERR_INVALID, "precision must be SG_ROUTE_FP32 or SG_ROUTE_BF16");
+  h->ix.route_precision = precision;
+  return SG_OK;
+}
+
+int sg_search(sg_index* h, uint32_t nq, const float* q768, const float* q256,
+              const sg_params* params, const uint64_t* allow_bits, uint64_t allow_words,
+              float* out_scores, uint32_t* out_ids, uint32_t* out_counts, sg_timing* timing) {
+  if (!h || !params) return fail(SG_ERR_INVALID, "null argument");
+  std::lock_guard<std::mutex> g(h->mu);
+  return search_impl(h, nq, q768, q256, *params, allow_bits, allow_words, out_scores, out_ids,
+                     out_counts, timing, false);
+}
+
+int sg_search_device(sg_index* h, uint32_t nq, const float* d_q768, const float* d_q256,
+                     const sg_params* params, const uint64_t* d_allow_bits, uint64_t allow_words,
+                     float* d_out_scores, uint32_t* d_out_ids, uint32_t* d_out_counts,
+                     void* stream) {
+  if (!h || !params) return fail(SG_ERR_INVALID, "null argument");
+  std::lock_guard<std::mutex> g(h->mu);
+  cudaStream_t user = (cudaStream_t)stream;
+  // order the index stream after the caller's stream, and the caller's after the results
+  cudaEvent_t ev;
+  CK(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+  CK(cudaEventRecord(ev, user));
+  CK(cudaStreamWaitEvent(h->stream, ev, 0));
+  int rc = search_impl(h, nq, d_q768, d_q256, *params, d_allow_bits, allow_words, d_out_scores,
+                       d_out_ids, d_out_counts, nullptr, true);
+  cudaEventDestroy(ev);
+  return rc;
+}
+
+int sg_route(sg_index* h, uint32_t nq, const float* q256, const sg_params* params,
+             float* out_scores, uint32_t* out_clusters, uint32_t* out_counts) {
+  if (!h || !params || !q256) return fail(SG_ERR_INVALID, "null argument");
+  std::lock_guard<std::mutex> g(h->mu);
+  int rc;
+  if ((rc = check_params(h, params))) return rc;
+  if (nq == 0) return SG_OK;
+  CK(cudaSetDevice(h->ix.device));
+  if ((rc = ensure_ws(h, nq, *params, 1))) return rc;
+  if ((rc = stage_inputs(h, nq, nullptr, q256, false))) return rc;
+  sg::Workspace& w = h->ws;
+  cudaStream_t st = h->stream;
+  CK(cudaMemsetAsync(w.counters, 0, 16, st));
+  sg::launch_prep(h->ix, w, nq, st);
+  sg::launch_route_scores(h->ix, w, nq, h->ix.route_precision, st);
+  sg::launch_route_select(h->ix, w, nq, *params, h->ix.route_precision, h->cfg.chunk_blocks, st);
+  CK(cudaGetLastError());
+  const uint32_t P = std::min<uint32_t>(params->nprobe, h->ix.k);
+  if (P) {
+    CK(cudaMemcpyAsync(out_scores, w.probe_sc, (size_t)nq * P * 4, cudaMemcpyDeviceToHost, st));
+    CK(cudaMemcpyAsync(out_clusters, w.probe_cl, (size_t)nq * P * 4, cudaMemcpyDeviceToHost, st));
+  }
+  CK(cudaMemcpyAsync(out_counts, w.probe_n, (size_t)nq * 4, cudaMemcpyDeviceToHost, st));
+  CK(cudaStreamSynchronize(st));
+  return SG_OK;
+}
+
+int sg_candidates(sg_index* h, uint32_t nq, const float* q256, const sg_params* params,
+                  const uint64_t* allow_bits, uint64_t allow_words, float* out_est,
+                  uint32_t* out_ids, float* out_err, uint32_t* out_counts) {
+  if (!h || !params || !q256) return fail(SG_ERR_INVALID, "null argument");
+  std::lock_guard<std::mutex> g(h->mu);
+  int rc;
+  if ((rc = check_params(h, params))) return rc;
+  if (nq == 0) return SG_OK;
+  CK(cudaSetDevice(h->ix.device));
+  const sg_params& p = *params;
+  uint32_t cap = full_cap(h, p);
+  for (uint32_t q0 = 0; q0 < nq; q0++) {
+    // one query at a time with the exact buffer bound: this entry point is for parity checks
+    if ((rc = ensure_ws(h, 1, p, cap))) return rc;
+    if ((rc = stage_inputs(h, 1, nullptr, q256 + (size_t)q0 * SG_PDIM, false))) return rc;
+    const uint64_t* d_allow;
+    if ((rc = stage_allow(h, allow_bits, allow_words, false, &d_allow))) return rc;
+    if ((rc = run_pipeline(h, 1, p, true, d_allow, allow_words, kToCandidates, false))) return rc;
+    sg::Workspace& w = h->ws;
+    const uint32_t c = std::max<uint32_t>(p.cand, 1);
+    if (p.cand) {
+      CK(cudaMemcpyAsync(out_est + (size_t)q0 * c, w.cest, (size_t)c * 4, cudaMemcpyDeviceToHost, h->stream));
+      CK(cudaMemcpyAsync(out_ids + (size_t)q0 * c, w.cid, (size_t)c * 4, cudaMemcpyDeviceToHost, h->stream));
+      CK(cudaMemcpyAsync(out_err + (size_t)q0 * c, w.cerr, (size_t)c * 4, cudaMemcpyDeviceToHost, h->stream));
+    }
+    CK(cudaMemcpyAsync(out_counts + q0, w.cn, 4, cudaMemcpyDeviceToHost, h->stream));
+    uint8_t o = 0;
+    CK(cudaMemcpyAsync(&o, w.overflow, 1, cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    if (o) return fail(SG_ERR_INVALID, "candidate buffer overflow at the exact bound");
+  }
+  return SG_OK;
+}
+
+int sg_query_prep(sg_index* h, uint32_t nq, const float* q256, uint8_t* out_tables,
+                  float* out_scale, float* out_bias, float* out_a, float* out_b) {
+  if (!h || !q256) return fail(SG_ERR_INVALID, "null argument");
+  std::lock_guard<std::mutex> g(h->mu);
+  if (nq == 0) return SG_OK;
+  CK(cudaSetDevice(h->ix.device));
+  sg_params p;
+  memset(&p, 0, sizeof p);
+  p.nprobe = 1;
+  p.cand = 1;
+  p.k = 1;
+  int rc;
+  if ((rc = ensure_ws(h, nq, p, 1))) return rc;
+  if ((rc = stage_inputs(h, nq, nullptr, q256, false))) return rc;
+  sg::launch_prep(h->ix, h->ws, nq, h->stream);
+  CK(cudaGetLastError());
+  std::vector<float4> qp(nq);
+  CK(cudaMemcpyAsync(out_tables, h->ws.tables, (size_t)nq * 1024, cudaMemcpyDeviceToHost, h->stream));
+  CK(cudaMemcpyAsync(qp.data(), h->ws.qp, nq * sizeof(float4), cudaMemcpyDeviceToHost, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  for (uint32_t i = 0; i < nq; i++) {
+    if (out_scale) out_scale[i] = qp[i].x;
+    if (out_bias) out_bias[i] = qp[i].y;
+    if (out_a) out_a[i] = qp[i].z;
+    if (out_b) out_b[i] = qp[i].w;
+  }
+  return SG_OK;
+}
+
+int sg_lut_scan(uint32_t groups, const uint8_t* tables, const uint8_t* blocks, uint64_t nblocks,
+                uint16_t* out_scores) {
+  if (groups != 64 && groups != 32) return fail(SG_ERR_INVALID, "groups must be 64 or 32");
+  if (!tables || (!blocks && nblocks) || (!out_scores && nblocks))
+    return fail(SG_ERR_INVALID, "null argument");
+  if (nblocks == 0) return SG_OK;
+  uint8_t *dt = nullptr, *db = nullptr;
+  uint16_t* dout = nullptr;
+  int rc;
+  if ((rc = dalloc(&dt, groups * 16)) || (rc = dalloc(&db, nblocks * groups * 16)) ||
+      (rc = dalloc(&dout, nblocks * SG_BLOCK))) {
+    dfree(dt); dfree(db); dfree(dout);
+    return rc;
+  }
+  cudaError_t e = cudaMemcpy(dt, tables, groups * 16, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMemcpy(db, blocks, nblocks * groups * 16, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) {
+    sg::launch_lut_scan(groups, dt, db, nblocks, dout, 0);
+    e = cudaGetLastError();
+  }
+  if (e == cudaSuccess)
+    e = cudaMemcpy(out_scores, dout, nblocks * SG_BLOCK * 2, cudaMemcpyDeviceToHost);
+  dfree(dt); dfree(db); dfree(dout);
+  if (e != cudaSuccess) return fail(SG_ERR_DEVICE, std::string("sg_lut_scan: ") + cudaGetErrorString(e));
+  return SG_OK;
+}
+
+int sg_dot_i8i8(const int8_t* query, const int8_t* rows, uint64_t nrows, uint32_t dim,
+                int32_t* out_dots) {
+  if (dim == 0 || dim % 4) return fail(SG_ERR_INVALID, "dim must be a positive multiple of 4");
+  if (!query || (!rows && nrows) || (!out_dots && nrows)) return fail(SG_ERR_INVALID, "null argument");
+  if (nrows == 0) return SG_OK;
+  int8_t *dq = nullptr, *dr = nullptr;
+  int32_t* dout = nullptr;
+  int rc;
+  if ((rc = dalloc(&dq, dim)) || (rc = dalloc(&dr, nrows * dim)) || (rc = dalloc(&dout, nrows))) {
+    dfree(dq); dfree(dr); dfree(dout);
+    return rc;
+  }
+  cudaError_t e = cudaMemcpy(dq, query, dim, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMemcpy(dr, rows, nrows * dim, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) {
+    sg::launch_dot_i8i8(dq, dr, nrows, dim, dout, 0);
+    e = cudaGetLastError();
+  }
+  if (e == cudaSuccess) e = cudaMemcpy(out_dots, dout, nrows * 4, cudaMemcpyDeviceToHost);
+  dfree(dq); dfree(dr); dfree(dout);
+  if (e != cudaSuccess) return fail(SG_ERR_DEVICE, std::string("sg_dot_i8i8: ") + cudaGetErrorString(e));
+  return SG_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,179 @@
+/*
+ * sieve_gpu.h — C ABI of the B200 (sm_100a) query path of the sieve IVF engine.
+ *
+ * The reference (a Rust crate) has no FFI; its query API is the in-process Rust API of
+ * `ivf::Index` / `ivf::Corpus` / `ivf::Params` / `filter::search` / `bigann::Index`. Each entry
+ * point below replaces one of those calls and names the reference item it stands for.
+ *
+ * Conventions
+ *   - Every function returns an int status: SG_OK (0) or a negative SG_ERR_* code. Nothing
+ *     aborts across the boundary; sg_last_error() gives a message for the calling thread.
+ *   - The library owns all device memory it allocates; callers own their host buffers.
+ *   - Functions named *_device take device pointers (inputs already resident in HBM) and a
+ *     cudaStream_t passed as void*; everything else takes host pointers and copies.
+ *   - Vectors are row-major float32 (queries) or int8 (rerank rows); ids are uint32 corpus rows.
+ *   - Results are (score, id) best first, ties broken by ascending id, exactly as the
+ *     reference's TopK::into_sorted orders them (src/topk.rs:57-61).
+ */
+#ifndef SIEVE_GPU_H
+#define SIEVE_GPU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ------------------------------------------------------------------------ */
+#define SG_OK 0
+#define SG_ERR_INVALID -1    /* bad argument or inconsistent index files                     */
+#define SG_ERR_IO -2         /* a file could not be read                                       */
+#define SG_ERR_OOM -3        /* device or host allocation failed                               */
+#define SG_ERR_DEVICE -4     /* a CUDA call failed                                             */
+#define SG_ERR_TIMEOUT -5    /* a bounded device-side wait gave up                             */
+#define SG_ERR_ADMISSION -6  /* serving: no scratch free for this request right now            */
+#define SG_ERR_UNSUPPORTED -7 /* the index lacks the files this request needs                  */
+
+/* ---- constants of the reference (src/lib.rs:21-26, src/lut.rs:42-44, src/ivf.rs:18) -------- */
+#define SG_DIM 768          /* full embedding width                                           */
+#define SG_PDIM 256         /* Matryoshka prefix the codes are built from                     */
+#define SG_CODE_BYTES 32    /* 1-bit code of the prefix                                       */
+#define SG_GROUPS 64        /* 4-dim LUT groups of the prefix                                 */
+#define SG_BLOCK 32         /* slots per nibble-transposed block                              */
+#define SG_BLOCK_BYTES 1024 /* GROUPS * 16                                                    */
+#define SG_TIER2_BYTES 64   /* 2-bit middle tier code (src/tier2.rs:7)                        */
+#define SG_PAD 0xFFFFFFFFu  /* id of a padding slot                                           */
+
+/* ---- ivf::Rerank (src/ivf.rs:425-439) --------------------------------------------------- */
+typedef enum {
+  SG_RERANK_NONE = 0,   /* Rerank::None: order by the code estimate                           */
+  SG_RERANK_PREFIX = 1, /* Rerank::Prefix: int8 256-d prefix cosine                           */
+  SG_RERANK_FULL = 2,   /* Rerank::Full: int8 768-d dot of every candidate                     */
+  SG_RERANK_TIERED = 3, /* Rerank::Tiered(r): 2-bit tier (or prefix) to r, then full           */
+  SG_RERANK_SSD = 4     /* Rerank::Ssd(r): best r by estimate, then full (rows are in HBM)     */
+} sg_rerank_kind;
+
+/* ---- ivf::Params (src/ivf.rs:441-460) --------------------------------------------------- */
+typedef struct {
+  uint32_t nprobe;      /* clusters probed (cap)                                                */
+  uint32_t cand;        /* candidates kept by the code scan                                     */
+  uint32_t rerank_kind; /* sg_rerank_kind                                                       */
+  uint32_t rerank_r;    /* r of Tiered(r) / Ssd(r)                                              */
+  uint32_t k;           /* results returned                                                     */
+  uint32_t has_prune;   /* prune: Some((prune_m, prune_w))                                      */
+  uint32_t prune_m;
+  float prune_w;
+  uint32_t has_margin;  /* margin: Some(margin)                                                 */
+  float margin;
+  uint32_t has_budget;  /* budget: Some(budget) in stored slots                                 */
+  uint32_t reserved;
+  uint64_t budget;
+} sg_params;
+
+/* ---- ivf::Timing (src/ivf.rs:521-538): device times of one call, in nanoseconds ----------- */
+typedef struct {
+  uint64_t route;    /* routing GEMM + probe selection                                         */
+  uint64_t scan;     /* query prep + LUT scan + candidate cut + dedup                          */
+  uint64_t rerank;   /* pruning + tier-2 + int8 rerank                                         */
+  uint64_t tier2;    /* part of rerank spent in the 2-bit tier                                 */
+  uint64_t scanned;  /* slots scanned (padding included), summed over queries                  */
+  uint64_t reranked; /* candidates reaching the rerank stage after dedup and pruning           */
+  uint64_t probed;   /* clusters scanned                                                       */
+  uint64_t fetch;    /* always 0: no SSD tier                                                  */
+  uint64_t wait;     /* always 0: no shard fan-out                                             */
+} sg_timing;
+
+/* Routing precision. FP32 scores every centroid with the reference's sequential f32 dot
+ * (src/blas.rs:43-54). BF16 runs the tensor-core GEMM, then rescores in FP32 every centroid
+ * whose BF16 score lies inside the rigorous error window of the nprobe-th best, so the probe
+ * set and the centroid scores equal the FP32 path's exactly. */
+typedef enum { SG_ROUTE_FP32 = 0, SG_ROUTE_BF16 = 1 } sg_route_precision;
+
+typedef struct sg_index sg_index;
+typedef struct sg_filter sg_filter;
+
+/* Host arrays of an IVF index plus its corpus, laid out exactly as the reference's files
+ * (src/ivf.rs:75-90 Corpus::open, src/ivf.rs:553-578 Index::open). Optional members may be
+ * NULL: tier2_* (no 2-bit tier), rotation/factors (global sign-code index, unsupported here),
+ * norm256 (no prefix rerank). */
+typedef struct {
+  uint64_t n;                 /* corpus rows                                                   */
+  uint32_t k;                 /* clusters                                                      */
+  const float* centroids;     /* centroids.f32   [k * 256]                                     */
+  const uint64_t* block_off;  /* block_off.u64   [k + 1]                                       */
+  const uint32_t* ids;        /* ids.u32         [nblocks * 32]                                */
+  const uint8_t* blocks;      /* blocks.bin      [nblocks * 1024]                              */
+  const float* factors;       /* factors.f32     [nblocks * 32 * 2] = [mul, err] per slot      */
+  const float* rotation;      /* rotation.f32    [3 * 256] signs                               */
+  const float* tier2_sigma;   /* tier2.sigma     [256]                                         */
+  const uint8_t* tier2_codes; /* tier2.bin       [n * 64]                                      */
+  const float* tier2_norm;    /* tier2.norm      [n]                                           */
+  const int8_t* rerank;       /* rerank.i8       [n * 768]                                     */
+  const float* norm256;       /* norm256.f32     [n]                                           */
+  const float* quant_scale;   /* quant.f32       [768]                                         */
+} sg_ivf_arrays;
+
+/* ---- errors ----------------------------------------------------------------------------- */
+const char* sg_last_error(void);
+/* Library version string and the device it was built for. */
+const char* sg_version(void);
+
+/* ---- open / close ----------------------------------------------------------------------- */
+/* ivf::Corpus::open(ingest_dir) + ivf::Index::open(index_dir) (src/ivf.rs:75-90, :553-578):
+ * reads the reference's files and uploads them to HBM on `device`. */
+int sg_open_ivf(const char* ingest_dir, const char* index_dir, int device, sg_index** out);
+/* The same from host arrays already in memory (the files' contents). */
+int sg_open_ivf_arrays(const sg_ivf_arrays* a, int device, sg_index** out);
+int sg_close(sg_index* index);
+/* Index facts: clusters, corpus rows, blocks, whether a 2-bit tier is resident. */
+int sg_index_info(const sg_index* index, uint32_t* k, uint64_t* n, uint64_t* nblocks,
+                  uint32_t* has_tier2);
+int sg_set_route_precision(sg_index* index, int precision);
+
+/* ---- search ----------------------------------------------------------------------------- */
+/* ivf::Index::search / search_view (src/ivf.rs:621-633) for nq queries at once.
+ * q768 [nq*768] and q256 [nq*256] are unit length (q256 may be NULL: it is then the
+ * renormalised prefix of q768, as quant::prefix, src/quant.rs:17-20). params is one sg_params
+ * shared by all queries. allow_bits (nullable, allow_words u64 words) is View::allow
+ * (src/ivf.rs:465-483): only rows with a set bit are returned. Outputs: out_scores/out_ids
+ * [nq * params.k], out_counts [nq] (results per query, <= k). timing is nullable. */
+int sg_search(sg_index* index, uint32_t nq, const float* q768, const float* q256,
+              const sg_params* params, const uint64_t* allow_bits, uint64_t allow_words,
+              float* out_scores, uint32_t* out_ids, uint32_t* out_counts, sg_timing* timing);
+/* The same with every pointer on the device and the work issued on `stream` (cudaStream_t). */
+int sg_search_device(sg_index* index, uint32_t nq, const float* d_q768, const float* d_q256,
+                     const sg_params* params, const uint64_t* d_allow_bits,
+                     uint64_t allow_words, float* d_out_scores, uint32_t* d_out_ids,
+                     uint32_t* d_out_counts, void* stream);
+
+/* ivf::Index::route (src/ivf.rs:589-613): the probe list of each query, best first, as
+ * (centroid score, cluster). out_scores/out_clusters [nq * params.nprobe], out_counts [nq]. */
+int sg_route(sg_index* index, uint32_t nq, const float* q256, const sg_params* params,
+             float* out_scores, uint32_t* out_clusters, uint32_t* out_counts);
+
+/* ivf::Index::candidates (src/ivf.rs:647-729) over the index's own routing: the best
+ * params.cand slots by RaBitQ estimate, deduplicated by row, in row order, as
+ * (estimate, row, error half-width). out_* [nq * params.cand], out_counts [nq]. */
+int sg_candidates(sg_index* index, uint32_t nq, const float* q256, const sg_params* params,
+                  const uint64_t* allow_bits, uint64_t allow_words, float* out_est,
+                  uint32_t* out_ids, float* out_err, uint32_t* out_counts);
+
+/* ---- kernel-level entry points (parity tests and micro-benchmarks) ----------------------- */
+/* rabitq::Query::new (src/rabitq.rs:119-125) on the device: rotated LUT tables [nq*64*16] u8,
+ * and per query scale, bias, a, b. */
+int sg_query_prep(sg_index* index, uint32_t nq, const float* q256, uint8_t* out_tables,
+                  float* out_scale, float* out_bias, float* out_a, float* out_b);
+/* lut::scan (src/lut.rs:96-126) for G = groups (64 or 32): u16 scores of nblocks blocks,
+ * 32 per block, against one u8 table set [groups * 16]. Stateless (no index needed). */
+int sg_lut_scan(uint32_t groups, const uint8_t* tables, const uint8_t* blocks, uint64_t nblocks,
+                uint16_t* out_scores);
+/* quant::dot_i8i8 (src/quant.rs:113-125) of one int8 query against `rows` int8 rows of
+ * length dim (a multiple of 4): exact int32 dots. Stateless. */
+int sg_dot_i8i8(const int8_t* query, const int8_t* rows, uint64_t nrows, uint32_t dim,
+                int32_t* out_dots);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* SIEVE_GPU_H */

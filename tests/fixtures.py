@@ -1,0 +1,54 @@
+"""Seeded small corpora and indexes shared by the tests (built on the CPU with the builder).
+
+INDEX_A: 20,000 rows, 64 clusters, SOAR, 2-bit tier — clusters of about one scan chunk.
+INDEX_B: 30,000 rows with 400 exact duplicates, 8 clusters — clusters span several scan chunks,
+         and the duplicates make exactly tied estimates and tied int8 scores.
+Queries come from the same mixtures (sigma 0.35) plus copies of corpus rows (self-matches).
+"""
+from __future__ import annotations
+
+import functools
+
+import numpy as np
+import torch
+
+from sieve_gpu import builder, synth
+
+import oracle as O
+
+
+def prefixes(q768: np.ndarray) -> np.ndarray:
+    return np.stack([O.prefix(v)[0] for v in q768]).astype(np.float32)
+
+
+@functools.lru_cache(maxsize=None)
+def index_a():
+    torch.manual_seed(0)
+    mix = synth.Mixture(n=20000, n_centers=64, seed=3)
+    corpus = builder.ingest(mix)
+    ix = builder.build_ivf(corpus, k=64, sample_n=20000, iters=8)
+    arrays = {**corpus, **ix}
+    q = mix.queries(48, sigma=0.35).numpy()
+    rows = mix.rows(100, 16).numpy()  # self-match queries
+    q768 = np.concatenate([q, rows]).astype(np.float32)
+    return arrays, q768, prefixes(q768), mix
+
+
+@functools.lru_cache(maxsize=None)
+def index_b():
+    mix = synth.Mixture(n=30000, n_centers=24, seed=5)
+    corpus = builder.ingest(mix)
+    # 400 exact duplicates: rows 0..99 repeated 4 more times at the end
+    dup = np.concatenate([corpus["rerank"][:100]] * 4)
+    corpus["rerank"] = np.concatenate([corpus["rerank"], dup])
+    corpus["norm256"] = np.concatenate([corpus["norm256"], np.tile(corpus["norm256"][:100], 4)])
+    corpus["codes"] = np.concatenate([corpus["codes"], np.tile(corpus["codes"][:100], (4, 1))])
+    corpus["n"] = corpus["rerank"].shape[0]
+    ix = builder.build_ivf(corpus, k=8, sample_n=30400, iters=6)
+    arrays = {**corpus, **ix}
+    q = mix.queries(24, sigma=0.35).numpy()
+    # queries near the duplicated rows: ties among their copies
+    rows = (corpus["rerank"][:8].astype(np.float32) / corpus["quant_scale"])
+    rows /= np.linalg.norm(rows, axis=1, keepdims=True)
+    q768 = np.concatenate([q, rows]).astype(np.float32)
+    return arrays, q768, prefixes(q768), mix
