@@ -13,8 +13,11 @@
 
 namespace sg {
 
-// Blocks (32 slots) a scan work item covers at most; the scan CTA holds one chunk's estimates.
-constexpr uint32_t kChunkBlocks = 64;
+// Blocks (32 slots) a scan work item covers at most; the scan CTA holds one chunk's estimates
+// in shared memory (4 B per slot), so kMaxChunkBlocks = 512 is 64 KB.
+constexpr uint32_t kMaxChunkBlocks = 512;
+constexpr uint32_t kChunkBlocks = 256;   // default chunk of the batched scan
+constexpr uint32_t kSeedBlocks = 512;    // rank-0 blocks each query's seed item covers
 // Largest cand / k / r the select kernels sort in shared memory.
 constexpr uint32_t kMaxCand = 4096;
 // Status bits a kernel raises in Workspace::status.
@@ -72,6 +75,7 @@ struct Workspace {
   uint32_t* probe_n = nullptr;   // [nq]
   uint64_t* scanned = nullptr;   // [nq]
   uint4* items = nullptr;        // [item_cap] (query, probe rank, first block, end block)
+  uint4* seed_items = nullptr;   // [nq] each query's first rank-0 chunk (the seed)
   uint32_t* counters = nullptr;  // [4]: nitems, next item, status, spare
   uint32_t* thr = nullptr;       // [nq] running lower bound of the cand-th estimate (ordered)
   uint32_t* ccount = nullptr;    // [nq] entries appended to a query's candidate buffer
@@ -92,13 +96,18 @@ struct Workspace {
   uint64_t allow_cap = 0;
   void* host_pinned = nullptr;   // pinned staging for host<->device copies
   size_t host_pinned_cap = 0;
-  cudaEvent_t ev[6] = {};
+  cudaEvent_t ev[10] = {};
   bool events = false;
+  sg_stats last = {};
 };
 
 struct Config {
-  uint32_t chunk_blocks = kChunkBlocks;  // autotuned
-  uint32_t scan_ctas_per_sm = 4;
+  uint32_t chunk_blocks = kChunkBlocks;  // batched scan chunk (autotuned)
+  uint32_t small_chunk_blocks = 64;      // chunk when few queries share the GPU
+  uint32_t small_batch = 64;             // below this many queries use the small chunk
+  uint32_t seed_blocks = kSeedBlocks;
+  uint32_t scan_ctas_per_sm = 2;
+  uint32_t soft_cap = 0;  // per-query buffer override (0: automatic); SIEVE_GPU_SOFT_CAP
 };
 
 std::string& last_error();
@@ -110,13 +119,16 @@ void launch_prep(const DevIndex& ix, Workspace& w, uint32_t nq, cudaStream_t st)
 void launch_route_scores(const DevIndex& ix, Workspace& w, uint32_t nq, int precision,
                          cudaStream_t st);
 void launch_route_select(const DevIndex& ix, Workspace& w, uint32_t nq, const sg_params& p,
-                         int precision, uint32_t chunk_blocks, cudaStream_t st);
+                         int precision, uint32_t chunk_blocks, uint32_t seed_blocks,
+                         cudaStream_t st);
+// The seed pass (one CTA per query, rank-0 seed item) then the persistent pass over the queue.
 void launch_scan(const DevIndex& ix, Workspace& w, uint32_t nq, const sg_params& p,
-                 const uint64_t* allow, uint64_t allow_words, int sms, cudaStream_t st);
+                 const uint64_t* allow, uint64_t allow_words, int sms, uint32_t chunk_blocks,
+                 uint32_t seed_blocks, int ctas_per_sm, cudaStream_t st);
 void launch_cut(const DevIndex& ix, Workspace& w, uint32_t nq, const sg_params& p,
                 cudaStream_t st);
-void launch_rerank(const DevIndex& ix, Workspace& w, uint32_t nq, const sg_params& p,
-                   cudaStream_t st, cudaEvent_t ev_t2_begin, cudaEvent_t ev_t2_end);
+int launch_rerank(const DevIndex& ix, Workspace& w, uint32_t nq, const sg_params& p,
+                  cudaStream_t st, cudaEvent_t ev_t2_begin, cudaEvent_t ev_t2_end);
 void launch_lut_scan(uint32_t groups, const uint8_t* tables, const uint8_t* blocks,
                      uint64_t nblocks, uint16_t* out, cudaStream_t st);
 void launch_dot_i8i8(const int8_t* q, const int8_t* rows, uint64_t nrows, uint32_t dim,

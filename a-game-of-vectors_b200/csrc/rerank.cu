@@ -221,20 +221,24 @@ static void dot_list(const DevIndex& ix, Workspace& w, uint32_t nq, uint32_t str
                                         w.lsc);
 }
 
-void launch_rerank(const DevIndex& ix, Workspace& w, uint32_t nq, const sg_params& p,
-                   cudaStream_t st, cudaEvent_t ev_t2_begin, cudaEvent_t ev_t2_end) {
+int launch_rerank(const DevIndex& ix, Workspace& w, uint32_t nq, const sg_params& p,
+                  cudaStream_t st, cudaEvent_t ev_t2_begin, cudaEvent_t ev_t2_end) {
   const uint32_t stride = p.cand;
+  int launches = 0;
   k_prune<<<nq, 256, 0, st>>>(w.cest, w.cid, w.cerr, w.cn, stride, p.has_prune, p.prune_m,
                               p.prune_w, w.lid, w.lsc, w.ln);
+  launches++;
   int kind = (int)p.rerank_kind;
   if (ev_t2_begin) cudaEventRecord(ev_t2_begin, st);
   if (kind == SG_RERANK_NONE) {
     // estimates are the scores
   } else if (kind == SG_RERANK_FULL) {
     dot_list(ix, w, nq, stride, false, st);
+    launches++;
   } else if (kind == SG_RERANK_SSD) {
     top_list(w.lsc, w.lid, w.ln, stride, p.rerank_r, w.lsc, w.lid, w.ln, stride, nq, st);
     dot_list(ix, w, nq, stride, false, st);
+    launches += 2;
   } else if (kind == SG_RERANK_TIERED && ix.has_t2) {
     static bool attr = false;
     size_t smem = (size_t)SG_TIER2_BYTES * 256 * sizeof(float);
@@ -248,16 +252,20 @@ void launch_rerank(const DevIndex& ix, Workspace& w, uint32_t nq, const sg_param
     top_list(w.lsc, w.lid, w.ln, stride, p.rerank_r, w.lsc, w.lid, w.ln, stride, nq, st);
     if (ev_t2_end) cudaEventRecord(ev_t2_end, st);
     dot_list(ix, w, nq, stride, false, st);
+    launches += 3;
   } else {  // Prefix, or Tiered without a tier-2 file
     dot_list(ix, w, nq, stride, true, st);
+    launches++;
     if (kind == SG_RERANK_TIERED) {
       top_list(w.lsc, w.lid, w.ln, stride, p.rerank_r, w.lsc, w.lid, w.ln, stride, nq, st);
       if (ev_t2_end) cudaEventRecord(ev_t2_end, st);
       dot_list(ix, w, nq, stride, false, st);
+      launches += 2;
     }
   }
-  if (ev_t2_end && !(kind == SG_RERANK_TIERED)) cudaEventRecord(ev_t2_end, st);
+  if (ev_t2_end && kind != SG_RERANK_TIERED) cudaEventRecord(ev_t2_end, st);
   top_list(w.lsc, w.lid, w.ln, stride, p.k, w.out_sc, w.out_id, w.out_n, p.k, nq, st);
+  return launches + 1;
 }
 
 // ---- stateless int8 dots for the parity tests --------------------------------------------------

@@ -164,6 +164,8 @@ struct SelectArgs {
   int bf16;
   sg_params p;
   uint32_t chunk_blocks;
+  uint32_t seed_blocks;
+  uint4* seed_items;
   float* probe_sc;
   uint32_t* probe_cl;
   uint32_t* probe_off;
@@ -280,12 +282,18 @@ __global__ void __launch_bounds__(256) k_route_select(SelectArgs a) {
   // probe list, admission offsets and chunk counts (block scans over probe ranks)
   uint32_t nloc = (m + blockDim.x - 1) / blockDim.x;  // probes per thread (contiguous)
   uint32_t r0 = threadIdx.x * nloc, r1 = min(m, r0 + nloc);
+  // Rank 0's first seed_blocks blocks form the query's seed item (scanned first, one CTA per
+  // query, to set a tight admission threshold); everything else is cut into chunks.
+  auto nchunks = [&](uint32_t r, uint32_t nb) {
+    uint32_t rest = r == 0 ? (nb > a.seed_blocks ? nb - a.seed_blocks : 0) : nb;
+    return (rest + a.chunk_blocks - 1) / a.chunk_blocks;
+  };
   uint32_t slots = 0, chunks = 0;
   for (uint32_t r = r0; r < r1; r++) {
     uint32_t c = key_id(keys[r]);
     uint32_t nb = a.block_off[c + 1] - a.block_off[c];
     slots += nb * SG_BLOCK;
-    chunks += (nb + a.chunk_blocks - 1) / a.chunk_blocks;
+    chunks += nchunks(r, nb);
   }
   uint32_t tot_slots, tot_chunks;
   uint32_t soff = block_exclusive_scan(slots, tmp, &tot_slots);
@@ -297,6 +305,7 @@ __global__ void __launch_bounds__(256) k_route_select(SelectArgs a) {
     s_base = base;
     a.probe_n[q] = m;
     a.scanned[q] = tot_slots;
+    if (m == 0) a.seed_items[q] = make_uint4(q, 0, 0, 0);
   }
   __syncthreads();
   uint64_t ibase = (uint64_t)s_base + coff;
@@ -307,6 +316,11 @@ __global__ void __launch_bounds__(256) k_route_select(SelectArgs a) {
     a.probe_off[(size_t)q * P + r] = soff;
     uint32_t b0 = a.block_off[c], b1 = a.block_off[c + 1];
     soff += (b1 - b0) * SG_BLOCK;
+    if (r == 0) {
+      uint32_t e = min(b1, b0 + a.seed_blocks);
+      a.seed_items[q] = make_uint4(q, 0, b0, e);
+      b0 = e;
+    }
     for (uint32_t b = b0; b < b1; b += a.chunk_blocks) {
       if (ibase < a.item_cap) a.items[ibase] = make_uint4(q, r, b, min(b1, b + a.chunk_blocks));
       ibase++;
@@ -332,7 +346,8 @@ void launch_route_scores(const DevIndex& ix, Workspace& w, uint32_t nq, int prec
 }
 
 void launch_route_select(const DevIndex& ix, Workspace& w, uint32_t nq, const sg_params& p,
-                         int precision, uint32_t chunk_blocks, cudaStream_t st) {
+                         int precision, uint32_t chunk_blocks, uint32_t seed_blocks,
+                         cudaStream_t st) {
   SelectArgs a;
   a.q256 = w.q256;
   a.cent = ix.cent;
@@ -345,6 +360,8 @@ void launch_route_select(const DevIndex& ix, Workspace& w, uint32_t nq, const sg
   a.bf16 = precision == SG_ROUTE_BF16;
   a.p = p;
   a.chunk_blocks = chunk_blocks;
+  a.seed_blocks = seed_blocks;
+  a.seed_items = w.seed_items;
   a.probe_sc = w.probe_sc;
   a.probe_cl = w.probe_cl;
   a.probe_off = w.probe_off;

@@ -33,6 +33,7 @@ struct ScanArgs {
   const uint32_t* probe_off;
   uint32_t P;
   const uint4* items;
+  const uint4* seed_items;
   uint64_t item_cap;
   uint32_t* counters;
   uint32_t* thr;
@@ -77,160 +78,152 @@ SG_DEV void score_block_quarter(const uint8_t* __restrict__ block, const uint4* 
   }
 }
 
-template <int CHB>
-__global__ void __launch_bounds__(256, 2) k_scan(ScanArgs a) {
-  constexpr int NS = CHB * 32;
-  constexpr int PER = NS / 256;  // slots per thread in the admission phase (contiguous)
-  __shared__ uint4 s_tab[SG_GROUPS];
-  __shared__ uint32_t s_key[NS];
-  __shared__ uint32_t hist[256], tmp[32];
-  __shared__ uint32_t s_item, s_base;
+// One CTA, one work item: score the item's blocks, then admit its best `cand` eligible slots.
+// Keys (ordered estimates, 0 = not eligible) live in dynamic shared memory, 4 B per slot.
+SG_DEV void scan_item(const ScanArgs& a, uint4 it, uint32_t* s_key, uint4* s_tab, uint32_t* hist,
+                      uint32_t* tmp, uint32_t* s_base) {
   const int tid = threadIdx.x, t4 = tid & 3, lbw = tid >> 2;
+  const uint32_t q = it.x, r = it.y, b0 = it.z, nb = it.w - it.z;
+  if (nb == 0) return;  // uniform
+  const uint32_t c = a.probe_cl[(size_t)q * a.P + r];
+  const float cent = a.probe_sc[(size_t)q * a.P + r];
+  const float4 qp = a.qp[q];
+  if (tid < SG_GROUPS)
+    s_tab[tid] = reinterpret_cast<const uint4*>(a.tables + (size_t)q * SG_GROUPS * 16)[tid];
+  const uint32_t cb0 = a.block_off[c];
+  const uint32_t cl = a.clen[c];
+  const uint32_t loc0 = (b0 - cb0) * SG_BLOCK;  // slot index of the item's first slot
+  const uint32_t kbase = a.probe_off[(size_t)q * a.P + r] + loc0;
+  __syncthreads();
+  // ---- scoring: 64 blocks per pass, four threads per block ----------------------------------
+  for (uint32_t pb = 0; pb < nb; pb += 64) {
+    const uint32_t lb = pb + lbw;
+    uint32_t acc[16];
+    if (lb < nb) {
+      score_block_quarter(a.blocks + (size_t)(b0 + lb) * SG_BLOCK_BYTES, s_tab, t4, acc);
+    } else {
+#pragma unroll
+      for (int e = 0; e < 16; e++) acc[e] = 0;
+    }
+#pragma unroll
+    for (int e = 0; e < 16; e++) {
+      acc[e] += __shfl_xor_sync(0xFFFFFFFFu, acc[e], 1);
+      acc[e] += __shfl_xor_sync(0xFFFFFFFFu, acc[e], 2);
+    }
+    if (lb < nb) {
+      uint32_t x0 = acc[0], x1 = acc[1], x2 = acc[2], x3 = acc[3];
+      if (t4 == 1) {
+        x0 = acc[4]; x1 = acc[5]; x2 = acc[6]; x3 = acc[7];
+      } else if (t4 == 2) {
+        x0 = acc[8]; x1 = acc[9]; x2 = acc[10]; x3 = acc[11];
+      } else if (t4 == 3) {
+        x0 = acc[12]; x1 = acc[13]; x2 = acc[14]; x3 = acc[15];
+      }
+      const float* mrow = a.mul + (size_t)(b0 + lb) * SG_BLOCK;
+      const float4 mlo = __ldg(reinterpret_cast<const float4*>(mrow + 4 * t4));
+      const float4 mhi = __ldg(reinterpret_cast<const float4*>(mrow + 16 + 4 * t4));
+      const uint32_t sc[8] = {x0 & 0xFFFFu, x0 >> 16, x2 & 0xFFFFu, x2 >> 16,
+                              x1 & 0xFFFFu, x1 >> 16, x3 & 0xFFFFu, x3 >> 16};
+      const float mv[8] = {mlo.x, mlo.y, mlo.z, mlo.w, mhi.x, mhi.y, mhi.z, mhi.w};
+#pragma unroll
+      for (int d = 0; d < 8; d++) {
+        const uint32_t doc = d < 4 ? 4 * t4 + d : 16 + 4 * t4 + (d - 4);
+        const uint32_t loc = lb * SG_BLOCK + doc;
+        const float est =
+            __fadd_rn(cent, __fmul_rn(mv[d], __fadd_rn(__fmul_rn(qp.z, (float)sc[d]), qp.w)));
+        s_key[loc] = (loc0 + loc < cl) ? ord(est) : 0u;
+      }
+    }
+  }
+  __syncthreads();
+  // ---- admission ------------------------------------------------------------------------------
+  const uint32_t thr = ld_cg(a.thr + q);
+  const uint32_t nloc = nb * SG_BLOCK;
+  const uint32_t per = (nloc + blockDim.x - 1) / blockDim.x;  // <= 64 slots per thread
+  const uint32_t i0 = tid * per, i1 = min(nloc, i0 + per);
+  uint32_t cnt = 0;
+  for (uint32_t i = i0; i < i1; i++) {
+    const uint32_t k = s_key[i];
+    bool surv = k != 0u && k >= thr;
+    if (surv && a.allow) surv = allowed(a.allow, a.allow_words, a.ids[(size_t)b0 * SG_BLOCK + i]);
+    if (!surv) s_key[i] = 0u;
+    cnt += surv;
+  }
+  const uint32_t n_s = block_sum(cnt, tmp);
+  if (n_s == 0) return;  // uniform
+  const bool cut = n_s > a.cand;
+  uint32_t T = 0, need = 0;
+  if (cut) {
+    T = block_select_nth_u32([&](uint32_t i) { return s_key[i]; }, nloc, a.cand, hist);
+    uint32_t gt = 0;
+    for (uint32_t i = i0; i < i1; i++) gt += s_key[i] > T;
+    need = a.cand - block_sum(gt, tmp);
+  }
+  uint32_t ties = 0;
+  if (cut)
+    for (uint32_t i = i0; i < i1; i++) ties += s_key[i] == T;
+  uint32_t tr = block_exclusive_scan(ties, tmp, nullptr);
+  uint64_t selmask = 0;
+  uint32_t nsel = 0;
+  for (uint32_t i = i0; i < i1; i++) {
+    const uint32_t k = s_key[i];
+    bool sel;
+    if (!cut) sel = k != 0u;
+    else if (k > T) sel = true;
+    else sel = (k == T) && (tr++ < need);
+    if (sel) {
+      selmask |= 1ull << (i - i0);
+      nsel++;
+    }
+  }
+  uint32_t total;
+  uint32_t off = block_exclusive_scan(nsel, tmp, &total);
+  if (tid == 0) {
+    *s_base = atomicAdd(a.ccount + q, total);
+    if (cut) atomicMax(a.thr + q, T);
+  }
+  __syncthreads();
+  const uint32_t base = *s_base;
+  uint4* dst = a.cbuf + (size_t)q * a.cap;
+  for (uint32_t i = i0; i < i1; i++) {
+    if (selmask & (1ull << (i - i0))) {
+      const uint32_t pos = base + off++;
+      if (pos < a.cap)
+        dst[pos] = make_uint4(__float_as_uint(unord(s_key[i])), kbase + i, b0 * SG_BLOCK + i, 0u);
+      else
+        a.overflow[q] = 1;
+    }
+  }
+}
+
+// Seed pass: CTA q scans query q's seed item (the first blocks of its best cluster).
+__global__ void __launch_bounds__(256, 2) k_scan_seed(ScanArgs a) {
+  extern __shared__ __align__(16) uint32_t s_key[];
+  __shared__ uint4 s_tab[SG_GROUPS];
+  __shared__ uint32_t hist[256], tmp[32], s_base;
+  scan_item(a, a.seed_items[blockIdx.x], s_key, s_tab, hist, tmp, &s_base);
+}
+
+// Main pass: a persistent grid drains the (query, probe, chunk) queue.
+__global__ void __launch_bounds__(256, 2) k_scan(ScanArgs a) {
+  extern __shared__ __align__(16) uint32_t s_key[];
+  __shared__ uint4 s_tab[SG_GROUPS];
+  __shared__ uint32_t hist[256], tmp[32], s_base, s_item;
   uint32_t nitems = a.counters[0];
   if (nitems > a.item_cap) nitems = (uint32_t)a.item_cap;
   for (;;) {
-    if (tid == 0) s_item = atomicAdd(&a.counters[1], 1u);
+    if (threadIdx.x == 0) s_item = atomicAdd(&a.counters[1], 1u);
     __syncthreads();
     const uint32_t item = s_item;
     if (item >= nitems) break;
-    const uint4 it = a.items[item];
-    const uint32_t q = it.x, r = it.y, b0 = it.z, nb = it.w - it.z;
-    const uint32_t c = a.probe_cl[(size_t)q * a.P + r];
-    const float cent = a.probe_sc[(size_t)q * a.P + r];
-    const float4 qp = a.qp[q];
-    if (tid < SG_GROUPS)
-      s_tab[tid] = reinterpret_cast<const uint4*>(a.tables + (size_t)q * SG_GROUPS * 16)[tid];
-    const uint32_t cb0 = a.block_off[c];
-    const uint32_t cl = a.clen[c];
-    const uint32_t loc0 = (b0 - cb0) * SG_BLOCK;  // slot index of the chunk's first slot
-    const uint32_t kbase = a.probe_off[(size_t)q * a.P + r] + loc0;
-    __syncthreads();
-    // ---- scoring --------------------------------------------------------------------------
-    for (int pb = 0; pb < CHB; pb += 64) {
-      const int lb = pb + lbw;
-      uint32_t acc[16];
-      if (lb < (int)nb) {
-        score_block_quarter(a.blocks + (size_t)(b0 + lb) * SG_BLOCK_BYTES, s_tab, t4, acc);
-      } else {
-#pragma unroll
-        for (int e = 0; e < 16; e++) acc[e] = 0;
-      }
-#pragma unroll
-      for (int e = 0; e < 16; e++) {
-        acc[e] += __shfl_xor_sync(0xFFFFFFFFu, acc[e], 1);
-        acc[e] += __shfl_xor_sync(0xFFFFFFFFu, acc[e], 2);
-      }
-      if (lb < (int)nb) {
-        uint32_t x0 = acc[0], x1 = acc[1], x2 = acc[2], x3 = acc[3];
-        if (t4 == 1) {
-          x0 = acc[4]; x1 = acc[5]; x2 = acc[6]; x3 = acc[7];
-        } else if (t4 == 2) {
-          x0 = acc[8]; x1 = acc[9]; x2 = acc[10]; x3 = acc[11];
-        } else if (t4 == 3) {
-          x0 = acc[12]; x1 = acc[13]; x2 = acc[14]; x3 = acc[15];
-        }
-        const float* mrow = a.mul + (size_t)(b0 + lb) * SG_BLOCK;
-        const float4 mlo = __ldg(reinterpret_cast<const float4*>(mrow + 4 * t4));
-        const float4 mhi = __ldg(reinterpret_cast<const float4*>(mrow + 16 + 4 * t4));
-        const uint32_t sc[8] = {x0 & 0xFFFFu, x0 >> 16, x2 & 0xFFFFu, x2 >> 16,
-                                x1 & 0xFFFFu, x1 >> 16, x3 & 0xFFFFu, x3 >> 16};
-        const float mv[8] = {mlo.x, mlo.y, mlo.z, mlo.w, mhi.x, mhi.y, mhi.z, mhi.w};
-#pragma unroll
-        for (int d = 0; d < 8; d++) {
-          const uint32_t doc = d < 4 ? 4 * t4 + d : 16 + 4 * t4 + (d - 4);
-          const uint32_t loc = lb * SG_BLOCK + doc;
-          const float est =
-              __fadd_rn(cent, __fmul_rn(mv[d], __fadd_rn(__fmul_rn(qp.z, (float)sc[d]), qp.w)));
-          s_key[loc] = (loc0 + loc < cl) ? ord(est) : 0u;
-        }
-      }
-    }
-    __syncthreads();
-    // ---- admission ----------------------------------------------------------------------------
-    const uint32_t thr = ld_cg(a.thr + q);
-    const uint32_t nloc = nb * SG_BLOCK;
-    const uint32_t i0 = tid * PER;
-    uint32_t cnt = 0;
-#pragma unroll
-    for (int j = 0; j < PER; j++) {
-      const uint32_t i = i0 + j;
-      if (i < nloc) {
-        const uint32_t k = s_key[i];
-        bool surv = k != 0u && k >= thr;
-        if (surv && a.allow) surv = allowed(a.allow, a.allow_words, a.ids[(size_t)b0 * SG_BLOCK + i]);
-        if (!surv) s_key[i] = 0u;
-        cnt += surv;
-      }
-    }
-    const uint32_t n_s = block_sum(cnt, tmp);
-    const bool cut = n_s > a.cand;
-    uint32_t T = 0, need = 0;
-    if (cut) {
-      T = block_select_nth_u32([&](uint32_t i) { return s_key[i]; }, nloc, a.cand, hist);
-      uint32_t gt = 0;
-#pragma unroll
-      for (int j = 0; j < PER; j++) {
-        const uint32_t i = i0 + j;
-        if (i < nloc && s_key[i] > T) gt++;
-      }
-      need = a.cand - block_sum(gt, tmp);
-    }
-    uint32_t ties = 0;
-    if (cut) {
-#pragma unroll
-      for (int j = 0; j < PER; j++) {
-        const uint32_t i = i0 + j;
-        if (i < nloc && s_key[i] == T) ties++;
-      }
-    }
-    uint32_t tie_rank = block_exclusive_scan(ties, tmp, nullptr);
-    uint32_t nsel = 0;
-    uint32_t selmask = 0;
-    {
-      uint32_t tr = tie_rank;
-#pragma unroll
-      for (int j = 0; j < PER; j++) {
-        const uint32_t i = i0 + j;
-        bool sel = false;
-        if (i < nloc) {
-          const uint32_t k = s_key[i];
-          if (!cut) sel = k != 0u;
-          else if (k > T) sel = true;
-          else if (k == T) sel = (tr++ < need);
-        }
-        if (sel) {
-          selmask |= 1u << j;
-          nsel++;
-        }
-      }
-    }
-    uint32_t total;
-    uint32_t off = block_exclusive_scan(nsel, tmp, &total);
-    if (tid == 0) {
-      s_base = total ? atomicAdd(a.ccount + q, total) : 0u;
-      if (cut) atomicMax(a.thr + q, T);
-    }
-    __syncthreads();
-    const uint32_t base = s_base;
-    uint4* dst = a.cbuf + (size_t)q * a.cap;
-#pragma unroll
-    for (int j = 0; j < PER; j++) {
-      if (selmask & (1u << j)) {
-        const uint32_t i = i0 + j;
-        const uint32_t pos = base + off++;
-        if (pos < a.cap)
-          dst[pos] = make_uint4(__float_as_uint(unord(s_key[i])), kbase + i,
-                                b0 * SG_BLOCK + i, 0u);
-        else
-          a.overflow[q] = 1;
-      }
-    }
+    scan_item(a, a.items[item], s_key, s_tab, hist, tmp, &s_base);
     __syncthreads();
   }
 }
 
 void launch_scan(const DevIndex& ix, Workspace& w, uint32_t nq, const sg_params& p,
-                 const uint64_t* allow, uint64_t allow_words, int sms, cudaStream_t st) {
+                 const uint64_t* allow, uint64_t allow_words, int sms, uint32_t chunk_blocks,
+                 uint32_t seed_blocks, int ctas_per_sm, cudaStream_t st) {
   ScanArgs a;
   a.blocks = ix.blocks;
   a.mul = ix.mul;
@@ -244,6 +237,7 @@ void launch_scan(const DevIndex& ix, Workspace& w, uint32_t nq, const sg_params&
   a.probe_off = w.probe_off;
   a.P = p.nprobe < ix.k ? p.nprobe : ix.k;
   a.items = w.items;
+  a.seed_items = w.seed_items;
   a.item_cap = w.item_cap;
   a.counters = w.counters;
   a.thr = w.thr;
@@ -254,7 +248,16 @@ void launch_scan(const DevIndex& ix, Workspace& w, uint32_t nq, const sg_params&
   a.cand = p.cand;
   a.allow = allow;
   a.allow_words = allow_words;
-  k_scan<kChunkBlocks><<<sms * 2, 256, 0, st>>>(a);
+  static bool attr = false;
+  if (!attr) {
+    cudaFuncSetAttribute(k_scan_seed, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)(kMaxChunkBlocks * SG_BLOCK * 4));
+    cudaFuncSetAttribute(k_scan, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)(kMaxChunkBlocks * SG_BLOCK * 4));
+    attr = true;
+  }
+  k_scan_seed<<<nq, 256, seed_blocks * SG_BLOCK * 4, st>>>(a);
+  k_scan<<<sms * ctas_per_sm, 256, chunk_blocks * SG_BLOCK * 4, st>>>(a);
 }
 
 // ---- stateless kernels for the parity tests ---------------------------------------------------

@@ -6,6 +6,7 @@
 //   drains the (query, probe, chunk) queue) -> cut + dedup -> prune / tier-2 / int8 rerank -> top-k.
 #include <cuda_bf16.h>
 #include <math.h>
+#include <stdlib.h>
 #include <string.h>
 
 #include <algorithm>
@@ -24,6 +25,7 @@ struct sg_index {
   std::mutex mu;
   cudaStream_t stream = nullptr;
   int sms = 148;
+  bool timing_on = false;
 };
 
 namespace sg {
@@ -114,6 +116,7 @@ void free_ws(sg::Workspace& w) {
   dfree(w.probe_n);
   dfree(w.scanned);
   dfree(w.items);
+  dfree(w.seed_items);
   dfree(w.counters);
   dfree(w.thr);
   dfree(w.ccount);
@@ -185,7 +188,7 @@ int build_index(const sg_ivf_arrays* a, int device, sg_index** out) {
   {
     std::vector<uint32_t> ch(K);
     for (uint32_t c = 0; c < K; c++)
-      ch[c] = (boff32[c + 1] - boff32[c] + h->cfg.chunk_blocks - 1) / h->cfg.chunk_blocks;
+      ch[c] = (boff32[c + 1] - boff32[c] + h->cfg.small_chunk_blocks - 1) / h->cfg.small_chunk_blocks;
     std::sort(ch.begin(), ch.end(), std::greater<uint32_t>());
     x.h_chunks_desc_prefix.assign(K + 1, 0);
     for (uint32_t c = 0; c < K; c++) x.h_chunks_desc_prefix[c + 1] = x.h_chunks_desc_prefix[c] + ch[c];
@@ -239,6 +242,7 @@ int build_index(const sg_ivf_arrays* a, int device, sg_index** out) {
     }
     x.has_t2 = true;
   }
+  if (const char* sc = getenv("SIEVE_GPU_SOFT_CAP")) h->cfg.soft_cap = (uint32_t)strtoul(sc, nullptr, 10);
   cudaDeviceProp prop;
   CK(cudaGetDeviceProperties(&prop, device));
   h->sms = prop.multiProcessorCount;
@@ -262,14 +266,14 @@ int ensure_ws(sg_index* h, uint32_t nq, const sg_params& p, uint32_t cbuf_per_q)
   if (nq > w.nq_cap) {
     uint32_t n = std::max(nq, w.nq_cap * 2);
     dfree(w.q768); dfree(w.q256); dfree(w.tables); dfree(w.qp); dfree(w.qnorm); dfree(w.wq);
-    dfree(w.winv); dfree(w.wq256); dfree(w.winv256); dfree(w.probe_n); dfree(w.scanned);
+    dfree(w.winv); dfree(w.wq256); dfree(w.winv256); dfree(w.probe_n); dfree(w.scanned); dfree(w.seed_items);
     dfree(w.thr); dfree(w.ccount); dfree(w.overflow); dfree(w.cn); dfree(w.ln); dfree(w.out_n);
     if ((rc = dalloc(&w.q768, (size_t)n * SG_DIM)) || (rc = dalloc(&w.q256, (size_t)n * SG_PDIM)) ||
         (rc = dalloc(&w.tables, (size_t)n * SG_GROUPS * 16)) || (rc = dalloc(&w.qp, n)) ||
         (rc = dalloc(&w.qnorm, n)) || (rc = dalloc(&w.wq, (size_t)n * SG_DIM)) ||
         (rc = dalloc(&w.winv, n)) || (rc = dalloc(&w.wq256, (size_t)n * SG_PDIM)) ||
         (rc = dalloc(&w.winv256, n)) || (rc = dalloc(&w.probe_n, n)) ||
-        (rc = dalloc(&w.scanned, n)) || (rc = dalloc(&w.thr, n)) || (rc = dalloc(&w.ccount, n)) ||
+        (rc = dalloc(&w.scanned, n)) || (rc = dalloc(&w.seed_items, n)) || (rc = dalloc(&w.thr, n)) || (rc = dalloc(&w.ccount, n)) ||
         (rc = dalloc(&w.overflow, n)) || (rc = dalloc(&w.cn, n)) || (rc = dalloc(&w.ln, n)) ||
         (rc = dalloc(&w.out_n, n)))
       return rc;
@@ -345,43 +349,72 @@ uint32_t full_cap(const sg_index* h, const sg_params& p) {
   return (uint32_t)std::min<uint64_t>(std::max<uint64_t>(b, 1), 0x7FFFFFFFull);
 }
 
+// Soft per-query buffer for batches: at least 16 x cand entries, and up to an 8 GiB budget
+// shared by the batch. A query that fills it is re-run (see search_impl) with the exact bound.
 uint32_t batch_cap(const sg_index* h, const sg_params& p, uint32_t nq) {
   uint32_t full = full_cap(h, p);
+  if (h->cfg.soft_cap) return std::min(full, h->cfg.soft_cap);
   if (nq <= 8) return full;
-  uint32_t soft = std::max<uint32_t>(16 * std::max<uint32_t>(p.cand, 1), 65536);
-  return std::min(full, soft);
+  uint64_t budget = (8ull << 30) / (sizeof(uint4) * (uint64_t)nq);
+  uint64_t soft = std::max<uint64_t>(16ull * std::max<uint32_t>(p.cand, 1), budget);
+  return (uint32_t)std::min<uint64_t>(full, soft);
 }
 
 enum Stage { kToCandidates = 1, kToSearch = 2 };
 
 // Runs the pipeline on queries already in ws.q768 / ws.q256 (have_q256 = false: derive it).
+// With `timed`, events ev[0..7] bracket the stages (see collect_stats).
 int run_pipeline(sg_index* h, uint32_t nq, const sg_params& p, bool have_q256,
                  const uint64_t* d_allow, uint64_t allow_words, Stage stage, bool timed) {
   sg::Workspace& w = h->ws;
   sg::DevIndex& x = h->ix;
   cudaStream_t st = h->stream;
+  uint32_t launches = 0;
   CK(cudaMemsetAsync(w.counters, 0, 4 * sizeof(uint32_t), st));
   CK(cudaMemsetAsync(w.thr, 0, nq * sizeof(uint32_t), st));
   CK(cudaMemsetAsync(w.ccount, 0, nq * sizeof(uint32_t), st));
   CK(cudaMemsetAsync(w.overflow, 0, nq, st));
   if (timed) CK(cudaEventRecord(w.ev[0], st));
-  if (!have_q256) sg::launch_prefix(w, nq, st);
+  if (!have_q256) {
+    sg::launch_prefix(w, nq, st);
+    launches++;
+  }
   sg::launch_prep(x, w, nq, st);
-  sg::launch_route_scores(x, w, nq, x.route_precision, st);
-  sg::launch_route_select(x, w, nq, p, x.route_precision, h->cfg.chunk_blocks, st);
   if (timed) CK(cudaEventRecord(w.ev[1], st));
+  sg::launch_route_scores(x, w, nq, x.route_precision, st);
+  if (timed) CK(cudaEventRecord(w.ev[2], st));
+  const uint32_t cb = nq < h->cfg.small_batch ? h->cfg.small_chunk_blocks : h->cfg.chunk_blocks;
+  sg::launch_route_select(x, w, nq, p, x.route_precision, cb, h->cfg.seed_blocks, st);
+  if (timed) CK(cudaEventRecord(w.ev[3], st));
+  launches += 3;
   if (p.cand > 0) {
-    sg::launch_scan(x, w, nq, p, d_allow, allow_words, h->sms, st);
+    sg::launch_scan(x, w, nq, p, d_allow, allow_words, h->sms, cb, h->cfg.seed_blocks,
+                    h->cfg.scan_ctas_per_sm, st);
+    if (timed) CK(cudaEventRecord(w.ev[4], st));
     sg::launch_cut(x, w, nq, p, st);
+    launches += 3;
   } else {
+    if (timed) CK(cudaEventRecord(w.ev[4], st));
     CK(cudaMemsetAsync(w.cn, 0, nq * sizeof(uint32_t), st));
   }
-  if (timed) CK(cudaEventRecord(w.ev[2], st));
+  if (timed) CK(cudaEventRecord(w.ev[5], st));
   if (stage == kToSearch)
-    sg::launch_rerank(x, w, nq, p, st, timed ? w.ev[4] : nullptr, timed ? w.ev[5] : nullptr);
-  if (timed) CK(cudaEventRecord(w.ev[3], st));
+    launches += sg::launch_rerank(x, w, nq, p, st, timed ? w.ev[7] : nullptr,
+                                  timed ? w.ev[8] : nullptr);
+  if (timed) CK(cudaEventRecord(w.ev[6], st));
   CK(cudaGetLastError());
+  w.last = sg_stats();
+  w.last.launches = launches;
   return SG_OK;
+}
+
+// After the stream has synchronised: stage times of a timed run_pipeline.
+void collect_stats(sg::Workspace& w, const sg_params& p) {
+  float* ms[6] = {&w.last.ms_prep, &w.last.ms_route_gemm, &w.last.ms_route_select,
+                  &w.last.ms_scan, &w.last.ms_cut, &w.last.ms_rerank};
+  for (int i = 0; i < 6; i++) cudaEventElapsedTime(ms[i], w.ev[i], w.ev[i + 1]);
+  cudaEventElapsedTime(&w.last.ms_total, w.ev[0], w.ev[6]);
+  if (p.rerank_kind == SG_RERANK_TIERED) cudaEventElapsedTime(&w.last.ms_tier2, w.ev[7], w.ev[8]);
 }
 
 int stage_inputs(sg_index* h, uint32_t nq, const float* q768, const float* q256, bool device) {
@@ -427,7 +460,8 @@ int search_impl(sg_index* h, uint32_t nq, const float* q768, const float* q256,
   if ((rc = stage_inputs(h, nq, q768, q256, device))) return rc;
   const uint64_t* d_allow;
   if ((rc = stage_allow(h, allow, allow_words, device, &d_allow))) return rc;
-  if ((rc = run_pipeline(h, nq, p, q256 != nullptr, d_allow, allow_words, kToSearch, t != nullptr)))
+  const bool timed_run = t != nullptr || h->timing_on;
+  if ((rc = run_pipeline(h, nq, p, q256 != nullptr, d_allow, allow_words, kToSearch, timed_run)))
     return rc;
   sg::Workspace& w = h->ws;
   std::vector<uint8_t> ovf(nq);
@@ -443,7 +477,7 @@ int search_impl(sg_index* h, uint32_t nq, const float* q768, const float* q256,
   CK(cudaMemcpyAsync(out_n, w.out_n, (size_t)nq * 4, okind, h->stream));
   std::vector<uint64_t> scanned;
   std::vector<uint32_t> probed, reranked;
-  if (t) {
+  if (timed_run) {
     scanned.resize(nq);
     probed.resize(nq);
     reranked.resize(nq);
@@ -453,45 +487,73 @@ int search_impl(sg_index* h, uint32_t nq, const float* q768, const float* q256,
   }
   CK(cudaStreamSynchronize(h->stream));
   if (status & sg::kStatusOverflow) return fail(SG_ERR_INVALID, "work queue overflow");
-  if (t) {
-    float ms[4] = {0, 0, 0, 0};
-    cudaEventElapsedTime(&ms[0], w.ev[0], w.ev[1]);
-    cudaEventElapsedTime(&ms[1], w.ev[1], w.ev[2]);
-    cudaEventElapsedTime(&ms[2], w.ev[2], w.ev[3]);
-    if (p.rerank_kind == SG_RERANK_TIERED) cudaEventElapsedTime(&ms[3], w.ev[4], w.ev[5]);
-    t->route += (uint64_t)(ms[0] * 1e6);
-    t->scan += (uint64_t)(ms[1] * 1e6);
-    t->rerank += (uint64_t)(ms[2] * 1e6);
-    t->tier2 += (uint64_t)(ms[3] * 1e6);
+  const bool timed = t != nullptr || h->timing_on;
+  if (timed) {
+    collect_stats(w, p);
+    uint64_t sc = 0, pr = 0, rr = 0;
     for (uint32_t i = 0; i < nq; i++) {
-      t->scanned += scanned[i];
-      t->probed += probed[i];
-      t->reranked += reranked[i];
+      sc += scanned[i];
+      pr += probed[i];
+      rr += reranked[i];
     }
+    w.last.scanned = sc;
+    w.last.probed = pr;
+    w.last.reranked = rr;
   }
-  // queries whose candidate buffer filled up run again alone with the exact bound
-  for (uint32_t i = 0; i < nq; i++) {
-    if (!ovf[i]) continue;
-    const uint64_t* al = allow;
-    const float* q1 = q768 + (size_t)i * SG_DIM;
-    const float* q2 = q256 ? q256 + (size_t)i * SG_PDIM : nullptr;
-    uint32_t fcap = full_cap(h, p);
-    if ((rc = ensure_ws(h, 1, p, fcap))) return rc;
-    if ((rc = stage_inputs(h, 1, q1, q2, device))) return rc;
-    if ((rc = stage_allow(h, al, allow_words, device, &d_allow))) return rc;
-    if ((rc = run_pipeline(h, 1, p, q2 != nullptr, d_allow, allow_words, kToSearch, false)))
-      return rc;
-    uint8_t o1 = 0;
-    CK(cudaMemcpyAsync(&o1, w.overflow, 1, cudaMemcpyDeviceToHost, h->stream));
-    if (k) {
-      CK(cudaMemcpyAsync(out_sc + (size_t)i * k, w.out_sc, k * 4, okind, h->stream));
-      CK(cudaMemcpyAsync(out_id + (size_t)i * k, w.out_id, k * 4, okind, h->stream));
+  if (t) {
+    t->route += (uint64_t)((w.last.ms_prep + w.last.ms_route_gemm + w.last.ms_route_select) * 1e6);
+    t->scan += (uint64_t)((w.last.ms_scan + w.last.ms_cut) * 1e6);
+    t->rerank += (uint64_t)(w.last.ms_rerank * 1e6);
+    t->tier2 += (uint64_t)(w.last.ms_tier2 * 1e6);
+    t->scanned += w.last.scanned;
+    t->probed += w.last.probed;
+    t->reranked += w.last.reranked;
+  }
+  // queries whose candidate buffer filled up run again, in batches, with the exact bound
+  const sg_stats saved = w.last;
+  uint32_t retry_launches = 0;
+  std::vector<uint32_t> redo;
+  for (uint32_t i = 0; i < nq; i++)
+    if (ovf[i]) redo.push_back(i);
+  if (!redo.empty()) {
+    const uint32_t fcap = full_cap(h, p);
+    const uint32_t per = (uint32_t)std::max<uint64_t>(
+        1, std::min<uint64_t>(redo.size(), (8ull << 30) / (sizeof(uint4) * (uint64_t)fcap)));
+    std::vector<float> hq768, hq256;
+    std::vector<float> osc((size_t)per * std::max<uint32_t>(k, 1));
+    std::vector<uint32_t> oid((size_t)per * std::max<uint32_t>(k, 1)), on(per);
+    for (size_t s0 = 0; s0 < redo.size(); s0 += per) {
+      const uint32_t m = (uint32_t)std::min<size_t>(per, redo.size() - s0);
+      if ((rc = ensure_ws(h, m, p, fcap))) return rc;
+      cudaMemcpyKind ik = device ? cudaMemcpyDeviceToDevice : cudaMemcpyDefault;
+      for (uint32_t j = 0; j < m; j++) {
+        const uint32_t i = redo[s0 + j];
+        CK(cudaMemcpyAsync(w.q768 + (size_t)j * SG_DIM, q768 + (size_t)i * SG_DIM, SG_DIM * 4, ik, h->stream));
+        if (q256)
+          CK(cudaMemcpyAsync(w.q256 + (size_t)j * SG_PDIM, q256 + (size_t)i * SG_PDIM, SG_PDIM * 4, ik, h->stream));
+      }
+      if ((rc = stage_allow(h, allow, allow_words, device, &d_allow))) return rc;
+      if ((rc = run_pipeline(h, m, p, q256 != nullptr, d_allow, allow_words, kToSearch, false)))
+        return rc;
+      std::vector<uint8_t> o1(m);
+      CK(cudaMemcpyAsync(o1.data(), w.overflow, m, cudaMemcpyDeviceToHost, h->stream));
+      for (uint32_t j = 0; j < m; j++) {
+        const uint32_t i = redo[s0 + j];
+        if (k) {
+          CK(cudaMemcpyAsync(out_sc + (size_t)i * k, w.out_sc + (size_t)j * k, k * 4, okind, h->stream));
+          CK(cudaMemcpyAsync(out_id + (size_t)i * k, w.out_id + (size_t)j * k, k * 4, okind, h->stream));
+        }
+        CK(cudaMemcpyAsync(out_n + i, w.out_n + j, 4, okind, h->stream));
+      }
+      CK(cudaStreamSynchronize(h->stream));
+      for (uint32_t j = 0; j < m; j++)
+        if (o1[j]) return fail(SG_ERR_INVALID, "candidate buffer overflow at the exact bound");
+      retry_launches += w.last.launches;
     }
-    CK(cudaMemcpyAsync(out_n + i, w.out_n, 4, okind, h->stream));
-    CK(cudaStreamSynchronize(h->stream));
-    if (o1) return fail(SG_ERR_INVALID, "candidate buffer overflow at the exact bound");
     if ((rc = ensure_ws(h, nq, p, cap))) return rc;
   }
+  w.last = saved;
+  w.last.launches += retry_launches;
   return SG_OK;
 }
 
@@ -615,6 +677,18 @@ int sg_set_route_precision(sg_index* h, int precision) {
   return SG_OK;
 }
 
+int sg_set_timing(sg_index* h, int on) {
+  if (!h) return fail(SG_ERR_INVALID, "null index");
+  h->timing_on = on != 0;
+  return SG_OK;
+}
+
+int sg_last_stats(const sg_index* h, sg_stats* out) {
+  if (!h || !out) return fail(SG_ERR_INVALID, "null argument");
+  *out = h->ws.last;
+  return SG_OK;
+}
+
 int sg_search(sg_index* h, uint32_t nq, const float* q768, const float* q256,
               const sg_params* params, const uint64_t* allow_bits, uint64_t allow_words,
               float* out_scores, uint32_t* out_ids, uint32_t* out_counts, sg_timing* timing) {
@@ -657,7 +731,8 @@ int sg_route(sg_index* h, uint32_t nq, const float* q256, const sg_params* param
   CK(cudaMemsetAsync(w.counters, 0, 16, st));
   sg::launch_prep(h->ix, w, nq, st);
   sg::launch_route_scores(h->ix, w, nq, h->ix.route_precision, st);
-  sg::launch_route_select(h->ix, w, nq, *params, h->ix.route_precision, h->cfg.chunk_blocks, st);
+  sg::launch_route_select(h->ix, w, nq, *params, h->ix.route_precision, h->cfg.chunk_blocks,
+                          h->cfg.seed_blocks, st);
   CK(cudaGetLastError());
   const uint32_t P = std::min<uint32_t>(params->nprobe, h->ix.k);
   if (P) {

@@ -61,6 +61,15 @@ class SgTiming(ctypes.Structure):
     ]
 
 
+class SgStats(ctypes.Structure):
+    """sg_stats: device stage times and counters of the last search."""
+
+    _fields_ = [(n, c_float) for n in ("ms_prep", "ms_route_gemm", "ms_route_select", "ms_scan",
+                                        "ms_cut", "ms_rerank", "ms_tier2", "ms_total")] + [
+        ("launches", c_uint32), ("reserved", c_uint32), ("scanned", c_uint64), ("probed", c_uint64),
+        ("reranked", c_uint64)]
+
+
 class SgIvfArrays(ctypes.Structure):
     """sg_ivf_arrays: the contents of the reference's corpus and index files."""
 
@@ -158,6 +167,8 @@ EXPORTS = [
     "sg_close",
     "sg_index_info",
     "sg_set_route_precision",
+    "sg_set_timing",
+    "sg_last_stats",
     "sg_search",
     "sg_search_device",
     "sg_route",

@@ -13,7 +13,7 @@ from dataclasses import dataclass, field
 import numpy as np
 
 from . import _abi
-from ._abi import SgParams, SgTiming, check, lib, make_arrays, ptr
+from ._abi import SgParams, SgStats, SgTiming, check, lib, make_arrays, ptr
 
 
 # ---- ivf::Rerank (src/ivf.rs:425-439) -----------------------------------------------------------
@@ -179,6 +179,15 @@ class Index:
         except Exception:
             pass
 
+    def set_timing(self, on: bool) -> None:
+        """Per-stage device timing of every search (read back with last_stats)."""
+        check(lib().sg_set_timing(self._h, c_int(1 if on else 0)))
+
+    def last_stats(self) -> dict:
+        st = SgStats()
+        check(lib().sg_last_stats(self._h, byref(st)))
+        return {name: getattr(st, name) for name, _ in SgStats._fields_ if name != "reserved"}
+
     def set_route_precision(self, bf16: bool) -> None:
         check(lib().sg_set_route_precision(self._h, c_int(_abi.ROUTE_BF16 if bf16 else _abi.ROUTE_FP32)))
 
@@ -202,6 +211,14 @@ class Index:
         if timing is not None:
             timing.add(t)
         return sc[:, : p.k], ids[:, : p.k], cnt
+
+    def search_into(self, q768: np.ndarray, params: Params, out_scores: np.ndarray,
+                    out_ids: np.ndarray, out_counts: np.ndarray, q256: np.ndarray | None = None) -> None:
+        """sg_search into caller-owned host buffers (pinned buffers make the copies direct)."""
+        nq = q768.shape[0]
+        p = params.to_c()
+        check(lib().sg_search(self._h, c_uint32(nq), ptr(q768), ptr(q256), byref(p), None, c_uint64(0),
+                              ptr(out_scores), ptr(out_ids), ptr(out_counts), None))
 
     def search(self, q768, q256, params: Params, allow=None, timing: Timing | None = None):
         """One query: list of (score, row) best first, like Index::search."""

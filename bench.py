@@ -1,0 +1,393 @@
+#!/usr/bin/env python
+"""Benchmark of the sieve query path on B200: QPS at R@10 >= 0.90 with p50/p99 latency, and the
+scan kernel's HBM roofline.
+
+Workloads (seeded synthetic Gaussian mixtures standing in for the reference's datasets, which are
+not available; shapes, sizes and noise model as the workloads name them):
+  c1  1M x 768, 1024 centres, 1024 clusters, SOAR, 10k queries   (the reference's CPU-sized case)
+  c2  18.4M x 768, 16384 centres, 4096 clusters, SOAR + 2-bit tier, 50k queries   (default)
+  c3  113.5M x 768, 65536 centres, 16384 clusters, SOAR + 2-bit tier, 100k queries (~105 GB HBM)
+
+One step = one batch of queries through the whole path (route, scan, cut, rerank) with the
+inputs resident in HBM (sg_search_device). `e2e` runs the same batches through the host API
+(sg_search) from pinned host memory, copies included. `plain` is the one-query-per-launch form.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--workload c2] [--impl ours|reference]
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+for p in (os.path.join(ROOT, "a-game-of-vectors_b200"), os.path.join(ROOT, "oracle")):
+    if p not in sys.path:
+        sys.path.insert(0, p)
+
+import numpy as np  # noqa: E402
+import torch  # noqa: E402
+
+WORKLOADS = {
+    "c1": dict(n=1_000_000, centers=1024, k=1024, queries=10_000, search="32:1000:full"),
+    "c2": dict(n=18_400_000, centers=16384, k=4096, queries=50_000, search="64:2000:full"),
+    "c3": dict(n=113_500_000, centers=65536, k=16384, queries=100_000, search="64:1000:full"),
+}
+SCAN_BYTES_PER_SLOT = 40  # 32 B code + 8 B [mul, err] factors per scanned slot
+
+
+def log(*a):
+    print(*a, file=sys.stderr, flush=True)
+
+
+# ---- clocks during the timed region ------------------------------------------------------------
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.lines: list[str] = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self) -> dict:
+        sm, mx, reasons = [], 0.0, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = max(mx, float(f[2]))
+            except ValueError:
+                continue
+            for name, val in zip(names, f[5:9]):
+                if val.lower() == "active":
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx or None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def measured_peaks() -> dict:
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return json.load(f)
+    except OSError:
+        return {}
+
+
+# ---- workload ----------------------------------------------------------------------------------
+def build_workload(name: str, device: str, rows: int | None, nq_pool: int, n_eval: int):
+    from sieve_gpu import builder, synth
+
+    w = dict(WORKLOADS[name])
+    if rows:
+        w["n"] = rows
+    t0 = time.time()
+    mix = synth.Mixture(n=w["n"], n_centers=w["centers"], dim=768, spread=1.0, sigma=0.3, seed=1,
+                        device=device)
+    corpus = builder.ingest(mix)
+    t_ingest = time.time() - t0
+    index = builder.build_ivf(corpus, k=w["k"], sample_n=min(w["n"], 262144), iters=10,
+                              soar_lambda=1.0, device=device)
+    t_build = time.time() - t0 - t_ingest
+    arrays = {**corpus, **index}
+    queries = mix.queries(nq_pool, sigma=0.35).float()
+    t1 = time.time()
+    gt = builder.ground_truth(mix, queries[:n_eval], k=10)
+    t_gt = time.time() - t1
+    log(f"workload {name}: n={w['n']} k={w['k']} ingest {t_ingest:.1f}s build {t_build:.1f}s "
+        f"gt {t_gt:.1f}s nblocks={int(arrays['block_off'][-1])}")
+    return w, arrays, queries, gt, {"ingest_s": round(t_ingest, 1), "build_s": round(t_build, 1)}
+
+
+def recall10(ids: np.ndarray, cnt: np.ndarray, gt: np.ndarray) -> float:
+    r = []
+    for i in range(gt.shape[0]):
+        got = set(int(x) for x in ids[i, : min(10, int(cnt[i]))])
+        truth = set(int(x) for x in gt[i, :10])
+        r.append(len(got & truth) / max(min(10, len(truth)), 1))
+    return float(np.mean(r))
+
+
+def int8_truth(arrays, q768: torch.Tensor, k: int = 10) -> np.ndarray:
+    """Exact top-k by the rerank's own int8 score (the ground truth filter::truth uses,
+    src/filter.rs:112-151): (query_i8(q / scale) . row) in exact integer arithmetic."""
+    dev = q768.device
+    scale = torch.as_tensor(arrays["quant_scale"], device=dev)
+    w = q768.float() / scale
+    m = torch.clamp(w.abs().amax(1, keepdim=True), min=1e-12)
+    s = 127.0 / m
+    v = w * s
+    wq = torch.where((v - torch.trunc(v)).abs() == 0.5, torch.trunc(v) + torch.sign(v), torch.round(v))
+    rows = arrays["rerank"]
+    best_v = torch.full((q768.shape[0], k), -float("inf"), device=dev)
+    best_i = torch.zeros((q768.shape[0], k), dtype=torch.int64, device=dev)
+    prev = torch.backends.cuda.matmul.allow_tf32
+    torch.backends.cuda.matmul.allow_tf32 = False  # products and sums stay exact integers in f32
+    try:
+        for s0 in range(0, rows.shape[0], 1 << 20):
+            x = torch.as_tensor(rows[s0:s0 + (1 << 20)], device=dev).float()
+            sc = wq @ x.T
+            v_, i_ = torch.topk(sc, min(k, sc.shape[1]), dim=1)
+            allv, alli = torch.cat((best_v, v_), 1), torch.cat((best_i, i_ + s0), 1)
+            # ties by ascending row id, as the reference's TopK order
+            order = torch.argsort(alli, dim=1, stable=True)
+            allv, alli = allv.gather(1, order), alli.gather(1, order)
+            tv, ti = torch.sort(allv, dim=1, descending=True, stable=True)
+            best_v, best_i = tv[:, :k], alli.gather(1, ti[:, :k])
+    finally:
+        torch.backends.cuda.matmul.allow_tf32 = prev
+    return best_i.cpu().numpy().astype(np.uint32)
+
+
+def cpu_reference(arrays, q768_host: np.ndarray, params, seconds: float, threads: int):
+    """The reference's portable CPU path (oracle restatement, -march=native, OpenMP over queries)
+    on a sample of queries sized to run about `seconds`."""
+    import oracle as O
+
+    oi = O.OracleIndex(arrays, native=True)
+    q256 = np.stack([O.prefix(v)[0] for v in q768_host]).astype(np.float32)
+    p = params.to_c()
+    probe = min(q768_host.shape[0], max(threads * 4, 64))
+    t = time.perf_counter()
+    oi.search_batch(q768_host[:probe], q256[:probe], p, threads=threads)
+    per_q = (time.perf_counter() - t) / probe
+    n = int(min(q768_host.shape[0], max(probe, seconds / max(per_q, 1e-9))))
+    t = time.perf_counter()
+    s, o, c, scanned = oi.search_batch(q768_host[:n], q256[:n], p, threads=threads)
+    dt = time.perf_counter() - t
+    return {"qps": n / dt, "queries": n, "seconds": dt, "ids": o, "cnt": c}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="c2", choices=sorted(WORKLOADS))
+    ap.add_argument("--rows", type=int, default=None, help="override the corpus size (smoke runs)")
+    ap.add_argument("--config", default=None, help="search config nprobe:cand:rerank[:...]")
+    ap.add_argument("--batch", type=int, default=4096)
+    ap.add_argument("--route", default="bf16", choices=["bf16", "fp32"])
+    ap.add_argument("--eval", type=int, default=1000, help="queries with exact ground truth")
+    ap.add_argument("--plain", type=int, default=512, help="queries timed one per launch")
+    ap.add_argument("--cpu-seconds", type=float, default=15.0)
+    args = ap.parse_args()
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+
+        torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    torch.cuda.set_device(local)
+    dev = f"cuda:{local}"
+    if args.impl == "reference" and rank != 0:
+        return finish(world)
+
+    from sieve_gpu import Index, parse_config
+
+    wl = WORKLOADS[args.workload]
+    config = args.config or wl["search"]
+    nq_pool = max(args.batch, args.eval, args.plain)
+    nq_pool = min(max(nq_pool, args.batch * 2), wl["queries"])
+    w, arrays, queries, gt, build_info = build_workload(args.workload, dev, args.rows, nq_pool, args.eval)
+    label, params = parse_config(config, w["k"])
+    params.k = 10
+    threads = os.cpu_count() or 1
+    cfg = {"workload": f"{args.workload}: {w['n']} x 768, {w['centers']} centres, {w['k']} clusters",
+           "search": config, "batch": args.batch, "route": args.route, "queries_pool": nq_pool,
+           "l2": "inputs larger than L2 (index and per-batch scan far above 126 MB)", **build_info}
+
+    if args.impl == "reference":
+        q_host = queries.cpu().numpy()
+        times = []
+        res = None
+        for i in range(args.warmup + args.steps):
+            res = cpu_reference(arrays, q_host[: max(args.eval, 256)], params,
+                                args.cpu_seconds / max(args.steps, 1), threads)
+            if i >= args.warmup:
+                times.append(res["qps"])
+        qps = float(np.mean(times))
+        rec = recall10(res["ids"][: gt.shape[0]], res["cnt"][: gt.shape[0]], gt[: res["ids"].shape[0]])
+        line = {"metric": "QPS at R@10>=0.90 (p50/p99 ms, scan GB/s vs HBM peak)", "impl": "reference",
+                "value": qps, "unit": "queries/s", "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+                "dtype": "f32/u8/i8", "data": "synthetic", "config": cfg, "recall_at_10": rec,
+                "cpu_baseline": {"value": qps, "unit": "queries/s", "cores": threads, "kind": "port",
+                                 "sample": f"{res['queries']} queries per step on {threads} threads"},
+                "e2e": {"value": qps, "unit": "queries/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+        print(json.dumps(line), flush=True)
+        return finish(world)
+
+    index = Index.from_arrays(arrays, device=local)
+    index.set_route_precision(args.route == "bf16")
+    index.set_timing(True)
+    q768 = queries.to(dev).contiguous()
+    B = args.batch
+    out_sc = torch.empty((B, params.k), dtype=torch.float32, device=dev)
+    out_id = torch.empty((B, params.k), dtype=torch.int32, device=dev)
+    out_n = torch.empty((B,), dtype=torch.int32, device=dev)
+    stream = torch.cuda.current_stream()
+
+    # recall on the ground-truth queries
+    ev = q768[: args.eval].cpu().numpy()
+    sc, ids, cnt = index.search_batch(ev, None, params)
+    rec = recall10(ids, cnt, gt)
+    rec_i8 = recall10(ids, cnt, int8_truth(arrays, q768[: args.eval]))
+    log(f"{label}: recall@10 {rec:.4f} (float truth), {rec_i8:.4f} (int8 truth)")
+
+    def step(i):
+        lo = (i * B) % (nq_pool - B + 1)
+        index.search_device(B, q768[lo].data_ptr(), None, params, out_sc.data_ptr(), out_id.data_ptr(),
+                            out_n.data_ptr(), stream.cuda_stream)
+
+    for i in range(args.warmup):
+        step(i)
+    torch.cuda.synchronize()
+    if world > 1:
+        torch.distributed.barrier()
+    step_ms, stats = [], []
+    with ClockSampler(local) as clocks:
+        torch.cuda.synchronize()
+        for i in range(args.steps):
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            step(args.warmup + i)
+            b.record(stream)
+            b.synchronize()
+            step_ms.append(a.elapsed_time(b))
+            stats.append(index.last_stats())
+        torch.cuda.synchronize()
+    total_ms = float(np.sum(step_ms))
+    if world > 1:
+        t = torch.tensor([total_ms], device=dev)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        total_ms = float(t.item())
+    qps = world * args.steps * B / (total_ms / 1e3)
+
+    # the scan kernel: algorithmic bytes over its event-timed duration, per launch
+    scan_ms = np.array([s["ms_scan"] for s in stats])
+    scanned = np.array([s["scanned"] for s in stats], dtype=np.float64)
+    achieved = float(np.mean(scanned * SCAN_BYTES_PER_SLOT / (scan_ms / 1e3)) / 1e9)
+    peaks = measured_peaks()
+    peak = peaks.get("hbm_gbs", 6650.0)
+    traffic = None
+    tpath = os.path.join(ROOT, "profiles", "scan_traffic.json")
+    if os.path.exists(tpath):
+        with open(tpath) as f:
+            t = json.load(f)
+        if t.get("workload") == args.workload and t.get("config") == config:
+            traffic = float(t["dram_bytes_per_slot"]) * float(np.mean(scanned))
+    stage = {k: round(float(np.mean([s[k] for s in stats])), 4)
+             for k in ("ms_prep", "ms_route_gemm", "ms_route_select", "ms_scan", "ms_cut", "ms_rerank",
+                       "ms_tier2", "ms_total")}
+
+    # one query per launch
+    plain_ms = []
+    for i in range(args.plain):
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        index.search_device(1, q768[i].data_ptr(), None, params, out_sc.data_ptr(), out_id.data_ptr(),
+                            out_n.data_ptr(), stream.cuda_stream)
+        b.record(stream)
+        b.synchronize()
+        plain_ms.append(a.elapsed_time(b))
+    plain_ms = np.array(plain_ms[min(8, len(plain_ms) // 4):] or [float("nan")])
+
+    # end to end through the host API from pinned memory
+    qh = torch.empty((B, 768), dtype=torch.float32).pin_memory()
+    osc = torch.empty((B, params.k), dtype=torch.float32).pin_memory()
+    oid = torch.empty((B, params.k), dtype=torch.int32).pin_memory()
+    ocn = torch.empty((B,), dtype=torch.int32).pin_memory()
+    host_pool = queries.cpu()
+    e2e_s = []
+    for i in range(args.warmup + args.steps):
+        lo = (i * B) % (nq_pool - B + 1)
+        qh.copy_(host_pool[lo:lo + B])
+        t = time.perf_counter()
+        index.search_into(qh.numpy(), params, osc.numpy(), oid.numpy().view(np.uint32), ocn.numpy().view(np.uint32))
+        if i >= args.warmup:
+            e2e_s.append(time.perf_counter() - t)
+    e2e_qps = world * args.steps * B / float(np.sum(e2e_s))
+
+    cpu = None
+    if rank == 0 and world == 1 and args.cpu_seconds > 0:
+        r = cpu_reference(arrays, queries[: max(args.eval, 256)].cpu().numpy(), params, args.cpu_seconds,
+                          threads)
+        cpu = {"value": r["qps"], "unit": "queries/s", "cores": threads, "kind": "port",
+               "sample": f"{r['queries']} queries of the same workload, {r['seconds']:.1f} s, "
+                         f"OpenMP over queries, oracle built -march=native"}
+    line = {
+        "metric": "QPS at R@10>=0.90 (p50/p99 ms, scan GB/s vs HBM peak)",
+        "value": qps, "unit": "queries/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": total_ms / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "u8 LUT / f32 estimate / i8 rerank", "data": "synthetic",
+        "config": cfg, "recall_at_10": rec, "recall_at_10_int8_truth": rec_i8,
+        "recall_note": "float truth = exact FP32 top-10 over the unit 768-d vectors; int8 truth = "
+                       "exact top-10 of the int8 rerank score over every row",
+        "p50_ms": float(np.percentile(step_ms, 50)), "p99_ms": float(np.percentile(step_ms, 99)),
+        "latency_note": "batched form: every query of a batch completes with its batch",
+        "plain": {"qps": float(1e3 / np.mean(plain_ms)), "p50_ms": float(np.percentile(plain_ms, 50)),
+                  "p99_ms": float(np.percentile(plain_ms, 99)), "queries": int(plain_ms.size)},
+        "stage_ms": stage,
+        "scanned_per_query": float(np.mean(scanned) / B),
+        "roofline": {"bound": "hbm", "kernel": "k_scan", "achieved": achieved, "peak": peak,
+                     "unit": "GB/s", "frac": achieved / peak,
+                     "peak_source": "MEASURED_PEAKS.json hbm_gbs" if "hbm_gbs" in peaks else "fallback",
+                     "traffic": traffic, "bytes_per_slot": SCAN_BYTES_PER_SLOT},
+        "cpu_baseline": cpu,
+        "e2e": {"value": e2e_qps, "unit": "queries/s", "h2d_bytes_per_step": B * 768 * 4,
+                "d2h_bytes_per_step": B * params.k * 8 + B * 4},
+        "gpu_launches": int(sum(s["launches"] for s in stats)),
+        "clocks": clocks.summary(),
+    }
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    index.close()
+    return finish(world)
+
+
+def finish(world: int):
+    if world > 1 and torch.distributed.is_initialized():
+        torch.distributed.barrier()
+        torch.distributed.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -90,8 +90,25 @@ typedef struct {
  * set and the centroid scores equal the FP32 path's exactly. */
 typedef enum { SG_ROUTE_FP32 = 0, SG_ROUTE_BF16 = 1 } sg_route_precision;
 
+/* Device-side stage times (ms) and work counters of the last search call, recorded when timing is
+ * on (sg_set_timing). No counterpart in the reference beyond ivf::Timing; used for rooflines. */
+typedef struct {
+  float ms_prep;          /* prefix + rotation + LUT + int8 query weights                       */
+  float ms_route_gemm;    /* routing scores (BF16 tensor-core GEMM or exact FP32)               */
+  float ms_route_select;  /* probe selection, FP32 rescoring window, work items                 */
+  float ms_scan;          /* LUT scan + estimate + admission (the persistent scan kernel)        */
+  float ms_cut;           /* candidate cut + SOAR dedup                                           */
+  float ms_rerank;        /* prune + tier-2 + int8 rerank + top-k                                 */
+  float ms_tier2;         /* part of ms_rerank in the 2-bit tier                                  */
+  float ms_total;
+  uint32_t launches;      /* kernels of this library launched by the call                          */
+  uint32_t reserved;
+  uint64_t scanned;       /* slots scanned, padding included, summed over queries                 */
+  uint64_t probed;        /* clusters probed, summed over queries                                 */
+  uint64_t reranked;      /* candidates reaching the rerank stage, summed over queries            */
+} sg_stats;
+
 typedef struct sg_index sg_index;
-typedef struct sg_filter sg_filter;
 
 /* Host arrays of an IVF index plus its corpus, laid out exactly as the reference's files
  * (src/ivf.rs:75-90 Corpus::open, src/ivf.rs:553-578 Index::open). Optional members may be
@@ -130,6 +147,10 @@ int sg_close(sg_index* index);
 int sg_index_info(const sg_index* index, uint32_t* k, uint64_t* n, uint64_t* nblocks,
                   uint32_t* has_tier2);
 int sg_set_route_precision(sg_index* index, int precision);
+/* Turns per-stage device timing of every search on (1) or off (0). */
+int sg_set_timing(sg_index* index, int on);
+/* Stage times and counters of the last sg_search / sg_search_device on this index. */
+int sg_last_stats(const sg_index* index, sg_stats* out);
 
 /* ---- search ----------------------------------------------------------------------------- */
 /* ivf::Index::search / search_view (src/ivf.rs:621-633) for nq queries at once.

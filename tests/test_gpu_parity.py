@@ -226,3 +226,16 @@ def test_invalid_params_are_rejected(gpu_a):
         ix.search_batch(q768[:1], q256[:1], Params(8, 5000))
     with pytest.raises(SieveError):
         ix.search_batch(q768[:1], q256[:1], Params(8, 100, Rerank(9)))
+
+
+def test_buffer_overflow_retry_gives_exact_results(monkeypatch):
+    """A candidate buffer too small for the batch makes queries overflow; they are re-run with
+    the exact bound and must still equal the oracle."""
+    arrays, q768, q256, _ = index_a()
+    monkeypatch.setenv("SIEVE_GPU_SOFT_CAP", "600")
+    ix = Index.from_arrays(arrays)
+    monkeypatch.delenv("SIEVE_GPU_SOFT_CAP")
+    try:
+        check_search(ix, O.OracleIndex(arrays), q768, q256, Params(16, 500, Rerank.full(), 10))
+    finally:
+        ix.close()
