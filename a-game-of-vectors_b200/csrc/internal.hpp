@@ -113,6 +113,12 @@ struct Config {
 std::string& last_error();
 int fail(int code, const std::string& msg);
 
+// Views of an open index for entry points in other translation units (sieve_gpu.cu defines them).
+const DevIndex* index_arrays(const sg_index* h);
+const Config* index_config(const sg_index* h);
+int index_sms(const sg_index* h);
+int index_check_params(const sg_index* h, const sg_params* p);
+
 // kernel launchers (one per .cu file section)
 void launch_prefix(Workspace& w, uint32_t nq, cudaStream_t st);
 void launch_prep(const DevIndex& ix, Workspace& w, uint32_t nq, cudaStream_t st);

@@ -575,6 +575,14 @@ bool read_file(const std::string& path, std::vector<char>& out, bool optional, i
 
 }  // namespace
 
+namespace sg {
+// Read-only views of an open index for entry points that live in other translation units.
+const DevIndex* index_arrays(const sg_index* h) { return &h->ix; }
+const Config* index_config(const sg_index* h) { return &h->cfg; }
+int index_sms(const sg_index* h) { return h->sms; }
+int index_check_params(const sg_index* h, const sg_params* p) { return check_params(h, p); }
+}  // namespace sg
+
 extern "C" {
 
 const char* sg_last_error(void) { return sg::last_error().c_str(); }

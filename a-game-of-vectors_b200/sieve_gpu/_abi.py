@@ -171,6 +171,7 @@ EXPORTS = [
     "sg_last_stats",
     "sg_search",
     "sg_search_device",
+    "sg_search_noalloc",
     "sg_route",
     "sg_candidates",
     "sg_query_prep",

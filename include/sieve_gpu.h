@@ -168,6 +168,21 @@ int sg_search_device(sg_index* index, uint32_t nq, const float* d_q768, const fl
                      uint64_t allow_words, float* d_out_scores, uint32_t* d_out_ids,
                      uint32_t* d_out_counts, void* stream);
 
+/* No counterpart in the reference. One query through the same path as sg_search, for callers
+ * that must not allocate device memory while serving: a latency-critical serving thread (cudaFree
+ * synchronises the device, cudaMalloc can wait behind running kernels) or a host whose device
+ * memory budget is fixed up front. All scratch comes from one fixed 32 MiB device array that
+ * every GPU loading the library holds until exit; the call allocates nothing (no cudaMalloc,
+ * cudaFree or allocating library routine). Params whose buffers exceed 32 MiB are rejected with
+ * SG_ERR_INVALID. Pointers are device pointers (d_q256 nullable); results (k scores, k ids, one
+ * count) are written on `stream` asynchronously, as sg_search orders them. The first call on a
+ * device looks up the array's device address (once per device, that device current), so make it
+ * before any stream capture. Calls share the array: calls that overlap on the GPU race. */
+int sg_search_noalloc(sg_index* index, const float* d_q768, const float* d_q256,
+                      const sg_params* params, const uint64_t* d_allow_bits, uint64_t allow_words,
+                      float* d_out_scores, uint32_t* d_out_ids, uint32_t* d_out_count,
+                      void* stream);
+
 /* ivf::Index::route (src/ivf.rs:589-613): the probe list of each query, best first, as
  * (centroid score, cluster). out_scores/out_clusters [nq * params.nprobe], out_counts [nq]. */
 int sg_route(sg_index* index, uint32_t nq, const float* q256, const sg_params* params,
