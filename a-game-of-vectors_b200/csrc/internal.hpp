@@ -36,6 +36,7 @@ struct DevIndex {
   uint32_t* block_off = nullptr;     // [k+1] first block of each cluster
   uint32_t* clen = nullptr;          // [k] real (non-PAD) slots of each cluster
   uint8_t* blocks = nullptr;         // [nblocks*1024] nibble-transposed codes (blocks.bin)
+  uint32_t* blocks_mma = nullptr;    // [nblocks*256] the same codes in the MMA scan's word order
   float* mul = nullptr;              // [nslots] factors.f32 [.., 0]
   float* err = nullptr;              // [nslots] factors.f32 [.., 1]
   uint32_t* ids = nullptr;           // [nslots] ids.u32
@@ -51,6 +52,7 @@ struct DevIndex {
   std::vector<uint64_t> h_block_off;
   std::vector<uint32_t> h_clen;
   std::vector<uint32_t> h_chunks_desc_prefix;  // prefix sums of per-cluster chunk counts, largest first
+  std::vector<uint64_t> h_slots_desc_prefix;   // prefix sums of per-cluster slot counts, largest first
   int route_precision = SG_ROUTE_BF16;
 };
 
@@ -76,7 +78,13 @@ struct Workspace {
   uint64_t* scanned = nullptr;   // [nq]
   uint4* items = nullptr;        // [item_cap] (query, probe rank, first block, end block)
   uint4* seed_items = nullptr;   // [nq] each query's first rank-0 chunk (the seed)
-  uint32_t* counters = nullptr;  // [4]: nitems, next item, status, spare
+  uint32_t* counters = nullptr;  // [8]: nitems, next item, status, -, mma groups, next group
+  uint32_t* inv_cnt = nullptr;   // [k] (query, probe >= 1) pairs per cluster
+  uint32_t* inv_fill = nullptr;  // [k]
+  uint32_t* inv_off = nullptr;   // [k+1]
+  uint32_t* inv_list = nullptr;  // [nq*P] (query << 12 | probe rank), grouped by cluster
+  uint2* gitems = nullptr;       // [gitems_cap] (cluster, group of 64 queries)
+  uint64_t gitems_cap = 0, inv_cap = 0;
   uint32_t* thr = nullptr;       // [nq] running lower bound of the cand-th estimate (ordered)
   uint32_t* ccount = nullptr;    // [nq] entries appended to a query's candidate buffer
   uint4* cbuf = nullptr;         // [nq*cbuf_per_q] (est bits, admission key, slot, 0)
@@ -108,6 +116,8 @@ struct Config {
   uint32_t seed_blocks = kSeedBlocks;
   uint32_t scan_ctas_per_sm = 2;
   uint32_t soft_cap = 0;  // per-query buffer override (0: automatic); SIEVE_GPU_SOFT_CAP
+  uint32_t mma_min_queries_per_cluster = 8;   // use the MMA scan at or above this average
+  int mma = 1;            // SIEVE_GPU_MMA: 0 ALU scan only, 1 automatic, 2 MMA whenever nprobe > 1
 };
 
 std::string& last_error();
@@ -124,9 +134,16 @@ void launch_prefix(Workspace& w, uint32_t nq, cudaStream_t st);
 void launch_prep(const DevIndex& ix, Workspace& w, uint32_t nq, cudaStream_t st);
 void launch_route_scores(const DevIndex& ix, Workspace& w, uint32_t nq, int precision,
                          cudaStream_t st);
+// alu_ranks = false leaves probe ranks >= 1 to the MMA scan (only rank-0 chunks past the seed
+// become ALU work items).
 void launch_route_select(const DevIndex& ix, Workspace& w, uint32_t nq, const sg_params& p,
                          int precision, uint32_t chunk_blocks, uint32_t seed_blocks,
-                         cudaStream_t st);
+                         bool alu_ranks, cudaStream_t st);
+// Inverts the probe lists and runs the tensor-core scan over (cluster, query group) items;
+// returns the kernels launched. Needs the seed pass first (it sets the thresholds).
+int launch_scan_mma(const DevIndex& ix, Workspace& w, uint32_t nq, const sg_params& p,
+                    const uint64_t* allow, uint64_t allow_words, int sms, cudaStream_t st);
+int transcode_mma(const uint8_t* blocks, uint64_t nblocks, uint32_t* out);
 // The seed pass (one CTA per query, rank-0 seed item) then the persistent pass over the queue.
 void launch_scan(const DevIndex& ix, Workspace& w, uint32_t nq, const sg_params& p,
                  const uint64_t* allow, uint64_t allow_words, int sms, uint32_t chunk_blocks,

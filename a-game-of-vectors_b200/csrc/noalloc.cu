@@ -72,7 +72,7 @@ void carve_workspace(Carve& c, sg::Workspace& w, const sg::DevIndex& x, uint32_t
   w.scanned = c.take<uint64_t>(1);
   w.items = c.take<uint4>(items);
   w.seed_items = c.take<uint4>(1);
-  w.counters = c.take<uint32_t>(4);
+  w.counters = c.take<uint32_t>(8);
   w.thr = c.take<uint32_t>(1);
   w.ccount = c.take<uint32_t>(1);
   w.cbuf = c.take<uint4>(cbuf);
@@ -130,7 +130,7 @@ extern "C" int sg_search_noalloc(sg_index* h, const float* d_q768, const float* 
 
   // The array keeps the previous call's contents: clear everything that must start at zero.
   cudaStream_t st = static_cast<cudaStream_t>(stream);
-  if ((e = cudaMemsetAsync(w.counters, 0, 4 * sizeof(uint32_t), st)) != cudaSuccess ||
+  if ((e = cudaMemsetAsync(w.counters, 0, 8 * sizeof(uint32_t), st)) != cudaSuccess ||
       (e = cudaMemsetAsync(w.thr, 0, sizeof(uint32_t), st)) != cudaSuccess ||
       (e = cudaMemsetAsync(w.ccount, 0, sizeof(uint32_t), st)) != cudaSuccess ||
       (e = cudaMemsetAsync(w.overflow, 0, 1, st)) != cudaSuccess)
@@ -138,7 +138,8 @@ extern "C" int sg_search_noalloc(sg_index* h, const float* d_q768, const float* 
   if (!d_q256) sg::launch_prefix(w, 1, st);
   sg::launch_prep(x, w, 1, st);
   sg::launch_route_scores(x, w, 1, x.route_precision, st);
-  sg::launch_route_select(x, w, 1, p, x.route_precision, cfg.small_chunk_blocks, cfg.seed_blocks, st);
+  sg::launch_route_select(x, w, 1, p, x.route_precision, cfg.small_chunk_blocks, cfg.seed_blocks,
+                          true, st);
   if (p.cand > 0) {
     sg::launch_scan(x, w, 1, p, d_allow_bits, allow_words, sg::index_sms(h), cfg.small_chunk_blocks,
                     cfg.seed_blocks, cfg.scan_ctas_per_sm, st);

@@ -165,6 +165,7 @@ struct SelectArgs {
   sg_params p;
   uint32_t chunk_blocks;
   uint32_t seed_blocks;
+  uint32_t alu_ranks;
   uint4* seed_items;
   float* probe_sc;
   uint32_t* probe_cl;
@@ -285,7 +286,7 @@ __global__ void __launch_bounds__(256) k_route_select(SelectArgs a) {
   // Rank 0's first seed_blocks blocks form the query's seed item (scanned first, one CTA per
   // query, to set a tight admission threshold); everything else is cut into chunks.
   auto nchunks = [&](uint32_t r, uint32_t nb) {
-    uint32_t rest = r == 0 ? (nb > a.seed_blocks ? nb - a.seed_blocks : 0) : nb;
+    uint32_t rest = r == 0 ? (nb > a.seed_blocks ? nb - a.seed_blocks : 0) : (a.alu_ranks ? nb : 0);
     return (rest + a.chunk_blocks - 1) / a.chunk_blocks;
   };
   uint32_t slots = 0, chunks = 0;
@@ -320,6 +321,8 @@ __global__ void __launch_bounds__(256) k_route_select(SelectArgs a) {
       uint32_t e = min(b1, b0 + a.seed_blocks);
       a.seed_items[q] = make_uint4(q, 0, b0, e);
       b0 = e;
+    } else if (!a.alu_ranks) {
+      continue;
     }
     for (uint32_t b = b0; b < b1; b += a.chunk_blocks) {
       if (ibase < a.item_cap) a.items[ibase] = make_uint4(q, r, b, min(b1, b + a.chunk_blocks));
@@ -347,7 +350,7 @@ void launch_route_scores(const DevIndex& ix, Workspace& w, uint32_t nq, int prec
 
 void launch_route_select(const DevIndex& ix, Workspace& w, uint32_t nq, const sg_params& p,
                          int precision, uint32_t chunk_blocks, uint32_t seed_blocks,
-                         cudaStream_t st) {
+                         bool alu_ranks, cudaStream_t st) {
   SelectArgs a;
   a.q256 = w.q256;
   a.cent = ix.cent;
@@ -361,6 +364,7 @@ void launch_route_select(const DevIndex& ix, Workspace& w, uint32_t nq, const sg
   a.p = p;
   a.chunk_blocks = chunk_blocks;
   a.seed_blocks = seed_blocks;
+  a.alu_ranks = alu_ranks ? 1u : 0u;
   a.seed_items = w.seed_items;
   a.probe_sc = w.probe_sc;
   a.probe_cl = w.probe_cl;

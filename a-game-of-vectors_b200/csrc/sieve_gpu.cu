@@ -87,6 +87,7 @@ void free_index(sg::DevIndex& x) {
   dfree(x.block_off);
   dfree(x.clen);
   dfree(x.blocks);
+  dfree(x.blocks_mma);
   dfree(x.mul);
   dfree(x.err);
   dfree(x.ids);
@@ -118,6 +119,11 @@ void free_ws(sg::Workspace& w) {
   dfree(w.items);
   dfree(w.seed_items);
   dfree(w.counters);
+  dfree(w.inv_cnt);
+  dfree(w.inv_fill);
+  dfree(w.inv_off);
+  dfree(w.inv_list);
+  dfree(w.gitems);
   dfree(w.thr);
   dfree(w.ccount);
   dfree(w.cbuf);
@@ -192,6 +198,11 @@ int build_index(const sg_ivf_arrays* a, int device, sg_index** out) {
     std::sort(ch.begin(), ch.end(), std::greater<uint32_t>());
     x.h_chunks_desc_prefix.assign(K + 1, 0);
     for (uint32_t c = 0; c < K; c++) x.h_chunks_desc_prefix[c + 1] = x.h_chunks_desc_prefix[c] + ch[c];
+    std::vector<uint64_t> sl(K);
+    for (uint32_t c = 0; c < K; c++) sl[c] = (uint64_t)(boff32[c + 1] - boff32[c]) * SG_BLOCK;
+    std::sort(sl.begin(), sl.end(), std::greater<uint64_t>());
+    x.h_slots_desc_prefix.assign(K + 1, 0);
+    for (uint32_t c = 0; c < K; c++) x.h_slots_desc_prefix[c + 1] = x.h_slots_desc_prefix[c] + sl[c];
   }
   // centroids: row-major, transposed, BF16; largest norm for the routing error window
   std::vector<float> ct((size_t)K * SG_PDIM);
@@ -229,6 +240,11 @@ int build_index(const sg_ivf_arrays* a, int device, sg_index** out) {
     free_index(x);
     return rc;
   }
+  if ((rc = dalloc(&x.blocks_mma, (size_t)nblocks * 256)) ||
+      sg::transcode_mma(x.blocks, nblocks, x.blocks_mma) || cudaDeviceSynchronize() != cudaSuccess) {
+    free_index(x);
+    return rc ? rc : fail(SG_ERR_DEVICE, "transcode of the code blocks failed");
+  }
   if (a->norm256 && (rc = upload(&x.norm256, a->norm256, a->n))) {
     free_index(x);
     return rc;
@@ -243,6 +259,7 @@ int build_index(const sg_ivf_arrays* a, int device, sg_index** out) {
     x.has_t2 = true;
   }
   if (const char* sc = getenv("SIEVE_GPU_SOFT_CAP")) h->cfg.soft_cap = (uint32_t)strtoul(sc, nullptr, 10);
+  if (const char* m = getenv("SIEVE_GPU_MMA")) h->cfg.mma = atoi(m);
   cudaDeviceProp prop;
   CK(cudaGetDeviceProperties(&prop, device));
   h->sms = prop.multiProcessorCount;
@@ -316,7 +333,21 @@ int ensure_ws(sg_index* h, uint32_t nq, const sg_params& p, uint32_t cbuf_per_q)
     if ((rc = dalloc(&w.items, want))) return rc;
     w.item_cap = want;
   }
-  if (!w.counters && (rc = dalloc(&w.counters, 4))) return rc;
+  if (!w.counters && (rc = dalloc(&w.counters, 8))) return rc;
+  if (!w.inv_cnt) {
+    if ((rc = dalloc(&w.inv_cnt, x.k)) || (rc = dalloc(&w.inv_fill, x.k)) ||
+        (rc = dalloc(&w.inv_off, (size_t)x.k + 1)))
+      return rc;
+  }
+  const uint64_t pairs = (uint64_t)nq * P;
+  if (pairs > w.inv_cap) {
+    dfree(w.inv_list);
+    dfree(w.gitems);
+    uint64_t want = std::max<uint64_t>(pairs, w.inv_cap * 2);
+    if ((rc = dalloc(&w.inv_list, want)) || (rc = dalloc(&w.gitems, want / 64 + x.k + 1))) return rc;
+    w.inv_cap = want;
+    w.gitems_cap = want / 64 + x.k + 1;
+  }
   const uint64_t cb = (uint64_t)nq * cbuf_per_q;
   if (cb > w.cbuf_cap) {
     dfree(w.cbuf);
@@ -342,17 +373,30 @@ int check_params(const sg_index* h, const sg_params* p) {
   return SG_OK;
 }
 
-// Per-query candidate buffer: every chunk appends at most `cand`, so chunks x cand is exact.
-uint32_t full_cap(const sg_index* h, const sg_params& p) {
+// Does a call of nq queries run the tensor-core scan? (It pays off once enough queries share each
+// probed cluster; SIEVE_GPU_MMA forces it off (0) or on (2).)
+bool use_mma(const sg_index* h, uint32_t nq, uint32_t P) {
+  const sg::DevIndex& x = h->ix;
+  if (!x.blocks_mma || P <= 1) return false;
+  if (h->cfg.mma == 2) return true;
+  return h->cfg.mma == 1 && nq >= 64 &&
+         (uint64_t)nq * (P - 1) >= (uint64_t)h->cfg.mma_min_queries_per_cluster * x.k;
+}
+
+// Exact per-query candidate-buffer bound. A slot is appended at most once, so the probed
+// clusters' slots bound it; the ALU scan also cuts every chunk to `cand`, so chunks x cand does.
+uint32_t full_cap(const sg_index* h, const sg_params& p, uint32_t nq) {
   const uint32_t P = std::min<uint32_t>(p.nprobe, h->ix.k);
-  uint64_t b = (uint64_t)h->ix.h_chunks_desc_prefix[P] * std::max<uint32_t>(p.cand, 1);
+  uint64_t b = h->ix.h_slots_desc_prefix[P];
+  if (!use_mma(h, nq, P))
+    b = std::min<uint64_t>(b, (uint64_t)h->ix.h_chunks_desc_prefix[P] * std::max<uint32_t>(p.cand, 1));
   return (uint32_t)std::min<uint64_t>(std::max<uint64_t>(b, 1), 0x7FFFFFFFull);
 }
 
 // Soft per-query buffer for batches: at least 16 x cand entries, and up to an 8 GiB budget
 // shared by the batch. A query that fills it is re-run (see search_impl) with the exact bound.
 uint32_t batch_cap(const sg_index* h, const sg_params& p, uint32_t nq) {
-  uint32_t full = full_cap(h, p);
+  uint32_t full = full_cap(h, p, nq);
   if (h->cfg.soft_cap) return std::min(full, h->cfg.soft_cap);
   if (nq <= 8) return full;
   uint64_t budget = (8ull << 30) / (sizeof(uint4) * (uint64_t)nq);
@@ -370,7 +414,7 @@ int run_pipeline(sg_index* h, uint32_t nq, const sg_params& p, bool have_q256,
   sg::DevIndex& x = h->ix;
   cudaStream_t st = h->stream;
   uint32_t launches = 0;
-  CK(cudaMemsetAsync(w.counters, 0, 4 * sizeof(uint32_t), st));
+  CK(cudaMemsetAsync(w.counters, 0, 8 * sizeof(uint32_t), st));
   CK(cudaMemsetAsync(w.thr, 0, nq * sizeof(uint32_t), st));
   CK(cudaMemsetAsync(w.ccount, 0, nq * sizeof(uint32_t), st));
   CK(cudaMemsetAsync(w.overflow, 0, nq, st));
@@ -384,12 +428,16 @@ int run_pipeline(sg_index* h, uint32_t nq, const sg_params& p, bool have_q256,
   sg::launch_route_scores(x, w, nq, x.route_precision, st);
   if (timed) CK(cudaEventRecord(w.ev[2], st));
   const uint32_t cb = nq < h->cfg.small_batch ? h->cfg.small_chunk_blocks : h->cfg.chunk_blocks;
-  sg::launch_route_select(x, w, nq, p, x.route_precision, cb, h->cfg.seed_blocks, st);
+  // The tensor-core scan pays off once enough queries share each probed cluster.
+  const uint32_t P = std::min<uint32_t>(p.nprobe, x.k);
+  const bool mma = use_mma(h, nq, P);
+  sg::launch_route_select(x, w, nq, p, x.route_precision, cb, h->cfg.seed_blocks, !mma, st);
   if (timed) CK(cudaEventRecord(w.ev[3], st));
   launches += 3;
   if (p.cand > 0) {
     sg::launch_scan(x, w, nq, p, d_allow, allow_words, h->sms, cb, h->cfg.seed_blocks,
                     h->cfg.scan_ctas_per_sm, st);
+    if (mma) launches += sg::launch_scan_mma(x, w, nq, p, d_allow, allow_words, h->sms, st);
     if (timed) CK(cudaEventRecord(w.ev[4], st));
     sg::launch_cut(x, w, nq, p, st);
     launches += 3;
@@ -476,11 +524,13 @@ int search_impl(sg_index* h, uint32_t nq, const float* q768, const float* q256,
   }
   CK(cudaMemcpyAsync(out_n, w.out_n, (size_t)nq * 4, okind, h->stream));
   std::vector<uint64_t> scanned;
-  std::vector<uint32_t> probed, reranked;
+  std::vector<uint32_t> probed, reranked, buffered;
   if (timed_run) {
     scanned.resize(nq);
     probed.resize(nq);
     reranked.resize(nq);
+    buffered.resize(nq);
+    CK(cudaMemcpyAsync(buffered.data(), w.ccount, nq * 4, cudaMemcpyDeviceToHost, h->stream));
     CK(cudaMemcpyAsync(scanned.data(), w.scanned, nq * 8, cudaMemcpyDeviceToHost, h->stream));
     CK(cudaMemcpyAsync(probed.data(), w.probe_n, nq * 4, cudaMemcpyDeviceToHost, h->stream));
     CK(cudaMemcpyAsync(reranked.data(), w.ln, nq * 4, cudaMemcpyDeviceToHost, h->stream));
@@ -490,15 +540,17 @@ int search_impl(sg_index* h, uint32_t nq, const float* q768, const float* q256,
   const bool timed = t != nullptr || h->timing_on;
   if (timed) {
     collect_stats(w, p);
-    uint64_t sc = 0, pr = 0, rr = 0;
+    uint64_t sc = 0, pr = 0, rr = 0, bu = 0;
     for (uint32_t i = 0; i < nq; i++) {
       sc += scanned[i];
       pr += probed[i];
       rr += reranked[i];
+      bu += buffered[i];
     }
     w.last.scanned = sc;
     w.last.probed = pr;
     w.last.reranked = rr;
+    w.last.buffered = bu;
   }
   if (t) {
     t->route += (uint64_t)((w.last.ms_prep + w.last.ms_route_gemm + w.last.ms_route_select) * 1e6);
@@ -516,9 +568,12 @@ int search_impl(sg_index* h, uint32_t nq, const float* q768, const float* q256,
   for (uint32_t i = 0; i < nq; i++)
     if (ovf[i]) redo.push_back(i);
   if (!redo.empty()) {
-    const uint32_t fcap = full_cap(h, p);
-    const uint32_t per = (uint32_t)std::max<uint64_t>(
-        1, std::min<uint64_t>(redo.size(), (8ull << 30) / (sizeof(uint4) * (uint64_t)fcap)));
+    uint32_t per = (uint32_t)redo.size();
+    uint32_t fcap = full_cap(h, p, per);
+    while (per > 1 && (uint64_t)per * fcap * sizeof(uint4) > (8ull << 30)) {
+      per = (per + 1) / 2;
+      fcap = full_cap(h, p, per);
+    }
     std::vector<float> hq768, hq256;
     std::vector<float> osc((size_t)per * std::max<uint32_t>(k, 1));
     std::vector<uint32_t> oid((size_t)per * std::max<uint32_t>(k, 1)), on(per);
@@ -736,11 +791,11 @@ int sg_route(sg_index* h, uint32_t nq, const float* q256, const sg_params* param
   if ((rc = stage_inputs(h, nq, nullptr, q256, false))) return rc;
   sg::Workspace& w = h->ws;
   cudaStream_t st = h->stream;
-  CK(cudaMemsetAsync(w.counters, 0, 16, st));
+  CK(cudaMemsetAsync(w.counters, 0, 32, st));
   sg::launch_prep(h->ix, w, nq, st);
   sg::launch_route_scores(h->ix, w, nq, h->ix.route_precision, st);
   sg::launch_route_select(h->ix, w, nq, *params, h->ix.route_precision, h->cfg.chunk_blocks,
-                          h->cfg.seed_blocks, st);
+                          h->cfg.seed_blocks, true, st);
   CK(cudaGetLastError());
   const uint32_t P = std::min<uint32_t>(params->nprobe, h->ix.k);
   if (P) {
@@ -762,7 +817,7 @@ int sg_candidates(sg_index* h, uint32_t nq, const float* q256, const sg_params* 
   if (nq == 0) return SG_OK;
   CK(cudaSetDevice(h->ix.device));
   const sg_params& p = *params;
-  uint32_t cap = full_cap(h, p);
+  uint32_t cap = full_cap(h, p, 1);
   for (uint32_t q0 = 0; q0 < nq; q0++) {
     // one query at a time with the exact buffer bound: this entry point is for parity checks
     if ((rc = ensure_ws(h, 1, p, cap))) return rc;

@@ -106,6 +106,7 @@ typedef struct {
   uint64_t scanned;       /* slots scanned, padding included, summed over queries                 */
   uint64_t probed;        /* clusters probed, summed over queries                                 */
   uint64_t reranked;      /* candidates reaching the rerank stage, summed over queries            */
+  uint64_t buffered;      /* scan entries appended to the candidate buffers, summed over queries  */
 } sg_stats;
 
 typedef struct sg_index sg_index;

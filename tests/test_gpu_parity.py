@@ -20,18 +20,33 @@ def cparams(p: Params) -> SgParams:
     return p.to_c()
 
 
-@pytest.fixture(scope="module")
-def gpu_a():
+def open_with(arrays, scan_mode: str):
+    """Opens an index with the scan chosen by SIEVE_GPU_MMA (0 ALU, 1 automatic, 2 tensor-core)."""
+    import os
+
+    old = os.environ.get("SIEVE_GPU_MMA")
+    os.environ["SIEVE_GPU_MMA"] = scan_mode
+    try:
+        return Index.from_arrays(arrays)
+    finally:
+        if old is None:
+            del os.environ["SIEVE_GPU_MMA"]
+        else:
+            os.environ["SIEVE_GPU_MMA"] = old
+
+
+@pytest.fixture(scope="module", params=["1", "2", "0"], ids=["auto", "mma", "alu"])
+def gpu_a(request):
     arrays, q768, q256, _ = index_a()
-    ix = Index.from_arrays(arrays)
+    ix = open_with(arrays, request.param)
     yield ix, O.OracleIndex(arrays), arrays, q768, q256
     ix.close()
 
 
-@pytest.fixture(scope="module")
-def gpu_b():
+@pytest.fixture(scope="module", params=["1", "2"], ids=["auto", "mma"])
+def gpu_b(request):
     arrays, q768, q256, _ = index_b()
-    ix = Index.from_arrays(arrays)
+    ix = open_with(arrays, request.param)
     yield ix, O.OracleIndex(arrays), arrays, q768, q256
     ix.close()
 
