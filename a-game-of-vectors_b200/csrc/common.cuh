@@ -271,4 +271,93 @@ SG_DEV void lut_word(uint32_t w, const uint4& t, uint32_t* acc) {
   acc[3] += prmt(rb, 0u, 0x4341u);
 }
 
+
+SG_DEV uint32_t block_reduce_min(uint32_t v, uint32_t* tmp) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v = min(v, __shfl_xor_sync(0xFFFFFFFFu, v, o));
+  __syncthreads();
+  if ((threadIdx.x & 31) == 0) tmp[threadIdx.x >> 5] = v;
+  __syncthreads();
+  uint32_t r = 0xFFFFFFFFu;
+  for (uint32_t w = 0; w < (blockDim.x >> 5); w++) r = min(r, tmp[w]);
+  __syncthreads();
+  return r;
+}
+
+SG_DEV uint32_t block_reduce_max(uint32_t v, uint32_t* tmp) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v = max(v, __shfl_xor_sync(0xFFFFFFFFu, v, o));
+  __syncthreads();
+  if ((threadIdx.x & 31) == 0) tmp[threadIdx.x >> 5] = v;
+  __syncthreads();
+  uint32_t r = 0;
+  for (uint32_t w = 0; w < (blockDim.x >> 5); w++) r = max(r, tmp[w]);
+  __syncthreads();
+  return r;
+}
+
+// Range-adaptive radix select: the n-th largest (1-based, n <= m) of m u32 keys read through
+// get(i). Keys of a query cluster in a narrow value range (the ordered bits of estimates that
+// agree in sign, exponent and leading mantissa bits), so the select first reduces min and max
+// and then runs 11-bit digits over (key - min) only: at most 3 passes, and the keys spread over
+// the bins instead of piling onto one (same-address shared atomics serialise). `hist` needs 2048
+// words and `tmp` 32 words of shared memory; every thread of the block calls it.
+template <typename Get>
+SG_DEV uint32_t block_select_nth_u32r(Get get, uint32_t m, uint32_t n, uint32_t* hist, uint32_t* tmp) {
+  uint32_t lo = 0xFFFFFFFFu, hi = 0;
+  for (uint32_t i = threadIdx.x; i < m; i += blockDim.x) {
+    const uint32_t k = get(i);
+    lo = min(lo, k);
+    hi = max(hi, k);
+  }
+  lo = block_reduce_min(lo, tmp);
+  hi = block_reduce_max(hi, tmp);
+  const uint32_t span = hi - lo;
+  int top = span ? 32 - __clz(span) : 0;  // significant bits of (key - lo)
+  uint32_t want = 0;                      // selected value of (key - lo) >> top
+  uint32_t remaining = n;
+  __shared__ uint32_t s_dig, s_above;
+  while (top > 0) {
+    const int shift = top > 11 ? top - 11 : 0;
+    const int width = top - shift;
+    const uint32_t nbins = 1u << width;
+    for (uint32_t i = threadIdx.x; i < nbins; i += blockDim.x) hist[i] = 0;
+    __syncthreads();
+    for (uint32_t i = threadIdx.x; i < m; i += blockDim.x) {
+      const uint32_t r = get(i) - lo;
+      if ((top >= 32 ? 0u : (r >> top)) == want) atomicAdd(&hist[(r >> shift) & (nbins - 1)], 1u);
+    }
+    __syncthreads();
+    // bins from the top: thread t owns bins nbins-1-t*per .. (descending), per <= 8
+    const uint32_t per = (nbins + blockDim.x - 1) / blockDim.x;
+    uint32_t loc = 0;
+    for (uint32_t j = 0; j < per; j++) {
+      const uint32_t b = threadIdx.x * per + j;
+      if (b < nbins) loc += hist[nbins - 1 - b];
+    }
+    uint32_t tot;
+    const uint32_t excl = block_exclusive_scan(loc, tmp, &tot);
+    if (excl < remaining && remaining <= excl + loc) {
+      uint32_t run = excl;
+      for (uint32_t j = 0; j < per; j++) {
+        const uint32_t b = threadIdx.x * per + j;
+        if (b >= nbins) break;
+        const uint32_t c = hist[nbins - 1 - b];
+        if (run < remaining && remaining <= run + c) {
+          s_dig = nbins - 1 - b;
+          s_above = run;
+          break;
+        }
+        run += c;
+      }
+    }
+    __syncthreads();
+    want = (want << width) | s_dig;
+    remaining -= s_above;
+    top = shift;
+    __syncthreads();
+  }
+  return lo + want;
+}
+
 }  // namespace sg

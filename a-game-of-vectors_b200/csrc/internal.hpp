@@ -17,7 +17,8 @@ namespace sg {
 // in shared memory (4 B per slot), so kMaxChunkBlocks = 512 is 64 KB.
 constexpr uint32_t kMaxChunkBlocks = 512;
 constexpr uint32_t kChunkBlocks = 256;   // default chunk of the batched scan
-constexpr uint32_t kSeedBlocks = 512;    // rank-0 blocks each query's seed item covers
+constexpr uint32_t kSeedBlocks = 512;    // block budget of each query's seed (its first probes)
+constexpr uint32_t kMaxSegs = 64;        // probes one seed can cover
 // Largest cand / k / r the select kernels sort in shared memory.
 constexpr uint32_t kMaxCand = 4096;
 // Status bits a kernel raises in Workspace::status.
@@ -87,8 +88,9 @@ struct Workspace {
   uint64_t gitems_cap = 0, inv_cap = 0;
   uint32_t* thr = nullptr;       // [nq] running lower bound of the cand-th estimate (ordered)
   uint32_t* ccount = nullptr;    // [nq] entries appended to a query's candidate buffer
-  uint4* cbuf = nullptr;         // [nq*cbuf_per_q] (est bits, admission key, slot, 0)
-  uint32_t cbuf_per_q = 0;
+  uint32_t* cbuf_est = nullptr;  // [nq*cbuf_per_q] candidate buffer: estimate (f32 bits)
+  uint2* cbuf_info = nullptr;    // [nq*cbuf_per_q] (admission key, slot) of the same entry
+  uint32_t cbuf_per_q = 0;       // a multiple of 4 (the cut reads estimates four at a time)
   uint8_t* overflow = nullptr;   // [nq]
   float* cest = nullptr;         // [nq*cand] candidates after cut + dedup, in row order
   uint32_t* cid = nullptr;
@@ -104,7 +106,7 @@ struct Workspace {
   uint64_t allow_cap = 0;
   void* host_pinned = nullptr;   // pinned staging for host<->device copies
   size_t host_pinned_cap = 0;
-  cudaEvent_t ev[10] = {};
+  cudaEvent_t ev[12] = {};
   bool events = false;
   sg_stats last = {};
 };
@@ -144,7 +146,8 @@ void launch_route_select(const DevIndex& ix, Workspace& w, uint32_t nq, const sg
 int launch_scan_mma(const DevIndex& ix, Workspace& w, uint32_t nq, const sg_params& p,
                     const uint64_t* allow, uint64_t allow_words, int sms, cudaStream_t st);
 int transcode_mma(const uint8_t* blocks, uint64_t nblocks, uint32_t* out);
-// The seed pass (one CTA per query, rank-0 seed item) then the persistent pass over the queue.
+// The seed pass (one CTA per query, rank-0 seed item; skipped when seed_blocks is 0) then the
+// persistent pass over the queue (skipped when chunk_blocks is 0).
 void launch_scan(const DevIndex& ix, Workspace& w, uint32_t nq, const sg_params& p,
                  const uint64_t* allow, uint64_t allow_words, int sms, uint32_t chunk_blocks,
                  uint32_t seed_blocks, int ctas_per_sm, cudaStream_t st);

@@ -75,7 +75,8 @@ void carve_workspace(Carve& c, sg::Workspace& w, const sg::DevIndex& x, uint32_t
   w.counters = c.take<uint32_t>(8);
   w.thr = c.take<uint32_t>(1);
   w.ccount = c.take<uint32_t>(1);
-  w.cbuf = c.take<uint4>(cbuf);
+  w.cbuf_est = c.take<uint32_t>(cbuf);
+  w.cbuf_info = c.take<uint2>(cbuf);
   w.overflow = c.take<uint8_t>(1);
   w.cest = c.take<float>(cand);
   w.cid = c.take<uint32_t>(cand);
@@ -108,7 +109,7 @@ extern "C" int sg_search_noalloc(sg_index* h, const float* d_q768, const float* 
   const uint32_t P = p.nprobe < x.k ? p.nprobe : x.k;
   const uint32_t cand = p.cand > 0 ? p.cand : 1;
   const uint64_t items = x.h_chunks_desc_prefix[P];
-  const uint64_t cbuf = items * cand;
+  const uint64_t cbuf = (items * cand + 3) & ~3ull;
   Carve sizing{nullptr};
   sg::Workspace w;
   carve_workspace(sizing, w, x, P, cand, items, (uint32_t)cbuf, d_q256 == nullptr);

@@ -198,10 +198,8 @@ __global__ void __launch_bounds__(256) k_route_select(SelectArgs a) {
   bool exact = !a.bf16;
   if (a.bf16) {
     // the P-th largest BF16 score and the window below it
-    uint64_t kth = block_select_nth_u64(
-        [&](uint32_t i) { return ((uint64_t)ord(row[i]) << 32) | (0xFFFFFFFFu - i); }, K, P, hist,
-        tmp);
-    float sP = unord((uint32_t)(kth >> 32));
+    const uint32_t kth = block_select_nth_u32([&](uint32_t i) { return ord(row[i]); }, K, P, hist);
+    const float sP = unord(kth);
     float delta = 0.0085f * a.qnorm[q] * a.cent_norm_max;
     float lim = sP - 2.0f * delta;
     for (uint32_t c = threadIdx.x; c < K; c += blockDim.x)
@@ -283,10 +281,33 @@ __global__ void __launch_bounds__(256) k_route_select(SelectArgs a) {
   // probe list, admission offsets and chunk counts (block scans over probe ranks)
   uint32_t nloc = (m + blockDim.x - 1) / blockDim.x;  // probes per thread (contiguous)
   uint32_t r0 = threadIdx.x * nloc, r1 = min(m, r0 + nloc);
-  // Rank 0's first seed_blocks blocks form the query's seed item (scanned first, one CTA per
-  // query, to set a tight admission threshold); everything else is cut into chunks.
+  // The seed: the first probes, whole clusters while they fit in seed_blocks (at most kMaxSegs),
+  // or the first seed_blocks blocks of probe 0 when that cluster alone is larger. It is scanned
+  // first, one CTA per query, to set a tight admission threshold; everything else is cut into
+  // chunks (or, with alu_ranks off, left to the tensor-core scan).
+  __shared__ uint32_t s_rs, s_partial;
+  if (threadIdx.x == 0) {
+    uint32_t used = 0, rs = 0, partial = 0;
+    for (uint32_t r = 0; r < m && r < kMaxSegs; r++) {
+      const uint32_t c = key_id(keys[r]);
+      const uint32_t nb = a.block_off[c + 1] - a.block_off[c];
+      if (r == 0 && nb > a.seed_blocks) {
+        rs = 1;
+        partial = a.seed_blocks;
+        break;
+      }
+      if (used + nb > a.seed_blocks) break;
+      used += nb;
+      rs++;
+    }
+    s_rs = rs;
+    s_partial = partial;
+    a.seed_items[q] = make_uint4(q, rs, partial, 0);
+  }
+  __syncthreads();
+  const uint32_t rs = s_rs, partial = s_partial;
   auto nchunks = [&](uint32_t r, uint32_t nb) {
-    uint32_t rest = r == 0 ? (nb > a.seed_blocks ? nb - a.seed_blocks : 0) : (a.alu_ranks ? nb : 0);
+    uint32_t rest = r < rs ? (r == 0 && partial ? nb - partial : 0) : (a.alu_ranks ? nb : 0);
     return (rest + a.chunk_blocks - 1) / a.chunk_blocks;
   };
   uint32_t slots = 0, chunks = 0;
@@ -306,7 +327,6 @@ __global__ void __launch_bounds__(256) k_route_select(SelectArgs a) {
     s_base = base;
     a.probe_n[q] = m;
     a.scanned[q] = tot_slots;
-    if (m == 0) a.seed_items[q] = make_uint4(q, 0, 0, 0);
   }
   __syncthreads();
   uint64_t ibase = (uint64_t)s_base + coff;
@@ -317,10 +337,9 @@ __global__ void __launch_bounds__(256) k_route_select(SelectArgs a) {
     a.probe_off[(size_t)q * P + r] = soff;
     uint32_t b0 = a.block_off[c], b1 = a.block_off[c + 1];
     soff += (b1 - b0) * SG_BLOCK;
-    if (r == 0) {
-      uint32_t e = min(b1, b0 + a.seed_blocks);
-      a.seed_items[q] = make_uint4(q, 0, b0, e);
-      b0 = e;
+    if (r < rs) {
+      if (!(r == 0 && partial)) continue;
+      b0 += partial;  // probe 0's blocks past the seed
     } else if (!a.alu_ranks) {
       continue;
     }

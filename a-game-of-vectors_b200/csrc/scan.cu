@@ -38,7 +38,8 @@ struct ScanArgs {
   uint32_t* counters;
   uint32_t* thr;
   uint32_t* ccount;
-  uint4* cbuf;
+  uint32_t* cbuf_est;
+  uint2* cbuf_info;
   uint32_t cap;
   uint8_t* overflow;
   uint32_t cand;
@@ -78,29 +79,61 @@ SG_DEV void score_block_quarter(const uint8_t* __restrict__ block, const uint4* 
   }
 }
 
-// One CTA, one work item: score the item's blocks, then admit its best `cand` eligible slots.
-// Keys (ordered estimates, 0 = not eligible) live in dynamic shared memory, 4 B per slot.
-SG_DEV void scan_item(const ScanArgs& a, uint4 it, uint32_t* s_key, uint4* s_tab, uint32_t* hist,
-                      uint32_t* tmp, uint32_t* s_base) {
-  const int tid = threadIdx.x, t4 = tid & 3, lbw = tid >> 2;
-  const uint32_t q = it.x, r = it.y, b0 = it.z, nb = it.w - it.z;
-  if (nb == 0) return;  // uniform
+// Up to kMaxSegs (probe, block range) segments scored into one key array: a work item is one
+// segment; a seed is the query's first probes (whole clusters, or the first blocks of one).
+struct Segs {
+  uint32_t start[kMaxSegs + 1];  // first block (in the key array) of each segment; [n] = total
+  uint32_t b0[kMaxSegs];         // first block of the segment in the index
+  int32_t cl[kMaxSegs];          // eligible (non-PAD) slots counted from the segment's first slot
+  uint32_t kb[kMaxSegs];         // admission key of the segment's first slot
+  float cent[kMaxSegs];          // centroid score of the segment's probe
+  uint32_t n;
+};
+
+SG_DEV uint32_t seg_of(const Segs& S, uint32_t gb) {
+  uint32_t lo = 0, hi = S.n - 1;
+  while (lo < hi) {
+    const uint32_t mid = (lo + hi + 1) >> 1;
+    if (S.start[mid] <= gb) lo = mid;
+    else hi = mid - 1;
+  }
+  return lo;
+}
+
+// Fills segment `i` for probe r of query q, blocks [b0, b1) of its cluster, starting at key block
+// `start`.
+SG_DEV void set_seg(const ScanArgs& a, Segs& S, uint32_t i, uint32_t q, uint32_t r, uint32_t b0,
+                    uint32_t start) {
   const uint32_t c = a.probe_cl[(size_t)q * a.P + r];
-  const float cent = a.probe_sc[(size_t)q * a.P + r];
+  const uint32_t cb0 = a.block_off[c];
+  S.start[i] = start;
+  S.b0[i] = b0;
+  S.cl[i] = (int32_t)a.clen[c] - (int32_t)((b0 - cb0) * SG_BLOCK);
+  S.kb[i] = a.probe_off[(size_t)q * a.P + r] + (b0 - cb0) * SG_BLOCK;
+  S.cent[i] = a.probe_sc[(size_t)q * a.P + r];
+}
+
+// One CTA: score every segment's blocks, then admit the best `cand` eligible slots at or above
+// the query's threshold (est desc, then admission order) and raise the threshold to their
+// cand-th estimate. Keys (ordered estimates, 0 = not eligible) live in dynamic shared memory.
+SG_DEV void scan_segments(const ScanArgs& a, uint32_t q, const Segs& S, uint32_t* s_key,
+                          uint4* s_tab, uint32_t* hist, uint32_t* tmp, uint32_t* s_base) {
+  const int tid = threadIdx.x, t4 = tid & 3, lbw = tid >> 2;
+  const uint32_t NB = S.start[S.n];
+  if (NB == 0) return;  // uniform
   const float4 qp = a.qp[q];
   if (tid < SG_GROUPS)
     s_tab[tid] = reinterpret_cast<const uint4*>(a.tables + (size_t)q * SG_GROUPS * 16)[tid];
-  const uint32_t cb0 = a.block_off[c];
-  const uint32_t cl = a.clen[c];
-  const uint32_t loc0 = (b0 - cb0) * SG_BLOCK;  // slot index of the item's first slot
-  const uint32_t kbase = a.probe_off[(size_t)q * a.P + r] + loc0;
   __syncthreads();
   // ---- scoring: 64 blocks per pass, four threads per block ----------------------------------
-  for (uint32_t pb = 0; pb < nb; pb += 64) {
-    const uint32_t lb = pb + lbw;
+  for (uint32_t pb = 0; pb < NB; pb += 64) {
+    const uint32_t gb = pb + lbw;
     uint32_t acc[16];
-    if (lb < nb) {
-      score_block_quarter(a.blocks + (size_t)(b0 + lb) * SG_BLOCK_BYTES, s_tab, t4, acc);
+    uint32_t sg = 0, blk = 0;
+    if (gb < NB) {
+      sg = seg_of(S, gb);
+      blk = S.b0[sg] + (gb - S.start[sg]);
+      score_block_quarter(a.blocks + (size_t)blk * SG_BLOCK_BYTES, s_tab, t4, acc);
     } else {
 #pragma unroll
       for (int e = 0; e < 16; e++) acc[e] = 0;
@@ -110,7 +143,7 @@ SG_DEV void scan_item(const ScanArgs& a, uint4 it, uint32_t* s_key, uint4* s_tab
       acc[e] += __shfl_xor_sync(0xFFFFFFFFu, acc[e], 1);
       acc[e] += __shfl_xor_sync(0xFFFFFFFFu, acc[e], 2);
     }
-    if (lb < nb) {
+    if (gb < NB) {
       uint32_t x0 = acc[0], x1 = acc[1], x2 = acc[2], x3 = acc[3];
       if (t4 == 1) {
         x0 = acc[4]; x1 = acc[5]; x2 = acc[6]; x3 = acc[7];
@@ -119,33 +152,38 @@ SG_DEV void scan_item(const ScanArgs& a, uint4 it, uint32_t* s_key, uint4* s_tab
       } else if (t4 == 3) {
         x0 = acc[12]; x1 = acc[13]; x2 = acc[14]; x3 = acc[15];
       }
-      const float* mrow = a.mul + (size_t)(b0 + lb) * SG_BLOCK;
+      const float* mrow = a.mul + (size_t)blk * SG_BLOCK;
       const float4 mlo = __ldg(reinterpret_cast<const float4*>(mrow + 4 * t4));
       const float4 mhi = __ldg(reinterpret_cast<const float4*>(mrow + 16 + 4 * t4));
       const uint32_t sc[8] = {x0 & 0xFFFFu, x0 >> 16, x2 & 0xFFFFu, x2 >> 16,
                               x1 & 0xFFFFu, x1 >> 16, x3 & 0xFFFFu, x3 >> 16};
       const float mv[8] = {mlo.x, mlo.y, mlo.z, mlo.w, mhi.x, mhi.y, mhi.z, mhi.w};
+      const float cent = S.cent[sg];
+      const int32_t rel0 = (int32_t)((gb - S.start[sg]) * SG_BLOCK);
 #pragma unroll
       for (int d = 0; d < 8; d++) {
         const uint32_t doc = d < 4 ? 4 * t4 + d : 16 + 4 * t4 + (d - 4);
-        const uint32_t loc = lb * SG_BLOCK + doc;
         const float est =
             __fadd_rn(cent, __fmul_rn(mv[d], __fadd_rn(__fmul_rn(qp.z, (float)sc[d]), qp.w)));
-        s_key[loc] = (loc0 + loc < cl) ? ord(est) : 0u;
+        s_key[gb * SG_BLOCK + doc] = (rel0 + (int32_t)doc < S.cl[sg]) ? ord(est) : 0u;
       }
     }
   }
   __syncthreads();
   // ---- admission ------------------------------------------------------------------------------
   const uint32_t thr = ld_cg(a.thr + q);
-  const uint32_t nloc = nb * SG_BLOCK;
+  const uint32_t nloc = NB * SG_BLOCK;
   const uint32_t per = (nloc + blockDim.x - 1) / blockDim.x;  // <= 64 slots per thread
   const uint32_t i0 = tid * per, i1 = min(nloc, i0 + per);
+  auto slot_of = [&](uint32_t i) {
+    const uint32_t gb = i / SG_BLOCK, sg = seg_of(S, gb);
+    return (S.b0[sg] + gb - S.start[sg]) * SG_BLOCK + (i % SG_BLOCK);
+  };
   uint32_t cnt = 0;
   for (uint32_t i = i0; i < i1; i++) {
     const uint32_t k = s_key[i];
     bool surv = k != 0u && k >= thr;
-    if (surv && a.allow) surv = allowed(a.allow, a.allow_words, a.ids[(size_t)b0 * SG_BLOCK + i]);
+    if (surv && a.allow) surv = allowed(a.allow, a.allow_words, a.ids[slot_of(i)]);
     if (!surv) s_key[i] = 0u;
     cnt += surv;
   }
@@ -184,24 +222,47 @@ SG_DEV void scan_item(const ScanArgs& a, uint4 it, uint32_t* s_key, uint4* s_tab
   }
   __syncthreads();
   const uint32_t base = *s_base;
-  uint4* dst = a.cbuf + (size_t)q * a.cap;
+  const size_t qbase = (size_t)q * a.cap;
   for (uint32_t i = i0; i < i1; i++) {
     if (selmask & (1ull << (i - i0))) {
       const uint32_t pos = base + off++;
-      if (pos < a.cap)
-        dst[pos] = make_uint4(__float_as_uint(unord(s_key[i])), kbase + i, b0 * SG_BLOCK + i, 0u);
-      else
+      if (pos < a.cap) {
+        const uint32_t gb = i / SG_BLOCK, sg = seg_of(S, gb);
+        const uint32_t rel = (gb - S.start[sg]) * SG_BLOCK + (i % SG_BLOCK);
+        a.cbuf_est[qbase + pos] = __float_as_uint(unord(s_key[i]));
+        a.cbuf_info[qbase + pos] = make_uint2(S.kb[sg] + rel, S.b0[sg] * SG_BLOCK + rel);
+      } else {
         a.overflow[q] = 1;
+      }
     }
   }
 }
 
-// Seed pass: CTA q scans query q's seed item (the first blocks of its best cluster).
+// Seed pass: CTA q scores query q's seed — its first probes, whole clusters while they fit in
+// the seed's block budget (or the first blocks of probe 0 when that one cluster is larger) —
+// so that its threshold is the cand-th estimate over enough slots to bound the rest tightly.
+// seed_items[q] = (q, probes covered, blocks of probe 0 when partial else 0, -).
 __global__ void __launch_bounds__(256, 2) k_scan_seed(ScanArgs a) {
   extern __shared__ __align__(16) uint32_t s_key[];
   __shared__ uint4 s_tab[SG_GROUPS];
   __shared__ uint32_t hist[256], tmp[32], s_base;
-  scan_item(a, a.seed_items[blockIdx.x], s_key, s_tab, hist, tmp, &s_base);
+  __shared__ Segs S;
+  const uint4 it = a.seed_items[blockIdx.x];
+  const uint32_t q = it.x, rs = it.y, partial = it.z;
+  if (threadIdx.x == 0) {
+    S.n = rs;
+    uint32_t start = 0;
+    for (uint32_t r = 0; r < rs; r++) {
+      const uint32_t c = a.probe_cl[(size_t)q * a.P + r];
+      const uint32_t b0 = a.block_off[c];
+      const uint32_t nb = partial ? partial : a.block_off[c + 1] - b0;
+      set_seg(a, S, r, q, r, b0, start);
+      start += nb;
+    }
+    S.start[rs] = start;
+  }
+  __syncthreads();
+  scan_segments(a, q, S, s_key, s_tab, hist, tmp, &s_base);
 }
 
 // Main pass: a persistent grid drains the (query, probe, chunk) queue.
@@ -209,14 +270,23 @@ __global__ void __launch_bounds__(256, 2) k_scan(ScanArgs a) {
   extern __shared__ __align__(16) uint32_t s_key[];
   __shared__ uint4 s_tab[SG_GROUPS];
   __shared__ uint32_t hist[256], tmp[32], s_base, s_item;
+  __shared__ Segs S;
   uint32_t nitems = a.counters[0];
   if (nitems > a.item_cap) nitems = (uint32_t)a.item_cap;
   for (;;) {
-    if (threadIdx.x == 0) s_item = atomicAdd(&a.counters[1], 1u);
+    if (threadIdx.x == 0) {
+      s_item = atomicAdd(&a.counters[1], 1u);
+      if (s_item < nitems) {
+        const uint4 it = a.items[s_item];
+        S.n = 1;
+        set_seg(a, S, 0, it.x, it.y, it.z, 0);
+        S.start[1] = it.w - it.z;
+      }
+    }
     __syncthreads();
     const uint32_t item = s_item;
     if (item >= nitems) break;
-    scan_item(a, a.items[item], s_key, s_tab, hist, tmp, &s_base);
+    scan_segments(a, a.items[item].x, S, s_key, s_tab, hist, tmp, &s_base);
     __syncthreads();
   }
 }
@@ -242,7 +312,8 @@ void launch_scan(const DevIndex& ix, Workspace& w, uint32_t nq, const sg_params&
   a.counters = w.counters;
   a.thr = w.thr;
   a.ccount = w.ccount;
-  a.cbuf = w.cbuf;
+  a.cbuf_est = w.cbuf_est;
+  a.cbuf_info = w.cbuf_info;
   a.cap = w.cbuf_per_q;
   a.overflow = w.overflow;
   a.cand = p.cand;
@@ -256,8 +327,8 @@ void launch_scan(const DevIndex& ix, Workspace& w, uint32_t nq, const sg_params&
                          (int)(kMaxChunkBlocks * SG_BLOCK * 4));
     attr = true;
   }
-  k_scan_seed<<<nq, 256, seed_blocks * SG_BLOCK * 4, st>>>(a);
-  k_scan<<<sms * ctas_per_sm, 256, chunk_blocks * SG_BLOCK * 4, st>>>(a);
+  if (seed_blocks) k_scan_seed<<<nq, 256, seed_blocks * SG_BLOCK * 4, st>>>(a);
+  if (chunk_blocks) k_scan<<<sms * ctas_per_sm, 256, chunk_blocks * SG_BLOCK * 4, st>>>(a);
 }
 
 // ---- stateless kernels for the parity tests ---------------------------------------------------

@@ -16,7 +16,8 @@
 // mma.sync.m16n8k32 u8 over 32 k-steps for 2 m-tiles x up to 8 n-tiles. The epilogue forms
 // est = cent + mul*(a*score + b) exactly as the ALU scan does and appends every eligible slot
 // at or above the query's threshold (set by the seed pass) to the query's candidate buffer.
-// Probe rank 0 is the seed pass's (scan.cu), so every (query, probe) pair is scanned once.
+// The probes the seed pass covered (scan.cu) are left out, so every (query, probe) pair is
+// scanned once.
 #include "common.cuh"
 #include "internal.hpp"
 
@@ -48,12 +49,14 @@ int transcode_mma(const uint8_t* blocks, uint64_t nblocks, uint32_t* out) {
 }
 
 // ---- inversion of the probe lists ----------------------------------------------------------
+// Probes the seed covered (seed_items[q].y) are not scanned again.
 __global__ void k_inv_count(const uint32_t* __restrict__ probe_cl, const uint32_t* __restrict__ probe_n,
-                            uint32_t P, uint32_t nq, uint32_t* __restrict__ cnt) {
+                            const uint4* __restrict__ seed, uint32_t P, uint32_t nq,
+                            uint32_t* __restrict__ cnt) {
   const uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= (uint64_t)nq * P) return;
   const uint32_t q = (uint32_t)(t / P), r = (uint32_t)(t % P);
-  if (r == 0 || r >= probe_n[q]) return;
+  if (r < seed[q].y || r >= probe_n[q]) return;
   atomicAdd(cnt + probe_cl[t], 1u);
 }
 
@@ -88,12 +91,13 @@ __global__ void __launch_bounds__(1024) k_inv_scan(const uint32_t* __restrict__ 
 }
 
 __global__ void k_inv_fill(const uint32_t* __restrict__ probe_cl, const uint32_t* __restrict__ probe_n,
-                           uint32_t P, uint32_t nq, const uint32_t* __restrict__ off,
-                           uint32_t* __restrict__ fill, uint32_t* __restrict__ list) {
+                           const uint4* __restrict__ seed, uint32_t P, uint32_t nq,
+                           const uint32_t* __restrict__ off, uint32_t* __restrict__ fill,
+                           uint32_t* __restrict__ list) {
   const uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= (uint64_t)nq * P) return;
   const uint32_t q = (uint32_t)(t / P), r = (uint32_t)(t % P);
-  if (r == 0 || r >= probe_n[q]) return;
+  if (r < seed[q].y || r >= probe_n[q]) return;
   const uint32_t c = probe_cl[t];
   list[off[c] + atomicAdd(fill + c, 1u)] = (q << 12) | r;
 }
@@ -145,7 +149,8 @@ struct MmaArgs {
   uint32_t* counters;
   uint32_t* thr;
   uint32_t* ccount;
-  uint4* cbuf;
+  uint32_t* cbuf_est;
+  uint2* cbuf_info;
   uint32_t cap;
   uint8_t* overflow;
   const uint64_t* allow;
@@ -294,11 +299,12 @@ __global__ void __launch_bounds__(256, 2) k_scan_mma(MmaArgs a) {
                 if (!a.allow || allowed(a.allow, a.allow_words, a.ids[gslot])) {
                   const uint32_t q = s_q[qi];
                   const uint32_t pos = atomicAdd(a.ccount + q, 1u);
-                  if (pos < a.cap)
-                    a.cbuf[(size_t)q * a.cap + pos] =
-                        make_uint4(__float_as_uint(est), s_kb[qi] + loc + slot, gslot, 0u);
-                  else
+                  if (pos < a.cap) {
+                    a.cbuf_est[(size_t)q * a.cap + pos] = __float_as_uint(est);
+                    a.cbuf_info[(size_t)q * a.cap + pos] = make_uint2(s_kb[qi] + loc + slot, gslot);
+                  } else {
                     a.overflow[q] = 1;
+                  }
                 }
               }
             }
@@ -316,9 +322,10 @@ int launch_scan_mma(const DevIndex& ix, Workspace& w, uint32_t nq, const sg_para
   cudaMemsetAsync(w.inv_cnt, 0, (size_t)ix.k * 4, st);
   cudaMemsetAsync(w.inv_fill, 0, (size_t)ix.k * 4, st);
   const unsigned grid = (unsigned)((pairs + 255) / 256);
-  k_inv_count<<<grid, 256, 0, st>>>(w.probe_cl, w.probe_n, P, nq, w.inv_cnt);
+  k_inv_count<<<grid, 256, 0, st>>>(w.probe_cl, w.probe_n, w.seed_items, P, nq, w.inv_cnt);
   k_inv_scan<<<1, 1024, 0, st>>>(w.inv_cnt, ix.k, w.inv_off, w.gitems, w.gitems_cap, w.counters);
-  k_inv_fill<<<grid, 256, 0, st>>>(w.probe_cl, w.probe_n, P, nq, w.inv_off, w.inv_fill, w.inv_list);
+  k_inv_fill<<<grid, 256, 0, st>>>(w.probe_cl, w.probe_n, w.seed_items, P, nq, w.inv_off, w.inv_fill,
+                                   w.inv_list);
   MmaArgs a;
   a.bmma = ix.blocks_mma;
   a.mul = ix.mul;
@@ -336,7 +343,8 @@ int launch_scan_mma(const DevIndex& ix, Workspace& w, uint32_t nq, const sg_para
   a.counters = w.counters;
   a.thr = w.thr;
   a.ccount = w.ccount;
-  a.cbuf = w.cbuf;
+  a.cbuf_est = w.cbuf_est;
+  a.cbuf_info = w.cbuf_info;
   a.cap = w.cbuf_per_q;
   a.overflow = w.overflow;
   a.allow = allow;

@@ -126,7 +126,8 @@ void free_ws(sg::Workspace& w) {
   dfree(w.gitems);
   dfree(w.thr);
   dfree(w.ccount);
-  dfree(w.cbuf);
+  dfree(w.cbuf_est);
+  dfree(w.cbuf_info);
   dfree(w.overflow);
   dfree(w.cest);
   dfree(w.cid);
@@ -271,6 +272,7 @@ int build_index(const sg_ivf_arrays* a, int device, sg_index** out) {
 // Sizes the workspace for nq queries under params p (grows, never shrinks).
 int ensure_ws(sg_index* h, uint32_t nq, const sg_params& p, uint32_t cbuf_per_q) {
   sg::Workspace& w = h->ws;
+  cbuf_per_q = (cbuf_per_q + 3) & ~3u;
   const sg::DevIndex& x = h->ix;
   const uint32_t P = std::min<uint32_t>(p.nprobe, x.k);
   const uint32_t cand = std::max<uint32_t>(p.cand, 1);
@@ -350,8 +352,9 @@ int ensure_ws(sg_index* h, uint32_t nq, const sg_params& p, uint32_t cbuf_per_q)
   }
   const uint64_t cb = (uint64_t)nq * cbuf_per_q;
   if (cb > w.cbuf_cap) {
-    dfree(w.cbuf);
-    if ((rc = dalloc(&w.cbuf, cb))) return rc;
+    dfree(w.cbuf_est);
+    dfree(w.cbuf_info);
+    if ((rc = dalloc(&w.cbuf_est, cb)) || (rc = dalloc(&w.cbuf_info, cb))) return rc;
     w.cbuf_cap = cb;
   }
   w.cbuf_per_q = cbuf_per_q;
@@ -435,13 +438,16 @@ int run_pipeline(sg_index* h, uint32_t nq, const sg_params& p, bool have_q256,
   if (timed) CK(cudaEventRecord(w.ev[3], st));
   launches += 3;
   if (p.cand > 0) {
-    sg::launch_scan(x, w, nq, p, d_allow, allow_words, h->sms, cb, h->cfg.seed_blocks,
+    sg::launch_scan(x, w, nq, p, d_allow, allow_words, h->sms, 0, h->cfg.seed_blocks,
                     h->cfg.scan_ctas_per_sm, st);
+    if (timed) CK(cudaEventRecord(w.ev[9], st));
+    sg::launch_scan(x, w, nq, p, d_allow, allow_words, h->sms, cb, 0, h->cfg.scan_ctas_per_sm, st);
     if (mma) launches += sg::launch_scan_mma(x, w, nq, p, d_allow, allow_words, h->sms, st);
     if (timed) CK(cudaEventRecord(w.ev[4], st));
     sg::launch_cut(x, w, nq, p, st);
     launches += 3;
   } else {
+    if (timed) CK(cudaEventRecord(w.ev[9], st));
     if (timed) CK(cudaEventRecord(w.ev[4], st));
     CK(cudaMemsetAsync(w.cn, 0, nq * sizeof(uint32_t), st));
   }
@@ -463,6 +469,7 @@ void collect_stats(sg::Workspace& w, const sg_params& p) {
   for (int i = 0; i < 6; i++) cudaEventElapsedTime(ms[i], w.ev[i], w.ev[i + 1]);
   cudaEventElapsedTime(&w.last.ms_total, w.ev[0], w.ev[6]);
   if (p.rerank_kind == SG_RERANK_TIERED) cudaEventElapsedTime(&w.last.ms_tier2, w.ev[7], w.ev[8]);
+  if (p.cand > 0) cudaEventElapsedTime(&w.last.ms_seed, w.ev[3], w.ev[9]);
 }
 
 int stage_inputs(sg_index* h, uint32_t nq, const float* q768, const float* q256, bool device) {
@@ -837,6 +844,26 @@ int sg_candidates(sg_index* h, uint32_t nq, const float* q256, const sg_params* 
     CK(cudaMemcpyAsync(&o, w.overflow, 1, cudaMemcpyDeviceToHost, h->stream));
     CK(cudaStreamSynchronize(h->stream));
     if (o) return fail(SG_ERR_INVALID, "candidate buffer overflow at the exact bound");
+    // the device list is unordered; Index::candidates returns it in row order
+    if (p.cand) {
+      const uint32_t n = out_counts[q0];
+      float* e = out_est + (size_t)q0 * c;
+      uint32_t* id = out_ids + (size_t)q0 * c;
+      float* er = out_err + (size_t)q0 * c;
+      std::vector<uint32_t> ord(n);
+      for (uint32_t i = 0; i < n; i++) ord[i] = i;
+      std::sort(ord.begin(), ord.end(), [&](uint32_t x, uint32_t y) { return id[x] < id[y]; });
+      std::vector<float> e2(n), er2(n);
+      std::vector<uint32_t> id2(n);
+      for (uint32_t i = 0; i < n; i++) {
+        e2[i] = e[ord[i]];
+        id2[i] = id[ord[i]];
+        er2[i] = er[ord[i]];
+      }
+      std::copy(e2.begin(), e2.end(), e);
+      std::copy(id2.begin(), id2.end(), id);
+      std::copy(er2.begin(), er2.end(), er);
+    }
   }
   return SG_OK;
 }

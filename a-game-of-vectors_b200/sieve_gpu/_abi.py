@@ -67,7 +67,7 @@ class SgStats(ctypes.Structure):
     _fields_ = [(n, c_float) for n in ("ms_prep", "ms_route_gemm", "ms_route_select", "ms_scan",
                                         "ms_cut", "ms_rerank", "ms_tier2", "ms_total")] + [
         ("launches", c_uint32), ("reserved", c_uint32), ("scanned", c_uint64), ("probed", c_uint64),
-        ("reranked", c_uint64), ("buffered", c_uint64)]
+        ("reranked", c_uint64), ("buffered", c_uint64), ("ms_seed", c_float), ("reserved2", c_uint32)]
 
 
 class SgIvfArrays(ctypes.Structure):

@@ -186,7 +186,7 @@ class Index:
     def last_stats(self) -> dict:
         st = SgStats()
         check(lib().sg_last_stats(self._h, byref(st)))
-        return {name: getattr(st, name) for name, _ in SgStats._fields_ if name != "reserved"}
+        return {name: getattr(st, name) for name, _ in SgStats._fields_ if not name.startswith("reserved")}
 
     def set_route_precision(self, bf16: bool) -> None:
         check(lib().sg_set_route_precision(self._h, c_int(_abi.ROUTE_BF16 if bf16 else _abi.ROUTE_FP32)))

@@ -35,7 +35,7 @@ import torch  # noqa: E402
 
 WORKLOADS = {
     "c1": dict(n=1_000_000, centers=1024, k=1024, queries=10_000, search="32:1000:full"),
-    "c2": dict(n=18_400_000, centers=16384, k=4096, queries=50_000, search="64:2000:full"),
+    "c2": dict(n=18_400_000, centers=16384, k=4096, queries=50_000, search="32:2000:full"),
     "c3": dict(n=113_500_000, centers=65536, k=16384, queries=100_000, search="64:1000:full"),
 }
 SCAN_BYTES_PER_SLOT = 40  # 32 B code + 8 B [mul, err] factors per scanned slot

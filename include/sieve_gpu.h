@@ -107,6 +107,8 @@ typedef struct {
   uint64_t probed;        /* clusters probed, summed over queries                                 */
   uint64_t reranked;      /* candidates reaching the rerank stage, summed over queries            */
   uint64_t buffered;      /* scan entries appended to the candidate buffers, summed over queries  */
+  float ms_seed;          /* part of ms_scan in the seed pass (each query's best cluster)         */
+  uint32_t reserved2;
 } sg_stats;
 
 typedef struct sg_index sg_index;

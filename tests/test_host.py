@@ -38,7 +38,7 @@ def test_library_reports_errors_without_aborting():
 def test_abi_struct_layouts():
     assert ctypes_size(_abi.SgParams) == 56
     assert ctypes_size(_abi.SgTiming) == 72
-    assert ctypes_size(_abi.SgStats) == 8 * 4 + 8 + 4 * 8
+    assert ctypes_size(_abi.SgStats) == 8 * 4 + 8 + 4 * 8 + 8
     assert ctypes_size(_abi.SgIvfArrays) == 8 + 8 + 12 * 8
 
 
