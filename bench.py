@@ -60,7 +60,7 @@ class ClockSampler:
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.FIELDS}",
-                 "--format=csv,noheader,nounits", "-lms", "200"],
+                 "--format=csv,noheader,nounits", "-lms", "100"],
                 stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.t = threading.Thread(target=self._read, daemon=True)
             self.t.start()
@@ -194,7 +194,7 @@ def cpu_reference(arrays, q768_host: np.ndarray, params, seconds: float, threads
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--steps", type=int, default=50)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="c2", choices=sorted(WORKLOADS))
@@ -311,7 +311,8 @@ def main():
     if os.path.exists(tpath):
         with open(tpath) as f:
             t = json.load(f)
-        if t.get("workload") == args.workload and t.get("config") == config:
+        if (t.get("workload") == args.workload and t.get("config") == config
+                and t.get("batch") == args.batch and not args.rows):
             traffic = float(t["dram_bytes_per_slot"]) * float(np.mean(scanned))
     stage = {k: round(float(np.mean([s[k] for s in stats])), 4)
              for k in ("ms_prep", "ms_route_gemm", "ms_route_select", "ms_scan", "ms_cut", "ms_rerank",
@@ -366,7 +367,8 @@ def main():
                   "p99_ms": float(np.percentile(plain_ms, 99)), "queries": int(plain_ms.size)},
         "stage_ms": stage,
         "scanned_per_query": float(np.mean(scanned) / B),
-        "roofline": {"bound": "hbm", "kernel": "k_scan", "achieved": achieved, "peak": peak,
+        "roofline": {"bound": "hbm", "kernel": "k_scan_seed + k_scan_mma (the scan stage)",
+                     "achieved": achieved, "peak": peak,
                      "unit": "GB/s", "frac": achieved / peak,
                      "peak_source": "MEASURED_PEAKS.json hbm_gbs" if "hbm_gbs" in peaks else "fallback",
                      "traffic": traffic, "bytes_per_slot": SCAN_BYTES_PER_SLOT},
