@@ -5,6 +5,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <string.h>
+
 #include <mutex>
 #include <string>
 #include <vector>
@@ -21,6 +23,8 @@ constexpr uint32_t kSeedBlocks = 512;    // block budget of each query's seed (i
 constexpr uint32_t kMaxSegs = 64;        // probes one seed can cover
 // Largest cand / k / r the select kernels sort in shared memory.
 constexpr uint32_t kMaxCand = 4096;
+// Most clusters the filter plan Expand sorts per query in shared memory (128 KB of keys).
+constexpr uint32_t kExpandMaxK = 16384;
 // Status bits a kernel raises in Workspace::status.
 constexpr uint32_t kStatusOverflow = 1u;   // a candidate buffer filled up (query is retried)
 constexpr uint32_t kStatusWindow = 2u;     // a BF16 routing window exceeded its buffer
@@ -104,6 +108,8 @@ struct Workspace {
   uint32_t* out_n = nullptr;
   uint64_t* allow = nullptr;     // [allow_words]
   uint64_t allow_cap = 0;
+  float* brute = nullptr;        // [brute_cap] exact scores of the filter plan Brute
+  uint64_t brute_cap = 0;
   void* host_pinned = nullptr;   // pinned staging for host<->device copies
   size_t host_pinned_cap = 0;
   cudaEvent_t ev[12] = {};
@@ -111,13 +117,47 @@ struct Workspace {
   sg_stats last = {};
 };
 
+// One execution context of an index: a workspace, the stream its work runs on, and the CUDA
+// graphs captured for the call shapes it has seen. sg_search uses the index's default context;
+// the serving loop runs several so that batches overlap on the device.
+struct GraphKey {
+  uint32_t nq;
+  sg_params p;
+  bool have_q256;
+  const uint64_t* allow;
+  uint64_t allow_words;
+  uint64_t gen;
+  bool same(const GraphKey& o) const {
+    return nq == o.nq && have_q256 == o.have_q256 && allow == o.allow &&
+           allow_words == o.allow_words && gen == o.gen &&
+           memcmp(&p, &o.p, sizeof(sg_params)) == 0;
+  }
+};
+
+// A pipeline captured as a CUDA graph for one call shape (exec is null until the shape has been
+// seen twice) and the launches it replays.
+struct GraphEntry {
+  GraphKey key;
+  cudaGraphExec_t exec;
+  uint32_t launches;
+};
+
+struct Ctx {
+  Workspace ws;
+  cudaStream_t stream = nullptr;
+  uint64_t gen = 1;  // bumped whenever a workspace buffer moves (captured graphs go stale)
+  std::vector<GraphEntry> graphs;
+};
+
 struct Config {
   uint32_t chunk_blocks = kChunkBlocks;  // batched scan chunk (autotuned)
   uint32_t small_chunk_blocks = 64;      // chunk when few queries share the GPU
   uint32_t small_batch = 64;             // below this many queries use the small chunk
   uint32_t seed_blocks = kSeedBlocks;
+  uint32_t small_seed_blocks = 256;      // seed budget below small_batch queries
   uint32_t scan_ctas_per_sm = 2;
   uint32_t soft_cap = 0;  // per-query buffer override (0: automatic); SIEVE_GPU_SOFT_CAP
+  int graphs = 1;         // capture and replay CUDA graphs per call shape (SIEVE_GPU_GRAPHS)
   uint32_t mma_min_queries_per_cluster = 8;   // use the MMA scan at or above this average
   int mma = 1;            // SIEVE_GPU_MMA: 0 ALU scan only, 1 automatic, 2 MMA whenever nprobe > 1
 };
@@ -138,6 +178,16 @@ void launch_route_scores(const DevIndex& ix, Workspace& w, uint32_t nq, int prec
                          cudaStream_t st);
 // alu_ranks = false leaves probe ranks >= 1 to the MMA scan (only rank-0 chunks past the seed
 // become ALU work items).
+inline uint32_t next_pow2_host(uint32_t x) {
+  uint32_t p = 1;
+  while (p < x) p <<= 1;
+  return p;
+}
+// filter::search Plan::Expand routing: needs exact f32 scores (launch_route_scores FP32) and a
+// probe-array stride of k.
+void launch_route_expand(const DevIndex& ix, Workspace& w, uint32_t nq, const sg_params& p,
+                         uint32_t chunk_blocks, uint32_t seed_blocks,
+                         const uint32_t* per_cluster, uint64_t target, cudaStream_t st);
 void launch_route_select(const DevIndex& ix, Workspace& w, uint32_t nq, const sg_params& p,
                          int precision, uint32_t chunk_blocks, uint32_t seed_blocks,
                          bool alu_ranks, cudaStream_t st);
@@ -157,6 +207,18 @@ int launch_rerank(const DevIndex& ix, Workspace& w, uint32_t nq, const sg_params
                   cudaStream_t st, cudaEvent_t ev_t2_begin, cudaEvent_t ev_t2_end);
 void launch_lut_scan(uint32_t groups, const uint8_t* tables, const uint8_t* blocks,
                      uint64_t nblocks, uint16_t* out, cudaStream_t st);
+// Filter::new on the device: allowed rows ascending (nrows of them) and allowed slots per cluster.
+int filter_build(const DevIndex& ix, const uint64_t* allow, uint64_t words, uint32_t** rows,
+                 uint64_t* nrows, uint32_t* per_cluster, cudaStream_t st);
+// filter::search Plan::Brute for queries [q0, q0+nq) prepared in w: exact int8 scores of the
+// `nrows` allowed rows, then the top k by (score desc, row asc) into w.out_*. `scores` holds
+// nq x nrows floats.
+int launch_brute(const DevIndex& ix, Workspace& w, uint32_t nq, const uint32_t* rows,
+                 uint32_t nrows, uint32_t k, float* scores, cudaStream_t st);
+// Top n of per-query scored lists by (score desc, id asc), sorted.
+void launch_top_list(const float* sc, const uint32_t* id, const uint32_t* n_in, uint64_t sc_stride,
+                     uint64_t id_stride, uint32_t nsel, float* out_sc, uint32_t* out_id,
+                     uint32_t* n_out, uint32_t stride_out, uint32_t nq, cudaStream_t st);
 void launch_dot_i8i8(const int8_t* q, const int8_t* rows, uint64_t nrows, uint32_t dim,
                      int32_t* out, cudaStream_t st);
 

@@ -161,7 +161,8 @@ __global__ void __launch_bounds__(256) k_tier2_list(const float* __restrict__ q2
 __global__ void __launch_bounds__(1024) k_top_list(const float* __restrict__ sc,
                                                    const uint32_t* __restrict__ id,
                                                    const uint32_t* __restrict__ n_in,
-                                                   uint32_t stride_in, uint32_t nsel,
+                                                   uint64_t stride_in, uint64_t id_stride,
+                                                   uint32_t nsel,
                                                    float* __restrict__ out_sc,
                                                    uint32_t* __restrict__ out_id,
                                                    uint32_t* __restrict__ n_out,
@@ -171,7 +172,7 @@ __global__ void __launch_bounds__(1024) k_top_list(const float* __restrict__ sc,
   __shared__ uint32_t hist[256], tmp[32], s_n;
   const uint32_t q = blockIdx.x, M = n_in[q];
   const float* S = sc + (size_t)q * stride_in;
-  const uint32_t* I = id + (size_t)q * stride_in;
+  const uint32_t* I = id + (size_t)q * id_stride;
   uint64_t T = 0;
   const bool cut = M > nsel;
   if (cut && nsel > 0) {
@@ -197,17 +198,24 @@ __global__ void __launch_bounds__(1024) k_top_list(const float* __restrict__ sc,
   if (threadIdx.x == 0) n_out[q] = n;
 }
 
-static void top_list(const float* sc, const uint32_t* id, const uint32_t* n_in, uint32_t stride_in,
-                     uint32_t nsel, float* out_sc, uint32_t* out_id, uint32_t* n_out,
-                     uint32_t stride_out, uint32_t nq, cudaStream_t st) {
+void launch_top_list(const float* sc, const uint32_t* id, const uint32_t* n_in, uint64_t sc_stride,
+                     uint64_t id_stride, uint32_t nsel, float* out_sc, uint32_t* out_id,
+                     uint32_t* n_out, uint32_t stride_out, uint32_t nq, cudaStream_t st) {
   static bool attr = false;
   size_t smem = (size_t)kMaxCand * 8;
   if (!attr) {
     cudaFuncSetAttribute(k_top_list, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     attr = true;
   }
-  k_top_list<<<nq, 1024, smem, st>>>(sc, id, n_in, stride_in, nsel, out_sc, out_id, n_out,
-                                     stride_out);
+  k_top_list<<<nq, 1024, smem, st>>>(sc, id, n_in, sc_stride, id_stride, nsel, out_sc, out_id,
+                                     n_out, stride_out);
+}
+
+static void top_list(const float* sc, const uint32_t* id, const uint32_t* n_in, uint32_t stride_in,
+                     uint32_t nsel, float* out_sc, uint32_t* out_id, uint32_t* n_out,
+                     uint32_t stride_out, uint32_t nq, cudaStream_t st) {
+  launch_top_list(sc, id, n_in, stride_in, stride_in, nsel, out_sc, out_id, n_out, stride_out, nq,
+                  st);
 }
 
 static void dot_list(const DevIndex& ix, Workspace& w, uint32_t nq, uint32_t stride, bool prefix,

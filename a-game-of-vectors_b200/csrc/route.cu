@@ -177,6 +177,84 @@ struct SelectArgs {
   uint32_t* counters;
 };
 
+// Writes query q's probe list (keys[0..m) sorted best first: probe ranks 0..m-1), the admission
+// offset of each probe's first slot, its seed descriptor and its ALU scan items. All threads of
+// the block call it.
+SG_DEV void emit_probes(const SelectArgs& a, const uint64_t* keys, uint32_t m, uint32_t q,
+                        uint32_t* tmp) {
+  const uint32_t P = a.P;
+  // probe list, admission offsets and chunk counts (block scans over probe ranks)
+  uint32_t nloc = (m + blockDim.x - 1) / blockDim.x;  // probes per thread (contiguous)
+  uint32_t r0 = threadIdx.x * nloc, r1 = min(m, r0 + nloc);
+  // The seed: the first probes, whole clusters while they fit in seed_blocks (at most kMaxSegs),
+  // or the first seed_blocks blocks of probe 0 when that cluster alone is larger. It is scanned
+  // first, one CTA per query, to set a tight admission threshold; everything else is cut into
+  // chunks (or, with alu_ranks off, left to the tensor-core scan).
+  __shared__ uint32_t s_rs, s_partial;
+  if (threadIdx.x == 0) {
+    uint32_t used = 0, rs = 0, partial = 0;
+    for (uint32_t r = 0; r < m && r < kMaxSegs; r++) {
+      const uint32_t c = key_id(keys[r]);
+      const uint32_t nb = a.block_off[c + 1] - a.block_off[c];
+      if (r == 0 && nb > a.seed_blocks) {
+        rs = 1;
+        partial = a.seed_blocks;
+        break;
+      }
+      if (used + nb > a.seed_blocks) break;
+      used += nb;
+      rs++;
+    }
+    s_rs = rs;
+    s_partial = partial;
+    a.seed_items[q] = make_uint4(q, rs, partial, 0);
+  }
+  __syncthreads();
+  const uint32_t rs = s_rs, partial = s_partial;
+  auto nchunks = [&](uint32_t r, uint32_t nb) {
+    uint32_t rest = r < rs ? (r == 0 && partial ? nb - partial : 0) : (a.alu_ranks ? nb : 0);
+    return (rest + a.chunk_blocks - 1) / a.chunk_blocks;
+  };
+  uint32_t slots = 0, chunks = 0;
+  for (uint32_t r = r0; r < r1; r++) {
+    uint32_t c = key_id(keys[r]);
+    uint32_t nb = a.block_off[c + 1] - a.block_off[c];
+    slots += nb * SG_BLOCK;
+    chunks += nchunks(r, nb);
+  }
+  uint32_t tot_slots, tot_chunks;
+  uint32_t soff = block_exclusive_scan(slots, tmp, &tot_slots);
+  uint32_t coff = block_exclusive_scan(chunks, tmp, &tot_chunks);
+  __shared__ uint32_t s_base;
+  if (threadIdx.x == 0) {
+    uint32_t base = atomicAdd(&a.counters[0], tot_chunks);
+    if ((uint64_t)base + tot_chunks > a.item_cap) atomicOr(&a.counters[2], kStatusOverflow);
+    s_base = base;
+    a.probe_n[q] = m;
+    a.scanned[q] = tot_slots;
+  }
+  __syncthreads();
+  uint64_t ibase = (uint64_t)s_base + coff;
+  for (uint32_t r = r0; r < r1; r++) {
+    uint32_t c = key_id(keys[r]);
+    a.probe_cl[(size_t)q * P + r] = c;
+    a.probe_sc[(size_t)q * P + r] = key_score(keys[r]);
+    a.probe_off[(size_t)q * P + r] = soff;
+    uint32_t b0 = a.block_off[c], b1 = a.block_off[c + 1];
+    soff += (b1 - b0) * SG_BLOCK;
+    if (r < rs) {
+      if (!(r == 0 && partial)) continue;
+      b0 += partial;  // probe 0's blocks past the seed
+    } else if (!a.alu_ranks) {
+      continue;
+    }
+    for (uint32_t b = b0; b < b1; b += a.chunk_blocks) {
+      if (ibase < a.item_cap) a.items[ibase] = make_uint4(q, r, b, min(b1, b + a.chunk_blocks));
+      ibase++;
+    }
+  }
+}
+
 __global__ void __launch_bounds__(256) k_route_select(SelectArgs a) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   uint64_t* keys = reinterpret_cast<uint64_t*>(smem_raw);  // [kWinCap]
@@ -192,6 +270,7 @@ __global__ void __launch_bounds__(256) k_route_select(SelectArgs a) {
     if (threadIdx.x == 0) {
       a.probe_n[q] = 0;
       a.scanned[q] = 0;
+      a.seed_items[q] = make_uint4(q, 0, 0, 0);
     }
     return;
   }
@@ -277,77 +356,47 @@ __global__ void __launch_bounds__(256) k_route_select(SelectArgs a) {
     s_keep = m;
   }
   __syncthreads();
-  const uint32_t m = s_keep;
-  // probe list, admission offsets and chunk counts (block scans over probe ranks)
-  uint32_t nloc = (m + blockDim.x - 1) / blockDim.x;  // probes per thread (contiguous)
-  uint32_t r0 = threadIdx.x * nloc, r1 = min(m, r0 + nloc);
-  // The seed: the first probes, whole clusters while they fit in seed_blocks (at most kMaxSegs),
-  // or the first seed_blocks blocks of probe 0 when that cluster alone is larger. It is scanned
-  // first, one CTA per query, to set a tight admission threshold; everything else is cut into
-  // chunks (or, with alu_ranks off, left to the tensor-core scan).
-  __shared__ uint32_t s_rs, s_partial;
-  if (threadIdx.x == 0) {
-    uint32_t used = 0, rs = 0, partial = 0;
-    for (uint32_t r = 0; r < m && r < kMaxSegs; r++) {
-      const uint32_t c = key_id(keys[r]);
-      const uint32_t nb = a.block_off[c + 1] - a.block_off[c];
-      if (r == 0 && nb > a.seed_blocks) {
-        rs = 1;
-        partial = a.seed_blocks;
-        break;
-      }
-      if (used + nb > a.seed_blocks) break;
-      used += nb;
-      rs++;
-    }
-    s_rs = rs;
-    s_partial = partial;
-    a.seed_items[q] = make_uint4(q, rs, partial, 0);
-  }
+  emit_probes(a, keys, s_keep, q, tmp);
+}
+
+// filter::search with Plan::Expand (src/filter.rs:79-93): every cluster in route order (exact f32
+// scores, score desc then cluster asc: the TopK(k) of Index::route with no margin or budget),
+// clusters without allowed slots dropped, kept while the allowed slots covered by the clusters
+// before it stay below the target (so the cluster that crosses the target is kept). One CTA per
+// query sorts the K keys in shared memory (K <= kExpandMaxK).
+__global__ void __launch_bounds__(1024) k_route_expand(SelectArgs a,
+                                                       const uint32_t* __restrict__ per_cluster,
+                                                       uint64_t target) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  uint64_t* keys = reinterpret_cast<uint64_t*>(smem_raw);  // [next_pow2(K)]
+  __shared__ uint32_t tmp[32], s_n;
+  const uint32_t q = blockIdx.x, K = a.K;
+  const float* row = a.scores + (size_t)q * K;
+  if (threadIdx.x == 0) s_n = 0;
   __syncthreads();
-  const uint32_t rs = s_rs, partial = s_partial;
-  auto nchunks = [&](uint32_t r, uint32_t nb) {
-    uint32_t rest = r < rs ? (r == 0 && partial ? nb - partial : 0) : (a.alu_ranks ? nb : 0);
-    return (rest + a.chunk_blocks - 1) / a.chunk_blocks;
-  };
-  uint32_t slots = 0, chunks = 0;
-  for (uint32_t r = r0; r < r1; r++) {
-    uint32_t c = key_id(keys[r]);
-    uint32_t nb = a.block_off[c + 1] - a.block_off[c];
-    slots += nb * SG_BLOCK;
-    chunks += nchunks(r, nb);
-  }
-  uint32_t tot_slots, tot_chunks;
-  uint32_t soff = block_exclusive_scan(slots, tmp, &tot_slots);
-  uint32_t coff = block_exclusive_scan(chunks, tmp, &tot_chunks);
-  __shared__ uint32_t s_base;
-  if (threadIdx.x == 0) {
-    uint32_t base = atomicAdd(&a.counters[0], tot_chunks);
-    if ((uint64_t)base + tot_chunks > a.item_cap) atomicOr(&a.counters[2], kStatusOverflow);
-    s_base = base;
-    a.probe_n[q] = m;
-    a.scanned[q] = tot_slots;
-  }
+  for (uint32_t c = threadIdx.x; c < K; c += blockDim.x)
+    if (per_cluster[c] > 0) keys[atomicAdd(&s_n, 1u)] = rank_key(row[c], c);
   __syncthreads();
-  uint64_t ibase = (uint64_t)s_base + coff;
-  for (uint32_t r = r0; r < r1; r++) {
-    uint32_t c = key_id(keys[r]);
-    a.probe_cl[(size_t)q * P + r] = c;
-    a.probe_sc[(size_t)q * P + r] = key_score(keys[r]);
-    a.probe_off[(size_t)q * P + r] = soff;
-    uint32_t b0 = a.block_off[c], b1 = a.block_off[c + 1];
-    soff += (b1 - b0) * SG_BLOCK;
-    if (r < rs) {
-      if (!(r == 0 && partial)) continue;
-      b0 += partial;  // probe 0's blocks past the seed
-    } else if (!a.alu_ranks) {
-      continue;
-    }
-    for (uint32_t b = b0; b < b1; b += a.chunk_blocks) {
-      if (ibase < a.item_cap) a.items[ibase] = make_uint4(q, r, b, min(b1, b + a.chunk_blocks));
-      ibase++;
-    }
+  const uint32_t n = s_n, n2 = next_pow2(n > 0 ? n : 1);
+  for (uint32_t i = n + threadIdx.x; i < n2; i += blockDim.x) keys[i] = 0;
+  __syncthreads();
+  block_bitonic_sort_desc(keys, n2);
+  // covered-before of each cluster in sorted order; it only grows, so the kept clusters are the
+  // prefix whose covered-before is below the target. (Allowed slots < 2^32: the index has fewer
+  // than 2^32 slots.)
+  const uint32_t per = (n + blockDim.x - 1) / blockDim.x;
+  const uint32_t i0 = min(n, threadIdx.x * per), i1 = min(n, i0 + per);
+  uint32_t loc = 0;
+  for (uint32_t i = i0; i < i1; i++) loc += per_cluster[key_id(keys[i])];
+  uint32_t total;
+  uint32_t before = block_exclusive_scan(loc, tmp, &total);
+  uint32_t take = 0;
+  for (uint32_t i = i0; i < i1; i++) {
+    take += (uint64_t)before < target;
+    before += per_cluster[key_id(keys[i])];
   }
+  const uint32_t m = block_sum(take, tmp);
+  emit_probes(a, keys, m, q, tmp);
 }
 
 void launch_route_scores(const DevIndex& ix, Workspace& w, uint32_t nq, int precision,
@@ -400,6 +449,43 @@ void launch_route_select(const DevIndex& ix, Workspace& w, uint32_t nq, const sg
     attr = true;
   }
   k_route_select<<<nq, 256, smem, st>>>(a);
+}
+
+void launch_route_expand(const DevIndex& ix, Workspace& w, uint32_t nq, const sg_params& p,
+                         uint32_t chunk_blocks, uint32_t seed_blocks,
+                         const uint32_t* per_cluster, uint64_t target, cudaStream_t st) {
+  SelectArgs a;
+  memset(&a, 0, sizeof a);
+  a.q256 = w.q256;
+  a.cent = ix.cent;
+  a.qnorm = w.qnorm;
+  a.cent_norm_max = ix.cent_norm_max;
+  a.block_off = ix.block_off;
+  a.K = ix.k;
+  a.scores = w.scores;
+  a.P = ix.k;
+  a.bf16 = 0;
+  a.p = p;
+  a.chunk_blocks = chunk_blocks;
+  a.seed_blocks = seed_blocks;
+  a.alu_ranks = 1;
+  a.seed_items = w.seed_items;
+  a.probe_sc = w.probe_sc;
+  a.probe_cl = w.probe_cl;
+  a.probe_off = w.probe_off;
+  a.probe_n = w.probe_n;
+  a.scanned = w.scanned;
+  a.items = w.items;
+  a.item_cap = w.item_cap;
+  a.counters = w.counters;
+  const size_t smem = (size_t)next_pow2_host(ix.k) * sizeof(uint64_t);
+  static bool attr = false;
+  if (!attr) {
+    cudaFuncSetAttribute(k_route_expand, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)(kExpandMaxK * sizeof(uint64_t)));
+    attr = true;
+  }
+  k_route_expand<<<nq, 1024, smem, st>>>(a, per_cluster, target);
 }
 
 }  // namespace sg

@@ -20,12 +20,21 @@
 
 struct sg_index {
   sg::DevIndex ix;
-  sg::Workspace ws;
+  sg::Ctx def;  // the context of sg_search / sg_search_device
   sg::Config cfg;
   std::mutex mu;
-  cudaStream_t stream = nullptr;
   int sms = 148;
   bool timing_on = false;
+};
+
+// filter::Filter (src/filter.rs:18-25) resident on its index's device.
+struct sg_filter {
+  sg_index* h = nullptr;
+  uint64_t words = 0;
+  uint64_t* allow = nullptr;        // [words] the allow bitset
+  uint32_t* rows = nullptr;         // [nrows] allowed rows, ascending
+  uint64_t nrows = 0;
+  uint32_t* per_cluster = nullptr;  // [k] allowed slots per cluster
 };
 
 namespace sg {
@@ -101,6 +110,8 @@ void free_index(sg::DevIndex& x) {
 }
 
 void free_ws(sg::Workspace& w) {
+  dfree(w.brute);
+  w.brute_cap = 0;
   dfree(w.q768);
   dfree(w.q256);
   dfree(w.tables);
@@ -261,17 +272,62 @@ int build_index(const sg_ivf_arrays* a, int device, sg_index** out) {
   }
   if (const char* sc = getenv("SIEVE_GPU_SOFT_CAP")) h->cfg.soft_cap = (uint32_t)strtoul(sc, nullptr, 10);
   if (const char* m = getenv("SIEVE_GPU_MMA")) h->cfg.mma = atoi(m);
+  if (const char* gr = getenv("SIEVE_GPU_GRAPHS")) h->cfg.graphs = atoi(gr);
+  if (const char* ss = getenv("SIEVE_GPU_SMALL_SEED"))
+    h->cfg.small_seed_blocks =
+        std::max<uint32_t>(1, std::min<uint32_t>((uint32_t)strtoul(ss, nullptr, 10), sg::kMaxChunkBlocks));
   cudaDeviceProp prop;
   CK(cudaGetDeviceProperties(&prop, device));
   h->sms = prop.multiProcessorCount;
-  CK(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));
+  CK(cudaStreamCreateWithFlags(&h->def.stream, cudaStreamNonBlocking));
   *out = h.release();
   return SG_OK;
 }
 
 // Sizes the workspace for nq queries under params p (grows, never shrinks).
-int ensure_ws(sg_index* h, uint32_t nq, const sg_params& p, uint32_t cbuf_per_q) {
-  sg::Workspace& w = h->ws;
+// How a call routes: the index's own probing (plain search, the Post plan), or the Expand plan
+// over a filter's per-cluster allowed slots.
+struct RoutePlan {
+  const uint32_t* per_cluster = nullptr;  // device [k]; set for Expand
+  uint64_t target = 0;
+  bool expand() const { return per_cluster != nullptr; }
+};
+
+// The device addresses a captured pipeline bakes in; when any moves, captured graphs are stale.
+uint64_t ws_signature(const sg::Workspace& w) {
+  const void* ptrs[] = {w.q768, w.q256, w.tables, w.qp, w.qnorm, w.wq, w.winv, w.wq256, w.winv256,
+                        w.scores, w.probe_sc, w.probe_cl, w.probe_off, w.probe_n, w.scanned,
+                        w.items, w.seed_items, w.counters, w.inv_cnt, w.inv_fill, w.inv_off,
+                        w.inv_list, w.gitems, w.thr, w.ccount, w.cbuf_est, w.cbuf_info,
+                        w.overflow, w.cest, w.cid, w.cerr, w.cn, w.lid, w.lsc, w.ln, w.out_sc,
+                        w.out_id, w.out_n};
+  uint64_t hsh = 1469598103934665603ull;
+  for (const void* q : ptrs) hsh = (hsh ^ (uint64_t)(uintptr_t)q) * 1099511628211ull;
+  hsh = (hsh ^ w.item_cap) * 1099511628211ull;
+  hsh = (hsh ^ w.cbuf_per_q) * 1099511628211ull;
+  return (hsh ^ w.gitems_cap) * 1099511628211ull;
+}
+
+void drop_graphs(sg::Ctx& c) {
+  for (auto& g : c.graphs)
+    if (g.exec) cudaGraphExecDestroy(g.exec);
+  c.graphs.clear();
+}
+
+int ensure_ws_impl(sg_index* h, sg::Ctx& c, uint32_t nq, const sg_params& p, uint32_t cbuf_per_q);
+
+int ensure_ws(sg_index* h, sg::Ctx& c, uint32_t nq, const sg_params& p, uint32_t cbuf_per_q) {
+  const uint64_t before = ws_signature(c.ws);
+  const int rc = ensure_ws_impl(h, c, nq, p, cbuf_per_q);
+  if (ws_signature(c.ws) != before) {
+    drop_graphs(c);
+    c.gen++;
+  }
+  return rc;
+}
+
+int ensure_ws_impl(sg_index* h, sg::Ctx& c, uint32_t nq, const sg_params& p, uint32_t cbuf_per_q) {
+  sg::Workspace& w = c.ws;
   cbuf_per_q = (cbuf_per_q + 3) & ~3u;
   const sg::DevIndex& x = h->ix;
   const uint32_t P = std::min<uint32_t>(p.nprobe, x.k);
@@ -380,7 +436,7 @@ int check_params(const sg_index* h, const sg_params* p) {
 // probed cluster; SIEVE_GPU_MMA forces it off (0) or on (2).)
 bool use_mma(const sg_index* h, uint32_t nq, uint32_t P) {
   const sg::DevIndex& x = h->ix;
-  if (!x.blocks_mma || P <= 1) return false;
+  if (!x.blocks_mma || P <= 1 || P > 4096) return false;  // inverted lists keep 12-bit ranks
   if (h->cfg.mma == 2) return true;
   return h->cfg.mma == 1 && nq >= 64 &&
          (uint64_t)nq * (P - 1) >= (uint64_t)h->cfg.mma_min_queries_per_cluster * x.k;
@@ -398,10 +454,10 @@ uint32_t full_cap(const sg_index* h, const sg_params& p, uint32_t nq) {
 
 // Soft per-query buffer for batches: at least 16 x cand entries, and up to an 8 GiB budget
 // shared by the batch. A query that fills it is re-run (see search_impl) with the exact bound.
-uint32_t batch_cap(const sg_index* h, const sg_params& p, uint32_t nq) {
+uint32_t batch_cap(const sg_index* h, const sg_params& p, uint32_t nq, bool soft_always = false) {
   uint32_t full = full_cap(h, p, nq);
   if (h->cfg.soft_cap) return std::min(full, h->cfg.soft_cap);
-  if (nq <= 8) return full;
+  if (nq <= 8 && !soft_always) return full;
   uint64_t budget = (8ull << 30) / (sizeof(uint4) * (uint64_t)nq);
   uint64_t soft = std::max<uint64_t>(16ull * std::max<uint32_t>(p.cand, 1), budget);
   return (uint32_t)std::min<uint64_t>(full, soft);
@@ -411,11 +467,12 @@ enum Stage { kToCandidates = 1, kToSearch = 2 };
 
 // Runs the pipeline on queries already in ws.q768 / ws.q256 (have_q256 = false: derive it).
 // With `timed`, events ev[0..7] bracket the stages (see collect_stats).
-int run_pipeline(sg_index* h, uint32_t nq, const sg_params& p, bool have_q256,
-                 const uint64_t* d_allow, uint64_t allow_words, Stage stage, bool timed) {
-  sg::Workspace& w = h->ws;
+int run_pipeline(sg_index* h, sg::Ctx& c, uint32_t nq, const sg_params& p, bool have_q256,
+                 const uint64_t* d_allow, uint64_t allow_words, Stage stage, bool timed,
+                 const RoutePlan& rp = RoutePlan()) {
+  sg::Workspace& w = c.ws;
   sg::DevIndex& x = h->ix;
-  cudaStream_t st = h->stream;
+  cudaStream_t st = c.stream;
   uint32_t launches = 0;
   CK(cudaMemsetAsync(w.counters, 0, 8 * sizeof(uint32_t), st));
   CK(cudaMemsetAsync(w.thr, 0, nq * sizeof(uint32_t), st));
@@ -428,17 +485,24 @@ int run_pipeline(sg_index* h, uint32_t nq, const sg_params& p, bool have_q256,
   }
   sg::launch_prep(x, w, nq, st);
   if (timed) CK(cudaEventRecord(w.ev[1], st));
-  sg::launch_route_scores(x, w, nq, x.route_precision, st);
+  sg::launch_route_scores(x, w, nq, rp.expand() ? SG_ROUTE_FP32 : x.route_precision, st);
   if (timed) CK(cudaEventRecord(w.ev[2], st));
-  const uint32_t cb = nq < h->cfg.small_batch ? h->cfg.small_chunk_blocks : h->cfg.chunk_blocks;
+  // Few queries leave most SMs to the chunked pass: a short seed (one CTA per query scans it
+  // alone) and short chunks keep the GPU busy.
+  const bool small = nq < h->cfg.small_batch;
+  const uint32_t cb = small ? h->cfg.small_chunk_blocks : h->cfg.chunk_blocks;
+  const uint32_t sb = small ? h->cfg.small_seed_blocks : h->cfg.seed_blocks;
   // The tensor-core scan pays off once enough queries share each probed cluster.
   const uint32_t P = std::min<uint32_t>(p.nprobe, x.k);
-  const bool mma = use_mma(h, nq, P);
-  sg::launch_route_select(x, w, nq, p, x.route_precision, cb, h->cfg.seed_blocks, !mma, st);
+  const bool mma = !rp.expand() && use_mma(h, nq, P);
+  if (rp.expand())
+    sg::launch_route_expand(x, w, nq, p, cb, sb, rp.per_cluster, rp.target, st);
+  else
+    sg::launch_route_select(x, w, nq, p, x.route_precision, cb, sb, !mma, st);
   if (timed) CK(cudaEventRecord(w.ev[3], st));
   launches += 3;
   if (p.cand > 0) {
-    sg::launch_scan(x, w, nq, p, d_allow, allow_words, h->sms, 0, h->cfg.seed_blocks,
+    sg::launch_scan(x, w, nq, p, d_allow, allow_words, h->sms, 0, sb,
                     h->cfg.scan_ctas_per_sm, st);
     if (timed) CK(cudaEventRecord(w.ev[9], st));
     sg::launch_scan(x, w, nq, p, d_allow, allow_words, h->sms, cb, 0, h->cfg.scan_ctas_per_sm, st);
@@ -472,16 +536,65 @@ void collect_stats(sg::Workspace& w, const sg_params& p) {
   if (p.cand > 0) cudaEventElapsedTime(&w.last.ms_seed, w.ev[3], w.ev[9]);
 }
 
-int stage_inputs(sg_index* h, uint32_t nq, const float* q768, const float* q256, bool device) {
-  sg::Workspace& w = h->ws;
+// Runs the search pipeline on c's stream: directly, or, for a call shape seen before and with
+// graphs on, by replaying the CUDA graph captured for it (the second time a shape occurs; the
+// first run of each kernel also sets its shared-memory attributes outside any capture).
+int launch_pipeline(sg_index* h, sg::Ctx& c, uint32_t nq, const sg_params& p, bool have_q256,
+                    const uint64_t* d_allow, uint64_t allow_words, bool timed) {
+  if (!h->cfg.graphs || timed)
+    return run_pipeline(h, c, nq, p, have_q256, d_allow, allow_words, kToSearch, timed);
+  sg::GraphKey key;
+  memset(&key, 0, sizeof key);
+  key.nq = nq;
+  key.p = p;
+  key.have_q256 = have_q256;
+  key.allow = d_allow;
+  key.allow_words = allow_words;
+  key.gen = c.gen;
+  for (auto& g : c.graphs)
+    if (g.key.same(key)) {
+      if (!g.exec) {  // seen once before: capture it now
+        cudaGraph_t graph = nullptr;
+        CK(cudaStreamBeginCapture(c.stream, cudaStreamCaptureModeThreadLocal));
+        int rc = run_pipeline(h, c, nq, p, have_q256, d_allow, allow_words, kToSearch, false);
+        cudaError_t e = cudaStreamEndCapture(c.stream, &graph);
+        if (rc) {
+          if (graph) cudaGraphDestroy(graph);
+          return rc;
+        }
+        if (e != cudaSuccess)
+          return fail(SG_ERR_DEVICE, std::string("cudaStreamEndCapture: ") + cudaGetErrorString(e));
+        cudaGraphExec_t exec = nullptr;
+        e = cudaGraphInstantiate(&exec, graph, 0);
+        cudaGraphDestroy(graph);
+        if (e != cudaSuccess)
+          return fail(SG_ERR_DEVICE, std::string("cudaGraphInstantiate: ") + cudaGetErrorString(e));
+        g.exec = exec;
+        g.launches = c.ws.last.launches;
+      }
+      CK(cudaGraphLaunch(g.exec, c.stream));
+      c.ws.last = sg_stats();
+      c.ws.last.launches = g.launches;
+      return SG_OK;
+    }
+  if (c.graphs.size() >= 32) {
+    if (c.graphs.front().exec) cudaGraphExecDestroy(c.graphs.front().exec);
+    c.graphs.erase(c.graphs.begin());
+  }
+  c.graphs.push_back({key, nullptr, 0});
+  return run_pipeline(h, c, nq, p, have_q256, d_allow, allow_words, kToSearch, false);
+}
+
+int stage_inputs(sg::Ctx& c, uint32_t nq, const float* q768, const float* q256, bool device) {
+  sg::Workspace& w = c.ws;
   cudaMemcpyKind kind = device ? cudaMemcpyDeviceToDevice : cudaMemcpyDefault;
-  if (q768) CK(cudaMemcpyAsync(w.q768, q768, (size_t)nq * SG_DIM * 4, kind, h->stream));
-  else CK(cudaMemsetAsync(w.q768, 0, (size_t)nq * SG_DIM * 4, h->stream));
-  if (q256) CK(cudaMemcpyAsync(w.q256, q256, (size_t)nq * SG_PDIM * 4, kind, h->stream));
+  if (q768) CK(cudaMemcpyAsync(w.q768, q768, (size_t)nq * SG_DIM * 4, kind, c.stream));
+  else CK(cudaMemsetAsync(w.q768, 0, (size_t)nq * SG_DIM * 4, c.stream));
+  if (q256) CK(cudaMemcpyAsync(w.q256, q256, (size_t)nq * SG_PDIM * 4, kind, c.stream));
   return SG_OK;
 }
 
-int stage_allow(sg_index* h, const uint64_t* allow, uint64_t words, bool device,
+int stage_allow(sg::Ctx& c, const uint64_t* allow, uint64_t words, bool device,
                 const uint64_t** d_allow) {
   *d_allow = nullptr;
   if (!allow) return SG_OK;
@@ -489,47 +602,58 @@ int stage_allow(sg_index* h, const uint64_t* allow, uint64_t words, bool device,
     *d_allow = allow;
     return SG_OK;
   }
-  sg::Workspace& w = h->ws;
+  sg::Workspace& w = c.ws;
   if (words > w.allow_cap) {
     dfree(w.allow);
     int rc = dalloc(&w.allow, words);
     if (rc) return rc;
     w.allow_cap = words;
   }
-  CK(cudaMemcpyAsync(w.allow, allow, words * 8, cudaMemcpyDefault, h->stream));
+  CK(cudaMemcpyAsync(w.allow, allow, words * 8, cudaMemcpyDefault, c.stream));
   *d_allow = w.allow;
   return SG_OK;
 }
 
 // Full search of nq queries with inputs staged; copies results out (kind: D2H or D2D).
-int search_impl(sg_index* h, uint32_t nq, const float* q768, const float* q256,
-                const sg_params& p, const uint64_t* allow, uint64_t allow_words, float* out_sc,
-                uint32_t* out_id, uint32_t* out_n, sg_timing* t, bool device) {
+int search_impl(sg_index* h, sg::Ctx& c, uint32_t nq, const float* q768, const float* q256,
+                const sg_params& user_p, const uint64_t* allow, uint64_t allow_words, float* out_sc,
+                uint32_t* out_id, uint32_t* out_n, sg_timing* t, bool device,
+                bool allow_dev = false, const RoutePlan& rp = RoutePlan()) {
   int rc;
-  if ((rc = check_params(h, &p))) return rc;
+  if ((rc = check_params(h, &user_p))) return rc;
   if (nq == 0) return SG_OK;
   if (!q768) return fail(SG_ERR_INVALID, "q768 is null");
   CK(cudaSetDevice(h->ix.device));
-  uint32_t cap = batch_cap(h, p, nq);
-  if ((rc = ensure_ws(h, nq, p, cap))) return rc;
-  if ((rc = stage_inputs(h, nq, q768, q256, device))) return rc;
+  allow_dev = allow_dev || device;
+  sg_params p = user_p;
+  if (rp.expand()) {  // Index::route over every cluster, no margin or budget (src/filter.rs:81)
+    p.nprobe = h->ix.k;
+    p.has_margin = 0;
+    p.has_budget = 0;
+  }
+  uint32_t cap = batch_cap(h, p, nq, rp.expand());
+  if ((rc = ensure_ws(h, c, nq, p, cap))) return rc;
+  if ((rc = stage_inputs(c, nq, q768, q256, device))) return rc;
   const uint64_t* d_allow;
-  if ((rc = stage_allow(h, allow, allow_words, device, &d_allow))) return rc;
+  if ((rc = stage_allow(c, allow, allow_words, allow_dev, &d_allow))) return rc;
   const bool timed_run = t != nullptr || h->timing_on;
-  if ((rc = run_pipeline(h, nq, p, q256 != nullptr, d_allow, allow_words, kToSearch, timed_run)))
-    return rc;
-  sg::Workspace& w = h->ws;
+  if (rp.expand())
+    rc = run_pipeline(h, c, nq, p, q256 != nullptr, d_allow, allow_words, kToSearch, timed_run, rp);
+  else
+    rc = launch_pipeline(h, c, nq, p, q256 != nullptr, d_allow, allow_words, timed_run);
+  if (rc) return rc;
+  sg::Workspace& w = c.ws;
   std::vector<uint8_t> ovf(nq);
-  CK(cudaMemcpyAsync(ovf.data(), w.overflow, nq, cudaMemcpyDeviceToHost, h->stream));
+  CK(cudaMemcpyAsync(ovf.data(), w.overflow, nq, cudaMemcpyDeviceToHost, c.stream));
   uint32_t status = 0;
-  CK(cudaMemcpyAsync(&status, w.counters + 2, 4, cudaMemcpyDeviceToHost, h->stream));
+  CK(cudaMemcpyAsync(&status, w.counters + 2, 4, cudaMemcpyDeviceToHost, c.stream));
   const uint32_t k = p.k;
   cudaMemcpyKind okind = device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost;
   if (k) {
-    CK(cudaMemcpyAsync(out_sc, w.out_sc, (size_t)nq * k * 4, okind, h->stream));
-    CK(cudaMemcpyAsync(out_id, w.out_id, (size_t)nq * k * 4, okind, h->stream));
+    CK(cudaMemcpyAsync(out_sc, w.out_sc, (size_t)nq * k * 4, okind, c.stream));
+    CK(cudaMemcpyAsync(out_id, w.out_id, (size_t)nq * k * 4, okind, c.stream));
   }
-  CK(cudaMemcpyAsync(out_n, w.out_n, (size_t)nq * 4, okind, h->stream));
+  CK(cudaMemcpyAsync(out_n, w.out_n, (size_t)nq * 4, okind, c.stream));
   std::vector<uint64_t> scanned;
   std::vector<uint32_t> probed, reranked, buffered;
   if (timed_run) {
@@ -537,12 +661,12 @@ int search_impl(sg_index* h, uint32_t nq, const float* q768, const float* q256,
     probed.resize(nq);
     reranked.resize(nq);
     buffered.resize(nq);
-    CK(cudaMemcpyAsync(buffered.data(), w.ccount, nq * 4, cudaMemcpyDeviceToHost, h->stream));
-    CK(cudaMemcpyAsync(scanned.data(), w.scanned, nq * 8, cudaMemcpyDeviceToHost, h->stream));
-    CK(cudaMemcpyAsync(probed.data(), w.probe_n, nq * 4, cudaMemcpyDeviceToHost, h->stream));
-    CK(cudaMemcpyAsync(reranked.data(), w.ln, nq * 4, cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaMemcpyAsync(buffered.data(), w.ccount, nq * 4, cudaMemcpyDeviceToHost, c.stream));
+    CK(cudaMemcpyAsync(scanned.data(), w.scanned, nq * 8, cudaMemcpyDeviceToHost, c.stream));
+    CK(cudaMemcpyAsync(probed.data(), w.probe_n, nq * 4, cudaMemcpyDeviceToHost, c.stream));
+    CK(cudaMemcpyAsync(reranked.data(), w.ln, nq * 4, cudaMemcpyDeviceToHost, c.stream));
   }
-  CK(cudaStreamSynchronize(h->stream));
+  CK(cudaStreamSynchronize(c.stream));
   if (status & sg::kStatusOverflow) return fail(SG_ERR_INVALID, "work queue overflow");
   const bool timed = t != nullptr || h->timing_on;
   if (timed) {
@@ -586,36 +710,105 @@ int search_impl(sg_index* h, uint32_t nq, const float* q768, const float* q256,
     std::vector<uint32_t> oid((size_t)per * std::max<uint32_t>(k, 1)), on(per);
     for (size_t s0 = 0; s0 < redo.size(); s0 += per) {
       const uint32_t m = (uint32_t)std::min<size_t>(per, redo.size() - s0);
-      if ((rc = ensure_ws(h, m, p, fcap))) return rc;
+      if ((rc = ensure_ws(h, c, m, p, fcap))) return rc;
       cudaMemcpyKind ik = device ? cudaMemcpyDeviceToDevice : cudaMemcpyDefault;
       for (uint32_t j = 0; j < m; j++) {
         const uint32_t i = redo[s0 + j];
-        CK(cudaMemcpyAsync(w.q768 + (size_t)j * SG_DIM, q768 + (size_t)i * SG_DIM, SG_DIM * 4, ik, h->stream));
+        CK(cudaMemcpyAsync(w.q768 + (size_t)j * SG_DIM, q768 + (size_t)i * SG_DIM, SG_DIM * 4, ik, c.stream));
         if (q256)
-          CK(cudaMemcpyAsync(w.q256 + (size_t)j * SG_PDIM, q256 + (size_t)i * SG_PDIM, SG_PDIM * 4, ik, h->stream));
+          CK(cudaMemcpyAsync(w.q256 + (size_t)j * SG_PDIM, q256 + (size_t)i * SG_PDIM, SG_PDIM * 4, ik, c.stream));
       }
-      if ((rc = stage_allow(h, allow, allow_words, device, &d_allow))) return rc;
-      if ((rc = run_pipeline(h, m, p, q256 != nullptr, d_allow, allow_words, kToSearch, false)))
+      if ((rc = stage_allow(c, allow, allow_words, allow_dev, &d_allow))) return rc;
+      if ((rc = run_pipeline(h, c, m, p, q256 != nullptr, d_allow, allow_words, kToSearch, false,
+                             rp)))
         return rc;
       std::vector<uint8_t> o1(m);
-      CK(cudaMemcpyAsync(o1.data(), w.overflow, m, cudaMemcpyDeviceToHost, h->stream));
+      CK(cudaMemcpyAsync(o1.data(), w.overflow, m, cudaMemcpyDeviceToHost, c.stream));
       for (uint32_t j = 0; j < m; j++) {
         const uint32_t i = redo[s0 + j];
         if (k) {
-          CK(cudaMemcpyAsync(out_sc + (size_t)i * k, w.out_sc + (size_t)j * k, k * 4, okind, h->stream));
-          CK(cudaMemcpyAsync(out_id + (size_t)i * k, w.out_id + (size_t)j * k, k * 4, okind, h->stream));
+          CK(cudaMemcpyAsync(out_sc + (size_t)i * k, w.out_sc + (size_t)j * k, k * 4, okind, c.stream));
+          CK(cudaMemcpyAsync(out_id + (size_t)i * k, w.out_id + (size_t)j * k, k * 4, okind, c.stream));
         }
-        CK(cudaMemcpyAsync(out_n + i, w.out_n + j, 4, okind, h->stream));
+        CK(cudaMemcpyAsync(out_n + i, w.out_n + j, 4, okind, c.stream));
       }
-      CK(cudaStreamSynchronize(h->stream));
+      CK(cudaStreamSynchronize(c.stream));
       for (uint32_t j = 0; j < m; j++)
         if (o1[j]) return fail(SG_ERR_INVALID, "candidate buffer overflow at the exact bound");
       retry_launches += w.last.launches;
     }
-    if ((rc = ensure_ws(h, nq, p, cap))) return rc;
+    if ((rc = ensure_ws(h, c, nq, p, cap))) return rc;
   }
   w.last = saved;
   w.last.launches += retry_launches;
+  return SG_OK;
+}
+
+// filter::search Plan::Brute (src/filter.rs:95-105): exact int8 scores of every allowed row, in
+// query batches whose score matrix stays under 1 GiB.
+int brute_impl(sg_index* h, sg::Ctx& c, const sg_filter* f, uint32_t nq, const float* q768,
+               const float* q256, const sg_params& p, float* out_sc, uint32_t* out_id,
+               uint32_t* out_n, sg_timing* t) {
+  int rc;
+  if ((rc = check_params(h, &p))) return rc;
+  if (nq == 0) return SG_OK;
+  if (!q768) return fail(SG_ERR_INVALID, "q768 is null");
+  CK(cudaSetDevice(h->ix.device));
+  const uint32_t R = (uint32_t)f->nrows;
+  const uint32_t per = (uint32_t)std::max<uint64_t>(
+      1, std::min<uint64_t>(nq, (256ull << 20) / std::max<uint64_t>(R, 1)));
+  if ((rc = ensure_ws(h, c, per, p, 1))) return rc;
+  sg::Workspace& w = c.ws;
+  if ((uint64_t)per * R > w.brute_cap) {
+    dfree(w.brute);
+    w.brute_cap = 0;
+    if ((rc = dalloc(&w.brute, (size_t)per * R))) return rc;
+    w.brute_cap = (uint64_t)per * R;
+  }
+  const bool timed = t != nullptr || h->timing_on;
+  if (timed && !w.events) {
+    for (auto& e : w.ev) CK(cudaEventCreate(&e));
+    w.events = true;
+  }
+  uint32_t launches = 0;
+  float ms = 0.0f;
+  for (uint32_t q0 = 0; q0 < nq; q0 += per) {
+    const uint32_t m = std::min(per, nq - q0);
+    if ((rc = stage_inputs(c, m, q768 + (size_t)q0 * SG_DIM, q256 ? q256 + (size_t)q0 * SG_PDIM : nullptr,
+                           false)))
+      return rc;
+    if (timed) CK(cudaEventRecord(w.ev[0], c.stream));
+    if (!q256) {
+      sg::launch_prefix(w, m, c.stream);
+      launches++;
+    }
+    sg::launch_prep(h->ix, w, m, c.stream);
+    launches += 1 + sg::launch_brute(h->ix, w, m, f->rows, R, p.k, w.brute, c.stream);
+    if (timed) CK(cudaEventRecord(w.ev[6], c.stream));
+    CK(cudaGetLastError());
+    if (p.k) {
+      CK(cudaMemcpyAsync(out_sc + (size_t)q0 * p.k, w.out_sc, (size_t)m * p.k * 4, cudaMemcpyDeviceToHost, c.stream));
+      CK(cudaMemcpyAsync(out_id + (size_t)q0 * p.k, w.out_id, (size_t)m * p.k * 4, cudaMemcpyDeviceToHost, c.stream));
+    }
+    CK(cudaMemcpyAsync(out_n + q0, w.out_n, (size_t)m * 4, cudaMemcpyDeviceToHost, c.stream));
+    CK(cudaStreamSynchronize(c.stream));
+    if (timed) {
+      float e = 0.0f;
+      CK(cudaEventElapsedTime(&e, w.ev[0], w.ev[6]));
+      ms += e;
+    }
+  }
+  w.last = sg_stats();
+  w.last.launches = launches;
+  w.last.reranked = (uint64_t)nq * R;
+  if (timed) {
+    w.last.ms_rerank = ms;
+    w.last.ms_total = ms;
+  }
+  if (t) {
+    t->rerank += (uint64_t)(ms * 1e6);
+    t->reranked += (uint64_t)nq * R;
+  }
   return SG_OK;
 }
 
@@ -721,10 +914,11 @@ int sg_open_ivf(const char* ingest_dir, const char* index_dir, int device, sg_in
 int sg_close(sg_index* h) {
   if (!h) return SG_OK;
   cudaSetDevice(h->ix.device);
-  if (h->stream) cudaStreamSynchronize(h->stream);
-  free_ws(h->ws);
+  if (h->def.stream) cudaStreamSynchronize(h->def.stream);
+  drop_graphs(h->def);
+  free_ws(h->def.ws);
   free_index(h->ix);
-  if (h->stream) cudaStreamDestroy(h->stream);
+  if (h->def.stream) cudaStreamDestroy(h->def.stream);
   delete h;
   return SG_OK;
 }
@@ -743,7 +937,12 @@ int sg_set_route_precision(sg_index* h, int precision) {
   if (!h) return fail(SG_ERR_INVALID, "null index");
   if (precision != SG_ROUTE_FP32 && precision != SG_ROUTE_BF16)
     return fail(SG_ERR_INVALID, "precision must be SG_ROUTE_FP32 or SG_ROUTE_BF16");
-  h->ix.route_precision = precision;
+  std::lock_guard<std::mutex> lk(h->mu);
+  if (h->ix.route_precision != precision) {
+    h->ix.route_precision = precision;
+    drop_graphs(h->def);  // captured pipelines launch the other routing kernel
+    h->def.gen++;
+  }
   return SG_OK;
 }
 
@@ -755,7 +954,7 @@ int sg_set_timing(sg_index* h, int on) {
 
 int sg_last_stats(const sg_index* h, sg_stats* out) {
   if (!h || !out) return fail(SG_ERR_INVALID, "null argument");
-  *out = h->ws.last;
+  *out = h->def.ws.last;
   return SG_OK;
 }
 
@@ -764,7 +963,7 @@ int sg_search(sg_index* h, uint32_t nq, const float* q768, const float* q256,
               float* out_scores, uint32_t* out_ids, uint32_t* out_counts, sg_timing* timing) {
   if (!h || !params) return fail(SG_ERR_INVALID, "null argument");
   std::lock_guard<std::mutex> g(h->mu);
-  return search_impl(h, nq, q768, q256, *params, allow_bits, allow_words, out_scores, out_ids,
+  return search_impl(h, h->def, nq, q768, q256, *params, allow_bits, allow_words, out_scores, out_ids,
                      out_counts, timing, false);
 }
 
@@ -779,8 +978,8 @@ int sg_search_device(sg_index* h, uint32_t nq, const float* d_q768, const float*
   cudaEvent_t ev;
   CK(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
   CK(cudaEventRecord(ev, user));
-  CK(cudaStreamWaitEvent(h->stream, ev, 0));
-  int rc = search_impl(h, nq, d_q768, d_q256, *params, d_allow_bits, allow_words, d_out_scores,
+  CK(cudaStreamWaitEvent(h->def.stream, ev, 0));
+  int rc = search_impl(h, h->def, nq, d_q768, d_q256, *params, d_allow_bits, allow_words, d_out_scores,
                        d_out_ids, d_out_counts, nullptr, true);
   cudaEventDestroy(ev);
   return rc;
@@ -794,10 +993,10 @@ int sg_route(sg_index* h, uint32_t nq, const float* q256, const sg_params* param
   if ((rc = check_params(h, params))) return rc;
   if (nq == 0) return SG_OK;
   CK(cudaSetDevice(h->ix.device));
-  if ((rc = ensure_ws(h, nq, *params, 1))) return rc;
-  if ((rc = stage_inputs(h, nq, nullptr, q256, false))) return rc;
-  sg::Workspace& w = h->ws;
-  cudaStream_t st = h->stream;
+  if ((rc = ensure_ws(h, h->def, nq, *params, 1))) return rc;
+  if ((rc = stage_inputs(h->def, nq, nullptr, q256, false))) return rc;
+  sg::Workspace& w = h->def.ws;
+  cudaStream_t st = h->def.stream;
   CK(cudaMemsetAsync(w.counters, 0, 32, st));
   sg::launch_prep(h->ix, w, nq, st);
   sg::launch_route_scores(h->ix, w, nq, h->ix.route_precision, st);
@@ -827,22 +1026,22 @@ int sg_candidates(sg_index* h, uint32_t nq, const float* q256, const sg_params* 
   uint32_t cap = full_cap(h, p, 1);
   for (uint32_t q0 = 0; q0 < nq; q0++) {
     // one query at a time with the exact buffer bound: this entry point is for parity checks
-    if ((rc = ensure_ws(h, 1, p, cap))) return rc;
-    if ((rc = stage_inputs(h, 1, nullptr, q256 + (size_t)q0 * SG_PDIM, false))) return rc;
+    if ((rc = ensure_ws(h, h->def, 1, p, cap))) return rc;
+    if ((rc = stage_inputs(h->def, 1, nullptr, q256 + (size_t)q0 * SG_PDIM, false))) return rc;
     const uint64_t* d_allow;
-    if ((rc = stage_allow(h, allow_bits, allow_words, false, &d_allow))) return rc;
-    if ((rc = run_pipeline(h, 1, p, true, d_allow, allow_words, kToCandidates, false))) return rc;
-    sg::Workspace& w = h->ws;
+    if ((rc = stage_allow(h->def, allow_bits, allow_words, false, &d_allow))) return rc;
+    if ((rc = run_pipeline(h, h->def, 1, p, true, d_allow, allow_words, kToCandidates, false))) return rc;
+    sg::Workspace& w = h->def.ws;
     const uint32_t c = std::max<uint32_t>(p.cand, 1);
     if (p.cand) {
-      CK(cudaMemcpyAsync(out_est + (size_t)q0 * c, w.cest, (size_t)c * 4, cudaMemcpyDeviceToHost, h->stream));
-      CK(cudaMemcpyAsync(out_ids + (size_t)q0 * c, w.cid, (size_t)c * 4, cudaMemcpyDeviceToHost, h->stream));
-      CK(cudaMemcpyAsync(out_err + (size_t)q0 * c, w.cerr, (size_t)c * 4, cudaMemcpyDeviceToHost, h->stream));
+      CK(cudaMemcpyAsync(out_est + (size_t)q0 * c, w.cest, (size_t)c * 4, cudaMemcpyDeviceToHost, h->def.stream));
+      CK(cudaMemcpyAsync(out_ids + (size_t)q0 * c, w.cid, (size_t)c * 4, cudaMemcpyDeviceToHost, h->def.stream));
+      CK(cudaMemcpyAsync(out_err + (size_t)q0 * c, w.cerr, (size_t)c * 4, cudaMemcpyDeviceToHost, h->def.stream));
     }
-    CK(cudaMemcpyAsync(out_counts + q0, w.cn, 4, cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaMemcpyAsync(out_counts + q0, w.cn, 4, cudaMemcpyDeviceToHost, h->def.stream));
     uint8_t o = 0;
-    CK(cudaMemcpyAsync(&o, w.overflow, 1, cudaMemcpyDeviceToHost, h->stream));
-    CK(cudaStreamSynchronize(h->stream));
+    CK(cudaMemcpyAsync(&o, w.overflow, 1, cudaMemcpyDeviceToHost, h->def.stream));
+    CK(cudaStreamSynchronize(h->def.stream));
     if (o) return fail(SG_ERR_INVALID, "candidate buffer overflow at the exact bound");
     // the device list is unordered; Index::candidates returns it in row order
     if (p.cand) {
@@ -868,6 +1067,102 @@ int sg_candidates(sg_index* h, uint32_t nq, const float* q256, const sg_params* 
   return SG_OK;
 }
 
+int sg_filter_new(sg_index* h, const uint64_t* allow_bits, uint64_t allow_words, sg_filter** out) {
+  if (!h || !out || (!allow_bits && allow_words)) return fail(SG_ERR_INVALID, "null argument");
+  *out = nullptr;
+  std::lock_guard<std::mutex> g(h->mu);
+  CK(cudaSetDevice(h->ix.device));
+  std::unique_ptr<sg_filter> f(new sg_filter());
+  f->h = h;
+  f->words = allow_words;
+  int rc;
+  auto cleanup = [&]() {
+    dfree(f->allow);
+    dfree(f->rows);
+    dfree(f->per_cluster);
+  };
+  if ((rc = dalloc(&f->allow, std::max<uint64_t>(allow_words, 1))) ||
+      (rc = dalloc(&f->per_cluster, std::max<uint32_t>(h->ix.k, 1)))) {
+    cleanup();
+    return rc;
+  }
+  cudaError_t e = cudaSuccess;
+  if (allow_words)
+    e = cudaMemcpyAsync(f->allow, allow_bits, allow_words * 8, cudaMemcpyHostToDevice, h->def.stream);
+  if (e != cudaSuccess) {
+    cleanup();
+    return fail(SG_ERR_DEVICE, std::string("filter upload: ") + cudaGetErrorString(e));
+  }
+  if ((rc = sg::filter_build(h->ix, f->allow, allow_words, &f->rows, &f->nrows, f->per_cluster,
+                             h->def.stream)) ||
+      (rc = cudaStreamSynchronize(h->def.stream) == cudaSuccess ? SG_OK
+                                                               : fail(SG_ERR_DEVICE, "filter build"))) {
+    cleanup();
+    return rc;
+  }
+  *out = f.release();
+  return SG_OK;
+}
+
+int sg_filter_info(const sg_filter* f, uint64_t* nrows, uint32_t* out_per_cluster, uint32_t* out_rows) {
+  if (!f) return fail(SG_ERR_INVALID, "null filter");
+  if (nrows) *nrows = f->nrows;
+  CK(cudaSetDevice(f->h->ix.device));
+  if (out_per_cluster)
+    CK(cudaMemcpy(out_per_cluster, f->per_cluster, (size_t)f->h->ix.k * 4, cudaMemcpyDeviceToHost));
+  if (out_rows && f->nrows)
+    CK(cudaMemcpy(out_rows, f->rows, (size_t)f->nrows * 4, cudaMemcpyDeviceToHost));
+  return SG_OK;
+}
+
+int sg_filter_free(sg_filter* f) {
+  if (!f) return SG_OK;
+  {
+    std::lock_guard<std::mutex> g(f->h->mu);
+    cudaSetDevice(f->h->ix.device);
+    cudaStreamSynchronize(f->h->def.stream);
+    dfree(f->allow);
+    dfree(f->rows);
+    dfree(f->per_cluster);
+  }
+  delete f;
+  return SG_OK;
+}
+
+int sg_plan_resolve(int plan, uint64_t allowed_rows, uint64_t n) {
+  if (plan != SG_PLAN_AUTO) return plan;
+  if (allowed_rows <= SG_BRUTE_MAX) return SG_PLAN_BRUTE;
+  if ((double)allowed_rows >= SG_POST_MIN * (double)n) return SG_PLAN_POST;
+  return SG_PLAN_EXPAND;
+}
+
+int sg_filter_search(sg_index* h, const sg_filter* f, int plan, uint64_t expand_target, uint32_t nq,
+                     const float* q768, const float* q256, const sg_params* params,
+                     float* out_scores, uint32_t* out_ids, uint32_t* out_counts, sg_timing* timing) {
+  if (!h || !f || !params) return fail(SG_ERR_INVALID, "null argument");
+  if (f->h != h) return fail(SG_ERR_INVALID, "the filter belongs to another index");
+  if (plan < SG_PLAN_POST || plan > SG_PLAN_AUTO) return fail(SG_ERR_INVALID, "unknown plan");
+  const int resolved = sg_plan_resolve(plan, f->nrows, h->ix.n);
+  if (plan == SG_PLAN_AUTO && resolved == SG_PLAN_EXPAND) expand_target = SG_EXPAND_TARGET;
+  std::lock_guard<std::mutex> g(h->mu);
+  try {
+    if (resolved == SG_PLAN_BRUTE)
+      return brute_impl(h, h->def, f, nq, q768, q256, *params, out_scores, out_ids, out_counts, timing);
+    if (resolved == SG_PLAN_POST)
+      return search_impl(h, h->def, nq, q768, q256, *params, f->allow, f->words, out_scores, out_ids,
+                         out_counts, timing, false, true);
+    if (h->ix.k > sg::kExpandMaxK)
+      return fail(SG_ERR_UNSUPPORTED, "plan Expand needs k <= 16384 clusters");
+    RoutePlan rp;
+    rp.per_cluster = f->per_cluster;
+    rp.target = expand_target;
+    return search_impl(h, h->def, nq, q768, q256, *params, f->allow, f->words, out_scores, out_ids,
+                       out_counts, timing, false, true, rp);
+  } catch (const std::exception& e) {
+    return fail(SG_ERR_OOM, e.what());
+  }
+}
+
 int sg_query_prep(sg_index* h, uint32_t nq, const float* q256, uint8_t* out_tables,
                   float* out_scale, float* out_bias, float* out_a, float* out_b) {
   if (!h || !q256) return fail(SG_ERR_INVALID, "null argument");
@@ -880,14 +1175,14 @@ int sg_query_prep(sg_index* h, uint32_t nq, const float* q256, uint8_t* out_tabl
   p.cand = 1;
   p.k = 1;
   int rc;
-  if ((rc = ensure_ws(h, nq, p, 1))) return rc;
-  if ((rc = stage_inputs(h, nq, nullptr, q256, false))) return rc;
-  sg::launch_prep(h->ix, h->ws, nq, h->stream);
+  if ((rc = ensure_ws(h, h->def, nq, p, 1))) return rc;
+  if ((rc = stage_inputs(h->def, nq, nullptr, q256, false))) return rc;
+  sg::launch_prep(h->ix, h->def.ws, nq, h->def.stream);
   CK(cudaGetLastError());
   std::vector<float4> qp(nq);
-  CK(cudaMemcpyAsync(out_tables, h->ws.tables, (size_t)nq * 1024, cudaMemcpyDeviceToHost, h->stream));
-  CK(cudaMemcpyAsync(qp.data(), h->ws.qp, nq * sizeof(float4), cudaMemcpyDeviceToHost, h->stream));
-  CK(cudaStreamSynchronize(h->stream));
+  CK(cudaMemcpyAsync(out_tables, h->def.ws.tables, (size_t)nq * 1024, cudaMemcpyDeviceToHost, h->def.stream));
+  CK(cudaMemcpyAsync(qp.data(), h->def.ws.qp, nq * sizeof(float4), cudaMemcpyDeviceToHost, h->def.stream));
+  CK(cudaStreamSynchronize(h->def.stream));
   for (uint32_t i = 0; i < nq; i++) {
     if (out_scale) out_scale[i] = qp[i].x;
     if (out_bias) out_bias[i] = qp[i].y;

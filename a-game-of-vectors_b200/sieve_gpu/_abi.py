@@ -174,6 +174,11 @@ EXPORTS = [
     "sg_search_noalloc",
     "sg_route",
     "sg_candidates",
+    "sg_filter_new",
+    "sg_filter_info",
+    "sg_filter_free",
+    "sg_plan_resolve",
+    "sg_filter_search",
     "sg_query_prep",
     "sg_lut_scan",
     "sg_dot_i8i8",

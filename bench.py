@@ -318,7 +318,8 @@ def main():
              for k in ("ms_prep", "ms_route_gemm", "ms_route_select", "ms_scan", "ms_cut", "ms_rerank",
                        "ms_tier2", "ms_total")}
 
-    # one query per launch
+    # one query per launch (timing off: repeated call shapes replay their captured CUDA graph)
+    index.set_timing(False)
     plain_ms = []
     for i in range(args.plain):
         a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)

@@ -198,6 +198,40 @@ int sg_candidates(sg_index* index, uint32_t nq, const float* q256, const sg_para
                   const uint64_t* allow_bits, uint64_t allow_words, float* out_est,
                   uint32_t* out_ids, float* out_err, uint32_t* out_counts);
 
+/* ---- filters: filter::Filter / Plan / search (src/filter.rs) ---------------------------- */
+/* filter::Plan (src/filter.rs:42-53). */
+typedef enum {
+  SG_PLAN_POST = 0,   /* the unfiltered probes, disallowed rows skipped at admission            */
+  SG_PLAN_EXPAND = 1, /* probe clusters in route order until expand_target allowed slots        */
+  SG_PLAN_BRUTE = 2,  /* exact int8 scores of every allowed row; no index                        */
+  SG_PLAN_AUTO = 3    /* one of the above from the filter's size (sg_plan_resolve)               */
+} sg_plan;
+#define SG_BRUTE_MAX 250000u     /* filter::BRUTE_MAX (src/filter.rs:55)                       */
+#define SG_POST_MIN 0.3          /* filter::POST_MIN (src/filter.rs:57)                        */
+#define SG_EXPAND_TARGET 200000u /* filter::EXPAND_TARGET (src/filter.rs:59)                   */
+
+typedef struct sg_filter sg_filter;
+/* filter::Filter::new (src/filter.rs:27-38) on the index's device: keeps the allow bitset, the
+ * allowed rows ascending and the allowed slots per cluster in HBM. Bits at rows >= n are
+ * ignored. The filter belongs to `index` and must be freed before it. */
+int sg_filter_new(sg_index* index, const uint64_t* allow_bits, uint64_t allow_words,
+                  sg_filter** out);
+/* The filter's allowed-row count, and (each nullable) per_cluster [k] and rows [nrows]. */
+int sg_filter_info(const sg_filter* filter, uint64_t* nrows, uint32_t* out_per_cluster,
+                   uint32_t* out_rows);
+int sg_filter_free(sg_filter* filter);
+/* filter::Plan::resolve (src/filter.rs:62-71): the plan Auto stands for, given the allowed rows
+ * and the corpus size (SG_PLAN_EXPAND then means Expand(SG_EXPAND_TARGET)); other plans are
+ * returned as they are. */
+int sg_plan_resolve(int plan, uint64_t allowed_rows, uint64_t n);
+/* filter::search (src/filter.rs:74-110) for nq queries: the top params.k allowed rows of each
+ * as (score, row), best first. expand_target is Expand's target (ignored by other plans; Auto
+ * uses SG_EXPAND_TARGET). Expand needs k <= 16384 clusters. Outputs as sg_search. */
+int sg_filter_search(sg_index* index, const sg_filter* filter, int plan, uint64_t expand_target,
+                     uint32_t nq, const float* q768, const float* q256, const sg_params* params,
+                     float* out_scores, uint32_t* out_ids, uint32_t* out_counts,
+                     sg_timing* timing);
+
 /* ---- kernel-level entry points (parity tests and micro-benchmarks) ----------------------- */
 /* rabitq::Query::new (src/rabitq.rs:119-125) on the device: rotated LUT tables [nq*64*16] u8,
  * and per query scale, bias, a, b. */

@@ -130,3 +130,22 @@ def test_oracle_search_is_sane():
     for i in range(0, len(q768), 9):
         s1, o1, _ = oi.search(q768[i], q256[i], p)
         assert np.array_equal(o1, o[i, : cnt[i]])
+
+
+def test_plan_resolve_is_the_reference_auto_plan():
+    """src/filter.rs:157-165 auto_plan, through the library's host-side sg_plan_resolve."""
+    from sieve_gpu import filter as F
+
+    class Fake:
+        def __init__(self, rows):
+            self.nrows = rows
+
+    n = 10_000_000
+    assert F.Plan.auto().resolve(Fake(F.BRUTE_MAX), n) == F.Plan.brute()
+    assert F.Plan.auto().resolve(Fake(1_000_000), n) == F.Plan.expand(F.EXPAND_TARGET)
+    assert F.Plan.auto().resolve(Fake(3_000_000), n) == F.Plan.post()
+    assert F.Plan.expand(7).resolve(Fake(1), n) == F.Plan.expand(7)
+    for rows in (0, 1, 250_000, 250_001, 2_999_999, 3_000_000, 10_000_000):
+        for plan in range(4):
+            got = _abi.lib().sg_plan_resolve(plan, _abi.c_uint64(rows), _abi.c_uint64(n))
+            assert got == O.plan_resolve(plan, rows, n)
