@@ -133,6 +133,75 @@ def make_arrays(arrays: dict) -> tuple[SgIvfArrays, list]:
     return st, keep
 
 
+# ---- bigann (src/bigann.rs) ----------------------------------------------------------------
+BG_DIM, BG_PDIM, BG_GROUPS, BG_CODE, BG_BLOCK_BYTES, BG_MAX_BITS = 100, 128, 32, 16, 512, 3
+
+
+class SgBigannParams(ctypes.Structure):
+    """sg_bigann_params: bigann::Params."""
+
+    _fields_ = [("nprobe", c_uint32), ("cand", c_uint32), ("k", c_uint32), ("refine", c_uint32),
+                ("margin", c_float), ("reserved", c_uint32)]
+
+
+class SgBigannTiming(ctypes.Structure):
+    """sg_bigann_timing: bigann::Timing, in nanoseconds."""
+
+    _fields_ = [(n, c_uint64) for n in ("route", "scan", "io_wait", "rerank", "scanned", "probes")]
+
+
+class SgBigannArrays(ctypes.Structure):
+    """sg_bigann_arrays: a bigann index's records (de-interleaved) and its base rows."""
+
+    _fields_ = [
+        ("n", c_uint64),
+        ("k", c_uint32),
+        ("bits", c_uint32),
+        ("leaves", c_void_p),
+        ("block_off", c_void_p),
+        ("ids", c_void_p),
+        ("blocks", c_void_p),
+        ("factors", c_void_p),
+        ("ext", c_void_p),
+        ("rotation", c_void_p),
+        ("base", c_void_p),
+    ]
+
+
+BIGANN_FIELDS = {
+    "leaves": np.float32,
+    "block_off": np.uint64,
+    "ids": np.uint32,
+    "blocks": np.uint8,
+    "factors": np.float32,
+    "ext": np.uint8,
+    "rotation": np.float32,
+    "base": np.int8,
+}
+
+
+def bg_extra(bits: int) -> int:
+    """bigann::refine_bytes (src/bigann.rs:110-113): planes of the low bits - 1 bits, then f."""
+    return (bits - 1) * BG_CODE + 4 if bits > 1 else 0
+
+
+def make_bigann_arrays(arrays: dict) -> tuple[SgBigannArrays, list]:
+    keep = []
+    st = SgBigannArrays()
+    st.n = int(arrays["n"])
+    st.k = int(arrays["k"])
+    st.bits = int(arrays["bits"])
+    for name, dt in BIGANN_FIELDS.items():
+        a = arrays.get(name)
+        if a is not None and a.size:
+            a = np.ascontiguousarray(a, dtype=dt)
+            keep.append(a)
+        else:
+            a = None
+        setattr(st, name, ptr(a))
+    return st, keep
+
+
 class SieveError(RuntimeError):
     def __init__(self, status: int, message: str):
         super().__init__(f"{STATUS_NAMES.get(status, status)}: {message}")
@@ -179,6 +248,14 @@ EXPORTS = [
     "sg_filter_free",
     "sg_plan_resolve",
     "sg_filter_search",
+    "sg_open_bigann",
+    "sg_open_bigann_arrays",
+    "sg_close_bigann",
+    "sg_bigann_info",
+    "sg_search_bigann",
+    "sg_search_bigann_device",
+    "sg_bigann_route",
+    "sg_bigann_candidates",
     "sg_query_prep",
     "sg_lut_scan",
     "sg_dot_i8i8",

@@ -134,6 +134,52 @@ typedef struct {
   const float* quant_scale;   /* quant.f32       [768]                                         */
 } sg_ivf_arrays;
 
+/* ---- bigann: L2 search over int8 rows (src/bigann.rs) ---------------------------------- */
+#define SG_BG_DIM 100          /* bigann::D: SPACEV row width                                   */
+#define SG_BG_PDIM 128         /* bigann::PD: padded width of the rotation and the codes        */
+#define SG_BG_GROUPS 32        /* LUT groups of a 128-bit code                                  */
+#define SG_BG_CODE 16          /* bigann::CODE: bytes of a 1-bit code                           */
+#define SG_BG_BLOCK_BYTES 512  /* bigann::BLOCK_BYTES                                           */
+#define SG_BG_MAX_BITS 3       /* bigann::MAX_BITS                                              */
+
+/* bigann::Params (src/bigann.rs:610-623). */
+typedef struct {
+  uint32_t nprobe;  /* leaves probed (cap)                                                      */
+  uint32_t cand;    /* candidates reranked exactly from the base rows                           */
+  uint32_t k;       /* results returned                                                         */
+  uint32_t refine;  /* multi-bit index: 1-bit shortlist re-estimated from all planes; 0 = off   */
+  float margin;     /* keep leaves with |q-c|^2 <= (1 + margin) |q-c1|^2; 0 = off               */
+  uint32_t reserved;
+} sg_bigann_params;
+
+/* bigann::Timing (src/bigann.rs:624-632): device times in nanoseconds. */
+typedef struct {
+  uint64_t route;
+  uint64_t scan;
+  uint64_t io_wait;  /* always 0: every record is resident in HBM                               */
+  uint64_t rerank;
+  uint64_t scanned;  /* slots scanned, padding included                                         */
+  uint64_t probes;   /* leaves probed                                                           */
+} sg_bigann_timing;
+
+/* Host arrays of a bigann index and its base, de-interleaved from the reference's postings.bin
+ * records (src/postings.rs:9-14, :31-34; src/bigann.rs:405-432): per slot, a 16-byte 1-bit
+ * code in 512-byte nibble-transposed blocks, [mul, |x|^2] factors, the row id and, with
+ * bits > 1, (bits - 1) * 16 bytes of refinement planes followed by the f32 scale f. */
+typedef struct {
+  uint64_t n;                 /* base rows                                                     */
+  uint32_t k;                 /* leaves                                                        */
+  uint32_t bits;              /* bits.u64: refinement width 1..3                               */
+  const float* leaves;        /* centroids.f32   [k * 100]                                     */
+  const uint64_t* block_off;  /* block_off.u64   [k + 1]                                       */
+  const uint32_t* ids;        /* record ids      [nblocks * 32]                                */
+  const uint8_t* blocks;      /* record blocks   [nblocks * 512]                               */
+  const float* factors;       /* record factors  [nblocks * 32 * 2] = [mul, |x|^2] per slot    */
+  const uint8_t* ext;         /* record extra    [nblocks * 32 * extra], extra = (bits-1)*16+4 */
+  const float* rotation;      /* rotation.f32    [3 * 128] signs                               */
+  const int8_t* base;         /* base.NN         [n * 100]                                     */
+} sg_bigann_arrays;
+
 /* ---- errors ----------------------------------------------------------------------------- */
 const char* sg_last_error(void);
 /* Library version string and the device it was built for. */
@@ -231,6 +277,37 @@ int sg_filter_search(sg_index* index, const sg_filter* filter, int plan, uint64_
                      uint32_t nq, const float* q768, const float* q256, const sg_params* params,
                      float* out_scores, uint32_t* out_ids, uint32_t* out_counts,
                      sg_timing* timing);
+
+/* ---- bigann: billion-scale L2 search over int8 rows (src/bigann.rs) -------------------- */
+typedef struct sg_bigann sg_bigann;
+/* bigann::Index::open(dir, base_dir, cache) (src/bigann.rs:635-641) with every record resident:
+ * reads centroids.f32, rotation.f32, bits.u64 (absent: 1), block_off.u64, postings.off and
+ * postings.bin from index_dir and base.NN (while base.NN.done exists) from base_dir, and uploads
+ * them to HBM on `device`. */
+int sg_open_bigann(const char* index_dir, const char* base_dir, int device, sg_bigann** out);
+/* The same from host arrays (the records already de-interleaved). */
+int sg_open_bigann_arrays(const sg_bigann_arrays* a, int device, sg_bigann** out);
+int sg_close_bigann(sg_bigann* index);
+int sg_bigann_info(const sg_bigann* index, uint32_t* k, uint64_t* n, uint64_t* nblocks,
+                   uint32_t* bits);
+/* bigann::Index::search (src/bigann.rs:653-657) for nq int8 queries q100 [nq * 100]: the top
+ * params.k rows by 2<q,x> - |x|^2 as (score, row), best first. out_* [nq * k], out_counts [nq]. */
+int sg_search_bigann(sg_bigann* index, uint32_t nq, const int8_t* q100,
+                     const sg_bigann_params* params, float* out_scores, uint32_t* out_ids,
+                     uint32_t* out_counts, sg_bigann_timing* timing);
+/* The same with device pointers, ordered after `stream` (cudaStream_t). */
+int sg_search_bigann_device(sg_bigann* index, uint32_t nq, const int8_t* d_q100,
+                            const sg_bigann_params* params, float* d_out_scores,
+                            uint32_t* d_out_ids, uint32_t* d_out_counts, void* stream);
+/* bigann::Index::route (src/bigann.rs:660-678): the probed leaves, best first.
+ * out_probe [nq * min(nprobe, k)], out_counts [nq]. */
+int sg_bigann_route(sg_bigann* index, uint32_t nq, const int8_t* q100,
+                    const sg_bigann_params* params, uint32_t* out_probe, uint32_t* out_counts);
+/* bigann::Index::candidates (src/bigann.rs:683-732) after the index's own routing: the best
+ * params.cand slots as (row, estimate, |x|^2), best first. out_* [nq * cand], out_counts [nq]. */
+int sg_bigann_candidates(sg_bigann* index, uint32_t nq, const int8_t* q100,
+                         const sg_bigann_params* params, uint32_t* out_ids, float* out_est,
+                         float* out_nx, uint32_t* out_counts);
 
 /* ---- kernel-level entry points (parity tests and micro-benchmarks) ----------------------- */
 /* rabitq::Query::new (src/rabitq.rs:119-125) on the device: rotated LUT tables [nq*64*16] u8,

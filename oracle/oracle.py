@@ -19,7 +19,8 @@ import numpy as np
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 sys.path.insert(0, os.path.join(ROOT, "a-game-of-vectors_b200"))
-from sieve_gpu._abi import SgIvfArrays, SgParams, SgTiming, make_arrays  # noqa: E402
+from sieve_gpu._abi import (SgBigannParams, SgBigannTiming, SgIvfArrays, SgParams, SgTiming,  # noqa: E402
+                            make_arrays, make_bigann_arrays)
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 
@@ -71,6 +72,12 @@ def lib(native: bool = False) -> ctypes.CDLL:
     L.or_plan_resolve.restype = c_int
     L.or_filter_search.restype = c_uint32
     L.or_recall_at.restype = c_double
+    for f in ("or_bg_refine_encode", "or_bg_refiner_estimate"):
+        getattr(L, f).restype = c_float
+    L.or_bg_refiner_estimate.argtypes = [c_void_p, c_float, c_uint32, c_void_p, c_void_p, c_float]
+    for f in ("or_bg_extra", "or_bg_route", "or_bg_candidates", "or_bg_rerank", "or_bg_search"):
+        getattr(L, f).restype = c_uint32
+    L.or_bg_search_batch.restype = c_uint64
     _libs[key] = L
     return L
 
@@ -389,3 +396,74 @@ class OracleIndex:
 
 
 __all__ = [name for name in dir() if not name.startswith("_")]
+
+
+# ---- bigann (src/bigann.rs) --------------------------------------------------------------------
+def bg_refine_encode(r, bits: int):
+    """refine_encode (src/bigann.rs:65-108): (planes [(MAX_BITS-1)*16] u8, f)."""
+    r = f32(r)
+    planes = np.zeros(2 * 16, np.uint8)
+    f = lib().or_bg_refine_encode(P(r), c_uint32(bits), P(planes))
+    return planes, f
+
+
+def bg_refiner(qr, bits: int):
+    """Refiner::new (src/bigann.rs:575-585): (tables [16, 256] f32, off)."""
+    qr = f32(qr)
+    tab = np.zeros((16, 256), np.float32)
+    off = c_float()
+    lib().or_bg_refiner_new(P(qr), c_uint32(bits), P(tab), ctypes.byref(off))
+    return tab, off.value
+
+
+def bg_refiner_estimate(tab, off: float, bits: int, sign, planes, f: float) -> float:
+    tab = f32(tab)
+    sign, planes = np.ascontiguousarray(sign, np.uint8), np.ascontiguousarray(planes, np.uint8)
+    return lib().or_bg_refiner_estimate(P(tab), off, bits, P(sign), P(planes), f)
+
+
+class OracleBigann:
+    """bigann::Index over in-memory arrays (the dict the GPU bigann index opens)."""
+
+    def __init__(self, arrays: dict, native: bool = False):
+        self.st, self._keep = make_bigann_arrays(arrays)
+        self.k = int(arrays["k"])
+        self.L = lib(native)
+
+    @staticmethod
+    def params(nprobe, cand, k, refine=0, margin=0.0) -> SgBigannParams:
+        return SgBigannParams(int(nprobe), int(cand), int(k), int(refine), float(margin), 0)
+
+    def route(self, q, p: SgBigannParams):
+        q = np.ascontiguousarray(q, np.int8)
+        probe = np.zeros(max(self.k, 1), np.uint32)
+        sc = np.zeros(max(self.k, 1), np.float32)
+        dots = np.zeros(max(self.k, 1), np.float32)
+        m = self.L.or_bg_route(ctypes.byref(self.st), P(q), ctypes.byref(p), P(probe), P(sc), P(dots))
+        return probe[:m], sc[:m], dots
+
+    def candidates(self, q, p: SgBigannParams):
+        q = np.ascontiguousarray(q, np.int8)
+        probe, _, dots = self.route(q, p)
+        c = max(p.cand, 1)
+        ids, est, nx = np.zeros(c, np.uint32), np.zeros(c, np.float32), np.zeros(c, np.float32)
+        scanned = c_uint64()
+        m = self.L.or_bg_candidates(ctypes.byref(self.st), P(q), P(probe), c_uint32(probe.size), P(dots),
+                                    ctypes.byref(p), P(ids), P(est), P(nx), ctypes.byref(scanned))
+        return ids[:m], est[:m], nx[:m], scanned.value
+
+    def search(self, q, p: SgBigannParams):
+        q = np.ascontiguousarray(q, np.int8)
+        k = max(p.k, 1)
+        s, o = np.zeros(k, np.float32), np.zeros(k, np.uint32)
+        t = SgBigannTiming()
+        m = self.L.or_bg_search(ctypes.byref(self.st), P(q), ctypes.byref(p), P(s), P(o), ctypes.byref(t))
+        return s[:m], o[:m], t
+
+    def search_batch(self, q, p: SgBigannParams, threads: int = 0):
+        q = np.ascontiguousarray(q, np.int8).reshape(-1, 100)
+        nq, k = q.shape[0], max(p.k, 1)
+        s, o, cnt = np.zeros((nq, k), np.float32), np.zeros((nq, k), np.uint32), np.zeros(nq, np.uint32)
+        scanned = self.L.or_bg_search_batch(ctypes.byref(self.st), c_uint32(nq), P(q), ctypes.byref(p),
+                                            c_int(threads or os.cpu_count() or 1), P(s), P(o), P(cnt))
+        return s[:, : p.k], o[:, : p.k], cnt, scanned

@@ -890,3 +890,268 @@ double or_recall_at(uint32_t k, const uint32_t* got, uint32_t ngot, const uint32
   uint32_t den = k < distinct ? k : distinct;
   return (double)hit / (double)(den > 0 ? den : 1);
 }
+
+/* ---- bigann.rs: L2 search over int8 rows ------------------------------------------------- */
+#define BG_D SG_BG_DIM
+#define BG_PD SG_BG_PDIM
+#define BG_CODE SG_BG_CODE
+#define BG_BB SG_BG_BLOCK_BYTES
+
+uint32_t or_bg_extra(uint32_t bits) { return bits > 1 ? (bits - 1) * BG_CODE + 4 : 0; }
+
+/* refine_encode: src/bigann.rs:65-108 (extended-RaBitQ step search over 24 deltas). */
+static inline uint32_t bg_level(float v, float delta, float h, uint32_t top) {
+  float x = floorf(v / delta + h + 0.5f);
+  float hi = (float)(2 * top - 1);
+  if (x < 0.0f) x = 0.0f;
+  if (x > hi) x = hi;
+  uint32_t u = (uint32_t)x;
+  return v > 0.0f ? (u | top) : (u & (top - 1));
+}
+
+float or_bg_refine_encode(const float* r, uint32_t bits, uint8_t* planes) {
+  memset(planes, 0, (SG_BG_MAX_BITS - 1) * BG_CODE);
+  const uint32_t top = 1u << (bits - 1);
+  const float h = (float)(2 * top - 1) / 2.0f;
+  float amax = 0.0f;
+  for (int i = 0; i < BG_PD; i++) amax = fmaxf(amax, fabsf(r[i]));
+  if (amax < 1e-12f) return 0.0f;
+  float best = -FLT_MAX, best_delta = amax / h;
+  for (int s = 0; s < 24; s++) {
+    const float delta = amax / h * (0.3f + 0.035f * (float)s);
+    float dot = 0.0f, n2 = 0.0f;
+    for (int i = 0; i < BG_PD; i++) {
+      const float w = (float)bg_level(r[i], delta, h, top) - h;
+      dot += r[i] * w;
+      n2 += w * w;
+    }
+    const float cosv = dot / sqrtf(n2);
+    if (cosv > best) {
+      best = cosv;
+      best_delta = delta;
+    }
+  }
+  float rr = 0.0f, dot = 0.0f;
+  for (int i = 0; i < BG_PD; i++) {
+    const uint32_t u = bg_level(r[i], best_delta, h, top);
+    for (uint32_t p = 0; p + 1 < bits; p++)
+      planes[p * BG_CODE + (i >> 3)] |= (uint8_t)(((u >> p) & 1u) << (i & 7));
+    rr += r[i] * r[i];
+    dot += r[i] * ((float)u - h);
+  }
+  return dot > 0.0f ? rr / dot : 0.0f;
+}
+
+/* Refiner::new / plane / estimate: src/bigann.rs:568-602. tab is [16][256]. */
+void or_bg_refiner_new(const float* qr, uint32_t bits, float* tab, float* off) {
+  for (int k = 0; k < BG_CODE; k++) {
+    float* t = tab + k * 256;
+    t[0] = 0.0f;
+    for (int v = 1; v < 256; v++) t[v] = t[v & (v - 1)] + qr[8 * k + __builtin_ctz((unsigned)v)];
+  }
+  const float h = (float)((1u << bits) - 1) / 2.0f;
+  float sum = NEG0;
+  for (int i = 0; i < BG_PD; i++) sum += qr[i];
+  *off = h * sum;
+}
+
+static float bg_plane(const float* tab, const uint8_t* p) {
+  float s = NEG0;
+  for (int k = 0; k < BG_CODE; k++) s += tab[k * 256 + p[k]];
+  return s;
+}
+
+float or_bg_refiner_estimate(const float* tab, float off, uint32_t bits, const uint8_t* sign,
+                             const uint8_t* planes, float f) {
+  float u = (float)(1u << (bits - 1)) * bg_plane(tab, sign);
+  for (uint32_t p = 0; p + 1 < bits; p++) u += (float)(1u << p) * bg_plane(tab, planes + p * BG_CODE);
+  return f * (u - off);
+}
+
+/* The rotated, padded query: pad_rotate(rot, q as f32) (src/bigann.rs:243-248). */
+static void bg_rotated_query(const sg_bigann_arrays* ix, const int8_t* q, float* qr) {
+  for (int i = 0; i < BG_PD; i++) qr[i] = i < BG_D ? (float)q[i] : 0.0f;
+  or_rotation_apply(ix->rotation, BG_PD, qr);
+}
+
+/* Index::route: src/bigann.rs:660-678. Returns the probe count; dots gets <q, c> of every leaf. */
+uint32_t or_bg_route(const sg_bigann_arrays* ix, const int8_t* q, const sg_bigann_params* p,
+                     uint32_t* out_probe, float* out_probe_scores, float* dots) {
+  const uint32_t K = ix->k;
+  float qf[BG_D];
+  for (int i = 0; i < BG_D; i++) qf[i] = (float)q[i];
+  or_gemm_abt(qf, ix->leaves, 1, K, BG_D, dots);
+  uint32_t np = p->nprobe < K ? p->nprobe : K;
+  if (np == 0) return 0;
+  topk t;
+  topk_init(&t, np);
+  for (uint32_t c = 0; c < K; c++) {
+    float n = NEG0;
+    for (int i = 0; i < BG_D; i++) n += ix->leaves[(uint64_t)c * BG_D + i] * ix->leaves[(uint64_t)c * BG_D + i];
+    topk_push(&t, 2.0f * dots[c] - n, c);
+  }
+  uint32_t m = topk_sorted(&t);
+  uint32_t keep = m;
+  if (p->margin > 0.0f && m > 0) {
+    float qq = NEG0;
+    for (int i = 0; i < BG_D; i++) qq += qf[i] * qf[i];
+    const float lim = (qq - t.items[0].s) * (1.0f + p->margin);
+    keep = 0;
+    for (uint32_t i = 0; i < m; i++)
+      if (qq - t.items[i].s <= lim) t.items[keep++] = t.items[i];
+  }
+  for (uint32_t i = 0; i < keep; i++) {
+    out_probe[i] = t.items[i].id;
+    if (out_probe_scores) out_probe_scores[i] = t.items[i].s;
+  }
+  topk_free(&t);
+  return keep;
+}
+
+/* Index::candidates: src/bigann.rs:683-732, the leaves scanned in probe order (every record
+ * resident). Out: (id, estimate, |x|^2) best first. */
+uint32_t or_bg_candidates(const sg_bigann_arrays* ix, const int8_t* q, const uint32_t* probe,
+                          uint32_t nprobe, const float* dots, const sg_bigann_params* p,
+                          uint32_t* out_ids, float* out_est, float* out_nx, uint64_t* scanned) {
+  float qp[BG_PD], qr[BG_PD];
+  for (int i = 0; i < BG_PD; i++) qp[i] = i < BG_D ? (float)q[i] : 0.0f;
+  uint8_t tables[SG_BG_GROUPS * 16];
+  float scale, bias, a, b;
+  or_query_new(ix->rotation, BG_PD, qp, tables, &scale, &bias, &a, &b);
+  const uint32_t bits = ix->bits;
+  const int refine = bits > 1 && p->refine > 0;
+  float* rtab = NULL;
+  float roff = 0.0f;
+  if (refine) {
+    bg_rotated_query(ix, q, qr);
+    rtab = (float*)malloc(sizeof(float) * BG_CODE * 256);
+    or_bg_refiner_new(qr, bits, rtab, &roff);
+  }
+  const uint32_t extra = or_bg_extra(bits);
+  /* info: (id, estimate, |x|^2) of every admitted slot, indexed by admission order */
+  uint64_t info_cap = 1024, ninfo = 0;
+  uint32_t* info_id = (uint32_t*)malloc(sizeof(uint32_t) * info_cap);
+  float* info_est = (float*)malloc(sizeof(float) * info_cap);
+  float* info_nx = (float*)malloc(sizeof(float) * info_cap);
+  const uint32_t kc = refine ? (p->refine > p->cand ? p->refine : p->cand) : p->cand;
+  topk cand, best;
+  topk_init(&cand, kc);
+  topk_init(&best, p->cand);
+  uint64_t sc_total = 0;
+  uint8_t sign[BG_CODE];
+  for (uint32_t i = 0; i < nprobe; i++) {
+    const uint32_t c = probe[i];
+    const float cent = dots[c];
+    const uint64_t b0 = ix->block_off[c], b1 = ix->block_off[c + 1];
+    for (uint64_t blk = b0; blk < b1; blk++) {
+      uint16_t scores[SG_BLOCK];
+      or_scan(tables, SG_BG_GROUPS, ix->blocks + blk * BG_BB, 1, scores);
+      for (uint32_t j = 0; j < SG_BLOCK; j++) {
+        const uint64_t s = blk * SG_BLOCK + j;
+        const uint32_t id = ix->ids[s];
+        if (id == SG_PAD) continue;
+        const float mul = ix->factors[2 * s], nx = ix->factors[2 * s + 1];
+        const float est = 2.0f * (cent + mul * (a * (float)scores[j] + b)) - nx;
+        if (!topk_admits(&cand, est, (uint32_t)ninfo)) continue;
+        topk_push(&cand, est, (uint32_t)ninfo);
+        float e = est;
+        if (refine) {
+          or_unpack_slot(ix->blocks + blk * BG_BB, SG_BG_GROUPS, j, sign);
+          const uint8_t* ex = ix->ext + s * extra;
+          float fs;
+          memcpy(&fs, ex + extra - 4, 4);
+          e = 2.0f * (cent + or_bg_refiner_estimate(rtab, roff, bits, sign, ex, fs)) - nx;
+          topk_push(&best, e, (uint32_t)ninfo);
+        }
+        if (ninfo == info_cap) {
+          info_cap *= 2;
+          info_id = (uint32_t*)realloc(info_id, sizeof(uint32_t) * info_cap);
+          info_est = (float*)realloc(info_est, sizeof(float) * info_cap);
+          info_nx = (float*)realloc(info_nx, sizeof(float) * info_cap);
+        }
+        info_id[ninfo] = id;
+        info_est[ninfo] = e;
+        info_nx[ninfo] = nx;
+        ninfo++;
+      }
+    }
+    sc_total += (b1 - b0) * SG_BLOCK;
+  }
+  topk* top = refine ? &best : &cand;
+  uint32_t m = p->cand ? topk_sorted(top) : 0;
+  for (uint32_t i = 0; i < m; i++) {
+    const uint32_t x = top->items[i].id;
+    out_ids[i] = info_id[x];
+    out_est[i] = info_est[x];
+    out_nx[i] = info_nx[x];
+  }
+  if (scanned) *scanned = sc_total;
+  topk_free(&cand);
+  topk_free(&best);
+  free(info_id);
+  free(info_est);
+  free(info_nx);
+  free(rtab);
+  return m;
+}
+
+/* Index::rerank: src/bigann.rs:735-747: 2 <q, x> - |x|^2 from the base rows, TopK(k). */
+uint32_t or_bg_rerank(const sg_bigann_arrays* ix, const int8_t* q, const uint32_t* ids,
+                      const float* nx, uint32_t n, const sg_bigann_params* p, float* out_scores,
+                      uint32_t* out_ids) {
+  if (p->k == 0) return 0;
+  topk t;
+  topk_init(&t, p->k);
+  for (uint32_t i = 0; i < n; i++) {
+    const int32_t dot = or_dot_i8i8(q, ix->base + (uint64_t)ids[i] * BG_D, BG_D);
+    topk_push(&t, 2.0f * (float)dot - nx[i], ids[i]);
+  }
+  uint32_t m = topk_sorted(&t);
+  for (uint32_t i = 0; i < m; i++) {
+    out_scores[i] = t.items[i].s;
+    out_ids[i] = t.items[i].id;
+  }
+  topk_free(&t);
+  return m;
+}
+
+/* Index::search: src/bigann.rs:653-657. */
+uint32_t or_bg_search(const sg_bigann_arrays* ix, const int8_t* q, const sg_bigann_params* p,
+                      float* out_scores, uint32_t* out_ids, sg_bigann_timing* t) {
+  uint32_t* probe = (uint32_t*)malloc(sizeof(uint32_t) * (ix->k ? ix->k : 1));
+  float* dots = (float*)malloc(sizeof(float) * (ix->k ? ix->k : 1));
+  const uint32_t np = or_bg_route(ix, q, p, probe, NULL, dots);
+  const uint32_t cap = p->cand ? p->cand : 1;
+  uint32_t* cid = (uint32_t*)malloc(sizeof(uint32_t) * cap);
+  float* cest = (float*)malloc(sizeof(float) * cap);
+  float* cnx = (float*)malloc(sizeof(float) * cap);
+  uint64_t scanned = 0;
+  const uint32_t n = or_bg_candidates(ix, q, probe, np, dots, p, cid, cest, cnx, &scanned);
+  const uint32_t k = or_bg_rerank(ix, q, cid, cnx, n, p, out_scores, out_ids);
+  if (t) {
+    t->probes += np;
+    t->scanned += scanned;
+  }
+  free(probe);
+  free(dots);
+  free(cid);
+  free(cest);
+  free(cnx);
+  return k;
+}
+
+uint64_t or_bg_search_batch(const sg_bigann_arrays* ix, uint32_t nq, const int8_t* q,
+                            const sg_bigann_params* p, int threads, float* out_scores,
+                            uint32_t* out_ids, uint32_t* out_counts) {
+  uint64_t scanned = 0;
+  if (threads < 1) threads = 1;
+#pragma omp parallel for schedule(dynamic, 4) num_threads(threads) reduction(+ : scanned)
+  for (int64_t i = 0; i < (int64_t)nq; i++) {
+    sg_bigann_timing t;
+    memset(&t, 0, sizeof t);
+    out_counts[i] = or_bg_search(ix, q + (uint64_t)i * BG_D, p, out_scores + (uint64_t)i * p->k,
+                                 out_ids + (uint64_t)i * p->k, &t);
+    scanned += t.scanned;
+  }
+  return scanned;
+}

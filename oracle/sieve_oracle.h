@@ -17,7 +17,7 @@
  *   Index::route/candidates/rerank/search .. src/ivf.rs:543-832
  *   filter::Filter/Plan/search ............. src/filter.rs:27-110
  *   recall_at .............................. src/eval.rs:7-10
- *   bigann route/candidates/rerank/Refiner . src/bigann.rs:65-108, :568-602, :660-747
+ *   bigann refine_encode/Refiner/route/candidates/rerank src/bigann.rs:65-108, :568-602, :653-747
  *
  * Floating point follows the Rust code operation for operation: f32 throughout, no FMA
  * contraction (built with -ffp-contract=off), sums sequential from -0.0 as Rust's
@@ -117,6 +117,28 @@ uint32_t or_filter_search(const sg_ivf_arrays* ix, const uint64_t* allow, uint64
                           int plan, uint64_t expand_target, const float* q768,
                           const float* q256, const sg_params* p, float* out_scores,
                           uint32_t* out_ids);
+
+/* bigann.rs: refinement codes, routing, candidates, rerank, search (src/bigann.rs:65-108,
+ * :568-602, :653-747). The scan visits the probed leaves in probe order, as Postings::fetch_each
+ * does when every record is resident (src/postings.rs:287-317). */
+uint32_t or_bg_extra(uint32_t bits);
+float or_bg_refine_encode(const float* r, uint32_t bits, uint8_t* planes);
+void or_bg_refiner_new(const float* qr, uint32_t bits, float* tab, float* off);
+float or_bg_refiner_estimate(const float* tab, float off, uint32_t bits, const uint8_t* sign,
+                             const uint8_t* planes, float f);
+uint32_t or_bg_route(const sg_bigann_arrays* ix, const int8_t* q, const sg_bigann_params* p,
+                     uint32_t* out_probe, float* out_probe_scores, float* dots);
+uint32_t or_bg_candidates(const sg_bigann_arrays* ix, const int8_t* q, const uint32_t* probe,
+                          uint32_t nprobe, const float* dots, const sg_bigann_params* p,
+                          uint32_t* out_ids, float* out_est, float* out_nx, uint64_t* scanned);
+uint32_t or_bg_rerank(const sg_bigann_arrays* ix, const int8_t* q, const uint32_t* ids,
+                      const float* nx, uint32_t n, const sg_bigann_params* p, float* out_scores,
+                      uint32_t* out_ids);
+uint32_t or_bg_search(const sg_bigann_arrays* ix, const int8_t* q, const sg_bigann_params* p,
+                      float* out_scores, uint32_t* out_ids, sg_bigann_timing* t);
+uint64_t or_bg_search_batch(const sg_bigann_arrays* ix, uint32_t nq, const int8_t* q,
+                            const sg_bigann_params* p, int threads, float* out_scores,
+                            uint32_t* out_ids, uint32_t* out_counts);
 
 double or_recall_at(uint32_t k, const uint32_t* got, uint32_t ngot, const uint32_t* truth,
                     uint32_t ntruth);

@@ -52,3 +52,29 @@ def index_b():
     rows /= np.linalg.norm(rows, axis=1, keepdims=True)
     q768 = np.concatenate([q, rows]).astype(np.float32)
     return arrays, q768, prefixes(q768), mix
+
+
+@functools.lru_cache(maxsize=None)
+def bigann_a(bits: int):
+    """bigann: 20,000 int8 rows (64 mixture centres) plus 200 exact duplicates, 8 x 16 leaves;
+    64 queries from the mixture and 16 copies of base rows."""
+    from sieve_gpu import bigann_builder as BB
+
+    sp = BB.Spacev(20000, 64, seed=5, device="cpu")
+    base = sp.rows(0, 20000)
+    base = torch.cat([base, base[:200]])
+    ix = BB.build_bigann(base, 8, 16, bits=bits, sample_n=20200, iters=6)
+    q = torch.cat([sp.queries(64), base[1000:1016]]).numpy()
+    return ix, q
+
+
+@functools.lru_cache(maxsize=None)
+def bigann_b():
+    """bigann with few, large leaves (2 x 4 of about 5,000 slots): scan steps span whole chunks
+    and the shortlist compacts many times inside one leaf."""
+    from sieve_gpu import bigann_builder as BB
+
+    sp = BB.Spacev(40000, 16, seed=9, device="cpu")
+    base = sp.rows(0, 40000)
+    ix = BB.build_bigann(base, 2, 4, bits=3, sample_n=40000, iters=5)
+    return ix, sp.queries(24).numpy()
