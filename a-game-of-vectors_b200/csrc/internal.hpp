@@ -108,6 +108,12 @@ struct Workspace {
   uint32_t* out_n = nullptr;
   uint64_t* allow = nullptr;     // [allow_words]
   uint64_t allow_cap = 0;
+  // Per-query allow bitsets (the serving loop batches queries with different filters): when
+  // per_query_allow is set the scans read allow_q[q] / allow_wq[q] instead of the call's bitset.
+  const uint64_t** allow_q = nullptr;  // [allow_q_cap] device pointers
+  uint64_t* allow_wq = nullptr;        // [allow_q_cap] words of each
+  uint64_t allow_q_cap = 0;
+  bool per_query_allow = false;
   float* brute = nullptr;        // [brute_cap] exact scores of the filter plan Brute
   uint64_t brute_cap = 0;
   void* host_pinned = nullptr;   // pinned staging for host<->device copies
@@ -222,4 +228,38 @@ void launch_top_list(const float* sc, const uint32_t* id, const uint32_t* n_in, 
 void launch_dot_i8i8(const int8_t* q, const int8_t* rows, uint64_t nrows, uint32_t dim,
                      int32_t* out, cudaStream_t st);
 
+}  // namespace sg
+
+// An open IVF index: its arrays in HBM, the default execution context of sg_search, and the
+// tuning of its kernels.
+struct sg_index {
+  sg::DevIndex ix;
+  sg::Ctx def;  // the context of sg_search / sg_search_device
+  sg::Config cfg;
+  std::mutex mu;
+  int sms = 148;
+  bool timing_on = false;
+};
+
+// filter::Filter (src/filter.rs:18-25) resident on its index's device.
+struct sg_filter {
+  sg_index* h = nullptr;
+  uint64_t words = 0;
+  uint64_t* allow = nullptr;        // [words] the allow bitset
+  uint32_t* rows = nullptr;         // [nrows] allowed rows, ascending
+  uint64_t nrows = 0;
+  uint32_t* per_cluster = nullptr;  // [k] allowed slots per cluster
+};
+
+namespace sg {
+// Execution-context entry points (sieve_gpu.cu) for the serving loop: grow c's scratch for a
+// batch, launch the whole pipeline on the queries already staged in c.ws (no host sync), run one
+// query synchronously (host queries, device allow bitset), and the scratch bytes of a batch.
+int ctx_prepare(sg_index* h, Ctx& c, uint32_t nq, const sg_params& p);
+int ctx_launch(sg_index* h, Ctx& c, uint32_t nq, const sg_params& p, bool have_q256);
+int ctx_search_one(sg_index* h, Ctx& c, const float* q768, const float* q256, const sg_params& p,
+                   const uint64_t* d_allow, uint64_t allow_words, float* out_sc, uint32_t* out_id,
+                   uint32_t* out_n);
+uint64_t ctx_bytes(const sg_index* h, const sg_params& p, uint32_t nq);
+void free_ctx(Ctx& c);
 }  // namespace sg

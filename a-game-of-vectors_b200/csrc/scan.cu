@@ -45,6 +45,8 @@ struct ScanArgs {
   uint32_t cand;
   const uint64_t* allow;
   uint64_t allow_words;
+  const uint64_t* const* allow_q;  // per-query allow bitsets (null entries: no filter), or null
+  const uint64_t* allow_wq;
 };
 
 SG_DEV uint4 ldg_nc(const uint4* p) {
@@ -172,6 +174,8 @@ SG_DEV void scan_segments(const ScanArgs& a, uint32_t q, const Segs& S, uint32_t
   __syncthreads();
   // ---- admission ------------------------------------------------------------------------------
   const uint32_t thr = ld_cg(a.thr + q);
+  const uint64_t* al = a.allow_q ? a.allow_q[q] : a.allow;
+  const uint64_t aw = a.allow_q ? a.allow_wq[q] : a.allow_words;
   const uint32_t nloc = NB * SG_BLOCK;
   const uint32_t per = (nloc + blockDim.x - 1) / blockDim.x;  // <= 64 slots per thread
   const uint32_t i0 = tid * per, i1 = min(nloc, i0 + per);
@@ -183,7 +187,7 @@ SG_DEV void scan_segments(const ScanArgs& a, uint32_t q, const Segs& S, uint32_t
   for (uint32_t i = i0; i < i1; i++) {
     const uint32_t k = s_key[i];
     bool surv = k != 0u && k >= thr;
-    if (surv && a.allow) surv = allowed(a.allow, a.allow_words, a.ids[slot_of(i)]);
+    if (surv && al) surv = allowed(al, aw, a.ids[slot_of(i)]);
     if (!surv) s_key[i] = 0u;
     cnt += surv;
   }
@@ -319,6 +323,8 @@ void launch_scan(const DevIndex& ix, Workspace& w, uint32_t nq, const sg_params&
   a.cand = p.cand;
   a.allow = allow;
   a.allow_words = allow_words;
+  a.allow_q = w.per_query_allow ? w.allow_q : nullptr;
+  a.allow_wq = w.allow_wq;
   static bool attr = false;
   if (!attr) {
     cudaFuncSetAttribute(k_scan_seed, cudaFuncAttributeMaxDynamicSharedMemorySize,

@@ -155,6 +155,8 @@ struct MmaArgs {
   uint8_t* overflow;
   const uint64_t* allow;
   uint64_t allow_words;
+  const uint64_t* const* allow_q;  // per-query allow bitsets (null entries: no filter), or null
+  const uint64_t* allow_wq;
 };
 
 // Per warp, two shared-memory stages of one block each: its 256 code words (1 KB) and its 32
@@ -296,8 +298,10 @@ __global__ void __launch_bounds__(256, 2) k_scan_mma(MmaArgs a) {
               const uint32_t key = ord(est);
               if (key >= s_thr[qi]) {
                 const uint32_t gslot = b * SG_BLOCK + slot;
-                if (!a.allow || allowed(a.allow, a.allow_words, a.ids[gslot])) {
-                  const uint32_t q = s_q[qi];
+                const uint32_t q = s_q[qi];
+                const uint64_t* al = a.allow_q ? a.allow_q[q] : a.allow;
+                const uint64_t aw = a.allow_q ? a.allow_wq[q] : a.allow_words;
+                if (!al || allowed(al, aw, a.ids[gslot])) {
                   const uint32_t pos = atomicAdd(a.ccount + q, 1u);
                   if (pos < a.cap) {
                     a.cbuf_est[(size_t)q * a.cap + pos] = __float_as_uint(est);
@@ -349,6 +353,8 @@ int launch_scan_mma(const DevIndex& ix, Workspace& w, uint32_t nq, const sg_para
   a.overflow = w.overflow;
   a.allow = allow;
   a.allow_words = allow_words;
+  a.allow_q = w.per_query_allow ? w.allow_q : nullptr;
+  a.allow_wq = w.allow_wq;
   static bool attr = false;
   const int smem = kQG * kBStride + 8 * 2 * kStageWords * 4;
   if (!attr) {

@@ -18,25 +18,6 @@
 
 #include "internal.hpp"
 
-struct sg_index {
-  sg::DevIndex ix;
-  sg::Ctx def;  // the context of sg_search / sg_search_device
-  sg::Config cfg;
-  std::mutex mu;
-  int sms = 148;
-  bool timing_on = false;
-};
-
-// filter::Filter (src/filter.rs:18-25) resident on its index's device.
-struct sg_filter {
-  sg_index* h = nullptr;
-  uint64_t words = 0;
-  uint64_t* allow = nullptr;        // [words] the allow bitset
-  uint32_t* rows = nullptr;         // [nrows] allowed rows, ascending
-  uint64_t nrows = 0;
-  uint32_t* per_cluster = nullptr;  // [k] allowed slots per cluster
-};
-
 namespace sg {
 
 std::string& last_error() {
@@ -110,6 +91,9 @@ void free_index(sg::DevIndex& x) {
 }
 
 void free_ws(sg::Workspace& w) {
+  dfree(w.allow_q);
+  dfree(w.allow_wq);
+  w.allow_q_cap = 0;
   dfree(w.brute);
   w.brute_cap = 0;
   dfree(w.q768);
@@ -836,6 +820,44 @@ const DevIndex* index_arrays(const sg_index* h) { return &h->ix; }
 const Config* index_config(const sg_index* h) { return &h->cfg; }
 int index_sms(const sg_index* h) { return h->sms; }
 int index_check_params(const sg_index* h, const sg_params* p) { return check_params(h, p); }
+
+// ---- execution-context entry points for the serving loop (serve.cu) -------------------------
+int ctx_prepare(sg_index* h, Ctx& c, uint32_t nq, const sg_params& p) {
+  int rc;
+  if ((rc = check_params(h, &p))) return rc;
+  CK(cudaSetDevice(h->ix.device));
+  return ensure_ws(h, c, nq, p, batch_cap(h, p, nq));
+}
+
+int ctx_launch(sg_index* h, Ctx& c, uint32_t nq, const sg_params& p, bool have_q256) {
+  return run_pipeline(h, c, nq, p, have_q256, nullptr, 0, kToSearch, false);
+}
+
+int ctx_search_one(sg_index* h, Ctx& c, const float* q768, const float* q256, const sg_params& p,
+                   const uint64_t* d_allow, uint64_t allow_words, float* out_sc, uint32_t* out_id,
+                   uint32_t* out_n) {
+  return search_impl(h, c, 1, q768, q256, p, d_allow, allow_words, out_sc, out_id, out_n, nullptr,
+                     false, true);
+}
+
+void free_ctx(Ctx& c) {
+  if (c.stream) cudaStreamSynchronize(c.stream);
+  drop_graphs(c);
+  free_ws(c.ws);
+  if (c.stream) cudaStreamDestroy(c.stream);
+  c.stream = nullptr;
+}
+
+// Device scratch of a batch of nq queries with params p (the workspace ensure_ws grows to).
+uint64_t ctx_bytes(const sg_index* h, const sg_params& p, uint32_t nq) {
+  const uint64_t P = std::min<uint32_t>(p.nprobe, h->ix.k);
+  const uint64_t cap = batch_cap(h, p, nq);
+  const uint64_t per_q = SG_DIM * 4 * 2 + SG_PDIM * 5 + 1024 + 64 + (uint64_t)h->ix.k * 4 + P * 16 +
+                         cap * 12 + (uint64_t)std::max<uint32_t>(p.cand, 1) * 20 +
+                         (uint64_t)std::max<uint32_t>(p.k, 1) * 8 + 64;
+  const uint64_t items = (uint64_t)h->ix.h_chunks_desc_prefix[P] * 16;
+  return (uint64_t)nq * (per_q + items) + (uint64_t)h->ix.k * 16 + 4096;
+}
 }  // namespace sg
 
 extern "C" {

@@ -248,6 +248,11 @@ EXPORTS = [
     "sg_filter_free",
     "sg_plan_resolve",
     "sg_filter_search",
+    "sg_server_start",
+    "sg_server_submit",
+    "sg_server_poll",
+    "sg_server_get_stats",
+    "sg_server_stop",
     "sg_open_bigann",
     "sg_open_bigann_arrays",
     "sg_close_bigann",

@@ -112,6 +112,13 @@ class BigannIndex:
             timing.add(t)
         return sc[:, : p.k], ids[:, : p.k], cnt
 
+    def search_into(self, q: np.ndarray, params: BigannParams, out_scores: np.ndarray,
+                    out_ids: np.ndarray, out_counts: np.ndarray) -> None:
+        """sg_search_bigann into caller-owned host buffers (pinned buffers make the copies direct)."""
+        p = params.to_c()
+        check(lib().sg_search_bigann(self._h, c_uint32(q.shape[0]), ptr(q), byref(p), ptr(out_scores),
+                                     ptr(out_ids), ptr(out_counts), None))
+
     def search(self, q, params: BigannParams, timing: BigannTiming | None = None):
         """One query: list of (score, row) best first, like bigann::Index::search."""
         sc, ids, cnt = self.search_batch(np.asarray(q)[None], params, timing)

@@ -118,21 +118,28 @@ def train(base: torch.Tensor, k1: int, k2: int, sample_n: int, iters: int = 8) -
 
 def assign(model: dict, x: torch.Tensor) -> torch.Tensor:
     """Model::assign (src/bigann.rs:263-290): best leaf among the children of the row's
-    TOP_COARSE nearest coarse cells."""
+    TOP_COARSE nearest coarse cells, one dense product per (coarse cell, rows choosing it)."""
     k2 = model["k2"]
     leaves = model["leaves"]
     ln = (leaves * leaves).sum(1)
     top = _nearest(x, model["coarse"], min(TOP_COARSE, model["coarse"].shape[0]))[0]  # [n, T]
-    best_s = torch.full((x.shape[0],), -float("inf"), device=x.device)
-    best_l = torch.zeros(x.shape[0], dtype=torch.int64, device=x.device)
+    n = x.shape[0]
+    best_s = torch.full((n,), -float("inf"), device=x.device)
+    best_l = torch.zeros(n, dtype=torch.int64, device=x.device)
     for t in range(top.shape[1]):
         cell = top[:, t]
-        cand = cell[:, None] * k2 + torch.arange(k2, device=x.device)[None, :]  # [n, k2]
-        sc = 2.0 * torch.einsum("nd,nkd->nk", x, leaves[cand]) - ln[cand]
-        v, j = sc.max(1)
-        better = v > best_s
-        best_s = torch.where(better, v, best_s)
-        best_l = torch.where(better, cand.gather(1, j[:, None])[:, 0], best_l)
+        order = torch.argsort(cell)
+        counts = torch.bincount(cell, minlength=model["coarse"].shape[0]).cpu().numpy()
+        start = 0
+        for c in np.nonzero(counts)[0]:
+            rows = order[start:start + counts[c]]
+            start += counts[c]
+            lv = leaves[c * k2:(c + 1) * k2]
+            sc = 2.0 * (x[rows] @ lv.T) - ln[c * k2:(c + 1) * k2]
+            v, j = sc.max(1)
+            better = v > best_s[rows]
+            best_s[rows] = torch.where(better, v, best_s[rows])
+            best_l[rows] = torch.where(better, j + c * k2, best_l[rows])
     return best_l
 
 
@@ -251,18 +258,26 @@ def build_bigann(base: torch.Tensor, k1: int, k2: int, bits: int = 2, sample_n: 
 
 
 def ground_truth(base: torch.Tensor, queries: torch.Tensor, k: int = 10, chunk: int = 1 << 20):
-    """Exact top-k rows by 2<q,x> - |x|^2 (integer-exact in f64), ties by ascending row."""
-    q = queries.double()
-    best_v = torch.full((q.shape[0], k), -float("inf"), dtype=torch.float64, device=q.device)
+    """Exact top-k rows by 2<q,x> - |x|^2, ties by ascending row: (ids [nq, k], scores [nq, k]).
+    Products and sums of int8 values stay below 2^24, so f32 (TF32 off) computes them exactly."""
+    q = queries.float()
+    best_v = torch.full((q.shape[0], k), -float("inf"), device=q.device)
     best_i = torch.zeros((q.shape[0], k), dtype=torch.int64, device=q.device)
-    for s in range(0, base.shape[0], chunk):
-        x = base[s:s + chunk].to(q.device).double()
-        sc = 2.0 * (q @ x.T) - (x * x).sum(1)[None, :]
-        v, i = torch.topk(sc, min(k, sc.shape[1]), dim=1)
-        allv = torch.cat((best_v, v), 1)
-        alli = torch.cat((best_i, i + s), 1)
-        tv, ti = torch.topk(allv, k, dim=1)
-        best_v, best_i = tv, alli.gather(1, ti)
+    prev = torch.backends.cuda.matmul.allow_tf32
+    torch.backends.cuda.matmul.allow_tf32 = False
+    try:
+        for s in range(0, base.shape[0], chunk):
+            x = base[s:s + chunk].to(q.device).float()
+            sc = 2.0 * (q @ x.T) - (x * x).sum(1)[None, :]
+            v, i = torch.topk(sc, min(k, sc.shape[1]), dim=1)
+            allv = torch.cat((best_v, v), 1)
+            alli = torch.cat((best_i, i + s), 1)
+            order = torch.argsort(alli, dim=1, stable=True)
+            allv, alli = allv.gather(1, order), alli.gather(1, order)
+            tv, ti = torch.sort(allv, dim=1, descending=True, stable=True)
+            best_v, best_i = tv[:, :k], alli.gather(1, ti[:, :k])
+    finally:
+        torch.backends.cuda.matmul.allow_tf32 = prev
     return best_i.cpu().numpy().astype(np.uint32), best_v.cpu().numpy()
 
 

@@ -7,6 +7,8 @@ not available; shapes, sizes and noise model as the workloads name them):
   c1  1M x 768, 1024 centres, 1024 clusters, SOAR, 10k queries   (the reference's CPU-sized case)
   c2  18.4M x 768, 16384 centres, 4096 clusters, SOAR + 2-bit tier, 50k queries   (default)
   c3  113.5M x 768, 65536 centres, 16384 clusters, SOAR + 2-bit tier, 100k queries (~105 GB HBM)
+  c4  bigann L2: int8 x 100 rows (100M by default, --rows up to the 1B shape), 131,072 leaves
+      (512 x 256), 2-bit refinement, 64 probes, 10k queries
 
 One step = one batch of queries through the whole path (route, scan, cut, rerank) with the
 inputs resident in HBM (sg_search_device). `e2e` runs the same batches through the host API
@@ -37,7 +39,12 @@ WORKLOADS = {
     "c1": dict(n=1_000_000, centers=1024, k=1024, queries=10_000, search="32:1000:full"),
     "c2": dict(n=18_400_000, centers=16384, k=4096, queries=50_000, search="32:2000:full"),
     "c3": dict(n=113_500_000, centers=65536, k=16384, queries=100_000, search="64:1000:full"),
+    # billion-scale L2 (bigann): 512 x 256 = 131,072 leaves, 2-bit refinement. The bench default
+    # is a 100M-row cut of the 1B shape (--rows sets it): the 1B build does not fit the run's time.
+    "c4": dict(n=100_000_000, centers=131072, k1=512, k2=256, bits=2, queries=10_000,
+               search="64:300:2000"),
 }
+BG_SCAN_BYTES_PER_SLOT = 24  # 16 B code + 8 B [mul, |x|^2] per scanned slot
 SCAN_BYTES_PER_SLOT = 40  # 32 B code + 8 B [mul, err] factors per scanned slot
 
 
@@ -191,6 +198,63 @@ def cpu_reference(arrays, q768_host: np.ndarray, params, seconds: float, threads
     return {"qps": n / dt, "queries": n, "seconds": dt, "ids": o, "cnt": c}
 
 
+def serve_load(index, arrays, queries_host: np.ndarray, params, rates, seconds: float, seed: int = 7):
+    """Open-loop Poisson arrivals into the serving loop (continuous batching): for each rate, the
+    achieved QPS and the p50/p99 latency from submit to results on the host. One request in ten
+    carries a filter (allowlists of 30%, 3% and 0.3% of the rows, seeded)."""
+    from sieve_gpu import Server
+    from sieve_gpu import filter as F
+    from sieve_gpu.index import allow_bitset
+
+    n = int(arrays["n"])
+    rng = np.random.default_rng(seed)
+    sys.setswitchinterval(0.0002)  # the spinning submitter must not starve the collector
+    filters = [F.Filter(allow_bitset(np.nonzero(rng.random(n) < f)[0], n), index) for f in (0.3, 0.03, 0.003)]
+    out = []
+    try:
+        for rate in rates:
+            srv = Server(index, max_batch=2048, contexts=3)
+            nreq = int(rate * seconds)
+            gaps = rng.exponential(1.0 / rate, nreq)
+            which = rng.integers(0, queries_host.shape[0], nreq)
+            filt = rng.random(nreq) < 0.1
+            fsel = rng.integers(0, len(filters), nreq)
+            tickets = [None] * nreq
+            lat = np.zeros(nreq)
+            t_sub = np.zeros(nreq)
+
+            def collector():
+                for i in range(nreq):
+                    while tickets[i] is None:
+                        time.sleep(0)
+                    r = srv.poll(tickets[i], wait_ms=-1)
+                    lat[i] = r[2].queue_ms + r[2].service_ms  # the library's own clock
+
+            th = threading.Thread(target=collector)
+            th.start()
+            t0 = time.perf_counter()
+            due = t0
+            for i in range(nreq):
+                due += gaps[i]
+                while time.perf_counter() < due:
+                    pass
+                t_sub[i] = time.perf_counter()
+                tickets[i] = srv.submit(queries_host[which[i]], None, params,
+                                        filters[fsel[i]] if filt[i] else None)
+            th.join()
+            wall = time.perf_counter() - t0
+            st = srv.stats()
+            srv.stop()
+            out.append({"offered_qps": rate, "achieved_qps": nreq / wall, "p50_ms": float(np.percentile(lat, 50)),
+                        "p99_ms": float(np.percentile(lat, 99)), "requests": nreq,
+                        "mean_batch": st["queries_batched"] / max(st["batches"], 1), "retried": st["retried"]})
+            log(f"serve {rate}/s: {out[-1]}")
+    finally:
+        for f in filters:
+            f.close()
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -205,6 +269,9 @@ def main():
     ap.add_argument("--eval", type=int, default=1000, help="queries with exact ground truth")
     ap.add_argument("--plain", type=int, default=512, help="queries timed one per launch")
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
+    ap.add_argument("--serve", default="20000,50000,100000",
+                    help="Poisson arrival rates (queries/s) for the serving loop; empty: skip")
+    ap.add_argument("--serve-seconds", type=float, default=2.0)
     args = ap.parse_args()
 
     rank = int(os.environ.get("RANK", "0"))
@@ -218,6 +285,9 @@ def main():
     dev = f"cuda:{local}"
     if args.impl == "reference" and rank != 0:
         return finish(world)
+
+    if args.workload == "c4":
+        return main_bigann(args, rank, world, local, dev)
 
     from sieve_gpu import Index, parse_config
 
@@ -347,6 +417,11 @@ def main():
             e2e_s.append(time.perf_counter() - t)
     e2e_qps = world * args.steps * B / float(np.sum(e2e_s))
 
+    serving = None
+    if args.serve:
+        rates = [float(x) for x in args.serve.split(",") if x]
+        serving = serve_load(index, arrays, queries.cpu().numpy(), params, rates, args.serve_seconds)
+
     cpu = None
     if rank == 0 and world == 1 and args.cpu_seconds > 0:
         r = cpu_reference(arrays, queries[: max(args.eval, 256)].cpu().numpy(), params, args.cpu_seconds,
@@ -367,6 +442,10 @@ def main():
         "plain": {"qps": float(1e3 / np.mean(plain_ms)), "p50_ms": float(np.percentile(plain_ms, 50)),
                   "p99_ms": float(np.percentile(plain_ms, 99)), "queries": int(plain_ms.size)},
         "stage_ms": stage,
+        "serving": serving,
+        "serving_note": "continuous batching (sg_server, 3 contexts): open-loop Poisson arrivals from a "
+                        "Python client, 10% filtered; latency = sg_server_submit to results on the "
+                        "host, on the library's clock",
         "scanned_per_query": float(np.mean(scanned) / B),
         "roofline": {"bound": "hbm", "kernel": "k_scan_seed + k_scan_mma (the scan stage)",
                      "achieved": achieved, "peak": peak,
@@ -377,6 +456,184 @@ def main():
         "e2e": {"value": e2e_qps, "unit": "queries/s", "h2d_bytes_per_step": B * 768 * 4,
                 "d2h_bytes_per_step": B * params.k * 8 + B * 4},
         "gpu_launches": int(sum(s["launches"] for s in stats)),
+        "clocks": clocks.summary(),
+    }
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    index.close()
+    return finish(world)
+
+
+# ---- bigann (billion-scale L2 over int8 rows) ----------------------------------------------------
+def recall10_ties(ids, cnt, gt_ids, gt_sc) -> tuple[float, float]:
+    """big-ann recall@10 with ties (any true row at most as far as the 10th nearest) and strict
+    recall@10 (src/bin/spacev.rs:108-119)."""
+    rt, rs = [], []
+    for i in range(gt_ids.shape[0]):
+        got = [int(x) for x in ids[i, : min(10, int(cnt[i]))]]
+        cut = gt_sc[i, 9]
+        ok = set(int(x) for x, sc in zip(gt_ids[i], gt_sc[i]) if sc >= cut)
+        rt.append(sum(g in ok for g in got) / 10.0)
+        rs.append(sum(g in set(int(x) for x in gt_ids[i, :10]) for g in got) / 10.0)
+    return float(np.mean(rt)), float(np.mean(rs))
+
+
+def main_bigann(args, rank: int, world: int, local: int, dev: str):
+    from sieve_gpu import bigann_builder as BB
+    from sieve_gpu.bigann import BigannIndex, BigannTiming, parse_config as bg_parse
+
+    wl = dict(WORKLOADS["c4"])
+    if args.rows:
+        wl["n"] = args.rows
+    config = args.config or wl["search"]
+    params = bg_parse(config, 10)
+    nq_pool = min(max(args.batch * 2, args.eval, args.plain), wl["queries"])
+    t0 = time.time()
+    sp = BB.Spacev(wl["n"], wl["centers"], spread=40.0, sigma=12.0, seed=1, device=dev)
+    base = sp.rows(0, wl["n"])
+    t_ingest = time.time() - t0
+    arrays = BB.build_bigann(base, wl["k1"], wl["k2"], bits=wl["bits"],
+                             sample_n=min(wl["n"], max(2_000_000, wl["n"] // 10)), iters=6)
+    t_build = time.time() - t0 - t_ingest
+    queries = sp.queries(nq_pool)
+    gt_ids, gt_sc = BB.ground_truth(base, queries[: args.eval], k=100)
+    del base
+    torch.cuda.empty_cache()
+    log(f"workload c4: n={wl['n']} leaves={arrays['k']} ingest {t_ingest:.1f}s build {t_build:.1f}s "
+        f"leaf sizes mean {arrays['sizes'].mean():.0f} max {arrays['sizes'].max()}")
+    threads = os.cpu_count() or 1
+    cfg = {"workload": f"c4: {wl['n']} x 100 int8 (1B shape cut to {wl['n']} rows), "
+                       f"{wl['centers']} centres, {wl['k1']}x{wl['k2']} leaves, {wl['bits']}-bit refine",
+           "search": config, "batch": args.batch, "queries_pool": nq_pool,
+           "l2": "inputs larger than L2 (records and base far above 126 MB)",
+           "ingest_s": round(t_ingest, 1), "build_s": round(t_build, 1)}
+    metric = "QPS at R@10>=0.90 (p50/p99 ms, scan GB/s vs HBM peak)"
+    qh_all = queries.cpu().numpy()
+
+    def cpu_ref(seconds: float):
+        import oracle as O
+
+        ob = O.OracleBigann(arrays, native=True)
+        p = params.to_c()
+        probe = min(qh_all.shape[0], max(threads * 4, 64))
+        t = time.perf_counter()
+        ob.search_batch(qh_all[:probe], p, threads=threads)
+        per_q = (time.perf_counter() - t) / probe
+        n = int(min(qh_all.shape[0], max(probe, seconds / max(per_q, 1e-9))))
+        t = time.perf_counter()
+        s_, o_, c_, _ = ob.search_batch(qh_all[:n], p, threads=threads)
+        dt = time.perf_counter() - t
+        return {"qps": n / dt, "queries": n, "seconds": dt, "ids": o_, "cnt": c_}
+
+    if args.impl == "reference":
+        times, res = [], None
+        for i in range(args.warmup + args.steps):
+            res = cpu_ref(args.cpu_seconds / max(args.steps, 1))
+            if i >= args.warmup:
+                times.append(res["qps"])
+        qps = float(np.mean(times))
+        m = min(res["ids"].shape[0], gt_ids.shape[0])
+        rec, rec_strict = recall10_ties(res["ids"][:m], res["cnt"][:m], gt_ids[:m], gt_sc[:m])
+        line = {"metric": metric, "impl": "reference", "value": qps, "unit": "queries/s", "n_gpus": world,
+                "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "i8/u8/f32", "data": "synthetic", "config": cfg,
+                "recall_at_10": rec, "recall_at_10_strict": rec_strict,
+                "cpu_baseline": {"value": qps, "unit": "queries/s", "cores": threads, "kind": "port",
+                                 "sample": f"{res['queries']} queries per step on {threads} threads"},
+                "e2e": {"value": qps, "unit": "queries/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+        print(json.dumps(line), flush=True)
+        return finish(world)
+
+    index = BigannIndex.from_arrays(arrays, device=local)
+    q = queries.to(dev).contiguous()
+    B = min(args.batch, nq_pool)
+    k = params.k
+    out_sc = torch.empty((B, k), dtype=torch.float32, device=dev)
+    out_id = torch.empty((B, k), dtype=torch.int32, device=dev)
+    out_n = torch.empty((B,), dtype=torch.int32, device=dev)
+    stream = torch.cuda.current_stream()
+    t_eval = BigannTiming()
+    sc, ids, cnt = index.search_batch(qh_all[: args.eval], params, t_eval)
+    rec, rec_strict = recall10_ties(ids, cnt, gt_ids, gt_sc)
+    log(f"{config}: recall@10 {rec:.4f} (ties), {rec_strict:.4f} (strict)")
+
+    def step(i):
+        lo = (i * B) % (nq_pool - B + 1)
+        index.search_device(B, q[lo].data_ptr(), params, out_sc.data_ptr(), out_id.data_ptr(),
+                            out_n.data_ptr(), stream.cuda_stream)
+
+    for i in range(args.warmup):
+        step(i)
+    torch.cuda.synchronize()
+    step_ms = []
+    with ClockSampler(local) as clocks:
+        torch.cuda.synchronize()
+        for i in range(args.steps):
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            step(args.warmup + i)
+            b.record(stream)
+            b.synchronize()
+            step_ms.append(a.elapsed_time(b))
+    total_ms = float(np.sum(step_ms))
+    qps = world * args.steps * B / (total_ms / 1e3)
+    # stage times of one timed batch (the scan kernel's share and its algorithmic bytes)
+    tb = BigannTiming()
+    index.search_batch(qh_all[:B], params, tb)
+    scan_s = tb.scan / 1e9
+    achieved = tb.scanned * BG_SCAN_BYTES_PER_SLOT / scan_s / 1e9 if scan_s > 0 else None
+    peaks = measured_peaks()
+    peak = peaks.get("hbm_gbs", 6650.0)
+    plain_ms = []
+    for i in range(args.plain):
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        index.search_device(1, q[i].data_ptr(), params, out_sc.data_ptr(), out_id.data_ptr(),
+                            out_n.data_ptr(), stream.cuda_stream)
+        b.record(stream)
+        b.synchronize()
+        plain_ms.append(a.elapsed_time(b))
+    plain_ms = np.array(plain_ms[min(8, len(plain_ms) // 4):] or [float("nan")])
+    qh = torch.empty((B, 100), dtype=torch.int8).pin_memory()
+    osc = torch.empty((B, k), dtype=torch.float32).pin_memory()
+    oid = torch.empty((B, k), dtype=torch.int32).pin_memory()
+    ocn = torch.empty((B,), dtype=torch.int32).pin_memory()
+    e2e_s = []
+    for i in range(args.warmup + args.steps):
+        lo = (i * B) % (nq_pool - B + 1)
+        qh.copy_(queries[lo:lo + B].cpu())
+        t = time.perf_counter()
+        index.search_into(qh.numpy(), params, osc.numpy(), oid.numpy().view(np.uint32),
+                          ocn.numpy().view(np.uint32))
+        if i >= args.warmup:
+            e2e_s.append(time.perf_counter() - t)
+    e2e_qps = world * args.steps * B / float(np.sum(e2e_s))
+    cpu = None
+    if rank == 0 and world == 1 and args.cpu_seconds > 0:
+        r = cpu_ref(args.cpu_seconds)
+        cpu = {"value": r["qps"], "unit": "queries/s", "cores": threads, "kind": "port",
+               "sample": f"{r['queries']} queries of the same workload, {r['seconds']:.1f} s, "
+                         f"OpenMP over queries, oracle built -march=native"}
+    line = {
+        "metric": metric, "value": qps, "unit": "queries/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "i8 route/rerank, u8 LUT, f32 estimate",
+        "data": "synthetic", "config": cfg, "recall_at_10": rec, "recall_at_10_strict": rec_strict,
+        "recall_note": "big-ann recall@10 with ties (spacev) and strict; truth = exact int8 L2 over every row",
+        "p50_ms": float(np.percentile(step_ms, 50)), "p99_ms": float(np.percentile(step_ms, 99)),
+        "latency_note": "batched form: every query of a batch completes with its batch",
+        "plain": {"qps": float(1e3 / np.mean(plain_ms)), "p50_ms": float(np.percentile(plain_ms, 50)),
+                  "p99_ms": float(np.percentile(plain_ms, 99)), "queries": int(plain_ms.size)},
+        "stage_ms": {"route": tb.route / 1e6, "scan": tb.scan / 1e6, "rerank": tb.rerank / 1e6},
+        "scanned_per_query": tb.scanned / B,
+        "roofline": {"bound": "hbm", "kernel": "k_bg_scan (the candidate scan)", "achieved": achieved,
+                     "peak": peak, "unit": "GB/s", "frac": (achieved / peak) if achieved else None,
+                     "peak_source": "MEASURED_PEAKS.json hbm_gbs" if "hbm_gbs" in peaks else "fallback",
+                     "traffic": None, "bytes_per_slot": BG_SCAN_BYTES_PER_SLOT},
+        "cpu_baseline": cpu,
+        "e2e": {"value": e2e_qps, "unit": "queries/s", "h2d_bytes_per_step": B * 100,
+                "d2h_bytes_per_step": B * k * 8 + B * 4},
+        "gpu_launches": 6 * args.steps * -(-B // min(65535, (1 << 28) // max(int(arrays["k"]), 1))),
         "clocks": clocks.summary(),
     }
     if rank == 0:

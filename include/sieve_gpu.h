@@ -278,6 +278,46 @@ int sg_filter_search(sg_index* index, const sg_filter* filter, int plan, uint64_
                      float* out_scores, uint32_t* out_ids, uint32_t* out_counts,
                      sg_timing* timing);
 
+/* ---- serving: continuous batching ------------------------------------------------------- */
+/* No counterpart in the reference beyond calling ivf::Index::search from many threads
+ * (src/bin/search.rs:272-323). A server queues single-query requests and a dispatcher thread
+ * batches whatever is pending each time one of `contexts` execution contexts (a stream with its
+ * own device scratch) frees up: requests that arrive while others run join the next batch, and
+ * batches on different contexts overlap on the GPU. A batch holds requests with the same params;
+ * each may carry its own filter (the Post plan). Every result equals the query run alone. */
+typedef struct sg_server sg_server;
+typedef struct {
+  uint32_t max_batch;      /* queries per batch (0: 1024)                                        */
+  uint32_t contexts;       /* batches in flight at once (0: 2)                                   */
+  uint64_t scratch_bytes;  /* HBM budget for all contexts' scratch (0: 8 GiB); batches are cut to
+                              fit a context's share, and a request that cannot fit alone is
+                              refused with SG_ERR_ADMISSION                                     */
+  uint32_t max_pending;    /* queued requests before submit refuses (0: 2^20)                    */
+  uint32_t reserved;
+} sg_server_config;
+typedef struct {
+  float queue_ms;    /* submit to the launch of its batch                                       */
+  float service_ms;  /* launch to results on the host                                           */
+  uint32_t batch;    /* queries in its batch                                                     */
+  uint32_t retried;  /* 1 when its candidate buffer filled up and it ran again alone            */
+} sg_request_info;
+typedef struct {
+  uint64_t submitted, completed, rejected, batches, queries_batched, retried;
+  uint32_t pending, in_flight;
+} sg_server_stats;
+int sg_server_start(sg_index* index, const sg_server_config* config, sg_server** out);
+/* Queues one query (q768 [768], q256 [256] nullable); filter (nullable) restricts it to the
+ * filter's rows. Returns a ticket for sg_server_poll. */
+int sg_server_submit(sg_server* server, const float* q768, const float* q256,
+                     const sg_params* params, const sg_filter* filter, uint64_t* ticket);
+/* Waits up to wait_ms (< 0: forever; 0: no wait) for the ticket's results: out_scores/out_ids
+ * [params.k], out_count. SG_ERR_TIMEOUT while it runs; after SG_OK the ticket is gone. */
+int sg_server_poll(sg_server* server, uint64_t ticket, int wait_ms, float* out_scores,
+                   uint32_t* out_ids, uint32_t* out_count, sg_request_info* info);
+int sg_server_get_stats(sg_server* server, sg_server_stats* out);
+/* Runs every queued request to completion, then stops the dispatcher and frees the contexts. */
+int sg_server_stop(sg_server* server);
+
 /* ---- bigann: billion-scale L2 search over int8 rows (src/bigann.rs) -------------------- */
 typedef struct sg_bigann sg_bigann;
 /* bigann::Index::open(dir, base_dir, cache) (src/bigann.rs:635-641) with every record resident:
