@@ -7,6 +7,7 @@
 
 #include <string.h>
 
+#include <algorithm>
 #include <mutex>
 #include <string>
 #include <vector>
@@ -28,6 +29,7 @@ constexpr uint32_t kExpandMaxK = 16384;
 // Status bits a kernel raises in Workspace::status.
 constexpr uint32_t kStatusOverflow = 1u;   // a candidate buffer filled up (query is retried)
 constexpr uint32_t kStatusWindow = 2u;     // a BF16 routing window exceeded its buffer
+constexpr uint32_t kStatusTimeout = 4u;    // a tensor-core scan wait ran out (the CTA stopped)
 
 // HBM layout of one IVF index (all arrays on the index's device).
 struct DevIndex {
@@ -41,8 +43,13 @@ struct DevIndex {
   uint32_t* block_off = nullptr;     // [k+1] first block of each cluster
   uint32_t* clen = nullptr;          // [k] real (non-PAD) slots of each cluster
   uint8_t* blocks = nullptr;         // [nblocks*1024] nibble-transposed codes (blocks.bin)
-  uint32_t* blocks_mma = nullptr;    // [nblocks*256] the same codes in the MMA scan's word order
+  uint32_t* blocks_mma = nullptr;    // [nblocks*256] the same codes in the mma.sync scan's word order
+  uint32_t* blocks_tc = nullptr;     // [nslots*8] the same codes slot-major (tcgen05 scan)
   float* mul = nullptr;              // [nslots] factors.f32 [.., 0]
+  float* bmax = nullptr;             // [nblocks] largest mul of each block's real slots (-1 where
+                                     // one is negative or not finite): the tcgen05 scan's floors
+  float2* mul_rng = nullptr;         // [k] (min, max) of mul over each cluster's real slots;
+                                     // min = -1 where the range bound does not apply
   float* err = nullptr;              // [nslots] factors.f32 [.., 1]
   uint32_t* ids = nullptr;           // [nslots] ids.u32
   float* rot = nullptr;              // [768] rotation.f32
@@ -166,6 +173,7 @@ struct Config {
   int graphs = 1;         // capture and replay CUDA graphs per call shape (SIEVE_GPU_GRAPHS)
   uint32_t mma_min_queries_per_cluster = 8;   // use the MMA scan at or above this average
   int mma = 1;            // SIEVE_GPU_MMA: 0 ALU scan only, 1 automatic, 2 MMA whenever nprobe > 1
+  int tc = 1;             // SIEVE_GPU_TC: 1 the tcgen05 scan, 0 the mma.sync scan (kept for comparison)
 };
 
 std::string& last_error();
@@ -202,6 +210,14 @@ void launch_route_select(const DevIndex& ix, Workspace& w, uint32_t nq, const sg
 int launch_scan_mma(const DevIndex& ix, Workspace& w, uint32_t nq, const sg_params& p,
                     const uint64_t* allow, uint64_t allow_words, int sms, cudaStream_t st);
 int transcode_mma(const uint8_t* blocks, uint64_t nblocks, uint32_t* out);
+void launch_invert(const DevIndex& ix, Workspace& w, uint32_t nq, uint32_t P, uint32_t qg, cudaStream_t st);
+// The batched scan on tcgen05 (scan_tc.cu): same work items and admission as launch_scan_mma.
+int launch_scan_tc(const DevIndex& ix, Workspace& w, uint32_t nq, const sg_params& p,
+                   const uint64_t* allow, uint64_t allow_words, int sms, cudaStream_t st);
+// Launch errors of these two are left for the caller's cudaGetLastError.
+void transcode_tc(const uint8_t* blocks, uint64_t nblocks, uint32_t* out, cudaStream_t st);
+void launch_lut_scan_tc(uint32_t nq, const uint8_t* tables, const uint32_t* codes, uint64_t nblocks,
+                        uint16_t* out, uint32_t* counters, int sms, cudaStream_t st);
 // The seed pass (one CTA per query, rank-0 seed item; skipped when seed_blocks is 0) then the
 // persistent pass over the queue (skipped when chunk_blocks is 0).
 void launch_scan(const DevIndex& ix, Workspace& w, uint32_t nq, const sg_params& p,

@@ -61,7 +61,7 @@ __global__ void k_inv_count(const uint32_t* __restrict__ probe_cl, const uint32_
 }
 
 // One CTA: exclusive scan of the per-cluster counts, and the (cluster, group) items.
-__global__ void __launch_bounds__(1024) k_inv_scan(const uint32_t* __restrict__ cnt, uint32_t K,
+__global__ void __launch_bounds__(1024) k_inv_scan(const uint32_t* __restrict__ cnt, uint32_t K, uint32_t qg,
                                                    uint32_t* __restrict__ off, uint2* __restrict__ gitems,
                                                    uint64_t gcap, uint32_t* __restrict__ counters) {
   __shared__ uint32_t tmp[32];
@@ -70,14 +70,14 @@ __global__ void __launch_bounds__(1024) k_inv_scan(const uint32_t* __restrict__ 
   uint32_t s = 0, gsum = 0;
   for (uint32_t c = c0; c < c1; c++) {
     s += cnt[c];
-    gsum += (cnt[c] + kQG - 1) / kQG;
+    gsum += (cnt[c] + qg - 1) / qg;
   }
   uint32_t tot, gtot;
   uint32_t base = block_exclusive_scan(s, tmp, &tot);
   uint32_t gbase = block_exclusive_scan(gsum, tmp, &gtot);
   for (uint32_t c = c0; c < c1; c++) {
     off[c] = base;
-    const uint32_t ng = (cnt[c] + kQG - 1) / kQG;
+    const uint32_t ng = (cnt[c] + qg - 1) / qg;
     for (uint32_t j = 0; j < ng; j++)
       if (gbase + j < gcap) gitems[gbase + j] = make_uint2(c, j);
     base += cnt[c];
@@ -109,6 +109,37 @@ SG_DEV uint32_t shl_clamp(uint32_t x, uint32_t s) {
   return d;
 }
 
+// Smallest LUT score `acc` at which some slot of a cluster whose mul values lie in [lo, hi] can
+// reach the admission key `thr` of a query (cent, a, b): est = cent + mul*(a*acc + b) rounded
+// operation by operation as the epilogue forms it. With a >= 0 and 0 <= lo <= hi, the bound
+// U(acc) = cent + m*(a*acc + b), m = hi where a*acc + b >= 0 and lo below, is at least every
+// slot's estimate (rounding is monotone in each operand) and is itself non-decreasing in acc,
+// so every slot with a score below the returned floor has ord(est) < thr and is rejected
+// without forming its estimate. Returns 0 where the bound does not apply, kMaxLutScore + 1
+// where no score can reach thr.
+constexpr uint32_t kMaxLutScore = SG_GROUPS * 255;
+
+SG_DEV uint32_t score_floor(float cent, float a, float b, float lo, float hi, uint32_t thr) {
+  if (thr == 0) return 0;
+  const float xmax = __fadd_rn(__fmul_rn(a, (float)kMaxLutScore), b);
+  if (!(lo >= 0.0f) || !(hi >= lo) || !(a >= 0.0f) || !isfinite(xmax) || !isfinite(b) ||
+      !isfinite(cent) || !isfinite(__fmul_rn(hi, xmax)) || !isfinite(__fmul_rn(hi, b)))
+    return 0;
+  auto U = [&](uint32_t acc) {
+    const float x = __fadd_rn(__fmul_rn(a, (float)acc), b);
+    return ord(__fadd_rn(cent, __fmul_rn(x >= 0.0f ? hi : lo, x)));
+  };
+  if (U(0) >= thr) return 0;
+  if (U(kMaxLutScore) < thr) return kMaxLutScore + 1;
+  uint32_t l = 0, h = kMaxLutScore;  // U(l) < thr <= U(h)
+  while (h - l > 1) {
+    const uint32_t m = (l + h) >> 1;
+    if (U(m) >= thr) h = m;
+    else l = m;
+  }
+  return h;
+}
+
 SG_DEV void mma_u8(int* d, const uint32_t* a, uint32_t b0, uint32_t b1) {
   asm volatile(
       "mma.sync.aligned.m16n8k32.row.col.s32.u8.u8.s32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
@@ -138,6 +169,7 @@ struct MmaArgs {
   const uint32_t* ids;
   const uint32_t* block_off;
   const uint32_t* clen;
+  const float2* mul_rng;
   const uint8_t* tables;
   const float4* qp;
   const float* probe_sc;
@@ -170,6 +202,7 @@ __global__ void __launch_bounds__(256, 2) k_scan_mma(MmaArgs a) {
   uint32_t* stage = reinterpret_cast<uint32_t*>(smem + kQG * kBStride);  // [8 warps][2][kStageWords]
   __shared__ float s_cent[kQG], s_a[kQG], s_b[kQG];
   __shared__ uint32_t s_thr[kQG], s_kb[kQG], s_q[kQG];
+  __shared__ __align__(8) int s_floor[kQG];  // score floor per query column (INT_MAX: empty column)
   __shared__ uint32_t s_item;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int g = lane >> 2, tig = lane & 3;
@@ -215,17 +248,23 @@ __global__ void __launch_bounds__(256, 2) k_scan_mma(MmaArgs a) {
     }
     if (threadIdx.x < kQG) {
       const int qi = threadIdx.x;
+      int fl = 0x7FFFFFFF;
       if (qi < (int)ng) {
         const uint32_t ent = a.inv_list[l0 + qi];
         const uint32_t q = ent >> 12, r = ent & 0xFFFu;
         const float4 p = a.qp[q];
-        s_cent[qi] = a.probe_sc[(size_t)q * a.P + r];
+        const float cent = a.probe_sc[(size_t)q * a.P + r];
+        const uint32_t thr = *(volatile const uint32_t*)(a.thr + q);
+        const float2 mr = a.mul_rng[c];
+        s_cent[qi] = cent;
         s_a[qi] = p.z;
         s_b[qi] = p.w;
-        s_thr[qi] = *(volatile const uint32_t*)(a.thr + q);
+        s_thr[qi] = thr;
         s_kb[qi] = a.probe_off[(size_t)q * a.P + r];
         s_q[qi] = q;
+        fl = (int)score_floor(cent, p.z, p.w, mr.x, mr.y, thr);
       }
+      s_floor[qi] = fl;
     }
     __syncthreads();
     const int ntiles = (int)((ng + 7) >> 3);
@@ -285,10 +324,12 @@ __global__ void __launch_bounds__(256, 2) k_scan_mma(MmaArgs a) {
 #pragma unroll
       for (int j = 0; j < 8; j++) {
         if (j >= ntiles) break;
+        const int2 fl = *reinterpret_cast<const int2*>(s_floor + 8 * j + 2 * tig);
 #pragma unroll
         for (int i = 0; i < 2; i++)
 #pragma unroll
           for (int e = 0; e < 4; e++) {
+            if (acc[i][j][e] < ((e & 1) ? fl.y : fl.x)) continue;  // below the cluster's floor
             const uint32_t slot = 16 * i + g + 8 * (e >> 1);
             const uint32_t qi = 8 * j + 2 * tig + (e & 1);
             if (qi < ng && loc + slot < cl) {
@@ -319,23 +360,30 @@ __global__ void __launch_bounds__(256, 2) k_scan_mma(MmaArgs a) {
   }
 }
 
-int launch_scan_mma(const DevIndex& ix, Workspace& w, uint32_t nq, const sg_params& p,
-                    const uint64_t* allow, uint64_t allow_words, int sms, cudaStream_t st) {
-  const uint32_t P = p.nprobe < ix.k ? p.nprobe : ix.k;
+// Per-cluster query lists of the (query, probe) pairs the seed left, cut into (cluster, group)
+// work items of up to qg queries (counters[4] items, counters[5] the next one to take).
+void launch_invert(const DevIndex& ix, Workspace& w, uint32_t nq, uint32_t P, uint32_t qg, cudaStream_t st) {
   const uint64_t pairs = (uint64_t)nq * P;
   cudaMemsetAsync(w.inv_cnt, 0, (size_t)ix.k * 4, st);
   cudaMemsetAsync(w.inv_fill, 0, (size_t)ix.k * 4, st);
   const unsigned grid = (unsigned)((pairs + 255) / 256);
   k_inv_count<<<grid, 256, 0, st>>>(w.probe_cl, w.probe_n, w.seed_items, P, nq, w.inv_cnt);
-  k_inv_scan<<<1, 1024, 0, st>>>(w.inv_cnt, ix.k, w.inv_off, w.gitems, w.gitems_cap, w.counters);
+  k_inv_scan<<<1, 1024, 0, st>>>(w.inv_cnt, ix.k, qg, w.inv_off, w.gitems, w.gitems_cap, w.counters);
   k_inv_fill<<<grid, 256, 0, st>>>(w.probe_cl, w.probe_n, w.seed_items, P, nq, w.inv_off, w.inv_fill,
                                    w.inv_list);
+}
+
+int launch_scan_mma(const DevIndex& ix, Workspace& w, uint32_t nq, const sg_params& p,
+                    const uint64_t* allow, uint64_t allow_words, int sms, cudaStream_t st) {
+  const uint32_t P = p.nprobe < ix.k ? p.nprobe : ix.k;
+  launch_invert(ix, w, nq, P, kQG, st);
   MmaArgs a;
   a.bmma = ix.blocks_mma;
   a.mul = ix.mul;
   a.ids = ix.ids;
   a.block_off = ix.block_off;
   a.clen = ix.clen;
+  a.mul_rng = ix.mul_rng;
   a.tables = w.tables;
   a.qp = w.qp;
   a.probe_sc = w.probe_sc;

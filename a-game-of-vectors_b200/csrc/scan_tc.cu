@@ -1,0 +1,654 @@
+// scan_tc.cu — the batched LUT scan on the 5th-generation tensor cores (tcgen05, sm_100a).
+//
+// The LUT score of a slot is sum_g T_g[nibble_g] (src/lut.rs:58-60, :116-126). In the one-hot
+// basis it is a dot product: the slot is a 1024-long 0/1 row (a 1 at g*16 + nibble_g for each of
+// its 64 groups) and the query is its 1024 u8 table entries, stored group-major already. One
+// cluster's slots times the tables of the queries that probe it is therefore a
+// [slots x 1024] x [1024 x queries] u8 x u8 -> s32 product: exact integers.
+//
+// This kernel runs that product as tcgen05.mma.kind::i8 with M = 128 slots (a tile of 4 blocks),
+// N = the item's queries (padded to 16, at most 64), K = 1024, in a persistent CTA per SM whose
+// warps each keep one role:
+//   - a loader warp takes (cluster, query group) work items from the queue and fills one of two
+//     item slots in shared memory: B (the query tables as K-major core matrices, 8 queries x
+//     16 B) and each query's constants, so an item's set-up overlaps the previous item's tiles;
+//   - four producer warps build A (the one-hot slots) in registers and write it straight into
+//     tensor memory with tcgen05.st: one-hot rows are 32x the size of the codes and never touch
+//     shared memory or HBM. Warp w owns TMEM lanes 32*w.. (block w of the tile) and fills the
+//     tile's four K chunks (16 groups = 256 one-hot bytes = 64 TMEM columns each);
+//   - one thread of the MMA warp issues the 32 MMAs (K = 32) of a tile into one of four TMEM
+//     accumulators and signals the A stages and the accumulator through mbarriers
+//     (tcgen05.commit);
+//   - eight epilogue warps (two per TMEM lane quarter, taking alternate tiles) read the s32
+//     scores with tcgen05.ld (one slot per thread, one query per column), reject every score
+//     below the (query, block) integer floor, and form est = cent + mul*(a*score + b) exactly as
+//     the ALU scan does for the rest. Each warp reserves room for its admitted slots with one
+//     atomic per query column, all columns' atomics in flight together, and appends every
+//     eligible slot at or above the query's threshold to the query's candidate buffer.
+// Every mbarrier wait is bounded: a wait that runs out raises kStatusTimeout, every role stops,
+// and the kernel frees its tensor memory and returns.
+//
+// A raw form of the same pipeline (kRaw) writes the u16 scores of every (query, slot) pair: it
+// is the batched lut::scan behind sg_lut_scan_batch and pins the contraction bit for bit.
+#include "common.cuh"
+#include "internal.hpp"
+
+namespace sg {
+
+constexpr int kTcQG = 64;           // queries per work item (MMA N, padded to a multiple of 16)
+constexpr int kTcChunks = 4;        // K chunks per tile: 16 groups = 256 one-hot bytes each
+constexpr uint32_t kTcCols = 512;   // TMEM columns: 4 x 64 (A stages) + 4 x 64 (D)
+constexpr uint32_t kTcDCol = 256;   // first D column
+constexpr int kTcDBufs = 4;         // accumulators
+constexpr int kTcProducers = 4;     // warps 0-3 build A
+constexpr int kTcEpi = 4;           // warps 4-11 drain D
+constexpr int kTcEpiWarps = 8;
+constexpr int kTcMma = 12;          // warp 12 issues the MMAs
+constexpr int kTcLoader = 13;       // warp 13 loads work items
+constexpr int kTcThreads = 14 * 32;
+constexpr int kTcBBytes = kTcQG * 1024;  // B of one item slot
+constexpr int kTcVStride = 36;      // words per lane row of the epilogue's score spill
+constexpr int kTcVBytes = kTcEpiWarps * 32 * kTcVStride * 4;  // the epilogue warps' spills
+constexpr uint64_t kTcWaitNs = 2000000000ull;  // a pipeline wait gives up after 2 s
+constexpr uint32_t kTcSpinLimit = 1u << 30;    // backstop on the number of polls
+constexpr uint32_t kTcMaxScore = SG_GROUPS * 255;
+
+// ---- slot-major codes ----------------------------------------------------------------------
+// Slot s's 64 nibbles in 8 words (32 B): group g at word g/8, bits 4*(g%8). Source: blocks.bin,
+// where group g's byte k holds the nibble of slot k (low) and of slot k+16 (high).
+__global__ void k_transcode_tc(const uint8_t* __restrict__ blocks, uint64_t nblocks,
+                               uint32_t* __restrict__ out) {
+  const uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= nblocks * 256) return;
+  const uint64_t b = t >> 8;
+  const uint32_t s = (uint32_t)(t >> 3) & 31, j = (uint32_t)t & 7;
+  const uint8_t* src = blocks + b * SG_BLOCK_BYTES + (s & 15);
+  const uint32_t sh = (s >> 4) * 4;
+  uint32_t w = 0;
+#pragma unroll
+  for (int p = 0; p < 8; p++) w |= (uint32_t)((src[(8 * j + p) * 16] >> sh) & 15u) << (4 * p);
+  out[t] = w;
+}
+
+void transcode_tc(const uint8_t* blocks, uint64_t nblocks, uint32_t* out, cudaStream_t st) {
+  if (nblocks == 0) return;
+  const uint64_t n = nblocks * 256;
+  k_transcode_tc<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(blocks, nblocks, out);
+}
+
+// ---- PTX wrappers ----------------------------------------------------------------------------
+SG_DEV uint32_t smem_addr(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+SG_DEV void mbar_init(uint64_t* bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(smem_addr(bar)), "r"(count));
+}
+SG_DEV void mbar_arrive(uint64_t* bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];\n" ::"r"(smem_addr(bar)) : "memory");
+}
+SG_DEV bool mbar_test(uint64_t* bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n.reg .pred p;\nmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\nselp.u32 %0, 1, 0, p;\n}\n"
+      : "=r"(ok)
+      : "r"(smem_addr(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+SG_DEV uint64_t globaltimer_ns() {
+  uint64_t t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+// Waits for the phase of `parity` to complete; false once the CTA aborts or the wait runs out
+// (kTcWaitNs on the global timer, or kTcSpinLimit polls).
+SG_DEV bool mbar_wait(uint64_t* bar, uint32_t parity, volatile int* abort_flag) {
+  uint64_t t0 = 0;
+  for (uint32_t i = 0; i < kTcSpinLimit; i++) {
+    if (mbar_test(bar, parity)) return true;
+    if (*abort_flag) return false;
+    if ((i & 255u) == 0) {
+      const uint64_t now = globaltimer_ns();
+      if (i == 0) t0 = now;
+      else if (now - t0 > kTcWaitNs) break;
+    }
+  }
+  *abort_flag = 1;
+  return false;
+}
+
+SG_DEV void tc_alloc(uint32_t* dst, uint32_t ncols) {
+  asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n" ::"r"(smem_addr(dst)),
+               "r"(ncols));
+}
+SG_DEV void tc_relinquish() { asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n" ::); }
+SG_DEV void tc_dealloc(uint32_t taddr, uint32_t ncols) {
+  asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(taddr), "r"(ncols));
+}
+SG_DEV void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory"); }
+SG_DEV void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory"); }
+SG_DEV void tc_commit(uint64_t* bar) {
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n" ::"r"(
+                   smem_addr(bar))
+               : "memory");
+}
+// D[tmem] (+)= A[tmem] x B[smem descriptor]; u8 x u8 -> s32, shape from the instruction descriptor.
+SG_DEV void tc_mma_i8(uint32_t d_tmem, uint32_t a_tmem, uint64_t b_desc, uint32_t idesc, uint32_t accumulate) {
+  asm volatile(
+      "{\n.reg .pred p;\nsetp.ne.b32 p, %4, 0;\n"
+      "tcgen05.mma.cta_group::1.kind::i8 [%0], [%1], %2, %3, {%5, %5, %5, %5}, p;\n}\n" ::"r"(d_tmem),
+      "r"(a_tmem), "l"(b_desc), "r"(idesc), "r"(accumulate), "r"(0u));
+}
+SG_DEV void tc_wait_st() { asm volatile("tcgen05.wait::st.sync.aligned;\n" ::: "memory"); }
+SG_DEV void tc_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory"); }
+SG_DEV void fence_proxy_async_smem() { asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory"); }
+SG_DEV void fence_mbar_init() { asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory"); }
+
+// 32 lanes x 32 columns: thread i writes lane (taddr lane + i), register j to column + j.
+SG_DEV void tc_st32(uint32_t taddr, const uint32_t* r) {
+  asm volatile(
+      "tcgen05.st.sync.aligned.32x32b.x32.b32 [%0], {%1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, "
+      "%13, %14, %15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31, %32};\n" ::"r"(
+          taddr),
+      "r"(r[0]), "r"(r[1]), "r"(r[2]), "r"(r[3]), "r"(r[4]), "r"(r[5]), "r"(r[6]), "r"(r[7]), "r"(r[8]),
+      "r"(r[9]), "r"(r[10]), "r"(r[11]), "r"(r[12]), "r"(r[13]), "r"(r[14]), "r"(r[15]), "r"(r[16]),
+      "r"(r[17]), "r"(r[18]), "r"(r[19]), "r"(r[20]), "r"(r[21]), "r"(r[22]), "r"(r[23]), "r"(r[24]),
+      "r"(r[25]), "r"(r[26]), "r"(r[27]), "r"(r[28]), "r"(r[29]), "r"(r[30]), "r"(r[31]));
+}
+SG_DEV void tc_ld32(uint32_t taddr, uint32_t* r) {
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, "
+      "%14, %15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, [%32];\n"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+        "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]),
+        "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]),
+        "=r"(r[23]), "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]),
+        "=r"(r[30]), "=r"(r[31])
+      : "r"(taddr));
+}
+
+// Shared-memory matrix descriptor, K-major without swizzle: core matrices of 8 rows x 16 B,
+// `lbo` bytes between the two K halves of an instruction, `sbo` bytes between 8-row groups.
+SG_DEV uint64_t smem_desc(uint32_t saddr, uint32_t lbo, uint32_t sbo) {
+  return (uint64_t)((saddr >> 4) & 0x3FFFu) | ((uint64_t)((lbo >> 4) & 0x3FFFu) << 16) |
+         ((uint64_t)((sbo >> 4) & 0x3FFFu) << 32) | (1ull << 46);
+}
+// Instruction descriptor of kind::i8: u8 A and B, both K-major, s32 accumulators, M = 128.
+SG_DEV uint32_t idesc_u8(uint32_t n) { return (2u << 4) | ((n >> 3) << 17) | ((128u >> 4) << 24); }
+
+SG_DEV uint32_t shl_sat(uint32_t x, uint32_t s) {
+  uint32_t d;  // PTX shl clamps shift amounts above 31 to 32: the result is then 0
+  asm("shl.b32 %0, %1, %2;" : "=r"(d) : "r"(x), "r"(s));
+  return d;
+}
+// One-hot of 8 groups (the 8 nibbles of w): group p's 16 bytes are 4 TMEM columns, the byte of
+// its nibble n set to 1 (column 4p + n/4, byte n%4).
+SG_DEV void onehot8(uint32_t w, uint32_t* r) {
+#pragma unroll
+  for (int p = 0; p < 8; p++) {
+    const uint32_t n8 = ((w >> (4 * p)) & 15u) << 3;
+    r[4 * p + 0] = shl_sat(1u, n8);
+    r[4 * p + 1] = shl_sat(1u, n8 - 32u);
+    r[4 * p + 2] = shl_sat(1u, n8 - 64u);
+    r[4 * p + 3] = shl_sat(1u, n8 - 96u);
+  }
+}
+
+
+// Integer floor on the LUT score of a (query, block): every slot of the block with a lower score
+// has est < T, the query's threshold. With est = fl(cent + fl(m * fl(fl(a*s) + b))), the real
+// value E = cent + m*(a*s + b) is within D = 2u*(M*(4*a*16320 + 3|b|) + |cent|) (u = 2^-24, M
+// the cluster's largest mul) of est, so est >= T needs m*(a*s + b) >= R = T - D - cent. For
+// R > 0, 0 <= m <= Mb (the block's largest mul) and a > 0 that means s >= (R/Mb - b)/a. The
+// loader precomputes R, b and 1/a per query in double; ia = 0 marks "no bound" (no threshold
+// yet, or inputs the bound does not cover), and a block with Mb < 0 holds a negative or non-finite
+// mul. One score unit is subtracted for the double rounding.
+SG_DEV int tc_floor(double R, double bd, double ia, float Mb) {
+  if (!(ia > 0.0) || !(Mb >= 0.0f) || !(R > 0.0)) return 0;
+  if (Mb == 0.0f) return (int)kTcMaxScore + 1;  // est = cent < T for every slot
+  const double x = (R / (double)Mb - bd) * ia;
+  if (!(x == x)) return 0;
+  if (x >= (double)(kTcMaxScore + 2)) return (int)kTcMaxScore + 1;
+  if (x <= 1.0) return 0;
+  return (int)floor(x - 1.0);
+}
+
+struct TcArgs {
+  const uint4* codes;  // [nslots * 2] slot-major codes
+  // admission form
+  const float* mul;
+  const float* bmax;   // [nblocks] largest mul of each block (-1: a negative or non-finite one)
+  const uint32_t* ids;
+  const uint32_t* block_off;
+  const uint32_t* clen;
+  const float2* mul_rng;
+  const uint8_t* tables;
+  const float4* qp;
+  const float* probe_sc;
+  const uint32_t* probe_off;
+  uint32_t P;
+  const uint32_t* inv_off;
+  const uint32_t* inv_list;
+  const uint2* gitems;
+  uint32_t* counters;  // [2] status, [4] items, [5] next item
+  uint32_t* thr;
+  uint32_t* ccount;
+  uint32_t* cbuf_est;
+  uint2* cbuf_info;
+  uint32_t cap;
+  uint8_t* overflow;
+  const uint64_t* allow;
+  uint64_t allow_words;
+  const uint64_t* const* allow_q;
+  const uint64_t* allow_wq;
+  // raw form: items are (query group, chunk of raw_chunk blocks); counters [0] status, [1] next
+  uint32_t nq;
+  uint64_t nblocks;
+  uint32_t raw_chunk;
+  uint16_t* out;  // [nq][nblocks * 32]
+};
+
+template <bool kRaw>
+__global__ void __launch_bounds__(kTcThreads, 1) k_scan_tc(TcArgs a) {
+  extern __shared__ __align__(1024) uint8_t smem[];  // B of the two item slots
+  __shared__ __align__(8) uint64_t bar_afull[kTcChunks], bar_aempty[kTcChunks], bar_dfull[kTcDBufs],
+      bar_dempty[kTcDBufs], bar_ifull[2], bar_iempty[2];
+  __shared__ uint32_t s_tmem;
+  __shared__ int s_abort;
+  __shared__ uint32_t s_meta[2][8];  // b0, nb, cl, ng, qbase, end
+  __shared__ float4 s_qc[2][kTcQG];  // cent, a, b, threshold key (as bits)
+  __shared__ uint2 s_qk[2][kTcQG];   // candidate order base, query
+  __shared__ double s_R[2][kTcQG], s_bd[2][kTcQG], s_ia[2][kTcQG];
+  __shared__ __align__(16) int s_wfl[kTcEpiWarps][kTcQG];  // (query, block) floors of the epilogue warps
+  __shared__ uint2 s_cb[kTcEpiWarps][32];                  // per column: reserved base, admitted lanes
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  volatile int* abort_flag = &s_abort;
+
+  if (warp == kTcMma) {
+    tc_alloc(&s_tmem, kTcCols);
+    tc_relinquish();
+  }
+  if (tid == 0) {
+    for (int i = 0; i < kTcChunks; i++) {
+      mbar_init(&bar_afull[i], 4);  // the four producer warps (lane quarters) of the chunk
+      mbar_init(&bar_aempty[i], 1);
+    }
+    for (int i = 0; i < kTcDBufs; i++) {
+      mbar_init(&bar_dfull[i], 1);
+      mbar_init(&bar_dempty[i], 4);
+    }
+    for (int i = 0; i < 2; i++) {
+      mbar_init(&bar_ifull[i], 1);
+      mbar_init(&bar_iempty[i], kTcProducers + kTcEpiWarps + 1);
+    }
+    s_abort = 0;
+    fence_mbar_init();
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = s_tmem;
+  const uint32_t bs_base = smem_addr(smem);
+  uint32_t* status = kRaw ? a.counters : a.counters + 2;
+
+  if (warp == kTcLoader) {
+    // ---- work items into the two item slots ------------------------------------------------
+    uint32_t nitems, nchunks = 0;
+    if (kRaw) {
+      nchunks = (uint32_t)((a.nblocks + a.raw_chunk - 1) / a.raw_chunk);
+      nitems = ((a.nq + kTcQG - 1) / kTcQG) * nchunks;
+    } else {
+      nitems = a.counters[4];
+    }
+    uint32_t* next_item = kRaw ? a.counters + 1 : a.counters + 5;
+    for (uint32_t it = 0;; it++) {
+      const uint32_t slot = it & 1, use = it >> 1;
+      if (!mbar_wait(&bar_iempty[slot], (use & 1) ^ 1, abort_flag)) break;
+      uint32_t item = 0;
+      if (lane == 0) item = atomicAdd(next_item, 1u);
+      item = __shfl_sync(0xFFFFFFFFu, item, 0);
+      if (item >= nitems) {
+        if (lane == 0) {
+          s_meta[slot][5] = 1;
+          mbar_arrive(&bar_ifull[slot]);
+        }
+        break;
+      }
+      uint32_t b0, nb, ng, cl, l0 = 0, qbase = 0, c = 0;
+      if (kRaw) {
+        const uint32_t qg = item / nchunks, ch = item % nchunks;
+        qbase = qg * kTcQG;
+        ng = min((uint32_t)kTcQG, a.nq - qbase);
+        b0 = ch * a.raw_chunk;
+        nb = (uint32_t)min((uint64_t)a.raw_chunk, a.nblocks - b0);
+        cl = nb * SG_BLOCK;
+      } else {
+        const uint2 gi = a.gitems[item];
+        c = gi.x;
+        l0 = a.inv_off[c] + gi.y * kTcQG;
+        ng = min((uint32_t)kTcQG, a.inv_off[c + 1] - l0);
+        b0 = a.block_off[c];
+        nb = a.block_off[c + 1] - b0;
+        cl = a.clen[c];
+      }
+      const uint32_t N = (ng + 15) & ~15u;
+      uint8_t* B = smem + slot * kTcBBytes;
+      if (nb > 0) {
+        // query n's table chunk g (16 B) at (n/8)*8192 + g*128 + (n%8)*16
+#pragma unroll 4
+        for (uint32_t e = lane; e < N * 64; e += 32) {
+          const uint32_t r = e & 7, g = (e >> 3) & 63, n = (e >> 9) * 8 + r;
+          uint4 v = make_uint4(0, 0, 0, 0);
+          if (n < ng) {
+            const uint32_t q = kRaw ? qbase + n : a.inv_list[l0 + n] >> 12;
+            v = reinterpret_cast<const uint4*>(a.tables + (size_t)q * SG_GROUPS * 16)[g];
+          }
+          *reinterpret_cast<uint4*>(B + (n >> 3) * 8192 + g * 128 + r * 16) = v;
+        }
+      }
+      if (!kRaw) {
+        for (uint32_t qi = lane; qi < ng; qi += 32) {
+          const uint32_t ent = a.inv_list[l0 + qi];
+          const uint32_t q = ent >> 12, r = ent & 0xFFFu;
+          const float4 p = a.qp[q];
+          const float cent = a.probe_sc[(size_t)q * a.P + r];
+          const uint32_t thr = *(volatile const uint32_t*)(a.thr + q);
+          s_qc[slot][qi] = make_float4(cent, p.z, p.w, __uint_as_float(thr));
+          s_qk[slot][qi] = make_uint2(a.probe_off[(size_t)q * a.P + r], q);
+          const float2 mr = a.mul_rng[c];
+          const float T = unord(thr);
+          double R = 0.0, ia = 0.0;
+          if (thr != 0 && mr.x >= 0.0f && isfinite(mr.y) && p.z > 0.0f && isfinite(p.z) && isfinite(p.w) &&
+              isfinite(cent) && isfinite(T)) {
+            const double u = 1.0 / 16777216.0;
+            const double d = 2.0 * u * ((double)mr.y * (4.0 * (double)p.z * kTcMaxScore + 3.0 * fabs((double)p.w)) +
+                                        fabs((double)cent)) + 1e-37;
+            R = (double)T - d - (double)cent;
+            ia = 1.0 / (double)p.z;
+          }
+          s_R[slot][qi] = R;
+          s_bd[slot][qi] = (double)p.w;
+          s_ia[slot][qi] = ia;
+        }
+      }
+      if (lane == 0) {
+        s_meta[slot][0] = b0;
+        s_meta[slot][1] = nb;
+        s_meta[slot][2] = cl;
+        s_meta[slot][3] = ng;
+        s_meta[slot][4] = qbase;
+        s_meta[slot][5] = 0;
+      }
+      fence_proxy_async_smem();
+      __syncwarp();
+      if (lane == 0) mbar_arrive(&bar_ifull[slot]);
+    }
+  } else {
+    // ---- consumers: items in order, tiles numbered across items ------------------------------
+    uint32_t ts = 0;  // tiles of earlier items
+    for (uint32_t it = 0;; it++) {
+      const uint32_t slot = it & 1, use = it >> 1;
+      if (!mbar_wait(&bar_ifull[slot], use & 1, abort_flag)) break;
+      if (s_meta[slot][5]) break;
+      const uint32_t b0 = s_meta[slot][0], nb = s_meta[slot][1], cl = s_meta[slot][2], ng = s_meta[slot][3];
+      const uint32_t qbase = s_meta[slot][4];
+      const uint32_t N = (ng + 15) & ~15u, ntiles = (nb + 3) >> 2;
+      bool ok = true;
+      if (warp < kTcProducers) {
+        // one-hot A: block 4t + warp of the tile, slot = lane, all four K chunks
+        const uint32_t qd = warp;
+        const uint32_t lane_base = (32u * qd) << 16;
+        auto codes_of = [&](uint32_t t, uint4& lo, uint4& hi) {
+          const uint32_t bl = 4 * t + qd;
+          lo = hi = make_uint4(0, 0, 0, 0);
+          if (t < ntiles && bl < nb) {
+            const uint64_t gs = (uint64_t)(b0 + bl) * SG_BLOCK + lane;
+            lo = a.codes[2 * gs];
+            hi = a.codes[2 * gs + 1];
+          }
+        };
+        uint4 lo, hi, nlo, nhi;
+        codes_of(0, lo, hi);
+        for (uint32_t t = 0; t < ntiles && ok; t++) {
+          codes_of(t + 1, nlo, nhi);
+          const uint32_t tp = (ts + t) & 1;
+          for (uint32_t ch = 0; ch < kTcChunks; ch++) {
+            if (!mbar_wait(&bar_aempty[ch], tp ^ 1, abort_flag)) {
+              ok = false;
+              break;
+            }
+            const uint4 cw = ch < 2 ? lo : hi;
+            uint32_t r[32];
+            onehot8((ch & 1) ? cw.z : cw.x, r);
+            tc_st32(tmem + lane_base + ch * 64, r);
+            onehot8((ch & 1) ? cw.w : cw.y, r);
+            tc_st32(tmem + lane_base + ch * 64 + 32, r);
+            tc_wait_st();
+            tc_fence_before();
+            __syncwarp();
+            if (lane == 0) mbar_arrive(&bar_afull[ch]);
+          }
+          lo = nlo;
+          hi = nhi;
+        }
+        if (lane == 0) mbar_arrive(&bar_iempty[slot]);
+      } else if (warp == kTcMma) {
+        const uint32_t idesc = idesc_u8(N);
+        const uint32_t bslot = bs_base + slot * kTcBBytes;
+        for (uint32_t t = 0; t < ntiles && ok; t++) {
+          const uint32_t ds = ts + t, dbuf = ds & (kTcDBufs - 1), duse = ds / kTcDBufs;
+          if (!mbar_wait(&bar_dempty[dbuf], (duse & 1) ^ 1, abort_flag)) break;
+          tc_fence_after();
+          for (uint32_t ch = 0; ch < kTcChunks; ch++) {
+            if (!mbar_wait(&bar_afull[ch], ds & 1, abort_flag)) {
+              ok = false;
+              break;
+            }
+            tc_fence_after();
+            if (lane == 0) {
+#pragma unroll
+              for (uint32_t kk = 0; kk < 8; kk++) {
+                const uint32_t kstep = ch * 8 + kk;  // K bytes 32*kstep.. = groups 2*kstep, +1
+                tc_mma_i8(tmem + kTcDCol + dbuf * kTcQG, tmem + ch * 64 + kk * 8,
+                          smem_desc(bslot + kstep * 256, 128, 8192), idesc, (ch | kk) != 0);
+              }
+              tc_commit(&bar_aempty[ch]);
+              if (ch == kTcChunks - 1) tc_commit(&bar_dfull[dbuf]);
+            }
+            __syncwarp();
+          }
+        }
+        if (lane == 0) mbar_arrive(&bar_iempty[slot]);
+      } else {
+        // ---- epilogue: slot (4t + qd)*32 + lane of the tiles of this warp's parity ----------
+        const uint32_t ew = warp - kTcEpi, qd = ew & 3, par = ew >> 2;
+        const uint32_t lane_base = (32u * qd) << 16;
+        const uint32_t ncc = (N + 31) >> 5;
+        int* wfl = s_wfl[ew];
+        uint2* cb = s_cb[ew];
+        uint32_t* vrow = reinterpret_cast<uint32_t*>(smem + 2 * kTcBBytes) + (ew * 32 + lane) * kTcVStride;
+        // the warp's next tile's mul and block maximum are loaded one tile ahead
+        auto tile_loads = [&](uint32_t t, float& mv, float& mb) {
+          const uint32_t bl = 4 * t + qd;
+          mv = 0.0f;
+          mb = -1.0f;
+          if (kRaw || t >= ntiles || bl >= nb) return;
+          mb = a.bmax[b0 + bl];
+          if (bl * SG_BLOCK + lane < cl) mv = a.mul[(b0 + bl) * SG_BLOCK + lane];
+        };
+        const uint32_t t0 = ((ts & 1) == par) ? 0 : 1;  // first tile of this warp's parity
+        float mv, mb, nmv, nmb;
+        tile_loads(t0, mv, mb);
+        for (uint32_t t = t0; t < ntiles; t += 2) {
+          const uint32_t ds = ts + t, dbuf = ds & (kTcDBufs - 1), duse = ds / kTcDBufs;
+          const uint32_t bl = 4 * t + qd;
+          const uint32_t loc = bl * SG_BLOCK + lane;
+          const bool lane_ok = bl < nb && loc < cl;
+          const uint32_t gslot = (b0 + bl) * SG_BLOCK + lane;
+          tile_loads(t + 2, nmv, nmb);
+          if (!kRaw) {
+            for (uint32_t qi = lane; qi < (uint32_t)kTcQG; qi += 32)
+              wfl[qi] = qi < ng ? tc_floor(s_R[slot][qi], s_bd[slot][qi], s_ia[slot][qi], mb) : 0x7FFFFFFF;
+            __syncwarp();
+          }
+          if (!mbar_wait(&bar_dfull[dbuf], duse & 1, abort_flag)) break;
+          tc_fence_after();
+          for (uint32_t cc = 0; cc < ncc; cc++) {
+            uint32_t v[32];
+            tc_ld32(tmem + lane_base + kTcDCol + dbuf * kTcQG + 32 * cc, v);
+            tc_wait_ld();
+            if (kRaw) {
+              if (lane_ok) {
+#pragma unroll
+                for (int j = 0; j < 32; j++)
+                  if (32 * cc + j < ng) a.out[(size_t)(qbase + 32 * cc + j) * (a.nblocks * SG_BLOCK) + gslot] = (uint16_t)v[j];
+              }
+              continue;
+            }
+            uint32_t m = 0;
+#pragma unroll
+            for (int j4 = 0; j4 < 8; j4++) {
+              const int4 f = *reinterpret_cast<const int4*>(wfl + 32 * cc + 4 * j4);
+              m |= ((int)v[4 * j4 + 0] >= f.x ? 1u : 0u) << (4 * j4 + 0);
+              m |= ((int)v[4 * j4 + 1] >= f.y ? 1u : 0u) << (4 * j4 + 1);
+              m |= ((int)v[4 * j4 + 2] >= f.z ? 1u : 0u) << (4 * j4 + 2);
+              m |= ((int)v[4 * j4 + 3] >= f.w ? 1u : 0u) << (4 * j4 + 3);
+            }
+            if (!lane_ok) m = 0;
+            if (!__any_sync(0xFFFFFFFFu, m != 0)) continue;
+#pragma unroll
+            for (int j4 = 0; j4 < 8; j4++)
+              *reinterpret_cast<uint4*>(vrow + 4 * j4) = make_uint4(v[4 * j4], v[4 * j4 + 1], v[4 * j4 + 2], v[4 * j4 + 3]);
+            // 1. exact admission of the lane's columns above the floor; an admitted column's
+            //    estimate replaces its score in the spill row
+            uint32_t adm = 0;
+            while (m) {
+              const uint32_t j = __ffs(m) - 1;
+              m &= m - 1;
+              const uint32_t qi = 32 * cc + j;
+              const float4 qc = s_qc[slot][qi];
+              const float est = __fadd_rn(qc.x, __fmul_rn(mv, __fadd_rn(__fmul_rn(qc.y, (float)vrow[j]), qc.z)));
+              if (ord(est) < __float_as_uint(qc.w)) continue;
+              const uint32_t q = s_qk[slot][qi].y;
+              const uint64_t* al = a.allow_q ? a.allow_q[q] : a.allow;
+              const uint64_t aw = a.allow_q ? a.allow_wq[q] : a.allow_words;
+              if (al && !allowed(al, aw, a.ids[gslot])) continue;
+              adm |= 1u << j;
+              vrow[j] = __float_as_uint(est);
+            }
+            __syncwarp();
+            const uint32_t amask = __reduce_or_sync(0xFFFFFFFFu, adm);
+            if (!amask) continue;
+            // 2. lane j takes column j's admitted lanes and reserves their room with one atomic;
+            //    the atomics of all columns are in flight together
+            uint32_t col = 0;
+            for (uint32_t r = amask; r; r &= r - 1) {
+              const uint32_t j = __ffs(r) - 1;
+              const uint32_t bal = __ballot_sync(0xFFFFFFFFu, (adm >> j) & 1u);
+              if (lane == j) col = bal;
+            }
+            uint32_t base = 0;
+            if (col) base = atomicAdd(a.ccount + s_qk[slot][32 * cc + lane].y, (uint32_t)__popc(col));
+            cb[lane] = make_uint2(base, col);
+            __syncwarp();
+            // 3. each admitted (slot, query) writes its entry at the column's base + its rank
+            for (uint32_t r = adm; r; r &= r - 1) {
+              const uint32_t j = __ffs(r) - 1;
+              const uint2 bc = cb[j];
+              const uint2 qk = s_qk[slot][32 * cc + j];
+              const uint32_t pos = bc.x + (uint32_t)__popc(bc.y & ((1u << lane) - 1u));
+              if (pos < a.cap) {
+                a.cbuf_est[(size_t)qk.y * a.cap + pos] = vrow[j];
+                a.cbuf_info[(size_t)qk.y * a.cap + pos] = make_uint2(qk.x + loc, gslot);
+              } else {
+                a.overflow[qk.y] = 1;
+              }
+            }
+            __syncwarp();
+          }
+          tc_fence_before();
+          __syncwarp();
+          if (lane == 0) mbar_arrive(&bar_dempty[dbuf]);
+          mv = nmv;
+          mb = nmb;
+        }
+        if (lane == 0) mbar_arrive(&bar_iempty[slot]);
+      }
+      ts += ntiles;
+      if (*abort_flag) break;
+    }
+  }
+  if (tid == 0 && *abort_flag) atomicOr(status, kStatusTimeout);
+  tc_fence_before();
+  __syncthreads();
+  if (warp == kTcMma) {
+    tc_fence_after();
+    tc_dealloc(tmem, kTcCols);
+  }
+}
+
+static int tc_smem_bytes() { return 2 * kTcBBytes + kTcVBytes; }
+
+template <bool kRaw>
+static void tc_set_attr() {
+  static bool done = false;  // per process; the attribute is per function, not per device
+  if (!done) {
+    cudaFuncSetAttribute(k_scan_tc<kRaw>, cudaFuncAttributeMaxDynamicSharedMemorySize, tc_smem_bytes());
+    done = true;
+  }
+}
+
+int launch_scan_tc(const DevIndex& ix, Workspace& w, uint32_t nq, const sg_params& p, const uint64_t* allow,
+                   uint64_t allow_words, int sms, cudaStream_t st) {
+  const uint32_t P = p.nprobe < ix.k ? p.nprobe : ix.k;
+  launch_invert(ix, w, nq, P, kTcQG, st);
+  TcArgs a{};
+  a.codes = reinterpret_cast<const uint4*>(ix.blocks_tc);
+  a.mul = ix.mul;
+  a.bmax = ix.bmax;
+  a.ids = ix.ids;
+  a.block_off = ix.block_off;
+  a.clen = ix.clen;
+  a.mul_rng = ix.mul_rng;
+  a.tables = w.tables;
+  a.qp = w.qp;
+  a.probe_sc = w.probe_sc;
+  a.probe_off = w.probe_off;
+  a.P = P;
+  a.inv_off = w.inv_off;
+  a.inv_list = w.inv_list;
+  a.gitems = w.gitems;
+  a.counters = w.counters;
+  a.thr = w.thr;
+  a.ccount = w.ccount;
+  a.cbuf_est = w.cbuf_est;
+  a.cbuf_info = w.cbuf_info;
+  a.cap = w.cbuf_per_q;
+  a.overflow = w.overflow;
+  a.allow = allow;
+  a.allow_words = allow_words;
+  a.allow_q = w.per_query_allow ? w.allow_q : nullptr;
+  a.allow_wq = w.allow_wq;
+  tc_set_attr<false>();
+  k_scan_tc<false><<<sms, kTcThreads, tc_smem_bytes(), st>>>(a);
+  return 4;
+}
+
+// Raw scores of nq query tables against nblocks blocks (slot-major codes already on the device);
+// counters: 2 words on the device, zeroed by the caller ([0] status, [1] next item).
+void launch_lut_scan_tc(uint32_t nq, const uint8_t* tables, const uint32_t* codes, uint64_t nblocks,
+                        uint16_t* out, uint32_t* counters, int sms, cudaStream_t st) {
+  TcArgs a{};
+  a.codes = reinterpret_cast<const uint4*>(codes);
+  a.tables = tables;
+  a.counters = counters;
+  a.nq = nq;
+  a.nblocks = nblocks;
+  a.raw_chunk = 64;
+  a.out = out;
+  tc_set_attr<true>();
+  const uint64_t items = (uint64_t)((nq + kTcQG - 1) / kTcQG) * ((nblocks + 63) / 64);
+  const unsigned grid = (unsigned)std::min<uint64_t>(items, (uint64_t)sms);
+  k_scan_tc<true><<<grid, kTcThreads, tc_smem_bytes(), st>>>(a);
+}
+
+}  // namespace sg

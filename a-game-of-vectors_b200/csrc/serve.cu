@@ -202,6 +202,10 @@ void complete_batch(sg_server* srv, Slot& s, int launch_rc) {
       r.status = fail(SG_ERR_INVALID, "work queue overflow");
       continue;
     }
+    if (*s.h_status & sg::kStatusTimeout) {
+      r.status = fail(SG_ERR_DEVICE, "tensor-core scan: a pipeline wait ran out");
+      continue;
+    }
     if (s.h_ovf[i]) {
       r.status = sg::ctx_search_one(srv->h, s.ctx, r.q768.data(), r.have_q256 ? r.q256.data() : nullptr,
                                     s.p, r.filter ? r.filter->allow : nullptr,

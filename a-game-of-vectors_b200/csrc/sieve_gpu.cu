@@ -10,6 +10,7 @@
 #include <string.h>
 
 #include <algorithm>
+#include <cmath>
 #include <cstdio>
 #include <fstream>
 #include <memory>
@@ -78,7 +79,10 @@ void free_index(sg::DevIndex& x) {
   dfree(x.clen);
   dfree(x.blocks);
   dfree(x.blocks_mma);
+  dfree(x.blocks_tc);
   dfree(x.mul);
+  dfree(x.mul_rng);
+  dfree(x.bmax);
   dfree(x.err);
   dfree(x.ids);
   dfree(x.rot);
@@ -221,6 +225,38 @@ int build_index(const sg_ivf_arrays* a, int device, sg_index** out) {
     mul[s] = a->factors[2 * s];
     err[s] = a->factors[2 * s + 1];
   }
+  // per-cluster range of mul over the real slots: the MMA scan turns it into an integer floor
+  // on the LUT score below which no slot of the cluster can reach a query's threshold
+  std::vector<float2> mrng(K);
+  for (uint32_t c = 0; c < K; c++) {
+    const uint64_t s0 = a->block_off[c] * SG_BLOCK;
+    float lo = INFINITY, hi = 0.0f;
+    bool ok = true;
+    for (uint64_t s = s0; s < s0 + x.h_clen[c]; s++) {
+      const float m = mul[s];
+      if (!(m >= 0.0f) || !std::isfinite(m)) ok = false;
+      lo = std::min(lo, m);
+      hi = std::max(hi, m);
+    }
+    if (x.h_clen[c] == 0) lo = 0.0f;
+    mrng[c] = ok ? make_float2(lo, hi) : make_float2(-1.0f, -1.0f);
+  }
+  std::vector<float> bmx(nblocks);
+  for (uint32_t c = 0; c < K; c++) {
+    const uint64_t s0 = a->block_off[c] * SG_BLOCK, s1 = s0 + x.h_clen[c];
+    for (uint64_t b = a->block_off[c]; b < a->block_off[c + 1]; b++) {
+      float hi = 0.0f;
+      for (uint64_t s = b * SG_BLOCK; s < (b + 1) * SG_BLOCK && s < s1; s++) {
+        const float m = mul[s];
+        if (!(m >= 0.0f) || !std::isfinite(m)) {
+          hi = -1.0f;
+          break;
+        }
+        hi = std::max(hi, m);
+      }
+      bmx[b] = hi;
+    }
+  }
   x.rot_norm = powf(256.0f, -1.5f);
   int rc;
   if ((rc = upload(&x.cent, a->centroids, (size_t)K * SG_PDIM)) ||
@@ -230,14 +266,28 @@ int build_index(const sg_ivf_arrays* a, int device, sg_index** out) {
       (rc = upload(&x.clen, x.h_clen.data(), x.h_clen.size())) ||
       (rc = upload(&x.blocks, a->blocks, (size_t)nblocks * SG_BLOCK_BYTES)) ||
       (rc = upload(&x.mul, mul.data(), mul.size())) || (rc = upload(&x.err, err.data(), err.size())) ||
+      (rc = upload(&x.mul_rng, mrng.data(), mrng.size())) || (rc = upload(&x.bmax, bmx.data(), bmx.size())) ||
       (rc = upload(&x.ids, a->ids, x.nslots)) || (rc = upload(&x.rot, a->rotation, 3 * SG_PDIM)) ||
       (rc = upload(&x.rerank, a->rerank, (size_t)a->n * SG_DIM)) ||
       (rc = upload(&x.qscale, a->quant_scale, SG_DIM))) {
     free_index(x);
     return rc;
   }
-  if ((rc = dalloc(&x.blocks_mma, (size_t)nblocks * 256)) ||
-      sg::transcode_mma(x.blocks, nblocks, x.blocks_mma) || cudaDeviceSynchronize() != cudaSuccess) {
+  // the batched tensor-core scan reads its own copy of the codes: slot-major for tcgen05 (the
+  // default), or the mma.sync word order when SIEVE_GPU_TC=0
+  if (const char* tc = getenv("SIEVE_GPU_TC")) h->cfg.tc = atoi(tc);
+  if (h->cfg.tc) {
+    if ((rc = dalloc(&x.blocks_tc, (size_t)nblocks * 256))) {
+      free_index(x);
+      return rc;
+    }
+    sg::transcode_tc(x.blocks, nblocks, x.blocks_tc, 0);
+    if (cudaGetLastError() != cudaSuccess || cudaDeviceSynchronize() != cudaSuccess) {
+      free_index(x);
+      return fail(SG_ERR_DEVICE, "transcode of the code blocks failed");
+    }
+  } else if ((rc = dalloc(&x.blocks_mma, (size_t)nblocks * 256)) ||
+             sg::transcode_mma(x.blocks, nblocks, x.blocks_mma) || cudaDeviceSynchronize() != cudaSuccess) {
     free_index(x);
     return rc ? rc : fail(SG_ERR_DEVICE, "transcode of the code blocks failed");
   }
@@ -420,7 +470,8 @@ int check_params(const sg_index* h, const sg_params* p) {
 // probed cluster; SIEVE_GPU_MMA forces it off (0) or on (2).)
 bool use_mma(const sg_index* h, uint32_t nq, uint32_t P) {
   const sg::DevIndex& x = h->ix;
-  if (!x.blocks_mma || P <= 1 || P > 4096) return false;  // inverted lists keep 12-bit ranks
+  if (!(h->cfg.tc ? x.blocks_tc : x.blocks_mma) || P <= 1 || P > 4096)
+    return false;  // inverted lists keep 12-bit ranks
   if (h->cfg.mma == 2) return true;
   return h->cfg.mma == 1 && nq >= 64 &&
          (uint64_t)nq * (P - 1) >= (uint64_t)h->cfg.mma_min_queries_per_cluster * x.k;
@@ -490,7 +541,9 @@ int run_pipeline(sg_index* h, sg::Ctx& c, uint32_t nq, const sg_params& p, bool 
                     h->cfg.scan_ctas_per_sm, st);
     if (timed) CK(cudaEventRecord(w.ev[9], st));
     sg::launch_scan(x, w, nq, p, d_allow, allow_words, h->sms, cb, 0, h->cfg.scan_ctas_per_sm, st);
-    if (mma) launches += sg::launch_scan_mma(x, w, nq, p, d_allow, allow_words, h->sms, st);
+    if (mma)
+      launches += h->cfg.tc ? sg::launch_scan_tc(x, w, nq, p, d_allow, allow_words, h->sms, st)
+                            : sg::launch_scan_mma(x, w, nq, p, d_allow, allow_words, h->sms, st);
     if (timed) CK(cudaEventRecord(w.ev[4], st));
     sg::launch_cut(x, w, nq, p, st);
     launches += 3;
@@ -652,6 +705,7 @@ int search_impl(sg_index* h, sg::Ctx& c, uint32_t nq, const float* q768, const f
   }
   CK(cudaStreamSynchronize(c.stream));
   if (status & sg::kStatusOverflow) return fail(SG_ERR_INVALID, "work queue overflow");
+  if (status & sg::kStatusTimeout) return fail(SG_ERR_DEVICE, "tensor-core scan: a pipeline wait ran out");
   const bool timed = t != nullptr || h->timing_on;
   if (timed) {
     collect_stats(w, p);
@@ -1238,6 +1292,46 @@ int sg_lut_scan(uint32_t groups, const uint8_t* tables, const uint8_t* blocks, u
     e = cudaMemcpy(out_scores, dout, nblocks * SG_BLOCK * 2, cudaMemcpyDeviceToHost);
   dfree(dt); dfree(db); dfree(dout);
   if (e != cudaSuccess) return fail(SG_ERR_DEVICE, std::string("sg_lut_scan: ") + cudaGetErrorString(e));
+  return SG_OK;
+}
+
+int sg_lut_scan_batch(uint32_t nq, const uint8_t* tables, const uint8_t* blocks, uint64_t nblocks,
+                      uint16_t* out_scores) {
+  if ((nq && !tables) || (nblocks && !blocks) || (nq && nblocks && !out_scores))
+    return fail(SG_ERR_INVALID, "null argument");
+  if (nq == 0 || nblocks == 0) return SG_OK;
+  if ((uint64_t)nq * nblocks * SG_BLOCK > (1ull << 34)) return fail(SG_ERR_INVALID, "output above 2^34 scores");
+  int dev = 0, sms = 0;
+  CK(cudaGetDevice(&dev));
+  CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+  uint8_t *dt = nullptr, *db = nullptr;
+  uint32_t *dc = nullptr, *dcnt = nullptr;
+  uint16_t* dout = nullptr;
+  const uint64_t nslots = nblocks * SG_BLOCK;
+  int rc;
+  if ((rc = dalloc(&dt, (size_t)nq * SG_GROUPS * 16)) || (rc = dalloc(&db, nblocks * SG_BLOCK_BYTES)) ||
+      (rc = dalloc(&dc, nblocks * 256)) || (rc = dalloc(&dcnt, 2)) || (rc = dalloc(&dout, nq * nslots))) {
+    dfree(dt); dfree(db); dfree(dc); dfree(dcnt); dfree(dout);
+    return rc;
+  }
+  cudaError_t e = cudaMemcpy(dt, tables, (size_t)nq * SG_GROUPS * 16, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMemcpy(db, blocks, nblocks * SG_BLOCK_BYTES, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMemset(dcnt, 0, 8);
+  if (e == cudaSuccess) {
+    sg::transcode_tc(db, nblocks, dc, 0);
+    e = cudaGetLastError();
+  }
+  if (e == cudaSuccess) {
+    sg::launch_lut_scan_tc(nq, dt, dc, nblocks, dout, dcnt, sms, 0);
+    e = cudaGetLastError();
+  }
+  if (e == cudaSuccess) e = cudaDeviceSynchronize();
+  uint32_t status = 0;
+  if (e == cudaSuccess) e = cudaMemcpy(&status, dcnt, 4, cudaMemcpyDeviceToHost);
+  if (e == cudaSuccess) e = cudaMemcpy(out_scores, dout, nq * nslots * 2, cudaMemcpyDeviceToHost);
+  dfree(dt); dfree(db); dfree(dc); dfree(dcnt); dfree(dout);
+  if (e != cudaSuccess) return fail(SG_ERR_DEVICE, std::string("sg_lut_scan_batch: ") + cudaGetErrorString(e));
+  if (status & sg::kStatusTimeout) return fail(SG_ERR_DEVICE, "sg_lut_scan_batch: a pipeline wait ran out");
   return SG_OK;
 }
 

@@ -4,10 +4,11 @@ reference's ivf module; `filter` mirrors filter::Filter / Plan / search; `Server
 loop (continuous batching); `bigann` is the billion-scale L2 path; `builder` and `bigann_builder`
 write the reference's index files; `synth` makes the seeded synthetic corpora the workloads run on.
 """
-from .index import Index, Params, Rerank, Timing, allow_bitset, dot_i8i8, lut_scan, parse_config
+from .index import (Index, Params, Rerank, Timing, allow_bitset, dot_i8i8, lut_scan, lut_scan_batch,
+                    parse_config)
 from ._abi import SieveError
 from . import filter
 from .server import Server
 
-__all__ = ["Index", "Params", "Rerank", "Timing", "parse_config", "allow_bitset", "lut_scan",
+__all__ = ["Index", "Params", "Rerank", "Timing", "parse_config", "allow_bitset", "lut_scan", "lut_scan_batch",
            "dot_i8i8", "SieveError", "filter", "Server"]

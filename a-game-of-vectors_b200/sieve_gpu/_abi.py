@@ -263,6 +263,7 @@ EXPORTS = [
     "sg_bigann_candidates",
     "sg_query_prep",
     "sg_lut_scan",
+    "sg_lut_scan_batch",
     "sg_dot_i8i8",
 ]
 

@@ -284,6 +284,17 @@ def lut_scan(tables: np.ndarray, blocks: np.ndarray) -> np.ndarray:
     return out
 
 
+def lut_scan_batch(tables: np.ndarray, blocks: np.ndarray) -> np.ndarray:
+    """lut::scan (src/lut.rs:96-102, 64 groups) of many queries at once on the tcgen05 tensor
+    cores: tables [nq, 1024] u8, blocks [nblocks * 1024] u8 -> u16 scores [nq, nblocks * 32]."""
+    tables = np.ascontiguousarray(tables, np.uint8).reshape(-1, 64 * 16)
+    blocks = np.ascontiguousarray(blocks, np.uint8)
+    nb = blocks.size // (64 * 16)
+    out = np.zeros((tables.shape[0], nb * 32), np.uint16)
+    check(lib().sg_lut_scan_batch(c_uint32(tables.shape[0]), ptr(tables), ptr(blocks), c_uint64(nb), ptr(out)))
+    return out
+
+
 def dot_i8i8(query: np.ndarray, rows: np.ndarray) -> np.ndarray:
     """quant::dot_i8i8 (src/quant.rs:113-125) of one query against many rows, on the GPU."""
     query = np.ascontiguousarray(query, np.int8)

@@ -191,11 +191,14 @@ def cpu_reference(arrays, q768_host: np.ndarray, params, seconds: float, threads
     t = time.perf_counter()
     oi.search_batch(q768_host[:probe], q256[:probe], p, threads=threads)
     per_q = (time.perf_counter() - t) / probe
-    n = int(min(q768_host.shape[0], max(probe, seconds / max(per_q, 1e-9))))
+    # the sample cycles through the query pool until it holds about `seconds` of work
+    n = int(max(probe, seconds / max(per_q, 1e-9)))
+    sel = np.arange(n) % q768_host.shape[0]
     t = time.perf_counter()
-    s, o, c, scanned = oi.search_batch(q768_host[:n], q256[:n], p, threads=threads)
+    s, o, c, scanned = oi.search_batch(q768_host[sel], q256[sel], p, threads=threads)
     dt = time.perf_counter() - t
-    return {"qps": n / dt, "queries": n, "seconds": dt, "ids": o, "cnt": c}
+    k = min(n, q768_host.shape[0])
+    return {"qps": n / dt, "queries": n, "seconds": dt, "ids": o[:k], "cnt": c[:k]}
 
 
 def serve_load(index, arrays, queries_host: np.ndarray, params, rates, seconds: float, seed: int = 7):

@@ -358,6 +358,11 @@ int sg_query_prep(sg_index* index, uint32_t nq, const float* q256, uint8_t* out_
  * 32 per block, against one u8 table set [groups * 16]. Stateless (no index needed). */
 int sg_lut_scan(uint32_t groups, const uint8_t* tables, const uint8_t* blocks, uint64_t nblocks,
                 uint16_t* out_scores);
+/* lut::scan (src/lut.rs:96-126, G = 64) of nq query table sets [nq * 64 * 16] against nblocks
+ * blocks, on the tcgen05 tensor cores (the contraction of the batched scan): u16 scores
+ * out_scores[q * nblocks * 32 + slot]. Stateless. */
+int sg_lut_scan_batch(uint32_t nq, const uint8_t* tables, const uint8_t* blocks, uint64_t nblocks,
+                      uint16_t* out_scores);
 /* quant::dot_i8i8 (src/quant.rs:113-125) of one int8 query against `rows` int8 rows of
  * length dim (a multiple of 4): exact int32 dots. Stateless. */
 int sg_dot_i8i8(const int8_t* query, const int8_t* rows, uint64_t nrows, uint32_t dim,

@@ -21,21 +21,24 @@ def cparams(p: Params) -> SgParams:
 
 
 def open_with(arrays, scan_mode: str):
-    """Opens an index with the scan chosen by SIEVE_GPU_MMA (0 ALU, 1 automatic, 2 tensor-core)."""
+    """Opens an index with the scan chosen by SIEVE_GPU_MMA (0 ALU, 1 automatic, 2 tensor-core);
+    a suffix "s" selects the mma.sync tensor-core scan instead of tcgen05 (SIEVE_GPU_TC=0)."""
     import os
 
-    old = os.environ.get("SIEVE_GPU_MMA")
-    os.environ["SIEVE_GPU_MMA"] = scan_mode
+    env = {"SIEVE_GPU_MMA": scan_mode.rstrip("s"), "SIEVE_GPU_TC": "0" if scan_mode.endswith("s") else "1"}
+    old = {k: os.environ.get(k) for k in env}
+    os.environ.update(env)
     try:
         return Index.from_arrays(arrays)
     finally:
-        if old is None:
-            del os.environ["SIEVE_GPU_MMA"]
-        else:
-            os.environ["SIEVE_GPU_MMA"] = old
+        for k, v in old.items():
+            if v is None:
+                del os.environ[k]
+            else:
+                os.environ[k] = v
 
 
-@pytest.fixture(scope="module", params=["1", "2", "0"], ids=["auto", "mma", "alu"])
+@pytest.fixture(scope="module", params=["1", "2", "2s", "0"], ids=["auto", "mma", "mma_sync", "alu"])
 def gpu_a(request):
     arrays, q768, q256, _ = index_a()
     ix = open_with(arrays, request.param)
@@ -43,7 +46,7 @@ def gpu_a(request):
     ix.close()
 
 
-@pytest.fixture(scope="module", params=["1", "2"], ids=["auto", "mma"])
+@pytest.fixture(scope="module", params=["1", "2", "2s"], ids=["auto", "mma", "mma_sync"])
 def gpu_b(request):
     arrays, q768, q256, _ = index_b()
     ix = open_with(arrays, request.param)
