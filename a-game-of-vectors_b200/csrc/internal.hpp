@@ -46,8 +46,6 @@ struct DevIndex {
   uint32_t* blocks_mma = nullptr;    // [nblocks*256] the same codes in the mma.sync scan's word order
   uint32_t* blocks_tc = nullptr;     // [nslots*8] the same codes slot-major (tcgen05 scan)
   float* mul = nullptr;              // [nslots] factors.f32 [.., 0]
-  float* bmax = nullptr;             // [nblocks] largest mul of each block's real slots (-1 where
-                                     // one is negative or not finite): the tcgen05 scan's floors
   float2* mul_rng = nullptr;         // [k] (min, max) of mul over each cluster's real slots;
                                      // min = -1 where the range bound does not apply
   float* err = nullptr;              // [nslots] factors.f32 [.., 1]
@@ -174,6 +172,7 @@ struct Config {
   uint32_t mma_min_queries_per_cluster = 8;   // use the MMA scan at or above this average
   int mma = 1;            // SIEVE_GPU_MMA: 0 ALU scan only, 1 automatic, 2 MMA whenever nprobe > 1
   int tc = 1;             // SIEVE_GPU_TC: 1 the tcgen05 scan, 0 the mma.sync scan (kept for comparison)
+  uint32_t tc_split = 0;  // SIEVE_GPU_TC_SPLIT (> 1): a first tcgen05 round over the ranks below it
 };
 
 std::string& last_error();
@@ -210,10 +209,13 @@ void launch_route_select(const DevIndex& ix, Workspace& w, uint32_t nq, const sg
 int launch_scan_mma(const DevIndex& ix, Workspace& w, uint32_t nq, const sg_params& p,
                     const uint64_t* allow, uint64_t allow_words, int sms, cudaStream_t st);
 int transcode_mma(const uint8_t* blocks, uint64_t nblocks, uint32_t* out);
-void launch_invert(const DevIndex& ix, Workspace& w, uint32_t nq, uint32_t P, uint32_t qg, cudaStream_t st);
+void launch_invert(const DevIndex& ix, Workspace& w, uint32_t nq, uint32_t P, uint32_t qg, uint32_t rlo,
+                   uint32_t rhi, cudaStream_t st);
 // The batched scan on tcgen05 (scan_tc.cu): same work items and admission as launch_scan_mma.
+// With split > 1 it scans probe ranks [1, split) first, raises every query's threshold to the
+// cand-th best estimate its buffer then holds, and scans the remaining ranks.
 int launch_scan_tc(const DevIndex& ix, Workspace& w, uint32_t nq, const sg_params& p,
-                   const uint64_t* allow, uint64_t allow_words, int sms, cudaStream_t st);
+                   const uint64_t* allow, uint64_t allow_words, int sms, uint32_t split, cudaStream_t st);
 // Launch errors of these two are left for the caller's cudaGetLastError.
 void transcode_tc(const uint8_t* blocks, uint64_t nblocks, uint32_t* out, cudaStream_t st);
 void launch_lut_scan_tc(uint32_t nq, const uint8_t* tables, const uint32_t* codes, uint64_t nblocks,

@@ -51,12 +51,12 @@ int transcode_mma(const uint8_t* blocks, uint64_t nblocks, uint32_t* out) {
 // ---- inversion of the probe lists ----------------------------------------------------------
 // Probes the seed covered (seed_items[q].y) are not scanned again.
 __global__ void k_inv_count(const uint32_t* __restrict__ probe_cl, const uint32_t* __restrict__ probe_n,
-                            const uint4* __restrict__ seed, uint32_t P, uint32_t nq,
+                            const uint4* __restrict__ seed, uint32_t P, uint32_t nq, uint32_t rlo, uint32_t rhi,
                             uint32_t* __restrict__ cnt) {
   const uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= (uint64_t)nq * P) return;
   const uint32_t q = (uint32_t)(t / P), r = (uint32_t)(t % P);
-  if (r < seed[q].y || r >= probe_n[q]) return;
+  if (r < seed[q].y || r >= probe_n[q] || r < rlo || r >= rhi) return;
   atomicAdd(cnt + probe_cl[t], 1u);
 }
 
@@ -91,13 +91,13 @@ __global__ void __launch_bounds__(1024) k_inv_scan(const uint32_t* __restrict__ 
 }
 
 __global__ void k_inv_fill(const uint32_t* __restrict__ probe_cl, const uint32_t* __restrict__ probe_n,
-                           const uint4* __restrict__ seed, uint32_t P, uint32_t nq,
+                           const uint4* __restrict__ seed, uint32_t P, uint32_t nq, uint32_t rlo, uint32_t rhi,
                            const uint32_t* __restrict__ off, uint32_t* __restrict__ fill,
                            uint32_t* __restrict__ list) {
   const uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= (uint64_t)nq * P) return;
   const uint32_t q = (uint32_t)(t / P), r = (uint32_t)(t % P);
-  if (r < seed[q].y || r >= probe_n[q]) return;
+  if (r < seed[q].y || r >= probe_n[q] || r < rlo || r >= rhi) return;
   const uint32_t c = probe_cl[t];
   list[off[c] + atomicAdd(fill + c, 1u)] = (q << 12) | r;
 }
@@ -360,23 +360,25 @@ __global__ void __launch_bounds__(256, 2) k_scan_mma(MmaArgs a) {
   }
 }
 
-// Per-cluster query lists of the (query, probe) pairs the seed left, cut into (cluster, group)
-// work items of up to qg queries (counters[4] items, counters[5] the next one to take).
-void launch_invert(const DevIndex& ix, Workspace& w, uint32_t nq, uint32_t P, uint32_t qg, cudaStream_t st) {
+// Per-cluster query lists of the (query, probe) pairs the seed left with probe rank in
+// [rlo, rhi), cut into (cluster, group) work items of up to qg queries (counters[4] items,
+// counters[5] the next one to take).
+void launch_invert(const DevIndex& ix, Workspace& w, uint32_t nq, uint32_t P, uint32_t qg, uint32_t rlo,
+                   uint32_t rhi, cudaStream_t st) {
   const uint64_t pairs = (uint64_t)nq * P;
   cudaMemsetAsync(w.inv_cnt, 0, (size_t)ix.k * 4, st);
   cudaMemsetAsync(w.inv_fill, 0, (size_t)ix.k * 4, st);
   const unsigned grid = (unsigned)((pairs + 255) / 256);
-  k_inv_count<<<grid, 256, 0, st>>>(w.probe_cl, w.probe_n, w.seed_items, P, nq, w.inv_cnt);
+  k_inv_count<<<grid, 256, 0, st>>>(w.probe_cl, w.probe_n, w.seed_items, P, nq, rlo, rhi, w.inv_cnt);
   k_inv_scan<<<1, 1024, 0, st>>>(w.inv_cnt, ix.k, qg, w.inv_off, w.gitems, w.gitems_cap, w.counters);
-  k_inv_fill<<<grid, 256, 0, st>>>(w.probe_cl, w.probe_n, w.seed_items, P, nq, w.inv_off, w.inv_fill,
+  k_inv_fill<<<grid, 256, 0, st>>>(w.probe_cl, w.probe_n, w.seed_items, P, nq, rlo, rhi, w.inv_off, w.inv_fill,
                                    w.inv_list);
 }
 
 int launch_scan_mma(const DevIndex& ix, Workspace& w, uint32_t nq, const sg_params& p,
                     const uint64_t* allow, uint64_t allow_words, int sms, cudaStream_t st) {
   const uint32_t P = p.nprobe < ix.k ? p.nprobe : ix.k;
-  launch_invert(ix, w, nq, P, kQG, st);
+  launch_invert(ix, w, nq, P, kQG, 0, P, st);
   MmaArgs a;
   a.bmma = ix.blocks_mma;
   a.mul = ix.mul;

@@ -20,11 +20,12 @@
 //     accumulators and signals the A stages and the accumulator through mbarriers
 //     (tcgen05.commit);
 //   - eight epilogue warps (two per TMEM lane quarter, taking alternate tiles) read the s32
-//     scores with tcgen05.ld (one slot per thread, one query per column), reject every score
-//     below the (query, block) integer floor, and form est = cent + mul*(a*score + b) exactly as
-//     the ALU scan does for the rest. Each warp reserves room for its admitted slots with one
-//     atomic per query column, all columns' atomics in flight together, and appends every
-//     eligible slot at or above the query's threshold to the query's candidate buffer.
+//     scores with tcgen05.ld (one slot per thread, one query per column) and form
+//     est = cent + mul*(a*score + b) for every column in straight-line code, exactly as the ALU
+//     scan does. The admitted (slot, query) bits are transposed across the warp so that each
+//     column reserves room for its admitted slots with one atomic, all columns' atomics in
+//     flight together, and the entries are written one chunk later, when the reservations have
+//     returned.
 // Every mbarrier wait is bounded: a wait that runs out raises kStatusTimeout, every role stops,
 // and the kernel frees its tensor memory and returns.
 //
@@ -47,11 +48,10 @@ constexpr int kTcMma = 12;          // warp 12 issues the MMAs
 constexpr int kTcLoader = 13;       // warp 13 loads work items
 constexpr int kTcThreads = 14 * 32;
 constexpr int kTcBBytes = kTcQG * 1024;  // B of one item slot
-constexpr int kTcVStride = 36;      // words per lane row of the epilogue's score spill
+constexpr int kTcVStride = 68;      // words per lane row of the epilogue's spills (2 x 32 + pad)
 constexpr int kTcVBytes = kTcEpiWarps * 32 * kTcVStride * 4;  // the epilogue warps' spills
 constexpr uint64_t kTcWaitNs = 2000000000ull;  // a pipeline wait gives up after 2 s
 constexpr uint32_t kTcSpinLimit = 1u << 30;    // backstop on the number of polls
-constexpr uint32_t kTcMaxScore = SG_GROUPS * 255;
 
 // ---- slot-major codes ----------------------------------------------------------------------
 // Slot s's 64 nibbles in 8 words (32 B): group g at word g/8, bits 4*(g%8). Source: blocks.bin,
@@ -194,29 +194,10 @@ SG_DEV void onehot8(uint32_t w, uint32_t* r) {
 }
 
 
-// Integer floor on the LUT score of a (query, block): every slot of the block with a lower score
-// has est < T, the query's threshold. With est = fl(cent + fl(m * fl(fl(a*s) + b))), the real
-// value E = cent + m*(a*s + b) is within D = 2u*(M*(4*a*16320 + 3|b|) + |cent|) (u = 2^-24, M
-// the cluster's largest mul) of est, so est >= T needs m*(a*s + b) >= R = T - D - cent. For
-// R > 0, 0 <= m <= Mb (the block's largest mul) and a > 0 that means s >= (R/Mb - b)/a. The
-// loader precomputes R, b and 1/a per query in double; ia = 0 marks "no bound" (no threshold
-// yet, or inputs the bound does not cover), and a block with Mb < 0 holds a negative or non-finite
-// mul. One score unit is subtracted for the double rounding.
-SG_DEV int tc_floor(double R, double bd, double ia, float Mb) {
-  if (!(ia > 0.0) || !(Mb >= 0.0f) || !(R > 0.0)) return 0;
-  if (Mb == 0.0f) return (int)kTcMaxScore + 1;  // est = cent < T for every slot
-  const double x = (R / (double)Mb - bd) * ia;
-  if (!(x == x)) return 0;
-  if (x >= (double)(kTcMaxScore + 2)) return (int)kTcMaxScore + 1;
-  if (x <= 1.0) return 0;
-  return (int)floor(x - 1.0);
-}
-
 struct TcArgs {
   const uint4* codes;  // [nslots * 2] slot-major codes
   // admission form
   const float* mul;
-  const float* bmax;   // [nblocks] largest mul of each block (-1: a negative or non-finite one)
   const uint32_t* ids;
   const uint32_t* block_off;
   const uint32_t* clen;
@@ -257,9 +238,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_scan_tc(TcArgs a) {
   __shared__ uint32_t s_meta[2][8];  // b0, nb, cl, ng, qbase, end
   __shared__ float4 s_qc[2][kTcQG];  // cent, a, b, threshold key (as bits)
   __shared__ uint2 s_qk[2][kTcQG];   // candidate order base, query
-  __shared__ double s_R[2][kTcQG], s_bd[2][kTcQG], s_ia[2][kTcQG];
-  __shared__ __align__(16) int s_wfl[kTcEpiWarps][kTcQG];  // (query, block) floors of the epilogue warps
-  __shared__ uint2 s_cb[kTcEpiWarps][32];                  // per column: reserved base, admitted lanes
+  __shared__ uint2 s_cb[kTcEpiWarps][2][32];               // per column: reserved base, admitted lanes
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   volatile int* abort_flag = &s_abort;
 
@@ -354,20 +333,6 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_scan_tc(TcArgs a) {
           const uint32_t thr = *(volatile const uint32_t*)(a.thr + q);
           s_qc[slot][qi] = make_float4(cent, p.z, p.w, __uint_as_float(thr));
           s_qk[slot][qi] = make_uint2(a.probe_off[(size_t)q * a.P + r], q);
-          const float2 mr = a.mul_rng[c];
-          const float T = unord(thr);
-          double R = 0.0, ia = 0.0;
-          if (thr != 0 && mr.x >= 0.0f && isfinite(mr.y) && p.z > 0.0f && isfinite(p.z) && isfinite(p.w) &&
-              isfinite(cent) && isfinite(T)) {
-            const double u = 1.0 / 16777216.0;
-            const double d = 2.0 * u * ((double)mr.y * (4.0 * (double)p.z * kTcMaxScore + 3.0 * fabs((double)p.w)) +
-                                        fabs((double)cent)) + 1e-37;
-            R = (double)T - d - (double)cent;
-            ia = 1.0 / (double)p.z;
-          }
-          s_R[slot][qi] = R;
-          s_bd[slot][qi] = (double)p.w;
-          s_ia[slot][qi] = ia;
         }
       }
       if (lane == 0) {
@@ -463,33 +428,49 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_scan_tc(TcArgs a) {
         const uint32_t ew = warp - kTcEpi, qd = ew & 3, par = ew >> 2;
         const uint32_t lane_base = (32u * qd) << 16;
         const uint32_t ncc = (N + 31) >> 5;
-        int* wfl = s_wfl[ew];
-        uint2* cb = s_cb[ew];
+        uint2* cb = &s_cb[ew][0][0];
         uint32_t* vrow = reinterpret_cast<uint32_t*>(smem + 2 * kTcBBytes) + (ew * 32 + lane) * kTcVStride;
-        // the warp's next tile's mul and block maximum are loaded one tile ahead
-        auto tile_loads = [&](uint32_t t, float& mv, float& mb) {
+        const uint32_t lt = (1u << lane) - 1u;
+        // A chunk's entries are written one chunk later, so the atomic that reserves their room
+        // is in flight meanwhile: p_* is the pending chunk (its spill row and column ballots in
+        // buffer p_buf, its reservation in p_base).
+        bool p_on = false;
+        uint32_t p_adm = 0, p_base = 0, p_loc = 0, p_gslot = 0, p_c0 = 0, p_buf = 0;
+        auto flush = [&]() {
+          if (!p_on) return;  // warp-uniform
+          uint2* cbp = cb + p_buf * 32;
+          cbp[lane].x = p_base;
+          __syncwarp();
+          for (uint32_t r = p_adm; r; r &= r - 1) {
+            const uint32_t j = __ffs(r) - 1;
+            const uint2 bc = cbp[j];
+            const uint2 qk = s_qk[slot][p_c0 + j];
+            const uint32_t pos = bc.x + (uint32_t)__popc(bc.y & lt);
+            if (pos < a.cap) {
+              a.cbuf_est[(size_t)qk.y * a.cap + pos] = vrow[p_buf * 32 + j];
+              a.cbuf_info[(size_t)qk.y * a.cap + pos] = make_uint2(qk.x + p_loc, p_gslot);
+            } else {
+              a.overflow[qk.y] = 1;
+            }
+          }
+          __syncwarp();
+          p_on = false;
+        };
+        // the warp's next tile's mul values are loaded one tile ahead
+        auto tile_mul = [&](uint32_t t) {
           const uint32_t bl = 4 * t + qd;
-          mv = 0.0f;
-          mb = -1.0f;
-          if (kRaw || t >= ntiles || bl >= nb) return;
-          mb = a.bmax[b0 + bl];
-          if (bl * SG_BLOCK + lane < cl) mv = a.mul[(b0 + bl) * SG_BLOCK + lane];
+          if (kRaw || t >= ntiles || bl >= nb || bl * SG_BLOCK + lane >= cl) return 0.0f;
+          return a.mul[(b0 + bl) * SG_BLOCK + lane];
         };
         const uint32_t t0 = ((ts & 1) == par) ? 0 : 1;  // first tile of this warp's parity
-        float mv, mb, nmv, nmb;
-        tile_loads(t0, mv, mb);
+        float mv = tile_mul(t0);
         for (uint32_t t = t0; t < ntiles; t += 2) {
           const uint32_t ds = ts + t, dbuf = ds & (kTcDBufs - 1), duse = ds / kTcDBufs;
           const uint32_t bl = 4 * t + qd;
           const uint32_t loc = bl * SG_BLOCK + lane;
           const bool lane_ok = bl < nb && loc < cl;
           const uint32_t gslot = (b0 + bl) * SG_BLOCK + lane;
-          tile_loads(t + 2, nmv, nmb);
-          if (!kRaw) {
-            for (uint32_t qi = lane; qi < (uint32_t)kTcQG; qi += 32)
-              wfl[qi] = qi < ng ? tc_floor(s_R[slot][qi], s_bd[slot][qi], s_ia[slot][qi], mb) : 0x7FFFFFFF;
-            __syncwarp();
-          }
+          const float nmv = tile_mul(t + 2);
           if (!mbar_wait(&bar_dfull[dbuf], duse & 1, abort_flag)) break;
           tc_fence_after();
           for (uint32_t cc = 0; cc < ncc; cc++) {
@@ -504,73 +485,67 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_scan_tc(TcArgs a) {
               }
               continue;
             }
-            uint32_t m = 0;
+            // 1. every column's estimate, exactly as the ALU scan forms it (the score is exact in
+            //    f32 through the 2^23 bias trick), and its admission test against the query's key
+            const uint32_t cbuf = p_on ? (p_buf ^ 1) : 0;
+            uint32_t* vr = vrow + cbuf * 32;
+            const uint32_t ncol = min(32u, ng - 32 * cc);
+            uint32_t adm = 0;
 #pragma unroll
             for (int j4 = 0; j4 < 8; j4++) {
-              const int4 f = *reinterpret_cast<const int4*>(wfl + 32 * cc + 4 * j4);
-              m |= ((int)v[4 * j4 + 0] >= f.x ? 1u : 0u) << (4 * j4 + 0);
-              m |= ((int)v[4 * j4 + 1] >= f.y ? 1u : 0u) << (4 * j4 + 1);
-              m |= ((int)v[4 * j4 + 2] >= f.z ? 1u : 0u) << (4 * j4 + 2);
-              m |= ((int)v[4 * j4 + 3] >= f.w ? 1u : 0u) << (4 * j4 + 3);
-            }
-            if (!lane_ok) m = 0;
-            if (!__any_sync(0xFFFFFFFFu, m != 0)) continue;
+              uint32_t e4[4];
 #pragma unroll
-            for (int j4 = 0; j4 < 8; j4++)
-              *reinterpret_cast<uint4*>(vrow + 4 * j4) = make_uint4(v[4 * j4], v[4 * j4 + 1], v[4 * j4 + 2], v[4 * j4 + 3]);
-            // 1. exact admission of the lane's columns above the floor; an admitted column's
-            //    estimate replaces its score in the spill row
-            uint32_t adm = 0;
-            while (m) {
-              const uint32_t j = __ffs(m) - 1;
-              m &= m - 1;
-              const uint32_t qi = 32 * cc + j;
-              const float4 qc = s_qc[slot][qi];
-              const float est = __fadd_rn(qc.x, __fmul_rn(mv, __fadd_rn(__fmul_rn(qc.y, (float)vrow[j]), qc.z)));
-              if (ord(est) < __float_as_uint(qc.w)) continue;
-              const uint32_t q = s_qk[slot][qi].y;
-              const uint64_t* al = a.allow_q ? a.allow_q[q] : a.allow;
-              const uint64_t aw = a.allow_q ? a.allow_wq[q] : a.allow_words;
-              if (al && !allowed(al, aw, a.ids[gslot])) continue;
-              adm |= 1u << j;
-              vrow[j] = __float_as_uint(est);
+              for (int e = 0; e < 4; e++) {
+                const int j = 4 * j4 + e;
+                const float4 qc = s_qc[slot][32 * cc + j];
+                const float sf = __fsub_rn(__uint_as_float(v[j] | 0x4B000000u), 8388608.0f);
+                const float est = __fadd_rn(qc.x, __fmul_rn(mv, __fadd_rn(__fmul_rn(qc.y, sf), qc.z)));
+                e4[e] = __float_as_uint(est);
+                adm |= (ord(est) >= __float_as_uint(qc.w) ? 1u : 0u) << j;
+              }
+              *reinterpret_cast<uint4*>(vr + 4 * j4) = make_uint4(e4[0], e4[1], e4[2], e4[3]);
             }
-            __syncwarp();
-            const uint32_t amask = __reduce_or_sync(0xFFFFFFFFu, adm);
-            if (!amask) continue;
-            // 2. lane j takes column j's admitted lanes and reserves their room with one atomic;
-            //    the atomics of all columns are in flight together
-            uint32_t col = 0;
-            for (uint32_t r = amask; r; r &= r - 1) {
-              const uint32_t j = __ffs(r) - 1;
-              const uint32_t bal = __ballot_sync(0xFFFFFFFFu, (adm >> j) & 1u);
-              if (lane == j) col = bal;
+            adm &= lane_ok ? (ncol == 32 ? 0xFFFFFFFFu : (1u << ncol) - 1u) : 0u;
+            if (adm && (a.allow || a.allow_q)) {  // allowlist filters (View::hidden)
+              const uint32_t id = a.ids[gslot];
+              for (uint32_t r = adm; r; r &= r - 1) {
+                const uint32_t j = __ffs(r) - 1;
+                const uint32_t q = s_qk[slot][32 * cc + j].y;
+                const uint64_t* al = a.allow_q ? a.allow_q[q] : a.allow;
+                const uint64_t aw = a.allow_q ? a.allow_wq[q] : a.allow_words;
+                if (al && !allowed(al, aw, id)) adm &= ~(1u << j);
+              }
+            }
+            if (!__any_sync(0xFFFFFFFFu, adm != 0)) continue;
+            // 2. the 32 x 32 bit matrix (lane = slot, bit = column) transposed across the warp:
+            //    lane j then holds column j's admitted lanes and reserves their room with one atomic
+            uint32_t col = adm;
+#pragma unroll
+            for (int w = 16; w >= 1; w >>= 1) {
+              const uint32_t lo = w == 16 ? 0x0000FFFFu : w == 8 ? 0x00FF00FFu : w == 4 ? 0x0F0F0F0Fu
+                                  : w == 2 ? 0x33333333u : 0x55555555u;
+              const uint32_t y = __shfl_xor_sync(0xFFFFFFFFu, col, w);
+              col = (lane & w) ? ((col & ~lo) | ((y & ~lo) >> w)) : ((col & lo) | ((y & lo) << w));
             }
             uint32_t base = 0;
             if (col) base = atomicAdd(a.ccount + s_qk[slot][32 * cc + lane].y, (uint32_t)__popc(col));
-            cb[lane] = make_uint2(base, col);
-            __syncwarp();
-            // 3. each admitted (slot, query) writes its entry at the column's base + its rank
-            for (uint32_t r = adm; r; r &= r - 1) {
-              const uint32_t j = __ffs(r) - 1;
-              const uint2 bc = cb[j];
-              const uint2 qk = s_qk[slot][32 * cc + j];
-              const uint32_t pos = bc.x + (uint32_t)__popc(bc.y & ((1u << lane) - 1u));
-              if (pos < a.cap) {
-                a.cbuf_est[(size_t)qk.y * a.cap + pos] = vrow[j];
-                a.cbuf_info[(size_t)qk.y * a.cap + pos] = make_uint2(qk.x + loc, gslot);
-              } else {
-                a.overflow[qk.y] = 1;
-              }
-            }
-            __syncwarp();
+            cb[cbuf * 32 + lane] = make_uint2(0, col);
+            // 3. the previous pending chunk's entries, then this chunk becomes the pending one
+            flush();
+            p_on = true;
+            p_adm = adm;
+            p_base = base;
+            p_loc = loc;
+            p_gslot = gslot;
+            p_c0 = 32 * cc;
+            p_buf = cbuf;
           }
           tc_fence_before();
           __syncwarp();
           if (lane == 0) mbar_arrive(&bar_dempty[dbuf]);
           mv = nmv;
-          mb = nmb;
         }
+        flush();
         if (lane == 0) mbar_arrive(&bar_iempty[slot]);
       }
       ts += ntiles;
@@ -597,14 +572,30 @@ static void tc_set_attr() {
   }
 }
 
+// A query's threshold raised to the cand-th largest estimate key its candidate buffer holds.
+// Every buffered entry is a scanned slot that stays in the buffer, and the cut takes the best
+// cand entries before the SOAR dedup (src/ivf.rs:698-726), so the final cand-th estimate is at
+// least this value: slots below it can never be among the candidates.
+__global__ void __launch_bounds__(1024) k_raise_thr(const uint32_t* __restrict__ cbuf_est, uint32_t cap,
+                                                    const uint32_t* __restrict__ ccount,
+                                                    const uint8_t* __restrict__ overflow, uint32_t cand,
+                                                    uint32_t* __restrict__ thr) {
+  __shared__ uint32_t hist[2048];
+  __shared__ uint32_t tmp[32];
+  const uint32_t q = blockIdx.x;
+  const uint32_t M = min(ccount[q], cap);
+  if (overflow[q] || cand == 0 || M < cand) return;
+  const uint32_t* E = cbuf_est + (size_t)q * cap;
+  const uint32_t T = block_select_nth_u32r([&](uint32_t i) { return ord(__uint_as_float(E[i])); }, M, cand, hist, tmp);
+  if (threadIdx.x == 0 && T > thr[q]) thr[q] = T;
+}
+
 int launch_scan_tc(const DevIndex& ix, Workspace& w, uint32_t nq, const sg_params& p, const uint64_t* allow,
-                   uint64_t allow_words, int sms, cudaStream_t st) {
+                   uint64_t allow_words, int sms, uint32_t split, cudaStream_t st) {
   const uint32_t P = p.nprobe < ix.k ? p.nprobe : ix.k;
-  launch_invert(ix, w, nq, P, kTcQG, st);
   TcArgs a{};
   a.codes = reinterpret_cast<const uint4*>(ix.blocks_tc);
   a.mul = ix.mul;
-  a.bmax = ix.bmax;
   a.ids = ix.ids;
   a.block_off = ix.block_off;
   a.clen = ix.clen;
@@ -629,8 +620,16 @@ int launch_scan_tc(const DevIndex& ix, Workspace& w, uint32_t nq, const sg_param
   a.allow_q = w.per_query_allow ? w.allow_q : nullptr;
   a.allow_wq = w.allow_wq;
   tc_set_attr<false>();
+  int launches = 0;
+  if (split > 1 && split < P) {
+    launch_invert(ix, w, nq, P, kTcQG, 1, split, st);
+    k_scan_tc<false><<<sms, kTcThreads, tc_smem_bytes(), st>>>(a);
+    k_raise_thr<<<nq, 1024, 0, st>>>(w.cbuf_est, w.cbuf_per_q, w.ccount, w.overflow, p.cand, w.thr);
+    launches += 5;
+  }
+  launch_invert(ix, w, nq, P, kTcQG, split > 1 && split < P ? split : 1, P, st);
   k_scan_tc<false><<<sms, kTcThreads, tc_smem_bytes(), st>>>(a);
-  return 4;
+  return launches + 4;
 }
 
 // Raw scores of nq query tables against nblocks blocks (slot-major codes already on the device);

@@ -82,7 +82,6 @@ void free_index(sg::DevIndex& x) {
   dfree(x.blocks_tc);
   dfree(x.mul);
   dfree(x.mul_rng);
-  dfree(x.bmax);
   dfree(x.err);
   dfree(x.ids);
   dfree(x.rot);
@@ -241,22 +240,6 @@ int build_index(const sg_ivf_arrays* a, int device, sg_index** out) {
     if (x.h_clen[c] == 0) lo = 0.0f;
     mrng[c] = ok ? make_float2(lo, hi) : make_float2(-1.0f, -1.0f);
   }
-  std::vector<float> bmx(nblocks);
-  for (uint32_t c = 0; c < K; c++) {
-    const uint64_t s0 = a->block_off[c] * SG_BLOCK, s1 = s0 + x.h_clen[c];
-    for (uint64_t b = a->block_off[c]; b < a->block_off[c + 1]; b++) {
-      float hi = 0.0f;
-      for (uint64_t s = b * SG_BLOCK; s < (b + 1) * SG_BLOCK && s < s1; s++) {
-        const float m = mul[s];
-        if (!(m >= 0.0f) || !std::isfinite(m)) {
-          hi = -1.0f;
-          break;
-        }
-        hi = std::max(hi, m);
-      }
-      bmx[b] = hi;
-    }
-  }
   x.rot_norm = powf(256.0f, -1.5f);
   int rc;
   if ((rc = upload(&x.cent, a->centroids, (size_t)K * SG_PDIM)) ||
@@ -266,7 +249,7 @@ int build_index(const sg_ivf_arrays* a, int device, sg_index** out) {
       (rc = upload(&x.clen, x.h_clen.data(), x.h_clen.size())) ||
       (rc = upload(&x.blocks, a->blocks, (size_t)nblocks * SG_BLOCK_BYTES)) ||
       (rc = upload(&x.mul, mul.data(), mul.size())) || (rc = upload(&x.err, err.data(), err.size())) ||
-      (rc = upload(&x.mul_rng, mrng.data(), mrng.size())) || (rc = upload(&x.bmax, bmx.data(), bmx.size())) ||
+      (rc = upload(&x.mul_rng, mrng.data(), mrng.size())) ||
       (rc = upload(&x.ids, a->ids, x.nslots)) || (rc = upload(&x.rot, a->rotation, 3 * SG_PDIM)) ||
       (rc = upload(&x.rerank, a->rerank, (size_t)a->n * SG_DIM)) ||
       (rc = upload(&x.qscale, a->quant_scale, SG_DIM))) {
@@ -276,6 +259,7 @@ int build_index(const sg_ivf_arrays* a, int device, sg_index** out) {
   // the batched tensor-core scan reads its own copy of the codes: slot-major for tcgen05 (the
   // default), or the mma.sync word order when SIEVE_GPU_TC=0
   if (const char* tc = getenv("SIEVE_GPU_TC")) h->cfg.tc = atoi(tc);
+  if (const char* sp = getenv("SIEVE_GPU_TC_SPLIT")) h->cfg.tc_split = (uint32_t)strtoul(sp, nullptr, 10);
   if (h->cfg.tc) {
     if ((rc = dalloc(&x.blocks_tc, (size_t)nblocks * 256))) {
       free_index(x);
@@ -542,7 +526,7 @@ int run_pipeline(sg_index* h, sg::Ctx& c, uint32_t nq, const sg_params& p, bool 
     if (timed) CK(cudaEventRecord(w.ev[9], st));
     sg::launch_scan(x, w, nq, p, d_allow, allow_words, h->sms, cb, 0, h->cfg.scan_ctas_per_sm, st);
     if (mma)
-      launches += h->cfg.tc ? sg::launch_scan_tc(x, w, nq, p, d_allow, allow_words, h->sms, st)
+      launches += h->cfg.tc ? sg::launch_scan_tc(x, w, nq, p, d_allow, allow_words, h->sms, h->cfg.tc_split, st)
                             : sg::launch_scan_mma(x, w, nq, p, d_allow, allow_words, h->sms, st);
     if (timed) CK(cudaEventRecord(w.ev[4], st));
     sg::launch_cut(x, w, nq, p, st);
