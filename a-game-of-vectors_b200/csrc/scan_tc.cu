@@ -126,17 +126,21 @@ SG_DEV void tc_dealloc(uint32_t taddr, uint32_t ncols) {
 }
 SG_DEV void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory"); }
 SG_DEV void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory"); }
-SG_DEV void tc_commit(uint64_t* bar) {
-  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n" ::"r"(
-                   smem_addr(bar))
-               : "memory");
-}
-// D[tmem] (+)= A[tmem] x B[smem descriptor]; u8 x u8 -> s32, shape from the instruction descriptor.
-SG_DEV void tc_mma_i8(uint32_t d_tmem, uint32_t a_tmem, uint64_t b_desc, uint32_t idesc, uint32_t accumulate) {
+// D[tmem] (+)= A[tmem] x B[smem descriptor], u8 x u8 -> s32 with the shape of the instruction
+// descriptor, issued by one elected lane of a converged warp (all lanes run the loop, so the
+// operands stay warp-uniform). The commit that signals the MMAs' completion on an mbarrier is
+// elected the same way, from the same (lowest) lane, which issued the MMAs it tracks.
+SG_DEV void tc_mma_i8_elect(uint32_t d_tmem, uint32_t a_tmem, uint64_t b_desc, uint32_t idesc, uint32_t accumulate) {
   asm volatile(
-      "{\n.reg .pred p;\nsetp.ne.b32 p, %4, 0;\n"
-      "tcgen05.mma.cta_group::1.kind::i8 [%0], [%1], %2, %3, {%5, %5, %5, %5}, p;\n}\n" ::"r"(d_tmem),
+      "{\n.reg .pred p, e;\nsetp.ne.b32 p, %4, 0;\nelect.sync _|e, 0xffffffff;\n"
+      "@e tcgen05.mma.cta_group::1.kind::i8 [%0], [%1], %2, %3, {%5, %5, %5, %5}, p;\n}\n" ::"r"(d_tmem),
       "r"(a_tmem), "l"(b_desc), "r"(idesc), "r"(accumulate), "r"(0u));
+}
+SG_DEV void tc_commit_elect(uint64_t* bar) {
+  asm volatile(
+      "{\n.reg .pred e;\nelect.sync _|e, 0xffffffff;\n"
+      "@e tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n}\n" ::"r"(smem_addr(bar))
+      : "memory");
 }
 SG_DEV void tc_wait_st() { asm volatile("tcgen05.wait::st.sync.aligned;\n" ::: "memory"); }
 SG_DEV void tc_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory"); }
@@ -398,7 +402,8 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_scan_tc(TcArgs a) {
         if (lane == 0) mbar_arrive(&bar_iempty[slot]);
       } else if (warp == kTcMma) {
         const uint32_t idesc = idesc_u8(N);
-        const uint32_t bslot = bs_base + slot * kTcBBytes;
+        // K step s starts 256 B (two core matrices) further on: 16 in the 16-byte address field
+        const uint64_t bdesc = smem_desc(bs_base + slot * kTcBBytes, 128, 8192);
         for (uint32_t t = 0; t < ntiles && ok; t++) {
           const uint32_t ds = ts + t, dbuf = ds & (kTcDBufs - 1), duse = ds / kTcDBufs;
           if (!mbar_wait(&bar_dempty[dbuf], (duse & 1) ^ 1, abort_flag)) break;
@@ -409,16 +414,12 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_scan_tc(TcArgs a) {
               break;
             }
             tc_fence_after();
-            if (lane == 0) {
 #pragma unroll
-              for (uint32_t kk = 0; kk < 8; kk++) {
-                const uint32_t kstep = ch * 8 + kk;  // K bytes 32*kstep.. = groups 2*kstep, +1
-                tc_mma_i8(tmem + kTcDCol + dbuf * kTcQG, tmem + ch * 64 + kk * 8,
-                          smem_desc(bslot + kstep * 256, 128, 8192), idesc, (ch | kk) != 0);
-              }
-              tc_commit(&bar_aempty[ch]);
-              if (ch == kTcChunks - 1) tc_commit(&bar_dfull[dbuf]);
-            }
+            for (uint32_t kk = 0; kk < 8; kk++)  // K bytes 32*(8ch + kk).. = groups 2*(8ch + kk), +1
+              tc_mma_i8_elect(tmem + kTcDCol + dbuf * kTcQG, tmem + ch * 64 + kk * 8,
+                              bdesc + (uint64_t)((ch * 8 + kk) * 16), idesc, (ch | kk) != 0);
+            tc_commit_elect(&bar_aempty[ch]);
+            if (ch == kTcChunks - 1) tc_commit_elect(&bar_dfull[dbuf]);
             __syncwarp();
           }
         }
