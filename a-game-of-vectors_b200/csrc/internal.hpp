@@ -173,6 +173,10 @@ struct Config {
   int mma = 1;            // SIEVE_GPU_MMA: 0 ALU scan only, 1 automatic, 2 MMA whenever nprobe > 1
   int tc = 1;             // SIEVE_GPU_TC: 1 the tcgen05 scan, 0 the mma.sync scan (kept for comparison)
   uint32_t tc_split = 0;  // SIEVE_GPU_TC_SPLIT (> 1): a first tcgen05 round over the ranks below it
+  // Clusters probed by fewer queries than this in a batch are scanned by the ALU kernel: a
+  // tcgen05 tile costs the same ~32 x 101 cycles per 128 slots for any query count up to 128,
+  // an ALU (slot, query) pair ~6 (SIEVE_GPU_TC_MIN overrides; the autotuner measures it)
+  uint32_t tc_min_queries = 6;
 };
 
 std::string& last_error();
@@ -210,12 +214,16 @@ int launch_scan_mma(const DevIndex& ix, Workspace& w, uint32_t nq, const sg_para
                     const uint64_t* allow, uint64_t allow_words, int sms, cudaStream_t st);
 int transcode_mma(const uint8_t* blocks, uint64_t nblocks, uint32_t* out);
 void launch_invert(const DevIndex& ix, Workspace& w, uint32_t nq, uint32_t P, uint32_t qg, uint32_t rlo,
-                   uint32_t rhi, cudaStream_t st);
-// The batched scan on tcgen05 (scan_tc.cu): same work items and admission as launch_scan_mma.
-// With split > 1 it scans probe ranks [1, split) first, raises every query's threshold to the
-// cand-th best estimate its buffer then holds, and scans the remaining ranks.
+                   uint32_t rhi, cudaStream_t st, uint32_t tmin = 1, uint32_t alu_chunk = 0);
+// The batched pass after the seed (scan_tc.cu): the (query, probe) pairs of clusters probed by
+// fewer than cfg.tc_min_queries queries go to the ALU chunk scan (with the routing kernel's
+// rank-0 chunks), the others to the tcgen05 scan, which has the same admission as
+// launch_scan_mma. With cfg.tc_split > 1 it scans probe ranks [1, split) first, raises every
+// query's threshold to the cand-th best estimate its buffer then holds, and scans the rest.
+struct Config;
 int launch_scan_tc(const DevIndex& ix, Workspace& w, uint32_t nq, const sg_params& p,
-                   const uint64_t* allow, uint64_t allow_words, int sms, uint32_t split, cudaStream_t st);
+                   const uint64_t* allow, uint64_t allow_words, int sms, const Config& cfg,
+                   uint32_t chunk_blocks, cudaStream_t st);
 // Launch errors of these two are left for the caller's cudaGetLastError.
 void transcode_tc(const uint8_t* blocks, uint64_t nblocks, uint32_t* out, cudaStream_t st);
 void launch_lut_scan_tc(uint32_t nq, const uint8_t* tables, const uint32_t* codes, uint64_t nblocks,

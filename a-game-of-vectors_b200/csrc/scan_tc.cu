@@ -592,8 +592,9 @@ __global__ void __launch_bounds__(1024) k_raise_thr(const uint32_t* __restrict__
 }
 
 int launch_scan_tc(const DevIndex& ix, Workspace& w, uint32_t nq, const sg_params& p, const uint64_t* allow,
-                   uint64_t allow_words, int sms, uint32_t split, cudaStream_t st) {
+                   uint64_t allow_words, int sms, const Config& cfg, uint32_t chunk_blocks, cudaStream_t st) {
   const uint32_t P = p.nprobe < ix.k ? p.nprobe : ix.k;
+  const uint32_t split = cfg.tc_split, tmin = std::max<uint32_t>(cfg.tc_min_queries, 1);
   TcArgs a{};
   a.codes = reinterpret_cast<const uint4*>(ix.blocks_tc);
   a.mul = ix.mul;
@@ -622,15 +623,24 @@ int launch_scan_tc(const DevIndex& ix, Workspace& w, uint32_t nq, const sg_param
   a.allow_wq = w.allow_wq;
   tc_set_attr<false>();
   int launches = 0;
+  // the ALU chunk pass: the routing kernel's rank-0 chunks past the seed, then the chunks of
+  // the pairs whose clusters too few queries probe (appended by k_alu_split)
+  auto alu_pass = [&]() {
+    launch_scan(ix, w, nq, p, allow, allow_words, sms, chunk_blocks, 0, (int)cfg.scan_ctas_per_sm, st);
+    // a later round's ALU pass starts where this one's queue ended
+    cudaMemcpyAsync(w.counters + 1, w.counters, 4, cudaMemcpyDeviceToDevice, st);
+  };
   if (split > 1 && split < P) {
-    launch_invert(ix, w, nq, P, kTcQG, 1, split, st);
+    launch_invert(ix, w, nq, P, kTcQG, 1, split, st, tmin, chunk_blocks);
+    alu_pass();
     k_scan_tc<false><<<sms, kTcThreads, tc_smem_bytes(), st>>>(a);
     k_raise_thr<<<nq, 1024, 0, st>>>(w.cbuf_est, w.cbuf_per_q, w.ccount, w.overflow, p.cand, w.thr);
-    launches += 5;
+    launches += 7;
   }
-  launch_invert(ix, w, nq, P, kTcQG, split > 1 && split < P ? split : 1, P, st);
+  launch_invert(ix, w, nq, P, kTcQG, split > 1 && split < P ? split : 1, P, st, tmin, chunk_blocks);
+  alu_pass();
   k_scan_tc<false><<<sms, kTcThreads, tc_smem_bytes(), st>>>(a);
-  return launches + 4;
+  return launches + 6;
 }
 
 // Raw scores of nq query tables against nblocks blocks (slot-major codes already on the device);

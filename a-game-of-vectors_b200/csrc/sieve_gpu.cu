@@ -260,6 +260,7 @@ int build_index(const sg_ivf_arrays* a, int device, sg_index** out) {
   // default), or the mma.sync word order when SIEVE_GPU_TC=0
   if (const char* tc = getenv("SIEVE_GPU_TC")) h->cfg.tc = atoi(tc);
   if (const char* sp = getenv("SIEVE_GPU_TC_SPLIT")) h->cfg.tc_split = (uint32_t)strtoul(sp, nullptr, 10);
+  if (const char* tm = getenv("SIEVE_GPU_TC_MIN")) h->cfg.tc_min_queries = (uint32_t)strtoul(tm, nullptr, 10);
   if (h->cfg.tc) {
     if ((rc = dalloc(&x.blocks_tc, (size_t)nblocks * 256))) {
       free_index(x);
@@ -457,8 +458,11 @@ bool use_mma(const sg_index* h, uint32_t nq, uint32_t P) {
   if (!(h->cfg.tc ? x.blocks_tc : x.blocks_mma) || P <= 1 || P > 4096)
     return false;  // inverted lists keep 12-bit ranks
   if (h->cfg.mma == 2) return true;
-  return h->cfg.mma == 1 && nq >= 64 &&
-         (uint64_t)nq * (P - 1) >= (uint64_t)h->cfg.mma_min_queries_per_cluster * x.k;
+  if (h->cfg.mma != 1 || nq < 64) return false;
+  // tcgen05: the batch splits per cluster on the device (few queries: ALU, many: tensor cores),
+  // so the inverted path pays off once some cluster can gather tc_min_queries queries
+  if (h->cfg.tc) return (uint64_t)nq * (P - 1) >= (uint64_t)h->cfg.tc_min_queries * 16;
+  return (uint64_t)nq * (P - 1) >= (uint64_t)h->cfg.mma_min_queries_per_cluster * x.k;
 }
 
 // Exact per-query candidate-buffer bound. A slot is appended at most once, so the probed
@@ -524,10 +528,12 @@ int run_pipeline(sg_index* h, sg::Ctx& c, uint32_t nq, const sg_params& p, bool 
     sg::launch_scan(x, w, nq, p, d_allow, allow_words, h->sms, 0, sb,
                     h->cfg.scan_ctas_per_sm, st);
     if (timed) CK(cudaEventRecord(w.ev[9], st));
-    sg::launch_scan(x, w, nq, p, d_allow, allow_words, h->sms, cb, 0, h->cfg.scan_ctas_per_sm, st);
-    if (mma)
-      launches += h->cfg.tc ? sg::launch_scan_tc(x, w, nq, p, d_allow, allow_words, h->sms, h->cfg.tc_split, st)
-                            : sg::launch_scan_mma(x, w, nq, p, d_allow, allow_words, h->sms, st);
+    if (mma && h->cfg.tc) {  // ALU chunks and tcgen05 tiles, split per cluster
+      launches += sg::launch_scan_tc(x, w, nq, p, d_allow, allow_words, h->sms, h->cfg, cb, st);
+    } else {
+      sg::launch_scan(x, w, nq, p, d_allow, allow_words, h->sms, cb, 0, h->cfg.scan_ctas_per_sm, st);
+      if (mma) launches += sg::launch_scan_mma(x, w, nq, p, d_allow, allow_words, h->sms, st);
+    }
     if (timed) CK(cudaEventRecord(w.ev[4], st));
     sg::launch_cut(x, w, nq, p, st);
     launches += 3;

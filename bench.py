@@ -130,9 +130,12 @@ def build_workload(name: str, device: str, rows: int | None, nq_pool: int, n_eva
                               soar_lambda=1.0, device=device)
     t_build = time.time() - t0 - t_ingest
     arrays = {**corpus, **index}
+    del corpus, index
+    torch.cuda.empty_cache()  # the index upload needs the build's cached device memory back
     queries = mix.queries(nq_pool, sigma=0.35).float()
     t1 = time.time()
     gt = builder.ground_truth(mix, queries[:n_eval], k=10)
+    torch.cuda.empty_cache()
     t_gt = time.time() - t1
     log(f"workload {name}: n={w['n']} k={w['k']} ingest {t_ingest:.1f}s build {t_build:.1f}s "
         f"gt {t_gt:.1f}s nblocks={int(arrays['block_off'][-1])}")
