@@ -138,9 +138,10 @@ struct GraphKey {
   const uint64_t* allow;
   uint64_t allow_words;
   uint64_t gen;
+  uint64_t cfg_gen;  // the index's Config generation the graph was captured under
   bool same(const GraphKey& o) const {
     return nq == o.nq && have_q256 == o.have_q256 && allow == o.allow &&
-           allow_words == o.allow_words && gen == o.gen &&
+           allow_words == o.allow_words && gen == o.gen && cfg_gen == o.cfg_gen &&
            memcmp(&p, &o.p, sizeof(sg_params)) == 0;
   }
 };
@@ -177,6 +178,7 @@ struct Config {
   // tcgen05 tile costs the same ~32 x 101 cycles per 128 slots for any query count up to 128,
   // an ALU (slot, query) pair ~6 (SIEVE_GPU_TC_MIN overrides; the autotuner measures it)
   uint32_t tc_min_queries = 6;
+  uint64_t gen = 1;  // bumped whenever a field changes (captured graphs of an older one are stale)
 };
 
 std::string& last_error();

@@ -578,6 +578,7 @@ int launch_pipeline(sg_index* h, sg::Ctx& c, uint32_t nq, const sg_params& p, bo
   key.allow = d_allow;
   key.allow_words = allow_words;
   key.gen = c.gen;
+  key.cfg_gen = h->cfg.gen;
   for (auto& g : c.graphs)
     if (g.key.same(key)) {
       if (!g.exec) {  // seen once before: capture it now
@@ -1283,6 +1284,111 @@ int sg_lut_scan(uint32_t groups, const uint8_t* tables, const uint8_t* blocks, u
   dfree(dt); dfree(db); dfree(dout);
   if (e != cudaSuccess) return fail(SG_ERR_DEVICE, std::string("sg_lut_scan: ") + cudaGetErrorString(e));
   return SG_OK;
+}
+
+int sg_get_tuning(const sg_index* h, sg_tuning* out) {
+  if (!h || !out) return fail(SG_ERR_INVALID, "null argument");
+  out->tc_min_queries = h->cfg.tc_min_queries;
+  out->chunk_blocks = h->cfg.chunk_blocks;
+  out->scan_ctas_per_sm = h->cfg.scan_ctas_per_sm;
+  out->seed_blocks = h->cfg.seed_blocks;
+  return SG_OK;
+}
+
+int sg_set_tuning(sg_index* h, const sg_tuning* t) {
+  if (!h || !t) return fail(SG_ERR_INVALID, "null argument");
+  // chunks of at least the small-batch chunk keep the work-queue capacity bound valid
+  if (t->chunk_blocks < h->cfg.small_chunk_blocks || t->chunk_blocks > sg::kMaxChunkBlocks)
+    return fail(SG_ERR_INVALID, "chunk_blocks must lie in [small chunk, 512]");
+  if (t->seed_blocks == 0 || t->seed_blocks > sg::kMaxChunkBlocks)
+    return fail(SG_ERR_INVALID, "seed_blocks must lie in [1, 512]");
+  if (t->scan_ctas_per_sm < 1 || t->scan_ctas_per_sm > 2) return fail(SG_ERR_INVALID, "scan_ctas_per_sm: 1 or 2");
+  if (t->tc_min_queries == 0) return fail(SG_ERR_INVALID, "tc_min_queries must be >= 1");
+  std::lock_guard<std::mutex> g(h->mu);
+  h->cfg.tc_min_queries = t->tc_min_queries;
+  h->cfg.chunk_blocks = t->chunk_blocks;
+  h->cfg.scan_ctas_per_sm = t->scan_ctas_per_sm;
+  h->cfg.seed_blocks = t->seed_blocks;
+  h->cfg.gen++;
+  return SG_OK;
+}
+
+// The autotuner: coordinate descent over the batched path's shapes, timing the caller's own
+// batch (device time of the whole pipeline, best of `reps` runs per candidate). Every shape
+// gives identical results, so only speed is compared.
+int sg_autotune(sg_index* h, uint32_t nq, const float* d_q768, const float* d_q256, const sg_params* params,
+                uint32_t reps, sg_tuning* out, float* out_ms) {
+  if (!h || !params || !d_q768 || nq == 0) return fail(SG_ERR_INVALID, "null argument or empty batch");
+  if (nq < h->cfg.small_batch) return fail(SG_ERR_INVALID, "the autotuner tunes batches of >= 64 queries");
+  int rc;
+  if ((rc = check_params(h, params))) return rc;
+  CK(cudaSetDevice(h->ix.device));
+  const uint32_t k = std::max<uint32_t>(params->k, 1);
+  float* osc = nullptr;
+  uint32_t *oid = nullptr, *on = nullptr;
+  if ((rc = dalloc(&osc, (size_t)nq * k)) || (rc = dalloc(&oid, (size_t)nq * k)) || (rc = dalloc(&on, nq))) {
+    dfree(osc); dfree(oid); dfree(on);
+    return rc;
+  }
+  reps = std::max<uint32_t>(reps, 1);
+  auto time_batch = [&](float* ms) -> int {
+    float best = INFINITY;
+    for (uint32_t r = 0; r < reps + 1; r++) {  // the first run warms the workspace
+      std::lock_guard<std::mutex> g(h->mu);
+      const bool was = h->timing_on;
+      h->timing_on = true;
+      int rc2 = search_impl(h, h->def, nq, d_q768, d_q256, *params, nullptr, 0, osc, oid, on, nullptr, true);
+      h->timing_on = was;
+      if (rc2) return rc2;
+      if (r > 0) best = std::min(best, h->def.ws.last.ms_total);
+    }
+    *ms = best;
+    return SG_OK;
+  };
+  sg_tuning t;
+  sg_get_tuning(h, &t);
+  float base_ms = 0.0f, cur = 0.0f;
+  if ((rc = time_batch(&base_ms))) goto done;
+  cur = base_ms;
+  {
+    const uint32_t tmins[] = {2, 3, 4, 6, 8, 12, 16, 24, 32, 0xFFFFFFFFu};
+    const uint32_t chunks[] = {64, 128, 256, 512};
+    const uint32_t seeds[] = {128, 256, 512};
+    const uint32_t ctas[] = {1, 2};
+    auto sweep = [&](uint32_t* field, const uint32_t* vals, size_t nv) -> int {
+      const uint32_t keep = *field;
+      uint32_t best_v = keep;
+      for (size_t i = 0; i < nv; i++) {
+        if (vals[i] == keep) continue;
+        if (field == &t.chunk_blocks && vals[i] < h->cfg.small_chunk_blocks) continue;
+        *field = vals[i];
+        int rc2 = sg_set_tuning(h, &t);
+        if (rc2) return rc2;
+        float ms;
+        if ((rc2 = time_batch(&ms))) return rc2;
+        if (ms < cur * 0.995f) {
+          cur = ms;
+          best_v = vals[i];
+        }
+      }
+      *field = best_v;
+      return sg_set_tuning(h, &t);
+    };
+    if ((rc = sweep(&t.tc_min_queries, tmins, sizeof tmins / 4)) ||
+        (rc = sweep(&t.chunk_blocks, chunks, sizeof chunks / 4)) ||
+        (rc = sweep(&t.seed_blocks, seeds, sizeof seeds / 4)) ||
+        (rc = sweep(&t.scan_ctas_per_sm, ctas, sizeof ctas / 4)))
+      goto done;
+  }
+  if (out) *out = t;
+  if (out_ms) {
+    out_ms[0] = base_ms;
+    out_ms[1] = cur;
+  }
+done:
+  cudaDeviceSynchronize();
+  dfree(osc); dfree(oid); dfree(on);
+  return rc;
 }
 
 int sg_lut_scan_batch(uint32_t nq, const uint8_t* tables, const uint8_t* blocks, uint64_t nblocks,

@@ -70,6 +70,13 @@ class SgStats(ctypes.Structure):
         ("reranked", c_uint64), ("buffered", c_uint64), ("ms_seed", c_float), ("reserved2", c_uint32)]
 
 
+class SgTuning(ctypes.Structure):
+    """sg_tuning: the autotuned shapes of the batched path."""
+
+    _fields_ = [("tc_min_queries", c_uint32), ("chunk_blocks", c_uint32), ("scan_ctas_per_sm", c_uint32),
+                ("seed_blocks", c_uint32)]
+
+
 class SgIvfArrays(ctypes.Structure):
     """sg_ivf_arrays: the contents of the reference's corpus and index files."""
 
@@ -262,6 +269,9 @@ EXPORTS = [
     "sg_bigann_route",
     "sg_bigann_candidates",
     "sg_query_prep",
+    "sg_get_tuning",
+    "sg_set_tuning",
+    "sg_autotune",
     "sg_lut_scan",
     "sg_lut_scan_batch",
     "sg_dot_i8i8",
@@ -277,6 +287,7 @@ def check(status: int) -> None:
 __all__ = [
     "SgParams",
     "SgTiming",
+    "SgTuning",
     "SgIvfArrays",
     "make_arrays",
     "ptr",

@@ -188,6 +188,27 @@ class Index:
         check(lib().sg_last_stats(self._h, byref(st)))
         return {name: getattr(st, name) for name, _ in SgStats._fields_ if not name.startswith("reserved")}
 
+    def tuning(self) -> dict:
+        t = _abi.SgTuning()
+        check(lib().sg_get_tuning(self._h, byref(t)))
+        return {name: getattr(t, name) for name, _ in _abi.SgTuning._fields_}
+
+    def set_tuning(self, **fields) -> None:
+        t = _abi.SgTuning(**{**self.tuning(), **fields})
+        check(lib().sg_set_tuning(self._h, byref(t)))
+
+    def autotune(self, nq: int, d_q768: int, params: Params, d_q256: int | None = None, reps: int = 2) -> dict:
+        """sg_autotune on nq device-resident queries: the chosen shapes and the batch's device
+        time before and after (ms)."""
+        p = params.to_c()
+        t = _abi.SgTuning()
+        ms = (ctypes.c_float * 2)()
+        check(lib().sg_autotune(self._h, c_uint32(nq), c_void_p(d_q768), c_void_p(d_q256) if d_q256 else None,
+                                byref(p), c_uint32(reps), byref(t), ms))
+        out = {name: getattr(t, name) for name, _ in _abi.SgTuning._fields_}
+        out.update(ms_before=round(ms[0], 4), ms_after=round(ms[1], 4))
+        return out
+
     def set_route_precision(self, bf16: bool) -> None:
         check(lib().sg_set_route_precision(self._h, c_int(_abi.ROUTE_BF16 if bf16 else _abi.ROUTE_FP32)))
 

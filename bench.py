@@ -67,7 +67,7 @@ class ClockSampler:
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.FIELDS}",
-                 "--format=csv,noheader,nounits", "-lms", "100"],
+                 "--format=csv,noheader,nounits", "-lms", "20"],
                 stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.t = threading.Thread(target=self._read, daemon=True)
             self.t.start()
@@ -283,7 +283,7 @@ def serve_load(index, arrays, queries_host: np.ndarray, params, rates, seconds: 
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=50)
+    ap.add_argument("--steps", type=int, default=200)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="c2", choices=sorted(WORKLOADS))
@@ -294,9 +294,10 @@ def main():
     ap.add_argument("--eval", type=int, default=1000, help="queries with exact ground truth")
     ap.add_argument("--plain", type=int, default=512, help="queries timed one per launch")
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
-    ap.add_argument("--serve", default="20000,50000,100000",
+    ap.add_argument("--serve", default="20000,50000,70000,85000",
                     help="Poisson arrival rates (queries/s) for the serving loop; empty: skip")
     ap.add_argument("--serve-seconds", type=float, default=2.0)
+    ap.add_argument("--no-tune", action="store_true", help="keep the default shapes (no autotuner)")
     args = ap.parse_args()
 
     rank = int(os.environ.get("RANK", "0"))
@@ -371,6 +372,13 @@ def main():
         index.search_device(B, q768[lo].data_ptr(), None, params, out_sc.data_ptr(), out_id.data_ptr(),
                             out_n.data_ptr(), stream.cuda_stream)
 
+    # the autotuner picks the batched path's shapes on this batch size (untimed; results are
+    # identical under every shape)
+    if B >= 64 and not args.no_tune:
+        index.set_timing(False)
+        cfg["tuning"] = index.autotune(B, q768[nq_pool - B].data_ptr(), params, reps=2)
+        index.set_timing(True)
+        log(f"autotune: {cfg['tuning']}")
     for i in range(args.warmup):
         step(i)
     torch.cuda.synchronize()

@@ -349,6 +349,24 @@ int sg_bigann_candidates(sg_bigann* index, uint32_t nq, const int8_t* q100,
                          const sg_bigann_params* params, uint32_t* out_ids, float* out_est,
                          float* out_nx, uint32_t* out_counts);
 
+/* ---- autotuner (no counterpart in the reference: the shapes of the batched GPU path) ------ */
+typedef struct {
+  uint32_t tc_min_queries;    /* clusters probed by fewer queries of a batch go to the ALU scan,
+                                 the others to the tcgen05 scan                                  */
+  uint32_t chunk_blocks;      /* ALU scan work-item size, blocks (64..512)                      */
+  uint32_t scan_ctas_per_sm;  /* ALU scan CTAs per SM (1 or 2)                                   */
+  uint32_t seed_blocks;       /* block budget of each query's seed pass (1..512)                */
+} sg_tuning;
+int sg_get_tuning(const sg_index* index, sg_tuning* out);
+/* Applies to batches of >= 64 queries; captured CUDA graphs of the previous tuning are retired. */
+int sg_set_tuning(sg_index* index, const sg_tuning* tuning);
+/* Times the caller's batch (nq device-resident queries, params) under candidate tunings, one
+ * field at a time (coordinate descent, best of `reps` device-timed runs each), and keeps the
+ * fastest. Results are identical under every tuning. out_ms[0], out_ms[1]: the batch's device
+ * time before and after, ms (either output may be null). */
+int sg_autotune(sg_index* index, uint32_t nq, const float* d_q768, const float* d_q256,
+                const sg_params* params, uint32_t reps, sg_tuning* out, float* out_ms);
+
 /* ---- kernel-level entry points (parity tests and micro-benchmarks) ----------------------- */
 /* rabitq::Query::new (src/rabitq.rs:119-125) on the device: rotated LUT tables [nq*64*16] u8,
  * and per query scale, bias, a, b. */
