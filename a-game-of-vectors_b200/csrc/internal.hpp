@@ -179,6 +179,9 @@ struct Config {
   // an ALU (slot, query) pair ~6 (SIEVE_GPU_TC_MIN overrides; the autotuner measures it)
   uint32_t tc_min_queries = 6;
   uint64_t gen = 1;  // bumped whenever a field changes (captured graphs of an older one are stale)
+  // device memory a batch's candidate buffers may take (a quarter of what the index leaves
+  // free at open, between 8 and 32 GiB); a query that fills its share is re-run alone
+  uint64_t cbuf_budget = 8ull << 30;
 };
 
 std::string& last_error();

@@ -290,6 +290,11 @@ int build_index(const sg_ivf_arrays* a, int device, sg_index** out) {
     x.has_t2 = true;
   }
   if (const char* sc = getenv("SIEVE_GPU_SOFT_CAP")) h->cfg.soft_cap = (uint32_t)strtoul(sc, nullptr, 10);
+  {
+    size_t free_b = 0, total_b = 0;
+    if (cudaMemGetInfo(&free_b, &total_b) == cudaSuccess)
+      h->cfg.cbuf_budget = std::min<uint64_t>(std::max<uint64_t>(free_b / 4, 8ull << 30), 32ull << 30);
+  }
   if (const char* m = getenv("SIEVE_GPU_MMA")) h->cfg.mma = atoi(m);
   if (const char* gr = getenv("SIEVE_GPU_GRAPHS")) h->cfg.graphs = atoi(gr);
   if (const char* ss = getenv("SIEVE_GPU_SMALL_SEED"))
@@ -481,7 +486,7 @@ uint32_t batch_cap(const sg_index* h, const sg_params& p, uint32_t nq, bool soft
   uint32_t full = full_cap(h, p, nq);
   if (h->cfg.soft_cap) return std::min(full, h->cfg.soft_cap);
   if (nq <= 8 && !soft_always) return full;
-  uint64_t budget = (8ull << 30) / (sizeof(uint4) * (uint64_t)nq);
+  uint64_t budget = h->cfg.cbuf_budget / (sizeof(uint4) * (uint64_t)nq);
   uint64_t soft = std::max<uint64_t>(16ull * std::max<uint32_t>(p.cand, 1), budget);
   return (uint32_t)std::min<uint64_t>(full, soft);
 }
@@ -730,7 +735,7 @@ int search_impl(sg_index* h, sg::Ctx& c, uint32_t nq, const float* q768, const f
   if (!redo.empty()) {
     uint32_t per = (uint32_t)redo.size();
     uint32_t fcap = full_cap(h, p, per);
-    while (per > 1 && (uint64_t)per * fcap * sizeof(uint4) > (8ull << 30)) {
+    while (per > 1 && (uint64_t)per * fcap * sizeof(uint4) > h->cfg.cbuf_budget) {
       per = (per + 1) / 2;
       fcap = full_cap(h, p, per);
     }
@@ -770,6 +775,7 @@ int search_impl(sg_index* h, sg::Ctx& c, uint32_t nq, const float* q768, const f
   }
   w.last = saved;
   w.last.launches += retry_launches;
+  w.last.retried = (uint32_t)redo.size();
   return SG_OK;
 }
 
@@ -1292,6 +1298,7 @@ int sg_get_tuning(const sg_index* h, sg_tuning* out) {
   out->chunk_blocks = h->cfg.chunk_blocks;
   out->scan_ctas_per_sm = h->cfg.scan_ctas_per_sm;
   out->seed_blocks = h->cfg.seed_blocks;
+  out->tc_split = h->cfg.tc_split;
   return SG_OK;
 }
 
@@ -1304,11 +1311,13 @@ int sg_set_tuning(sg_index* h, const sg_tuning* t) {
     return fail(SG_ERR_INVALID, "seed_blocks must lie in [1, 512]");
   if (t->scan_ctas_per_sm < 1 || t->scan_ctas_per_sm > 2) return fail(SG_ERR_INVALID, "scan_ctas_per_sm: 1 or 2");
   if (t->tc_min_queries == 0) return fail(SG_ERR_INVALID, "tc_min_queries must be >= 1");
+  if (t->tc_split > 4096) return fail(SG_ERR_INVALID, "tc_split must be <= 4096");
   std::lock_guard<std::mutex> g(h->mu);
   h->cfg.tc_min_queries = t->tc_min_queries;
   h->cfg.chunk_blocks = t->chunk_blocks;
   h->cfg.scan_ctas_per_sm = t->scan_ctas_per_sm;
   h->cfg.seed_blocks = t->seed_blocks;
+  h->cfg.tc_split = t->tc_split;
   h->cfg.gen++;
   return SG_OK;
 }
@@ -1355,6 +1364,7 @@ int sg_autotune(sg_index* h, uint32_t nq, const float* d_q768, const float* d_q2
     const uint32_t chunks[] = {64, 128, 256, 512};
     const uint32_t seeds[] = {128, 256, 512};
     const uint32_t ctas[] = {1, 2};
+    const uint32_t splits[] = {0, 3, 6};
     auto sweep = [&](uint32_t* field, const uint32_t* vals, size_t nv) -> int {
       const uint32_t keep = *field;
       uint32_t best_v = keep;
@@ -1377,7 +1387,8 @@ int sg_autotune(sg_index* h, uint32_t nq, const float* d_q768, const float* d_q2
     if ((rc = sweep(&t.tc_min_queries, tmins, sizeof tmins / 4)) ||
         (rc = sweep(&t.chunk_blocks, chunks, sizeof chunks / 4)) ||
         (rc = sweep(&t.seed_blocks, seeds, sizeof seeds / 4)) ||
-        (rc = sweep(&t.scan_ctas_per_sm, ctas, sizeof ctas / 4)))
+        (rc = sweep(&t.scan_ctas_per_sm, ctas, sizeof ctas / 4)) ||
+        (rc = sweep(&t.tc_split, splits, sizeof splits / 4)))
       goto done;
   }
   if (out) *out = t;

@@ -67,14 +67,14 @@ class SgStats(ctypes.Structure):
     _fields_ = [(n, c_float) for n in ("ms_prep", "ms_route_gemm", "ms_route_select", "ms_scan",
                                         "ms_cut", "ms_rerank", "ms_tier2", "ms_total")] + [
         ("launches", c_uint32), ("reserved", c_uint32), ("scanned", c_uint64), ("probed", c_uint64),
-        ("reranked", c_uint64), ("buffered", c_uint64), ("ms_seed", c_float), ("reserved2", c_uint32)]
+        ("reranked", c_uint64), ("buffered", c_uint64), ("ms_seed", c_float), ("retried", c_uint32)]
 
 
 class SgTuning(ctypes.Structure):
     """sg_tuning: the autotuned shapes of the batched path."""
 
     _fields_ = [("tc_min_queries", c_uint32), ("chunk_blocks", c_uint32), ("scan_ctas_per_sm", c_uint32),
-                ("seed_blocks", c_uint32)]
+                ("seed_blocks", c_uint32), ("tc_split", c_uint32)]
 
 
 class SgIvfArrays(ctypes.Structure):

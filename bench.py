@@ -480,6 +480,7 @@ def main():
                         "Python client, 10% filtered, after 0.5 s of unmeasured warm-up at the same "
                         "rate; latency = sg_server_submit to results on the host, on the library's clock",
         "scanned_per_query": float(np.mean(scanned) / B),
+        "retried_queries_per_step": float(np.mean([s["retried"] for s in stats])),
         "roofline": {"bound": "hbm", "kernel": "k_scan_seed + k_scan + k_scan_tc (the scan stage)",
                      "achieved": achieved, "peak": peak,
                      "unit": "GB/s", "frac": achieved / peak,

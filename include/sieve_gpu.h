@@ -108,7 +108,8 @@ typedef struct {
   uint64_t reranked;      /* candidates reaching the rerank stage, summed over queries            */
   uint64_t buffered;      /* scan entries appended to the candidate buffers, summed over queries  */
   float ms_seed;          /* part of ms_scan in the seed pass (each query's best cluster)         */
-  uint32_t reserved2;
+  uint32_t retried;       /* queries re-run with their exact buffer bound after a batch's buffer
+                             filled up                                                      */
 } sg_stats;
 
 typedef struct sg_index sg_index;
@@ -356,6 +357,8 @@ typedef struct {
   uint32_t chunk_blocks;      /* ALU scan work-item size, blocks (64..512)                      */
   uint32_t scan_ctas_per_sm;  /* ALU scan CTAs per SM (1 or 2)                                   */
   uint32_t seed_blocks;       /* block budget of each query's seed pass (1..512)                */
+  uint32_t tc_split;          /* > 1: probe ranks below it are scanned first and each query's
+                                 threshold raised to its buffer's cand-th estimate (0: off)      */
 } sg_tuning;
 int sg_get_tuning(const sg_index* index, sg_tuning* out);
 /* Applies to batches of >= 64 queries; captured CUDA graphs of the previous tuning are retired. */
