@@ -17,7 +17,8 @@
 namespace sg {
 
 // Blocks (32 slots) a scan work item covers at most; the scan CTA holds one chunk's estimates
-// in shared memory (4 B per slot), so kMaxChunkBlocks = 512 is 64 KB.
+// in shared memory (4 B per slot plus one padding word per block), so kMaxChunkBlocks = 512
+// is 66 KB.
 constexpr uint32_t kMaxChunkBlocks = 512;
 constexpr uint32_t kChunkBlocks = 256;   // default chunk of the batched scan
 constexpr uint32_t kSeedBlocks = 512;    // block budget of each query's seed (its first probes)

@@ -63,6 +63,12 @@ SG_DEV uint32_t ld_cg(const uint32_t* p) {
   return v;
 }
 
+// Slot i's key lives at word i + i/32 of the key array: one padding word per block, so the
+// admission loops (thread t walks its own contiguous range of slots) and the per-block key
+// writes of the scoring spread over the shared-memory banks instead of hitting one bank.
+constexpr uint32_t kKeyWordsPerBlock = SG_BLOCK + 1;
+SG_DEV uint32_t kx(uint32_t i) { return i + (i >> 5); }
+
 // Scores one block's 32 slots into 16 packed accumulators (sum over this thread's 16 groups).
 SG_DEV void score_block_quarter(const uint8_t* __restrict__ block, const uint4* s_tab, int t4,
                                 uint32_t* acc) {
@@ -167,7 +173,7 @@ SG_DEV void scan_segments(const ScanArgs& a, uint32_t q, const Segs& S, uint32_t
         const uint32_t doc = d < 4 ? 4 * t4 + d : 16 + 4 * t4 + (d - 4);
         const float est =
             __fadd_rn(cent, __fmul_rn(mv[d], __fadd_rn(__fmul_rn(qp.z, (float)sc[d]), qp.w)));
-        s_key[gb * SG_BLOCK + doc] = (rel0 + (int32_t)doc < S.cl[sg]) ? ord(est) : 0u;
+        s_key[gb * kKeyWordsPerBlock + doc] = (rel0 + (int32_t)doc < S.cl[sg]) ? ord(est) : 0u;
       }
     }
   }
@@ -185,10 +191,10 @@ SG_DEV void scan_segments(const ScanArgs& a, uint32_t q, const Segs& S, uint32_t
   };
   uint32_t cnt = 0;
   for (uint32_t i = i0; i < i1; i++) {
-    const uint32_t k = s_key[i];
+    const uint32_t k = s_key[kx(i)];
     bool surv = k != 0u && k >= thr;
     if (surv && al) surv = allowed(al, aw, a.ids[slot_of(i)]);
-    if (!surv) s_key[i] = 0u;
+    if (!surv) s_key[kx(i)] = 0u;
     cnt += surv;
   }
   const uint32_t n_s = block_sum(cnt, tmp);
@@ -196,19 +202,19 @@ SG_DEV void scan_segments(const ScanArgs& a, uint32_t q, const Segs& S, uint32_t
   const bool cut = n_s > a.cand;
   uint32_t T = 0, need = 0;
   if (cut) {
-    T = block_select_nth_u32([&](uint32_t i) { return s_key[i]; }, nloc, a.cand, hist);
+    T = block_select_nth_u32([&](uint32_t i) { return s_key[kx(i)]; }, nloc, a.cand, hist);
     uint32_t gt = 0;
-    for (uint32_t i = i0; i < i1; i++) gt += s_key[i] > T;
+    for (uint32_t i = i0; i < i1; i++) gt += s_key[kx(i)] > T;
     need = a.cand - block_sum(gt, tmp);
   }
   uint32_t ties = 0;
   if (cut)
-    for (uint32_t i = i0; i < i1; i++) ties += s_key[i] == T;
+    for (uint32_t i = i0; i < i1; i++) ties += s_key[kx(i)] == T;
   uint32_t tr = block_exclusive_scan(ties, tmp, nullptr);
   uint64_t selmask = 0;
   uint32_t nsel = 0;
   for (uint32_t i = i0; i < i1; i++) {
-    const uint32_t k = s_key[i];
+    const uint32_t k = s_key[kx(i)];
     bool sel;
     if (!cut) sel = k != 0u;
     else if (k > T) sel = true;
@@ -233,7 +239,7 @@ SG_DEV void scan_segments(const ScanArgs& a, uint32_t q, const Segs& S, uint32_t
       if (pos < a.cap) {
         const uint32_t gb = i / SG_BLOCK, sg = seg_of(S, gb);
         const uint32_t rel = (gb - S.start[sg]) * SG_BLOCK + (i % SG_BLOCK);
-        a.cbuf_est[qbase + pos] = __float_as_uint(unord(s_key[i]));
+        a.cbuf_est[qbase + pos] = __float_as_uint(unord(s_key[kx(i)]));
         a.cbuf_info[qbase + pos] = make_uint2(S.kb[sg] + rel, S.b0[sg] * SG_BLOCK + rel);
       } else {
         a.overflow[q] = 1;
@@ -328,13 +334,13 @@ void launch_scan(const DevIndex& ix, Workspace& w, uint32_t nq, const sg_params&
   static bool attr = false;
   if (!attr) {
     cudaFuncSetAttribute(k_scan_seed, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         (int)(kMaxChunkBlocks * SG_BLOCK * 4));
+                         (int)(kMaxChunkBlocks * kKeyWordsPerBlock * 4));
     cudaFuncSetAttribute(k_scan, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         (int)(kMaxChunkBlocks * SG_BLOCK * 4));
+                         (int)(kMaxChunkBlocks * kKeyWordsPerBlock * 4));
     attr = true;
   }
-  if (seed_blocks) k_scan_seed<<<nq, 256, seed_blocks * SG_BLOCK * 4, st>>>(a);
-  if (chunk_blocks) k_scan<<<sms * ctas_per_sm, 256, chunk_blocks * SG_BLOCK * 4, st>>>(a);
+  if (seed_blocks) k_scan_seed<<<nq, 256, seed_blocks * kKeyWordsPerBlock * 4, st>>>(a);
+  if (chunk_blocks) k_scan<<<sms * ctas_per_sm, 256, chunk_blocks * kKeyWordsPerBlock * 4, st>>>(a);
 }
 
 // ---- stateless kernels for the parity tests ---------------------------------------------------
