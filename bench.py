@@ -106,6 +106,21 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
+def max_over_ranks(value: float, world: int, device) -> float:
+    """The largest of every rank's `value` (a timed region's length): each GPU runs an independent
+    replica of the workload (no data-path collective), so the job's time is its slowest rank's."""
+    if world <= 1:
+        return value
+    t = torch.tensor([value], dtype=torch.float64, device=device)
+    torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+    return float(t.item())
+
+
+def replica_qps(per_rank_queries: int, seconds: float, world: int, device) -> float:
+    """Whole-job throughput of `world` replicas: all ranks' queries over the slowest rank's time."""
+    return world * per_rank_queries / max_over_ranks(seconds, world, device)
+
+
 def measured_peaks() -> dict:
     try:
         with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
@@ -396,11 +411,7 @@ def main():
             step_ms.append(a.elapsed_time(b))
             stats.append(index.last_stats())
         torch.cuda.synchronize()
-    total_ms = float(np.sum(step_ms))
-    if world > 1:
-        t = torch.tensor([total_ms], device=dev)
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        total_ms = float(t.item())
+    total_ms = max_over_ranks(float(np.sum(step_ms)), world, dev)
     qps = world * args.steps * B / (total_ms / 1e3)
 
     # the scan kernel: algorithmic bytes over its event-timed duration, per launch
@@ -448,7 +459,7 @@ def main():
         index.search_into(qh.numpy(), params, osc.numpy(), oid.numpy().view(np.uint32), ocn.numpy().view(np.uint32))
         if i >= args.warmup:
             e2e_s.append(time.perf_counter() - t)
-    e2e_qps = world * args.steps * B / float(np.sum(e2e_s))
+    e2e_qps = replica_qps(args.steps * B, float(np.sum(e2e_s)), world, dev)
 
     serving = None
     if args.serve:
@@ -612,7 +623,7 @@ def main_bigann(args, rank: int, world: int, local: int, dev: str):
             b.record(stream)
             b.synchronize()
             step_ms.append(a.elapsed_time(b))
-    total_ms = float(np.sum(step_ms))
+    total_ms = max_over_ranks(float(np.sum(step_ms)), world, dev)
     qps = world * args.steps * B / (total_ms / 1e3)
     # stage times of one timed batch (the scan kernel's share and its algorithmic bytes)
     tb = BigannTiming()
@@ -644,7 +655,7 @@ def main_bigann(args, rank: int, world: int, local: int, dev: str):
                           ocn.numpy().view(np.uint32))
         if i >= args.warmup:
             e2e_s.append(time.perf_counter() - t)
-    e2e_qps = world * args.steps * B / float(np.sum(e2e_s))
+    e2e_qps = replica_qps(args.steps * B, float(np.sum(e2e_s)), world, dev)
     cpu = None
     if rank == 0 and world == 1 and args.cpu_seconds > 0:
         r = cpu_ref(args.cpu_seconds)
