@@ -16,9 +16,11 @@
 //     tensor memory with tcgen05.st: one-hot rows are 32x the size of the codes and never touch
 //     shared memory or HBM. Warp w owns TMEM lanes 32*w.. (block w of the tile) and fills the
 //     tile's four K chunks (16 groups = 256 one-hot bytes = 64 TMEM columns each);
-//   - one thread of the MMA warp issues the 32 MMAs (K = 32) of a tile into one of four TMEM
-//     accumulators and signals the A stages and the accumulator through mbarriers
-//     (tcgen05.commit);
+//   - the MMA warp, converged, issues the 32 MMAs (K = 32) of a tile from one elected lane into
+//     one of four TMEM accumulators and signals the A stages and the accumulator through
+//     mbarriers (tcgen05.commit). Each MMA costs ~100 SM cycles whatever N up to 128, so a tile
+//     costs ~3.2k cycles however many queries share the cluster: the per-cluster split sends
+//     clusters that few queries probe to the ALU scan instead;
 //   - eight epilogue warps (two per TMEM lane quarter, taking alternate tiles) read the s32
 //     scores with tcgen05.ld (one slot per thread, one query per column) and form
 //     est = cent + mul*(a*score + b) for every column in straight-line code, exactly as the ALU
@@ -205,7 +207,6 @@ struct TcArgs {
   const uint32_t* ids;
   const uint32_t* block_off;
   const uint32_t* clen;
-  const float2* mul_rng;
   const uint8_t* tables;
   const float4* qp;
   const float* probe_sc;
@@ -601,7 +602,6 @@ int launch_scan_tc(const DevIndex& ix, Workspace& w, uint32_t nq, const sg_param
   a.ids = ix.ids;
   a.block_off = ix.block_off;
   a.clen = ix.clen;
-  a.mul_rng = ix.mul_rng;
   a.tables = w.tables;
   a.qp = w.qp;
   a.probe_sc = w.probe_sc;
