@@ -30,7 +30,7 @@ constexpr uint32_t kExpandMaxK = 16384;
 // Status bits a kernel raises in Workspace::status.
 constexpr uint32_t kStatusOverflow = 1u;   // a candidate buffer filled up (query is retried)
 constexpr uint32_t kStatusWindow = 2u;     // a BF16 routing window exceeded its buffer
-constexpr uint32_t kStatusTimeout = 4u;    // a tensor-core scan wait ran out (the CTA stopped)
+constexpr uint32_t kStatusTimeout = 4u;    // a tensor-core wait ran out (the CTA stopped)
 
 // HBM layout of one IVF index (all arrays on the index's device).
 struct DevIndex {

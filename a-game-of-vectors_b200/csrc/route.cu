@@ -3,9 +3,9 @@
 // Two ways to score q256 against the K centroids:
 //   FP32: every (query, centroid) dot in the reference's order — a sequential f32 sum from -0.0
 //         of rounded products (blas::gemm_abt portable, src/blas.rs:43-54). Exact by construction.
-//   BF16: a tensor-core GEMM [nq x 256] x [256 x K] with FP32 accumulation, then, per query,
-//         every centroid whose BF16 score lies within 2*delta of the nprobe-th best BF16 score is
-//         rescored with the FP32 sequential dot. delta bounds |BF16 score - FP32 score|:
+//   BF16: a tcgen05 tensor-core GEMM [nq x 256] x [256 x K] with FP32 accumulation, then, per
+//         query, every centroid whose BF16 score lies within 2*delta of the nprobe-th best BF16
+//         score is rescored with the FP32 sequential dot. delta bounds |BF16 score - FP32 score|:
 //         inputs rounded to bf16 (unit roundoff 2^-8) give a product error <= (2^-7 + 2^-16)|q_i c_i|;
 //         FP32 accumulation of 256 exact bf16 products adds <= 256*2^-23 * sum|q_i c_i|, and the
 //         reference's own sequential sum differs from the real dot by <= 256*2^-24 * sum|q_i c_i|.
@@ -19,6 +19,7 @@
 
 #include "common.cuh"
 #include "internal.hpp"
+#include "tcgen05.cuh"
 
 namespace sg {
 
@@ -50,89 +51,108 @@ __global__ void __launch_bounds__(256) k_route_fp32(const float* __restrict__ q2
     if (q0 + j < nq) scores[(size_t)(q0 + j) * K + c] = acc[j];
 }
 
-// ---- BF16 tensor-core GEMM: 64 queries x 128 centroids per CTA, 8 warps of 32x32 -------------
-constexpr int kBM = 64, kBN = 128, kLD = SG_PDIM + 8;  // padded rows: conflict-free fragments
+// ---- BF16 GEMM on the tcgen05 tensor cores: 128 centroids x 64 queries per CTA --------------
+// D[centroid][query] = sum_k c_bf16[k] * bf16(q[k]) in FP32 tensor memory (M = 128 TMEM lanes,
+// N = 64 columns), both operands in shared memory as K-major core matrices without swizzle:
+// 8 rows x 16 B (8 bf16) per core matrix, 128 B apart along K, 4096 B (32 along K) apart along
+// the rows. Chunk e of a tile (row 8*(e>>8) + (e&7), k-chunk (e>>3)&31) sits at byte 16*e, so
+// the loads write shared memory linearly. One elected lane issues the 16 MMAs (K = 16 each);
+// all warps then read the accumulators with tcgen05.ld: warp w takes TMEM lanes 32*(w&3).. (the
+// tile's centroids), columns 32*(w>>2).. (queries), and stores each query's 32 centroid scores
+// as one coalesced 128 B row segment.
+constexpr int kRtM = 128, kRtN = 64, kRtThreads = 256;
+constexpr uint32_t kRtCols = 64;  // TMEM columns: the f32 accumulators
+constexpr int kRtABytes = kRtM * SG_PDIM * 2, kRtBBytes = kRtN * SG_PDIM * 2;
+constexpr int kRtSmem = kRtABytes + kRtBBytes;  // 96 KB: two CTAs per SM
 
-SG_DEV void mma_bf16(float* d, const uint32_t* a, const uint32_t* b) {
-  asm volatile(
-      "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, "
-      "{%8,%9}, {%0,%1,%2,%3};\n"
-      : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
-      : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b[0]), "r"(b[1]));
+SG_DEV uint32_t pack_bf16x2(float lo, float hi) {
+  __nv_bfloat162 p = __floats2bfloat162_rn(lo, hi);  // round to nearest even
+  return *reinterpret_cast<uint32_t*>(&p);
 }
 
-__global__ void __launch_bounds__(256) k_route_bf16(const float* __restrict__ q256,
-                                                    const __nv_bfloat16* __restrict__ cb,
-                                                    uint32_t K, uint32_t nq,
-                                                    float* __restrict__ scores) {
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  __nv_bfloat16* As = reinterpret_cast<__nv_bfloat16*>(smem_raw);
-  __nv_bfloat16* Bs = As + kBM * kLD;
-  const uint32_t m0 = blockIdx.y * kBM, n0 = blockIdx.x * kBN;
-  // A: queries f32 -> bf16 (round to nearest even)
-  for (int i = threadIdx.x; i < kBM * SG_PDIM / 4; i += blockDim.x) {
-    int r = i / (SG_PDIM / 4), c4 = i % (SG_PDIM / 4);
-    float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
-    if (m0 + r < nq) v = *reinterpret_cast<const float4*>(q256 + (size_t)(m0 + r) * SG_PDIM + 4 * c4);
-    __nv_bfloat162 lo = __floats2bfloat162_rn(v.x, v.y), hi = __floats2bfloat162_rn(v.z, v.w);
-    *reinterpret_cast<__nv_bfloat162*>(As + r * kLD + 4 * c4) = lo;
-    *reinterpret_cast<__nv_bfloat162*>(As + r * kLD + 4 * c4 + 2) = hi;
+__global__ void __launch_bounds__(kRtThreads) k_route_tc(const float* __restrict__ q256,
+                                                         const __nv_bfloat16* __restrict__ cb,
+                                                         uint32_t K, uint32_t nq,
+                                                         float* __restrict__ scores,
+                                                         uint32_t* __restrict__ status) {
+  extern __shared__ __align__(1024) uint8_t smem[];
+  __shared__ __align__(8) uint64_t bar_done;
+  __shared__ uint32_t s_tmem;
+  __shared__ int s_abort;
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const uint32_t m0 = blockIdx.x * kRtM, q0 = blockIdx.y * kRtN;
+  if (warp == 0) {
+    tc_alloc(&s_tmem, kRtCols);
+    tc_relinquish();
   }
-  // B: centroid rows (k contiguous = the col-major B operand)
-  for (int i = threadIdx.x; i < kBN * SG_PDIM / 8; i += blockDim.x) {
-    int r = i / (SG_PDIM / 8), c8 = i % (SG_PDIM / 8);
-    uint4 v = make_uint4(0, 0, 0, 0);
-    if (n0 + r < K) v = *reinterpret_cast<const uint4*>(cb + (size_t)(n0 + r) * SG_PDIM + 8 * c8);
-    *reinterpret_cast<uint2*>(Bs + r * kLD + 8 * c8) = make_uint2(v.x, v.y);
-    *reinterpret_cast<uint2*>(Bs + r * kLD + 8 * c8 + 4) = make_uint2(v.z, v.w);
+  if (tid == 0) {
+    mbar_init(&bar_done, 1);
+    s_abort = 0;
+    fence_mbar_init();
   }
-  __syncthreads();
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int g = lane >> 2, tig = lane & 3;
-  const int wm = (warp >> 2) * 32, wn = (warp & 3) * 32;
-  float acc[2][4][4];
-#pragma unroll
-  for (int i = 0; i < 2; i++)
-#pragma unroll
-    for (int j = 0; j < 4; j++)
-#pragma unroll
-      for (int e = 0; e < 4; e++) acc[i][j][e] = 0.0f;
+  uint4* As = reinterpret_cast<uint4*>(smem);
+  uint4* Bs = reinterpret_cast<uint4*>(smem + kRtABytes);
+  // A: centroid rows, already bf16 (rows past K are zero)
 #pragma unroll 4
-  for (int k0 = 0; k0 < SG_PDIM; k0 += 16) {
-    uint32_t a[2][4], b[4][2];
-#pragma unroll
-    for (int i = 0; i < 2; i++) {
-      const __nv_bfloat16* base = As + (wm + 16 * i + g) * kLD + k0 + 2 * tig;
-      a[i][0] = *reinterpret_cast<const uint32_t*>(base);
-      a[i][1] = *reinterpret_cast<const uint32_t*>(base + 8 * kLD);
-      a[i][2] = *reinterpret_cast<const uint32_t*>(base + 8);
-      a[i][3] = *reinterpret_cast<const uint32_t*>(base + 8 * kLD + 8);
-    }
-#pragma unroll
-    for (int j = 0; j < 4; j++) {
-      const __nv_bfloat16* base = Bs + (wn + 8 * j + g) * kLD + k0 + 2 * tig;
-      b[j][0] = *reinterpret_cast<const uint32_t*>(base);
-      b[j][1] = *reinterpret_cast<const uint32_t*>(base + 8);
-    }
-#pragma unroll
-    for (int i = 0; i < 2; i++)
-#pragma unroll
-      for (int j = 0; j < 4; j++) mma_bf16(acc[i][j], a[i], b[j]);
+  for (int e = tid; e < kRtM * (SG_PDIM / 8); e += kRtThreads) {
+    const uint32_t r = 8 * (e >> 8) + (e & 7), c = (e >> 3) & 31;
+    uint4 v = make_uint4(0, 0, 0, 0);
+    if (m0 + r < K) v = __ldg(reinterpret_cast<const uint4*>(cb + (size_t)(m0 + r) * SG_PDIM) + c);
+    As[e] = v;
   }
-#pragma unroll
-  for (int i = 0; i < 2; i++)
-#pragma unroll
-    for (int j = 0; j < 4; j++) {
-      uint32_t r = m0 + wm + 16 * i + g, c = n0 + wn + 8 * j + 2 * tig;
-      if (r < nq) {
-        if (c < K) scores[(size_t)r * K + c] = acc[i][j][0];
-        if (c + 1 < K) scores[(size_t)r * K + c + 1] = acc[i][j][1];
-      }
-      if (r + 8 < nq) {
-        if (c < K) scores[(size_t)(r + 8) * K + c] = acc[i][j][2];
-        if (c + 1 < K) scores[(size_t)(r + 8) * K + c + 1] = acc[i][j][3];
-      }
+  // B: query rows, f32 -> bf16 (rows past nq are zero)
+#pragma unroll 4
+  for (int e = tid; e < kRtN * (SG_PDIM / 8); e += kRtThreads) {
+    const uint32_t r = 8 * (e >> 8) + (e & 7), c = (e >> 3) & 31;
+    uint4 v = make_uint4(0, 0, 0, 0);
+    if (q0 + r < nq) {
+      const float4* src = reinterpret_cast<const float4*>(q256 + (size_t)(q0 + r) * SG_PDIM + 8 * c);
+      const float4 x = src[0], y = src[1];
+      v = make_uint4(pack_bf16x2(x.x, x.y), pack_bf16x2(x.z, x.w), pack_bf16x2(y.x, y.y),
+                     pack_bf16x2(y.z, y.w));
     }
+    Bs[e] = v;
+  }
+  fence_proxy_async_smem();  // the tiles' generic-proxy stores, visible to the tensor cores
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = s_tmem;
+  if (warp == 0) {
+    // kind::f16 instruction descriptor: F32 accumulators, BF16 A and B, both K-major
+    const uint32_t idesc = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(kRtN >> 3) << 17) |
+                           ((uint32_t)(kRtM >> 4) << 24);
+    const uint64_t ad = smem_desc(smem_addr(smem), 128, 4096);
+    const uint64_t bd = smem_desc(smem_addr(smem + kRtABytes), 128, 4096);
+    // K step s starts 32 B of K (two core matrices, 256 B) further on: 16 in the address field
+#pragma unroll
+    for (uint32_t s = 0; s < SG_PDIM / 16; s++)
+      tc_mma_bf16_ss_elect(tmem, ad + 16 * s, bd + 16 * s, idesc, s != 0);
+    tc_commit_elect(&bar_done);
+    __syncwarp();
+  }
+  const bool ok = __all_sync(0xffffffffu, mbar_wait(&bar_done, 0, &s_abort));
+  tc_fence_after();
+  if (ok) {
+    const uint32_t qd = warp & 3, n0 = 32u * (warp >> 2);
+    uint32_t r[32];
+    tc_ld32(tmem + ((32u * qd) << 16) + n0, r);
+    tc_wait_ld();
+    const uint32_t c = m0 + 32 * qd + lane;
+    if (c < K) {
+#pragma unroll
+      for (uint32_t j = 0; j < 32; j++)
+        if (q0 + n0 + j < nq) scores[(size_t)(q0 + n0 + j) * K + c] = __uint_as_float(r[j]);
+    }
+  } else if (lane == 0) {
+    atomicOr(status, kStatusTimeout);
+  }
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 0) {
+    tc_fence_after();
+    tc_dealloc(tmem, kRtCols);
+  }
 }
 
 // The reference's sequential FP32 dot of one query with one centroid row.
@@ -402,14 +422,14 @@ __global__ void __launch_bounds__(1024) k_route_expand(SelectArgs a,
 void launch_route_scores(const DevIndex& ix, Workspace& w, uint32_t nq, int precision,
                          cudaStream_t st) {
   if (precision == SG_ROUTE_BF16) {
-    static bool attr = false;
-    size_t smem = (size_t)(kBM + kBN) * kLD * sizeof(__nv_bfloat16);
+    static bool attr = false;  // per process; the attribute is per function, not per device
     if (!attr) {
-      cudaFuncSetAttribute(k_route_bf16, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+      cudaFuncSetAttribute(k_route_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, kRtSmem);
       attr = true;
     }
-    dim3 grid((ix.k + kBN - 1) / kBN, (nq + kBM - 1) / kBM);
-    k_route_bf16<<<grid, 256, smem, st>>>(w.q256, ix.cent_bf16, ix.k, nq, w.scores);
+    dim3 grid((ix.k + kRtM - 1) / kRtM, (nq + kRtN - 1) / kRtN);
+    k_route_tc<<<grid, kRtThreads, kRtSmem, st>>>(w.q256, ix.cent_bf16, ix.k, nq, w.scores,
+                                                  w.counters + 2);
   } else {
     dim3 grid((ix.k + 255) / 256, (nq + kRouteQB - 1) / kRouteQB);
     k_route_fp32<<<grid, 256, 0, st>>>(w.q256, ix.cent_t, ix.k, nq, w.scores);

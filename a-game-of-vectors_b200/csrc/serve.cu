@@ -203,7 +203,7 @@ void complete_batch(sg_server* srv, Slot& s, int launch_rc) {
       continue;
     }
     if (*s.h_status & sg::kStatusTimeout) {
-      r.status = fail(SG_ERR_DEVICE, "tensor-core scan: a pipeline wait ran out");
+      r.status = fail(SG_ERR_DEVICE, "a tensor-core wait ran out (routing GEMM or scan)");
       continue;
     }
     if (s.h_ovf[i]) {

@@ -701,7 +701,7 @@ int search_impl(sg_index* h, sg::Ctx& c, uint32_t nq, const float* q768, const f
   }
   CK(cudaStreamSynchronize(c.stream));
   if (status & sg::kStatusOverflow) return fail(SG_ERR_INVALID, "work queue overflow");
-  if (status & sg::kStatusTimeout) return fail(SG_ERR_DEVICE, "tensor-core scan: a pipeline wait ran out");
+  if (status & sg::kStatusTimeout) return fail(SG_ERR_DEVICE, "a tensor-core wait ran out (routing GEMM or scan)");
   const bool timed = t != nullptr || h->timing_on;
   if (timed) {
     collect_stats(w, p);
@@ -1082,7 +1082,36 @@ int sg_route(sg_index* h, uint32_t nq, const float* q256, const sg_params* param
     CK(cudaMemcpyAsync(out_clusters, w.probe_cl, (size_t)nq * P * 4, cudaMemcpyDeviceToHost, st));
   }
   CK(cudaMemcpyAsync(out_counts, w.probe_n, (size_t)nq * 4, cudaMemcpyDeviceToHost, st));
+  uint32_t status = 0;
+  CK(cudaMemcpyAsync(&status, w.counters + 2, 4, cudaMemcpyDeviceToHost, st));
   CK(cudaStreamSynchronize(st));
+  if (status & sg::kStatusTimeout) return fail(SG_ERR_DEVICE, "routing GEMM: a tensor-core wait ran out");
+  return SG_OK;
+}
+
+int sg_route_scores(sg_index* h, uint32_t nq, const float* q256, float* out_scores) {
+  if (!h || !q256 || !out_scores) return fail(SG_ERR_INVALID, "null argument");
+  std::lock_guard<std::mutex> g(h->mu);
+  int rc;
+  if (nq == 0) return SG_OK;
+  CK(cudaSetDevice(h->ix.device));
+  sg_params p;
+  memset(&p, 0, sizeof p);
+  p.nprobe = 1;
+  p.cand = 1;
+  p.k = 1;
+  if ((rc = ensure_ws(h, h->def, nq, p, 1))) return rc;
+  if ((rc = stage_inputs(h->def, nq, nullptr, q256, false))) return rc;
+  sg::Workspace& w = h->def.ws;
+  cudaStream_t st = h->def.stream;
+  CK(cudaMemsetAsync(w.counters, 0, 32, st));
+  sg::launch_route_scores(h->ix, w, nq, h->ix.route_precision, st);
+  CK(cudaGetLastError());
+  uint32_t status = 0;
+  CK(cudaMemcpyAsync(out_scores, w.scores, (size_t)nq * h->ix.k * 4, cudaMemcpyDeviceToHost, st));
+  CK(cudaMemcpyAsync(&status, w.counters + 2, 4, cudaMemcpyDeviceToHost, st));
+  CK(cudaStreamSynchronize(st));
+  if (status & sg::kStatusTimeout) return fail(SG_ERR_DEVICE, "routing GEMM: a tensor-core wait ran out");
   return SG_OK;
 }
 

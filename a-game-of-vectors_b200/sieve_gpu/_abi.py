@@ -249,6 +249,7 @@ EXPORTS = [
     "sg_search_device",
     "sg_search_noalloc",
     "sg_route",
+    "sg_route_scores",
     "sg_candidates",
     "sg_filter_new",
     "sg_filter_info",

@@ -268,6 +268,15 @@ class Index:
         check(lib().sg_route(self._h, c_uint32(nq), ptr(q), byref(p), ptr(sc), ptr(cl), ptr(cnt)))
         return [(sc[i, : cnt[i]], cl[i, : cnt[i]]) for i in range(nq)]
 
+    # the centroid scores of Index::route (src/ivf.rs:592, blas::gemm_abt) at the routing precision
+    def route_scores(self, q256) -> np.ndarray:
+        q = np.ascontiguousarray(q256, np.float32).reshape(-1, _abi.PDIM)
+        nq = q.shape[0]
+        out = np.zeros((nq, self.k), np.float32)
+        if nq:
+            check(lib().sg_route_scores(self._h, c_uint32(nq), ptr(q), ptr(out)))
+        return out
+
     # Index::candidates (src/ivf.rs:647-729) after the index's own routing
     def candidates(self, q256, params: Params, allow=None):
         q = np.ascontiguousarray(q256, np.float32).reshape(-1, _abi.PDIM)

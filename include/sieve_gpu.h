@@ -238,6 +238,13 @@ int sg_search_noalloc(sg_index* index, const float* d_q768, const float* d_q256,
 int sg_route(sg_index* index, uint32_t nq, const float* q256, const sg_params* params,
              float* out_scores, uint32_t* out_clusters, uint32_t* out_counts);
 
+/* The centroid scores behind ivf::Index::route (src/ivf.rs:592: blas::gemm_abt of the queries
+ * against the centroids, src/blas.rs:46-52) at the index's routing precision: out_scores
+ * [nq * k], query-major. FP32 gives the reference's sequential sums bit for bit; BF16 gives the
+ * tensor-core GEMM's scores, within 0.0085 |q| max|c| of them (the window that sg_route
+ * rescores exactly). */
+int sg_route_scores(sg_index* index, uint32_t nq, const float* q256, float* out_scores);
+
 /* ivf::Index::candidates (src/ivf.rs:647-729) over the index's own routing: the best
  * params.cand slots by RaBitQ estimate, deduplicated by row, in row order, as
  * (estimate, row, error half-width). out_* [nq * params.cand], out_counts [nq]. */

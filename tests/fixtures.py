@@ -3,6 +3,7 @@
 INDEX_A: 20,000 rows, 64 clusters, SOAR, 2-bit tier — clusters of about one scan chunk.
 INDEX_B: 30,000 rows with 400 exact duplicates, 8 clusters — clusters span several scan chunks,
          and the duplicates make exactly tied estimates and tied int8 scores.
+INDEX_C: 12,000 rows, 300 clusters, 150 queries — several routing GEMM tiles on both axes.
 Queries come from the same mixtures (sigma 0.35) plus copies of corpus rows (self-matches).
 """
 from __future__ import annotations
@@ -51,6 +52,19 @@ def index_b():
     rows = (corpus["rerank"][:8].astype(np.float32) / corpus["quant_scale"])
     rows /= np.linalg.norm(rows, axis=1, keepdims=True)
     q768 = np.concatenate([q, rows]).astype(np.float32)
+    return arrays, q768, prefixes(q768), mix
+
+
+@functools.lru_cache(maxsize=None)
+def index_c():
+    """300 clusters over 12,000 rows and 150 queries: routing tiles of 128 centroids x 64 queries
+    with a partial last tile on both axes."""
+    torch.manual_seed(1)
+    mix = synth.Mixture(n=12000, n_centers=96, seed=11)
+    corpus = builder.ingest(mix)
+    ix = builder.build_ivf(corpus, k=300, sample_n=12000, iters=3)
+    arrays = {**corpus, **ix}
+    q768 = mix.queries(150, sigma=0.35).numpy().astype(np.float32)
     return arrays, q768, prefixes(q768), mix
 
 

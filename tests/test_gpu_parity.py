@@ -9,7 +9,7 @@ import numpy as np
 import pytest
 
 import oracle as O
-from fixtures import index_a, index_b
+from fixtures import index_a, index_b, index_c
 from sieve_gpu import Index, Params, Rerank, allow_bitset, dot_i8i8, lut_scan
 from sieve_gpu._abi import SgParams
 
@@ -117,6 +117,68 @@ def test_route_matches_oracle(gpu_a, bf16, case):
     ix.set_route_precision(bf16)
     got = ix.route(q256, p)
     ix.set_route_precision(True)
+    for i in range(q256.shape[0]):
+        s, c = oi.route(q256[i], cparams(p))
+        assert np.array_equal(got[i][1], c), f"query {i}"
+        assert np.array_equal(got[i][0], s), f"query {i}"
+
+
+def _bf16(x: np.ndarray) -> np.ndarray:
+    """f32 -> bf16 (round to nearest even), returned as f32; finite inputs."""
+    u = np.ascontiguousarray(x, np.float32).view(np.uint32).astype(np.uint64)
+    r = ((u + 0x7FFF + ((u >> 16) & 1)) >> 16) << 16
+    return r.astype(np.uint32).view(np.float32)
+
+
+@pytest.fixture(scope="module", params=["a", "c"])
+def gpu_route(request):
+    arrays, q768, q256, _ = (index_a if request.param == "a" else index_c)()
+    ix = Index.from_arrays(arrays)
+    yield ix, O.OracleIndex(arrays), arrays, q768, q256
+    ix.close()
+
+
+def test_route_scores_fp32_bit_exact(gpu_route):
+    """FP32 routing scores are blas::gemm_abt's sequential sums (src/blas.rs:46-52) bit for bit."""
+    ix, oi, arrays, q768, q256 = gpu_route
+    ix.set_route_precision(False)
+    try:
+        got = ix.route_scores(q256)
+    finally:
+        ix.set_route_precision(True)
+    want = O.gemm_abt(q256, arrays["centroids"])
+    assert got.shape == want.shape
+    assert np.array_equal(got.view(np.uint32), want.view(np.uint32))
+
+
+def test_route_scores_bf16_gemm(gpu_route):
+    """The tcgen05 BF16 GEMM: every (query, centroid) score equals the exact product of the
+    bf16-rounded operands up to FP32 accumulation error (512 * 2^-23 * sum|q_i c_i|), and lies
+    within the rescoring window's delta = 0.0085 |q| max|c| of the FP32 score."""
+    ix, oi, arrays, q768, q256 = gpu_route
+    got = ix.route_scores(q256)
+    cent = np.asarray(arrays["centroids"], np.float32)
+    qb, cb = _bf16(q256).astype(np.float64), _bf16(cent).astype(np.float64)
+    exact = qb @ cb.T
+    acc_tol = 512 * 2.0**-23 * (np.abs(qb) @ np.abs(cb).T) + 1e-30
+    err = np.abs(got.astype(np.float64) - exact)
+    assert np.all(err <= acc_tol), f"max excess {np.max(err - acc_tol)}"
+    fp32 = O.gemm_abt(q256, cent).astype(np.float64)
+    delta = 0.0085 * np.linalg.norm(q256, axis=1)[:, None] * np.max(np.linalg.norm(cent, axis=1))
+    assert np.all(np.abs(got - fp32) <= delta)
+    # the scores differ from FP32's (the GEMM ran in bf16), so the check above is not vacuous
+    assert np.any(got != fp32.astype(np.float32))
+
+
+@pytest.mark.parametrize("bf16", [False, True])
+@pytest.mark.parametrize("p", [Params(20, 100), Params(300, 100), Params(40, 100, margin=0.1)])
+def test_route_many_tiles_matches_oracle(gpu_route, bf16, p):
+    ix, oi, arrays, q768, q256 = gpu_route
+    ix.set_route_precision(bf16)
+    try:
+        got = ix.route(q256, p)
+    finally:
+        ix.set_route_precision(True)
     for i in range(q256.shape[0]):
         s, c = oi.route(q256[i], cparams(p))
         assert np.array_equal(got[i][1], c), f"query {i}"
