@@ -70,7 +70,7 @@ SG_DEV uint32_t pack_bf16x2(float lo, float hi) {
   return *reinterpret_cast<uint32_t*>(&p);
 }
 
-__global__ void __launch_bounds__(kRtThreads) k_route_tc(const float* __restrict__ q256,
+__global__ void __launch_bounds__(kRtThreads, 2) k_route_tc(const float* __restrict__ q256,
                                                          const __nv_bfloat16* __restrict__ cb,
                                                          uint32_t K, uint32_t nq,
                                                          float* __restrict__ scores,
@@ -92,26 +92,44 @@ __global__ void __launch_bounds__(kRtThreads) k_route_tc(const float* __restrict
   }
   uint4* As = reinterpret_cast<uint4*>(smem);
   uint4* Bs = reinterpret_cast<uint4*>(smem + kRtABytes);
-  // A: centroid rows, already bf16 (rows past K are zero)
-#pragma unroll 4
-  for (int e = tid; e < kRtM * (SG_PDIM / 8); e += kRtThreads) {
-    const uint32_t r = 8 * (e >> 8) + (e & 7), c = (e >> 3) & 31;
-    uint4 v = make_uint4(0, 0, 0, 0);
-    if (m0 + r < K) v = __ldg(reinterpret_cast<const uint4*>(cb + (size_t)(m0 + r) * SG_PDIM) + c);
-    As[e] = v;
-  }
-  // B: query rows, f32 -> bf16 (rows past nq are zero)
-#pragma unroll 4
-  for (int e = tid; e < kRtN * (SG_PDIM / 8); e += kRtThreads) {
-    const uint32_t r = 8 * (e >> 8) + (e & 7), c = (e >> 3) & 31;
-    uint4 v = make_uint4(0, 0, 0, 0);
-    if (q0 + r < nq) {
-      const float4* src = reinterpret_cast<const float4*>(q256 + (size_t)(q0 + r) * SG_PDIM + 8 * c);
-      const float4 x = src[0], y = src[1];
-      v = make_uint4(pack_bf16x2(x.x, x.y), pack_bf16x2(x.z, x.w), pack_bf16x2(y.x, y.y),
-                     pack_bf16x2(y.z, y.w));
+  // A: centroid rows, already bf16; B: query rows, f32 -> bf16. Each thread issues all its loads
+  // of a tile before its stores (rows clamped into range, zeroed past K or nq at the store), so a
+  // CTA keeps 64 KB of loads in flight rather than waiting for each few.
+  {
+    uint4 v[kRtM * (SG_PDIM / 8) / kRtThreads];
+#pragma unroll
+    for (int i = 0; i < kRtM * (SG_PDIM / 8) / kRtThreads; i++) {
+      const int e = tid + i * kRtThreads;
+      const uint32_t r = 8 * (e >> 8) + (e & 7), c = (e >> 3) & 31;
+      const uint32_t row = min(m0 + r, K - 1);
+      v[i] = __ldg(reinterpret_cast<const uint4*>(cb + (size_t)row * SG_PDIM) + c);
     }
-    Bs[e] = v;
+#pragma unroll
+    for (int i = 0; i < kRtM * (SG_PDIM / 8) / kRtThreads; i++) {
+      const int e = tid + i * kRtThreads;
+      const uint32_t r = 8 * (e >> 8) + (e & 7);
+      As[e] = m0 + r < K ? v[i] : make_uint4(0, 0, 0, 0);
+    }
+  }
+  {
+    float4 x[kRtN * (SG_PDIM / 8) / kRtThreads], y[kRtN * (SG_PDIM / 8) / kRtThreads];
+#pragma unroll
+    for (int i = 0; i < kRtN * (SG_PDIM / 8) / kRtThreads; i++) {
+      const int e = tid + i * kRtThreads;
+      const uint32_t r = 8 * (e >> 8) + (e & 7), c = (e >> 3) & 31;
+      const uint32_t row = min(q0 + r, nq - 1);
+      const float4* src = reinterpret_cast<const float4*>(q256 + (size_t)row * SG_PDIM + 8 * c);
+      x[i] = __ldg(src);
+      y[i] = __ldg(src + 1);
+    }
+#pragma unroll
+    for (int i = 0; i < kRtN * (SG_PDIM / 8) / kRtThreads; i++) {
+      const int e = tid + i * kRtThreads;
+      const uint32_t r = 8 * (e >> 8) + (e & 7);
+      Bs[e] = q0 + r < nq ? make_uint4(pack_bf16x2(x[i].x, x[i].y), pack_bf16x2(x[i].z, x[i].w),
+                                       pack_bf16x2(y[i].x, y[i].y), pack_bf16x2(y[i].z, y[i].w))
+                          : make_uint4(0, 0, 0, 0);
+    }
   }
   fence_proxy_async_smem();  // the tiles' generic-proxy stores, visible to the tensor cores
   tc_fence_before();
@@ -421,6 +439,7 @@ __global__ void __launch_bounds__(1024) k_route_expand(SelectArgs a,
 
 void launch_route_scores(const DevIndex& ix, Workspace& w, uint32_t nq, int precision,
                          cudaStream_t st) {
+  if (nq == 0 || ix.k == 0) return;
   if (precision == SG_ROUTE_BF16) {
     static bool attr = false;  // per process; the attribute is per function, not per device
     if (!attr) {
