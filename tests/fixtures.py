@@ -4,6 +4,7 @@ INDEX_A: 20,000 rows, 64 clusters, SOAR, 2-bit tier — clusters of about one sc
 INDEX_B: 30,000 rows with 400 exact duplicates, 8 clusters — clusters span several scan chunks,
          and the duplicates make exactly tied estimates and tied int8 scores.
 INDEX_C: 12,000 rows, 300 clusters, 150 queries — several routing GEMM tiles on both axes.
+INDEX_D: 16,384 rows, 4096 clusters, 4096 queries — the routing GEMM at full size.
 Queries come from the same mixtures (sigma 0.35) plus copies of corpus rows (self-matches).
 """
 from __future__ import annotations
@@ -65,6 +66,19 @@ def index_c():
     ix = builder.build_ivf(corpus, k=300, sample_n=12000, iters=3)
     arrays = {**corpus, **ix}
     q768 = mix.queries(150, sigma=0.35).numpy().astype(np.float32)
+    return arrays, q768, prefixes(q768), mix
+
+
+@functools.lru_cache(maxsize=None)
+def index_d():
+    """4096 clusters over 16,384 rows and a batch of 4096 queries: the routing GEMM at full size
+    (K = 4096 centroids x 4096 queries, 32 x 64 tiles)."""
+    torch.manual_seed(2)
+    mix = synth.Mixture(n=16384, n_centers=256, seed=13)
+    corpus = builder.ingest(mix)
+    ix = builder.build_ivf(corpus, k=4096, sample_n=16384, iters=1)
+    arrays = {**corpus, **ix}
+    q768 = mix.queries(4096, sigma=0.35).numpy().astype(np.float32)
     return arrays, q768, prefixes(q768), mix
 
 

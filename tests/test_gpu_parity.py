@@ -9,7 +9,7 @@ import numpy as np
 import pytest
 
 import oracle as O
-from fixtures import index_a, index_b, index_c
+from fixtures import index_a, index_b, index_c, index_d
 from sieve_gpu import Index, Params, Rerank, allow_bitset, dot_i8i8, lut_scan
 from sieve_gpu._abi import SgParams
 
@@ -138,9 +138,17 @@ def gpu_route(request):
     ix.close()
 
 
-def test_route_scores_fp32_bit_exact(gpu_route):
+@pytest.fixture(scope="module", params=["a", "c", "d"])
+def gpu_route_scores(request):
+    arrays, q768, q256, _ = {"a": index_a, "c": index_c, "d": index_d}[request.param]()
+    ix = Index.from_arrays(arrays)
+    yield ix, None, arrays, q768, q256
+    ix.close()
+
+
+def test_route_scores_fp32_bit_exact(gpu_route_scores):
     """FP32 routing scores are blas::gemm_abt's sequential sums (src/blas.rs:46-52) bit for bit."""
-    ix, oi, arrays, q768, q256 = gpu_route
+    ix, _, arrays, q768, q256 = gpu_route_scores
     ix.set_route_precision(False)
     try:
         got = ix.route_scores(q256)
@@ -151,11 +159,11 @@ def test_route_scores_fp32_bit_exact(gpu_route):
     assert np.array_equal(got.view(np.uint32), want.view(np.uint32))
 
 
-def test_route_scores_bf16_gemm(gpu_route):
+def test_route_scores_bf16_gemm(gpu_route_scores):
     """The tcgen05 BF16 GEMM: every (query, centroid) score equals the exact product of the
     bf16-rounded operands up to FP32 accumulation error (512 * 2^-23 * sum|q_i c_i|), and lies
     within the rescoring window's delta = 0.0085 |q| max|c| of the FP32 score."""
-    ix, oi, arrays, q768, q256 = gpu_route
+    ix, _, arrays, q768, q256 = gpu_route_scores
     got = ix.route_scores(q256)
     cent = np.asarray(arrays["centroids"], np.float32)
     qb, cb = _bf16(q256).astype(np.float64), _bf16(cent).astype(np.float64)
