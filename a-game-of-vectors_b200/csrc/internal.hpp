@@ -80,6 +80,7 @@ struct Workspace {
   float* winv = nullptr;       // [nq]
   int8_t* wq256 = nullptr;     // [nq*256]
   float* winv256 = nullptr;    // [nq]
+  __nv_bfloat16* q16 = nullptr;  // [nq*256] q256 rounded to bf16: the routing GEMM's B operand
   float* scores = nullptr;     // [nq*k] routing scores
   uint64_t scores_cap = 0;
   float* probe_sc = nullptr;   // [nq*P]
@@ -197,8 +198,13 @@ int index_check_params(const sg_index* h, const sg_params* p);
 // kernel launchers (one per .cu file section)
 void launch_prefix(Workspace& w, uint32_t nq, cudaStream_t st);
 void launch_prep(const DevIndex& ix, Workspace& w, uint32_t nq, cudaStream_t st);
-void launch_route_scores(const DevIndex& ix, Workspace& w, uint32_t nq, int precision,
-                         cudaStream_t st);
+// Looks up the driver's tensor-map encoder the BF16 routing GEMM needs (once per process);
+// false if the driver does not provide it.
+bool route_gemm_ready();
+// BF16: two launches (the queries to bf16, then the tcgen05 GEMM); FP32: one. Returns the
+// launch error, or cudaErrorInvalidValue if the GEMM's TMA tensor maps cannot be encoded.
+cudaError_t launch_route_scores(const DevIndex& ix, Workspace& w, uint32_t nq, int precision,
+                                cudaStream_t st);
 // alu_ranks = false leaves probe ranks >= 1 to the MMA scan (only rank-0 chunks past the seed
 // become ALU work items).
 inline uint32_t next_pow2_host(uint32_t x) {

@@ -57,6 +57,7 @@ struct Carve {
 void carve_workspace(Carve& c, sg::Workspace& w, const sg::DevIndex& x, uint32_t P, uint32_t cand,
                      uint64_t items, uint32_t cbuf, bool need_q256) {
   if (need_q256) w.q256 = c.take<float>(SG_PDIM);
+  w.q16 = c.take<__nv_bfloat16>(SG_PDIM);
   w.tables = c.take<uint8_t>(SG_GROUPS * 16);
   w.qp = c.take<float4>(1);
   w.qnorm = c.take<float>(1);
@@ -138,7 +139,8 @@ extern "C" int sg_search_noalloc(sg_index* h, const float* d_q768, const float* 
     return sg::fail(SG_ERR_DEVICE, std::string("cudaMemsetAsync: ") + cudaGetErrorString(e));
   if (!d_q256) sg::launch_prefix(w, 1, st);
   sg::launch_prep(x, w, 1, st);
-  sg::launch_route_scores(x, w, 1, x.route_precision, st);
+  if ((e = sg::launch_route_scores(x, w, 1, x.route_precision, st)) != cudaSuccess)
+    return sg::fail(SG_ERR_DEVICE, std::string("sg_search_noalloc routing: ") + cudaGetErrorString(e));
   sg::launch_route_select(x, w, 1, p, x.route_precision, cfg.small_chunk_blocks, cfg.seed_blocks,
                           true, st);
   if (p.cand > 0) {

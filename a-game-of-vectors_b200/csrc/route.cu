@@ -15,7 +15,10 @@
 // Then TopK(nprobe) ordering (score desc, id asc), the margin cut v >= best - m, and the slot
 // budget (take while the running slot count stays <= b, keep at least one), and the scan work
 // items of each probe (chunks of at most chunk_blocks blocks).
+#include <cudaTypedefs.h>
 #include <float.h>
+
+#include <mutex>
 
 #include "common.cuh"
 #include "internal.hpp"
@@ -53,13 +56,15 @@ __global__ void __launch_bounds__(256) k_route_fp32(const float* __restrict__ q2
 
 // ---- BF16 GEMM on the tcgen05 tensor cores: 128 centroids x 64 queries per CTA --------------
 // D[centroid][query] = sum_k c_bf16[k] * bf16(q[k]) in FP32 tensor memory (M = 128 TMEM lanes,
-// N = 64 columns), both operands in shared memory as K-major core matrices without swizzle:
-// 8 rows x 16 B (8 bf16) per core matrix, 128 B apart along K, 4096 B (32 along K) apart along
-// the rows. Chunk e of a tile (row 8*(e>>8) + (e&7), k-chunk (e>>3)&31) sits at byte 16*e, so
-// the loads write shared memory linearly. One elected lane issues the 16 MMAs (K = 16 each);
-// all warps then read the accumulators with tcgen05.ld: warp w takes TMEM lanes 32*(w&3).. (the
-// tile's centroids), columns 32*(w>>2).. (queries), and stores each query's 32 centroid scores
-// as one coalesced 128 B row segment.
+// N = 64 columns). Both operands come into shared memory by TMA as K-major core matrices without
+// swizzle (8 rows x 16 B = 8 bf16 each): one tiled copy per 16-byte k-chunk c brings that chunk
+// of all the tile's rows, row after row, to c * rows * 16 B. So the core matrices of a chunk
+// are 128 B apart along the rows (SBO) and the chunks rows * 16 B apart along K (LBO). The
+// copies bypass the load/store pipe, which register-staged loads of this layout saturate (each
+// warp-wide load touches 8 rows). One elected lane issues the 16 MMAs (K = 16 each). All warps
+// then read the accumulators with tcgen05.ld: warp w takes TMEM lanes 32*(w&3).. (the tile's
+// centroids) and columns 32*(w>>2).. (queries), and stores each query's 32 centroid scores as
+// one coalesced 128 B row segment. Rows past K or nq come in as zeros (the maps' bounds).
 constexpr int kRtM = 128, kRtN = 64, kRtThreads = 256;
 constexpr uint32_t kRtCols = 64;  // TMEM columns: the f32 accumulators
 constexpr int kRtABytes = kRtM * SG_PDIM * 2, kRtBBytes = kRtN * SG_PDIM * 2;
@@ -70,13 +75,21 @@ SG_DEV uint32_t pack_bf16x2(float lo, float hi) {
   return *reinterpret_cast<uint32_t*>(&p);
 }
 
-__global__ void __launch_bounds__(kRtThreads, 2) k_route_tc(const float* __restrict__ q256,
-                                                         const __nv_bfloat16* __restrict__ cb,
+// q256 -> bf16, 4 values per thread.
+__global__ void k_q_bf16(const float4* __restrict__ q, uint32_t n4, uint2* __restrict__ out) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n4) return;
+  const float4 v = q[i];
+  out[i] = make_uint2(pack_bf16x2(v.x, v.y), pack_bf16x2(v.z, v.w));
+}
+
+__global__ void __launch_bounds__(kRtThreads) k_route_tc(const __grid_constant__ CUtensorMap map_c,
+                                                         const __grid_constant__ CUtensorMap map_q,
                                                          uint32_t K, uint32_t nq,
                                                          float* __restrict__ scores,
                                                          uint32_t* __restrict__ status) {
   extern __shared__ __align__(1024) uint8_t smem[];
-  __shared__ __align__(8) uint64_t bar_done;
+  __shared__ __align__(8) uint64_t bar_load, bar_done;
   __shared__ uint32_t s_tmem;
   __shared__ int s_abort;
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
@@ -86,67 +99,37 @@ __global__ void __launch_bounds__(kRtThreads, 2) k_route_tc(const float* __restr
     tc_relinquish();
   }
   if (tid == 0) {
+    mbar_init(&bar_load, 1);
     mbar_init(&bar_done, 1);
     s_abort = 0;
     fence_mbar_init();
   }
-  uint4* As = reinterpret_cast<uint4*>(smem);
-  uint4* Bs = reinterpret_cast<uint4*>(smem + kRtABytes);
-  // A: centroid rows, already bf16; B: query rows, f32 -> bf16. Each thread issues all its loads
-  // of a tile before its stores (rows clamped into range, zeroed past K or nq at the store), so a
-  // CTA keeps 64 KB of loads in flight rather than waiting for each few.
-  {
-    uint4 v[kRtM * (SG_PDIM / 8) / kRtThreads];
-#pragma unroll
-    for (int i = 0; i < kRtM * (SG_PDIM / 8) / kRtThreads; i++) {
-      const int e = tid + i * kRtThreads;
-      const uint32_t r = 8 * (e >> 8) + (e & 7), c = (e >> 3) & 31;
-      const uint32_t row = min(m0 + r, K - 1);
-      v[i] = __ldg(reinterpret_cast<const uint4*>(cb + (size_t)row * SG_PDIM) + c);
-    }
-#pragma unroll
-    for (int i = 0; i < kRtM * (SG_PDIM / 8) / kRtThreads; i++) {
-      const int e = tid + i * kRtThreads;
-      const uint32_t r = 8 * (e >> 8) + (e & 7);
-      As[e] = m0 + r < K ? v[i] : make_uint4(0, 0, 0, 0);
-    }
-  }
-  {
-    float4 x[kRtN * (SG_PDIM / 8) / kRtThreads], y[kRtN * (SG_PDIM / 8) / kRtThreads];
-#pragma unroll
-    for (int i = 0; i < kRtN * (SG_PDIM / 8) / kRtThreads; i++) {
-      const int e = tid + i * kRtThreads;
-      const uint32_t r = 8 * (e >> 8) + (e & 7), c = (e >> 3) & 31;
-      const uint32_t row = min(q0 + r, nq - 1);
-      const float4* src = reinterpret_cast<const float4*>(q256 + (size_t)row * SG_PDIM + 8 * c);
-      x[i] = __ldg(src);
-      y[i] = __ldg(src + 1);
-    }
-#pragma unroll
-    for (int i = 0; i < kRtN * (SG_PDIM / 8) / kRtThreads; i++) {
-      const int e = tid + i * kRtThreads;
-      const uint32_t r = 8 * (e >> 8) + (e & 7);
-      Bs[e] = q0 + r < nq ? make_uint4(pack_bf16x2(x[i].x, x[i].y), pack_bf16x2(x[i].z, x[i].w),
-                                       pack_bf16x2(y[i].x, y[i].y), pack_bf16x2(y[i].z, y[i].w))
-                          : make_uint4(0, 0, 0, 0);
-    }
-  }
-  fence_proxy_async_smem();  // the tiles' generic-proxy stores, visible to the tensor cores
   tc_fence_before();
   __syncthreads();
   tc_fence_after();
   const uint32_t tmem = s_tmem;
   if (warp == 0) {
-    // kind::f16 instruction descriptor: F32 accumulators, BF16 A and B, both K-major
-    const uint32_t idesc = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(kRtN >> 3) << 17) |
-                           ((uint32_t)(kRtM >> 4) << 24);
-    const uint64_t ad = smem_desc(smem_addr(smem), 128, 4096);
-    const uint64_t bd = smem_desc(smem_addr(smem + kRtABytes), 128, 4096);
-    // K step s starts 32 B of K (two core matrices, 256 B) further on: 16 in the address field
+    const uint32_t a = smem_addr(smem), b = a + kRtABytes;
+    if (lane == 0) {
+      mbar_expect_tx(&bar_load, kRtABytes + kRtBBytes);
+      for (int c = 0; c < SG_PDIM / 8; c++) {
+        tma_load_2d(a + c * (kRtM * 16), &map_c, 8 * c, (int32_t)m0, &bar_load);
+        tma_load_2d(b + c * (kRtN * 16), &map_q, 8 * c, (int32_t)q0, &bar_load);
+      }
+    }
+    __syncwarp();
+    if (__all_sync(0xffffffffu, mbar_wait(&bar_load, 0, &s_abort))) {
+      tc_fence_after();
+      // kind::f16 instruction descriptor: F32 accumulators, BF16 A and B, both K-major
+      const uint32_t idesc = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(kRtN >> 3) << 17) |
+                             ((uint32_t)(kRtM >> 4) << 24);
+      const uint64_t ad = smem_desc(a, kRtM * 16, 128), bd = smem_desc(b, kRtN * 16, 128);
+      // K step s covers k-chunks 2s and 2s + 1: the start moves two chunks (2 * rows * 16 B)
 #pragma unroll
-    for (uint32_t s = 0; s < SG_PDIM / 16; s++)
-      tc_mma_bf16_ss_elect(tmem, ad + 16 * s, bd + 16 * s, idesc, s != 0);
-    tc_commit_elect(&bar_done);
+      for (uint32_t s = 0; s < SG_PDIM / 16; s++)
+        tc_mma_bf16_ss_elect(tmem, ad + 2 * s * kRtM, bd + 2 * s * kRtN, idesc, s != 0);
+      tc_commit_elect(&bar_done);
+    }
     __syncwarp();
   }
   const bool ok = __all_sync(0xffffffffu, mbar_wait(&bar_done, 0, &s_abort));
@@ -171,6 +154,38 @@ __global__ void __launch_bounds__(kRtThreads, 2) k_route_tc(const float* __restr
     tc_fence_after();
     tc_dealloc(tmem, kRtCols);
   }
+}
+
+// cuTensorMapEncodeTiled from the driver, looked up once (the library links the CUDA runtime
+// statically and has no link-time dependency on the driver library).
+static PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
+  static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q = cudaDriverEntryPointSymbolNotFound;
+    if (cudaGetDriverEntryPointByVersion("cuTensorMapEncodeTiled", &p, 12000, cudaEnableDefault, &q) ==
+            cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+  });
+  return fn;
+}
+
+bool route_gemm_ready() { return tensor_map_encoder() != nullptr; }
+
+// A 2-D map over a row-major [rows x 256] bf16 matrix (16-byte aligned) whose box is one 16-byte
+// k-chunk (8 elements) of box_rows rows; rows past `rows` read as zeros.
+static bool encode_rows(CUtensorMap* m, const __nv_bfloat16* base, uint64_t rows, uint32_t box_rows) {
+  const PFN_cuTensorMapEncodeTiled_v12000 enc = tensor_map_encoder();
+  if (!enc) return false;
+  const cuuint64_t dims[2] = {SG_PDIM, rows};
+  const cuuint64_t strides[1] = {SG_PDIM * sizeof(__nv_bfloat16)};
+  const cuuint32_t box[2] = {8, box_rows};
+  const cuuint32_t estr[2] = {1, 1};
+  return enc(m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<__nv_bfloat16*>(base), dims, strides,
+             box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+             CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
 // The reference's sequential FP32 dot of one query with one centroid row.
@@ -437,22 +452,28 @@ __global__ void __launch_bounds__(1024) k_route_expand(SelectArgs a,
   emit_probes(a, keys, m, q, tmp);
 }
 
-void launch_route_scores(const DevIndex& ix, Workspace& w, uint32_t nq, int precision,
-                         cudaStream_t st) {
-  if (nq == 0 || ix.k == 0) return;
+cudaError_t launch_route_scores(const DevIndex& ix, Workspace& w, uint32_t nq, int precision,
+                                cudaStream_t st) {
+  if (nq == 0 || ix.k == 0) return cudaSuccess;
   if (precision == SG_ROUTE_BF16) {
     static bool attr = false;  // per process; the attribute is per function, not per device
     if (!attr) {
       cudaFuncSetAttribute(k_route_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, kRtSmem);
       attr = true;
     }
+    CUtensorMap map_c, map_q;
+    if (!encode_rows(&map_c, ix.cent_bf16, ix.k, kRtM) || !encode_rows(&map_q, w.q16, nq, kRtN))
+      return cudaErrorInvalidValue;
+    const uint32_t n4 = nq * (SG_PDIM / 4);
+    k_q_bf16<<<(n4 + 255) / 256, 256, 0, st>>>(reinterpret_cast<const float4*>(w.q256), n4,
+                                               reinterpret_cast<uint2*>(w.q16));
     dim3 grid((ix.k + kRtM - 1) / kRtM, (nq + kRtN - 1) / kRtN);
-    k_route_tc<<<grid, kRtThreads, kRtSmem, st>>>(w.q256, ix.cent_bf16, ix.k, nq, w.scores,
-                                                  w.counters + 2);
+    k_route_tc<<<grid, kRtThreads, kRtSmem, st>>>(map_c, map_q, ix.k, nq, w.scores, w.counters + 2);
   } else {
     dim3 grid((ix.k + 255) / 256, (nq + kRouteQB - 1) / kRouteQB);
     k_route_fp32<<<grid, 256, 0, st>>>(w.q256, ix.cent_t, ix.k, nq, w.scores);
   }
+  return cudaGetLastError();
 }
 
 void launch_route_select(const DevIndex& ix, Workspace& w, uint32_t nq, const sg_params& p,

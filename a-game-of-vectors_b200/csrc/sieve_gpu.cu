@@ -101,6 +101,7 @@ void free_ws(sg::Workspace& w) {
   w.brute_cap = 0;
   dfree(w.q768);
   dfree(w.q256);
+  dfree(w.q16);
   dfree(w.tables);
   dfree(w.qp);
   dfree(w.qnorm);
@@ -256,6 +257,10 @@ int build_index(const sg_ivf_arrays* a, int device, sg_index** out) {
     free_index(x);
     return rc;
   }
+  if (!sg::route_gemm_ready()) {
+    free_index(x);
+    return fail(SG_ERR_DEVICE, "cuTensorMapEncodeTiled (the routing GEMM's TMA maps) is unavailable");
+  }
   // the batched tensor-core scan reads its own copy of the codes: slot-major for tcgen05 (the
   // default), or the mma.sync word order when SIEVE_GPU_TC=0
   if (const char* tc = getenv("SIEVE_GPU_TC")) h->cfg.tc = atoi(tc);
@@ -364,10 +369,11 @@ int ensure_ws_impl(sg_index* h, sg::Ctx& c, uint32_t nq, const sg_params& p, uin
   }
   if (nq > w.nq_cap) {
     uint32_t n = std::max(nq, w.nq_cap * 2);
-    dfree(w.q768); dfree(w.q256); dfree(w.tables); dfree(w.qp); dfree(w.qnorm); dfree(w.wq);
+    dfree(w.q768); dfree(w.q256); dfree(w.q16); dfree(w.tables); dfree(w.qp); dfree(w.qnorm); dfree(w.wq);
     dfree(w.winv); dfree(w.wq256); dfree(w.winv256); dfree(w.probe_n); dfree(w.scanned); dfree(w.seed_items);
     dfree(w.thr); dfree(w.ccount); dfree(w.overflow); dfree(w.cn); dfree(w.ln); dfree(w.out_n);
     if ((rc = dalloc(&w.q768, (size_t)n * SG_DIM)) || (rc = dalloc(&w.q256, (size_t)n * SG_PDIM)) ||
+        (rc = dalloc(&w.q16, (size_t)n * SG_PDIM)) ||
         (rc = dalloc(&w.tables, (size_t)n * SG_GROUPS * 16)) || (rc = dalloc(&w.qp, n)) ||
         (rc = dalloc(&w.qnorm, n)) || (rc = dalloc(&w.wq, (size_t)n * SG_DIM)) ||
         (rc = dalloc(&w.winv, n)) || (rc = dalloc(&w.wq256, (size_t)n * SG_PDIM)) ||
@@ -513,7 +519,8 @@ int run_pipeline(sg_index* h, sg::Ctx& c, uint32_t nq, const sg_params& p, bool 
   }
   sg::launch_prep(x, w, nq, st);
   if (timed) CK(cudaEventRecord(w.ev[1], st));
-  sg::launch_route_scores(x, w, nq, rp.expand() ? SG_ROUTE_FP32 : x.route_precision, st);
+  const int route_prec = rp.expand() ? SG_ROUTE_FP32 : x.route_precision;
+  CK(sg::launch_route_scores(x, w, nq, route_prec, st));
   if (timed) CK(cudaEventRecord(w.ev[2], st));
   // Few queries leave most SMs to the chunked pass: a short seed (one CTA per query scans it
   // alone) and short chunks keep the GPU busy.
@@ -528,7 +535,7 @@ int run_pipeline(sg_index* h, sg::Ctx& c, uint32_t nq, const sg_params& p, bool 
   else
     sg::launch_route_select(x, w, nq, p, x.route_precision, cb, sb, !mma, st);
   if (timed) CK(cudaEventRecord(w.ev[3], st));
-  launches += 3;
+  launches += route_prec == SG_ROUTE_BF16 ? 4 : 3;  // prep, routing (BF16: + the bf16 queries), select
   if (p.cand > 0) {
     sg::launch_scan(x, w, nq, p, d_allow, allow_words, h->sms, 0, sb,
                     h->cfg.scan_ctas_per_sm, st);
@@ -1072,7 +1079,7 @@ int sg_route(sg_index* h, uint32_t nq, const float* q256, const sg_params* param
   cudaStream_t st = h->def.stream;
   CK(cudaMemsetAsync(w.counters, 0, 32, st));
   sg::launch_prep(h->ix, w, nq, st);
-  sg::launch_route_scores(h->ix, w, nq, h->ix.route_precision, st);
+  CK(sg::launch_route_scores(h->ix, w, nq, h->ix.route_precision, st));
   sg::launch_route_select(h->ix, w, nq, *params, h->ix.route_precision, h->cfg.chunk_blocks,
                           h->cfg.seed_blocks, true, st);
   CK(cudaGetLastError());
@@ -1105,7 +1112,7 @@ int sg_route_scores(sg_index* h, uint32_t nq, const float* q256, float* out_scor
   sg::Workspace& w = h->def.ws;
   cudaStream_t st = h->def.stream;
   CK(cudaMemsetAsync(w.counters, 0, 32, st));
-  sg::launch_route_scores(h->ix, w, nq, h->ix.route_precision, st);
+  CK(sg::launch_route_scores(h->ix, w, nq, h->ix.route_precision, st));
   CK(cudaGetLastError());
   uint32_t status = 0;
   CK(cudaMemcpyAsync(out_scores, w.scores, (size_t)nq * h->ix.k * 4, cudaMemcpyDeviceToHost, st));

@@ -1,7 +1,9 @@
 // tcgen05.cuh — inline-PTX wrappers for the 5th-generation tensor cores (sm_100a) shared by the
 // tcgen05 kernels of this library: mbarriers with bounded waits, tensor-memory allocation, loads
-// and stores, shared-memory matrix descriptors and MMAs issued from one elected lane.
+// and stores, shared-memory matrix descriptors, MMAs issued from one elected lane, and tiled TMA
+// loads (no multicast).
 #pragma once
+#include <cuda.h>
 #include <stdint.h>
 
 #include "common.cuh"
@@ -119,6 +121,22 @@ SG_DEV void tc_mma_bf16_ss_elect(uint32_t d_tmem, uint64_t a_desc, uint64_t b_de
       "{\n.reg .pred p, e;\nsetp.ne.b32 p, %4, 0;\nelect.sync _|e, 0xffffffff;\n"
       "@e tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %5, %5, %5}, p;\n}\n" ::"r"(d_tmem),
       "l"(a_desc), "l"(b_desc), "r"(idesc), "r"(accumulate), "r"(0u));
+}
+
+// Adds `bytes` to the transaction count the current phase of `bar` waits for, and arrives.
+SG_DEV void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(smem_addr(bar)), "r"(bytes)
+               : "memory");
+}
+// Tiled TMA load of the box at (x, y) of a 2-D tensor map into this CTA's shared memory at `dst`
+// (128-byte aligned); completion is counted in bytes on `bar`. x * element size must be a
+// multiple of 16 bytes.
+SG_DEV void tma_load_2d(uint32_t dst, const CUtensorMap* map, int32_t x, int32_t y, uint64_t* bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];\n" ::"r"(
+          dst),
+      "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(smem_addr(bar))
+      : "memory");
 }
 
 }  // namespace sg
