@@ -824,16 +824,19 @@ int bg_run(sg_bigann* h, uint32_t nq, const sg_bigann_params& p, BgStage stage, 
                                     w.qp, w.qq, w.rtab, w.roff);
   dim3 g1((h->k + 255) / 256, (nq + sg::kBgRouteQ - 1) / sg::kBgRouteQ);
   sg::k_bg_scores<<<g1, 256, 0, st>>>(w.q, nq, h->leaves_t, h->leaf_norm, h->k, w.scores);
-  static bool attr = false;
-  if (!attr) {
-    BG_CK(cudaFuncSetAttribute(sg::k_bg_select, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                               (int)(sg::kBgMax * 8)));
-    BG_CK(cudaFuncSetAttribute(sg::k_bg_scan<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                               (int)bg_scan_smem(sg::kBgMax, sg::kBgMax, true)));
-    BG_CK(cudaFuncSetAttribute(sg::k_bg_scan<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                               (int)bg_scan_smem(sg::kBgMax, sg::kBgMax, false)));
-    attr = true;
-  }
+  static sg::PerDeviceOnce attr;
+  const cudaError_t smem_limits = attr([] {
+    cudaError_t e = cudaFuncSetAttribute(sg::k_bg_select, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)(sg::kBgMax * 8));
+    if (e == cudaSuccess)
+      e = cudaFuncSetAttribute(sg::k_bg_scan<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               (int)bg_scan_smem(sg::kBgMax, sg::kBgMax, true));
+    if (e == cudaSuccess)
+      e = cudaFuncSetAttribute(sg::k_bg_scan<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               (int)bg_scan_smem(sg::kBgMax, sg::kBgMax, false));
+    return e;
+  });
+  BG_CK(smem_limits);
   const size_t sel_smem = (size_t)sg::next_pow2_host(std::max<uint32_t>(P, 1)) * 8;
   sg::k_bg_select<<<nq, 1024, sel_smem, st>>>(w.scores, h->k, P, p.margin, w.qq, w.q, h->leaves,
                                               w.probe, w.probe_cent, w.probe_n);

@@ -164,12 +164,9 @@ void launch_cut(const DevIndex& ix, Workspace& w, uint32_t nq, const sg_params& 
   a.cid = w.cid;
   a.cerr = w.cerr;
   a.cn = w.cn;
-  static bool attr = false;
-  size_t smem = (size_t)kHash * 12 + (size_t)kMaxCand * 4;
-  if (!attr) {
-    cudaFuncSetAttribute(k_cut, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    attr = true;
-  }
+  static PerDeviceOnce attr;
+  const size_t smem = (size_t)kHash * 12 + (size_t)kMaxCand * 4;
+  attr([&] { return cudaFuncSetAttribute(k_cut, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem); });
   k_cut<<<nq, 1024, smem, st>>>(a);
 }
 

@@ -8,6 +8,7 @@
 #include <string.h>
 
 #include <algorithm>
+#include <atomic>
 #include <mutex>
 #include <string>
 #include <vector>
@@ -15,6 +16,25 @@
 #include "../../include/sieve_gpu.h"
 
 namespace sg {
+
+// Runs a kernel-attribute setter (such as raising the dynamic shared-memory limit) once per
+// device: an attribute set on one device does not carry over to a kernel launched on another.
+// Racing first calls may both run the setter, which is idempotent. A device index past 63 runs
+// it every time.
+struct PerDeviceOnce {
+  std::atomic<uint64_t> done{0};
+  template <typename F>
+  cudaError_t operator()(F&& set) {
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    const uint64_t bit = dev >= 0 && dev < 64 ? 1ull << dev : 0;
+    if (bit && (done.load(std::memory_order_acquire) & bit)) return cudaSuccess;
+    e = set();
+    if (e == cudaSuccess && bit) done.fetch_or(bit, std::memory_order_acq_rel);
+    return e;
+  }
+};
 
 // Blocks (32 slots) a scan work item covers at most; the scan CTA holds one chunk's estimates
 // in shared memory (4 B per slot plus one padding word per block), so kMaxChunkBlocks = 512

@@ -201,12 +201,9 @@ __global__ void __launch_bounds__(1024) k_top_list(const float* __restrict__ sc,
 void launch_top_list(const float* sc, const uint32_t* id, const uint32_t* n_in, uint64_t sc_stride,
                      uint64_t id_stride, uint32_t nsel, float* out_sc, uint32_t* out_id,
                      uint32_t* n_out, uint32_t stride_out, uint32_t nq, cudaStream_t st) {
-  static bool attr = false;
-  size_t smem = (size_t)kMaxCand * 8;
-  if (!attr) {
-    cudaFuncSetAttribute(k_top_list, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    attr = true;
-  }
+  static PerDeviceOnce attr;
+  const size_t smem = (size_t)kMaxCand * 8;
+  attr([&] { return cudaFuncSetAttribute(k_top_list, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem); });
   k_top_list<<<nq, 1024, smem, st>>>(sc, id, n_in, sc_stride, id_stride, nsel, out_sc, out_id,
                                      n_out, stride_out);
 }
@@ -248,12 +245,11 @@ int launch_rerank(const DevIndex& ix, Workspace& w, uint32_t nq, const sg_params
     dot_list(ix, w, nq, stride, false, st);
     launches += 2;
   } else if (kind == SG_RERANK_TIERED && ix.has_t2) {
-    static bool attr = false;
-    size_t smem = (size_t)SG_TIER2_BYTES * 256 * sizeof(float);
-    if (!attr) {
-      cudaFuncSetAttribute(k_tier2_list, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-      attr = true;
-    }
+    static PerDeviceOnce attr;
+    const size_t smem = (size_t)SG_TIER2_BYTES * 256 * sizeof(float);
+    attr([&] {
+      return cudaFuncSetAttribute(k_tier2_list, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    });
     dim3 grid((stride + 127) / 128, nq);
     k_tier2_list<<<grid, 256, smem, st>>>(w.q256, ix.t2_sigma, ix.t2_codes, ix.t2_norm, w.lid,
                                           w.ln, stride, w.lsc);

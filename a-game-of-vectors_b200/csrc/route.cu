@@ -456,11 +456,8 @@ cudaError_t launch_route_scores(const DevIndex& ix, Workspace& w, uint32_t nq, i
                                 cudaStream_t st) {
   if (nq == 0 || ix.k == 0) return cudaSuccess;
   if (precision == SG_ROUTE_BF16) {
-    static bool attr = false;  // per process; the attribute is per function, not per device
-    if (!attr) {
-      cudaFuncSetAttribute(k_route_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, kRtSmem);
-      attr = true;
-    }
+    static PerDeviceOnce attr;
+    attr([] { return cudaFuncSetAttribute(k_route_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, kRtSmem); });
     CUtensorMap map_c, map_q;
     if (!encode_rows(&map_c, ix.cent_bf16, ix.k, kRtM) || !encode_rows(&map_q, w.q16, nq, kRtN))
       return cudaErrorInvalidValue;
@@ -502,12 +499,11 @@ void launch_route_select(const DevIndex& ix, Workspace& w, uint32_t nq, const sg
   a.items = w.items;
   a.item_cap = w.item_cap;
   a.counters = w.counters;
-  static bool attr = false;
-  size_t smem = kWinCap * sizeof(uint64_t);
-  if (!attr) {
-    cudaFuncSetAttribute(k_route_select, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    attr = true;
-  }
+  static PerDeviceOnce attr;
+  const size_t smem = kWinCap * sizeof(uint64_t);
+  attr([&] {
+    return cudaFuncSetAttribute(k_route_select, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  });
   k_route_select<<<nq, 256, smem, st>>>(a);
 }
 
@@ -539,12 +535,11 @@ void launch_route_expand(const DevIndex& ix, Workspace& w, uint32_t nq, const sg
   a.item_cap = w.item_cap;
   a.counters = w.counters;
   const size_t smem = (size_t)next_pow2_host(ix.k) * sizeof(uint64_t);
-  static bool attr = false;
-  if (!attr) {
-    cudaFuncSetAttribute(k_route_expand, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         (int)(kExpandMaxK * sizeof(uint64_t)));
-    attr = true;
-  }
+  static PerDeviceOnce attr;
+  attr([] {
+    return cudaFuncSetAttribute(k_route_expand, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)(kExpandMaxK * sizeof(uint64_t)));
+  });
   k_route_expand<<<nq, 1024, smem, st>>>(a, per_cluster, target);
 }
 

@@ -331,14 +331,15 @@ void launch_scan(const DevIndex& ix, Workspace& w, uint32_t nq, const sg_params&
   a.allow_words = allow_words;
   a.allow_q = w.per_query_allow ? w.allow_q : nullptr;
   a.allow_wq = w.allow_wq;
-  static bool attr = false;
-  if (!attr) {
-    cudaFuncSetAttribute(k_scan_seed, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         (int)(kMaxChunkBlocks * kKeyWordsPerBlock * 4));
-    cudaFuncSetAttribute(k_scan, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         (int)(kMaxChunkBlocks * kKeyWordsPerBlock * 4));
-    attr = true;
-  }
+  static PerDeviceOnce attr;
+  attr([] {
+    cudaError_t e = cudaFuncSetAttribute(k_scan_seed, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)(kMaxChunkBlocks * kKeyWordsPerBlock * 4));
+    if (e == cudaSuccess)
+      e = cudaFuncSetAttribute(k_scan, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               (int)(kMaxChunkBlocks * kKeyWordsPerBlock * 4));
+    return e;
+  });
   if (seed_blocks) k_scan_seed<<<nq, 256, seed_blocks * kKeyWordsPerBlock * 4, st>>>(a);
   if (chunk_blocks) k_scan<<<sms * ctas_per_sm, 256, chunk_blocks * kKeyWordsPerBlock * 4, st>>>(a);
 }

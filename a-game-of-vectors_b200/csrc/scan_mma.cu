@@ -447,12 +447,9 @@ int launch_scan_mma(const DevIndex& ix, Workspace& w, uint32_t nq, const sg_para
   a.allow_words = allow_words;
   a.allow_q = w.per_query_allow ? w.allow_q : nullptr;
   a.allow_wq = w.allow_wq;
-  static bool attr = false;
+  static PerDeviceOnce attr;
   const int smem = kQG * kBStride + 8 * 2 * kStageWords * 4;
-  if (!attr) {
-    cudaFuncSetAttribute(k_scan_mma, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-    attr = true;
-  }
+  attr([&] { return cudaFuncSetAttribute(k_scan_mma, cudaFuncAttributeMaxDynamicSharedMemorySize, smem); });
   k_scan_mma<<<sms * 2, 256, smem, st>>>(a);
   return 4;
 }

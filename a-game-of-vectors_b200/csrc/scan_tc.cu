@@ -466,11 +466,10 @@ static int tc_smem_bytes() { return 2 * kTcBBytes + kTcVBytes; }
 
 template <bool kRaw>
 static void tc_set_attr() {
-  static bool done = false;  // per process; the attribute is per function, not per device
-  if (!done) {
-    cudaFuncSetAttribute(k_scan_tc<kRaw>, cudaFuncAttributeMaxDynamicSharedMemorySize, tc_smem_bytes());
-    done = true;
-  }
+  static PerDeviceOnce attr;
+  attr([] {
+    return cudaFuncSetAttribute(k_scan_tc<kRaw>, cudaFuncAttributeMaxDynamicSharedMemorySize, tc_smem_bytes());
+  });
 }
 
 // A query's threshold raised to the cand-th largest estimate key its candidate buffer holds.
