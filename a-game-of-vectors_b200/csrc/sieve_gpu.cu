@@ -486,8 +486,9 @@ uint32_t full_cap(const sg_index* h, const sg_params& p, uint32_t nq) {
   return (uint32_t)std::min<uint64_t>(std::max<uint64_t>(b, 1), 0x7FFFFFFFull);
 }
 
-// Soft per-query buffer for batches: at least 16 x cand entries, and up to an 8 GiB budget
-// shared by the batch. A query that fills it is re-run (see search_impl) with the exact bound.
+// Soft per-query buffer for batches: at least 16 x cand entries, and up to the index's
+// candidate-buffer budget (a quarter of the device memory free at open, 8 to 32 GiB) shared by
+// the batch. A query that fills it is re-run (see search_impl) with the exact bound.
 uint32_t batch_cap(const sg_index* h, const sg_params& p, uint32_t nq, bool soft_always = false) {
   uint32_t full = full_cap(h, p, nq);
   if (h->cfg.soft_cap) return std::min(full, h->cfg.soft_cap);
