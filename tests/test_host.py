@@ -33,6 +33,9 @@ def test_library_reports_errors_without_aborting():
     assert rc == -2 and b"cannot open" in L.sg_last_error()
     assert L.sg_lut_scan(7, None, None, 0, None) == -1
     assert L.sg_dot_i8i8(None, None, 0, 3, None) == -1
+    # argument checks come before any device call
+    assert L.sg_route_scores(None, 1, None, None) == -1 and b"null" in L.sg_last_error()
+    assert L.sg_route(None, 1, None, None, None, None, None) == -1
 
 
 def test_abi_struct_layouts():
