@@ -19,6 +19,8 @@ struct CutArgs {
   const uint32_t* ids;
   const float* err;
   uint32_t cand;
+  const float4* qp;  // (scale, bias, a, b): global codes report lut.to_float(score)
+  uint32_t global;   // global sign codes: the admission key is the row, copies differ by slot
   float* cest;
   uint32_t* cid;
   float* cerr;
@@ -106,7 +108,8 @@ __global__ void __launch_bounds__(1024, 2) k_cut(CutArgs a) {
     const uint32_t i = sel[j];
     const uint2 info = Ei[i];
     const uint32_t id = a.ids[info.y];
-    const uint64_t pack = ((uint64_t)ord(__uint_as_float(Ee[i])) << 32) | (0xFFFFFFFFu - info.x);
+    const uint64_t pack = ((uint64_t)ord(__uint_as_float(Ee[i])) << 32) |
+                          (0xFFFFFFFFu - (a.global ? info.y : info.x));
     uint32_t h = hash_row(id);
     for (uint32_t probe = 0; probe < kHash; probe++) {
       const uint32_t prev = atomicCAS(&h_id[h], kEmpty, id);
@@ -124,7 +127,8 @@ __global__ void __launch_bounds__(1024, 2) k_cut(CutArgs a) {
     const uint32_t i = sel[j];
     const uint2 info = Ei[i];
     const uint32_t id = a.ids[info.y];
-    const uint64_t pack = ((uint64_t)ord(__uint_as_float(Ee[i])) << 32) | (0xFFFFFFFFu - info.x);
+    const uint64_t pack = ((uint64_t)ord(__uint_as_float(Ee[i])) << 32) |
+                          (0xFFFFFFFFu - (a.global ? info.y : info.x));
     uint32_t h = hash_row(id);
     for (uint32_t probe = 0; probe < kHash && h_id[h] != id; probe++) h = (h + 1) & (kHash - 1);
     *id_out = id;
@@ -141,7 +145,9 @@ __global__ void __launch_bounds__(1024, 2) k_cut(CutArgs a) {
     uint32_t id, slot;
     if (winner(j, &id, &slot)) {
       const size_t o = (size_t)q * cand + off++;
-      a.cest[o] = __uint_as_float(Ee[sel[j]]);
+      const float e = __uint_as_float(Ee[sel[j]]);
+      // Lut::to_float (src/lut.rs:62-64) of a global code's score
+      a.cest[o] = a.global ? __fadd_rn(__fdiv_rn(e, a.qp[q].x), a.qp[q].y) : e;
       a.cid[o] = id;
       a.cerr[o] = a.err[slot];
     }
@@ -160,6 +166,8 @@ void launch_cut(const DevIndex& ix, Workspace& w, uint32_t nq, const sg_params& 
   a.ids = ix.ids;
   a.err = ix.err;
   a.cand = p.cand;
+  a.qp = w.qp;
+  a.global = ix.global;
   a.cest = w.cest;
   a.cid = w.cid;
   a.cerr = w.cerr;

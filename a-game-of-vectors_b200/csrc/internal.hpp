@@ -71,8 +71,12 @@ struct DevIndex {
                                      // min = -1 where the range bound does not apply
   float* err = nullptr;              // [nslots] factors.f32 [.., 1]
   uint32_t* ids = nullptr;           // [nslots] ids.u32
-  float* rot = nullptr;              // [768] rotation.f32
+  float* rot = nullptr;              // [768] rotation.f32 (null for global sign codes)
   float rot_norm = 0.0f;             // (256 as f32).powf(-1.5)
+  // Global sign codes (an index without rotation.f32 / factors.f32, src/ivf.rs:700-717): slots
+  // hold their rows' sign codes, the LUT is built on the unrotated prefix, candidates are ranked
+  // by the u16 LUT score with ties by row, and mul = 1, err = +inf fill the factor planes.
+  bool global = false;
   bool has_t2 = false;
   float* t2_sigma = nullptr;         // [256]
   uint8_t* t2_codes = nullptr;       // [n*64]
@@ -80,11 +84,11 @@ struct DevIndex {
   int8_t* rerank = nullptr;          // [n*768]
   float* norm256 = nullptr;          // [n]
   float* qscale = nullptr;           // [768]
+  uint8_t* codes = nullptr;          // [n*32] codes.bin, when given (the flat Hamming baseline)
   std::vector<uint64_t> h_block_off;
   std::vector<uint32_t> h_clen;
   std::vector<uint32_t> h_chunks_desc_prefix;  // prefix sums of per-cluster chunk counts, largest first
   std::vector<uint64_t> h_slots_desc_prefix;   // prefix sums of per-cluster slot counts, largest first
-  int route_precision = SG_ROUTE_BF16;
 };
 
 // Device buffers of one batched call, grown on demand and reused.
@@ -101,6 +105,9 @@ struct Workspace {
   int8_t* wq256 = nullptr;     // [nq*256]
   float* winv256 = nullptr;    // [nq]
   __nv_bfloat16* q16 = nullptr;  // [nq*256] q256 rounded to bf16: the routing GEMM's B operand
+  uint32_t* w8 = nullptr;      // [nq*64] s8 weights of the tensor-core bound, 4 per word
+  float4* fq = nullptr;        // [nq] (gamma, R_hi, R_lo, -) of the bound
+  uint32_t* tc_start = nullptr;  // [nq] candidate-buffer entries before the bound pass
   float* scores = nullptr;     // [nq*k] routing scores
   uint64_t scores_cap = 0;
   float* probe_sc = nullptr;   // [nq*P]
@@ -179,6 +186,7 @@ struct GraphEntry {
 struct Ctx {
   Workspace ws;
   cudaStream_t stream = nullptr;
+  cudaEvent_t order_ev = nullptr;  // orders this stream after a caller's stream (created on first use)
   uint64_t gen = 1;  // bumped whenever a workspace buffer moves (captured graphs go stale)
   std::vector<GraphEntry> graphs;
 };
@@ -194,12 +202,15 @@ struct Config {
   int graphs = 1;         // capture and replay CUDA graphs per call shape (SIEVE_GPU_GRAPHS)
   uint32_t mma_min_queries_per_cluster = 8;   // use the MMA scan at or above this average
   int mma = 1;            // SIEVE_GPU_MMA: 0 ALU scan only, 1 automatic, 2 MMA whenever nprobe > 1
-  int tc = 1;             // SIEVE_GPU_TC: 1 the tcgen05 scan, 0 the mma.sync scan (kept for comparison)
+  int tc = 1;             // SIEVE_GPU_TC: 1 the tcgen05 bound scan, 2 the tcgen05 one-hot scan,
+                          // 0 the mma.sync scan (the last two kept for comparison)
   uint32_t tc_split = 0;  // SIEVE_GPU_TC_SPLIT (> 1): a first tcgen05 round over the ranks below it
   // Clusters probed by fewer queries than this in a batch are scanned by the ALU kernel: a
   // tcgen05 tile costs the same ~32 x 101 cycles per 128 slots for any query count up to 128,
   // an ALU (slot, query) pair ~6 (SIEVE_GPU_TC_MIN overrides; the autotuner measures it)
   uint32_t tc_min_queries = 6;
+  int route_precision = SG_ROUTE_BF16;  // sg_set_route_precision
+  bool timing = false;                  // per-stage device timing (sg_set_timing) of this call
   uint64_t gen = 1;  // bumped whenever a field changes (captured graphs of an older one are stale)
   // device memory a batch's candidate buffers may take (a quarter of what the index leaves
   // free at open, between 8 and 32 GiB); a query that fills its share is re-run alone
@@ -211,7 +222,9 @@ int fail(int code, const std::string& msg);
 
 // Views of an open index for entry points in other translation units (sieve_gpu.cu defines them).
 const DevIndex* index_arrays(const sg_index* h);
-const Config* index_config(const sg_index* h);
+// A copy of the index's tuning and routing precision, taken under the index's config lock: a call
+// works from one snapshot, so a concurrent sg_set_tuning / sg_autotune cannot change it midway.
+Config index_config(const sg_index* h);
 int index_sms(const sg_index* h);
 int index_check_params(const sg_index* h, const sg_params* p);
 
@@ -240,6 +253,13 @@ void launch_route_expand(const DevIndex& ix, Workspace& w, uint32_t nq, const sg
 void launch_route_select(const DevIndex& ix, Workspace& w, uint32_t nq, const sg_params& p,
                          int precision, uint32_t chunk_blocks, uint32_t seed_blocks,
                          bool alu_ranks, cudaStream_t st);
+// The caller's probe lists (device arrays [nq * P], counts [nq], P = min(nprobe, k)) in place of
+// routing: Index::candidates over given probes. Cluster numbers must be < k.
+// The lists may be w.probe_sc / w.probe_cl / w.probe_n themselves: each CTA reads its query's
+// list before it writes the probe list.
+void launch_route_given(const DevIndex& ix, Workspace& w, uint32_t nq, const sg_params& p, uint32_t chunk_blocks,
+                        uint32_t seed_blocks, bool alu_ranks, const float* given_sc, const uint32_t* given_cl,
+                        const uint32_t* given_n, cudaStream_t st);
 // Inverts the probe lists and runs the tensor-core scan over (cluster, query group) items;
 // returns the kernels launched. Needs the seed pass first (it sets the thresholds).
 int launch_scan_mma(const DevIndex& ix, Workspace& w, uint32_t nq, const sg_params& p,
@@ -256,6 +276,12 @@ struct Config;
 int launch_scan_tc(const DevIndex& ix, Workspace& w, uint32_t nq, const sg_params& p,
                    const uint64_t* allow, uint64_t allow_words, int sms, const Config& cfg,
                    uint32_t chunk_blocks, cudaStream_t st);
+// scan_tcf.cu: per-query weights and residual bounds of the tensor-core bound (after
+// launch_prep), and one bound pass over launch_invert's items with the exact recheck of what it
+// admitted (returns the kernels launched).
+void launch_filter_prep(Workspace& w, uint32_t nq, cudaStream_t st);
+int launch_scan_tcf(const DevIndex& ix, Workspace& w, uint32_t nq, uint32_t P, const uint64_t* allow,
+                    uint64_t allow_words, int sms, cudaStream_t st);
 // Launch errors of these two are left for the caller's cudaGetLastError.
 void transcode_tc(const uint8_t* blocks, uint64_t nblocks, uint32_t* out, cudaStream_t st);
 void launch_lut_scan_tc(uint32_t nq, const uint8_t* tables, const uint32_t* codes, uint64_t nblocks,
@@ -285,18 +311,32 @@ void launch_top_list(const float* sc, const uint32_t* id, const uint32_t* n_in, 
                      uint32_t* n_out, uint32_t stride_out, uint32_t nq, cudaStream_t st);
 void launch_dot_i8i8(const int8_t* q, const int8_t* rows, uint64_t nrows, uint32_t dim,
                      int32_t* out, cudaStream_t st);
+// hamming.cu: the flat Hamming baseline for the queries staged in w (q768 and q256): rows in
+// w.lid / w.ln (stride cand), scores in w.lsc, the top k in w.out_* (stride k).
+int launch_flat_hamming(const DevIndex& ix, Workspace& w, uint32_t nq, uint32_t cand, uint32_t k,
+                        cudaStream_t st);
 
 }  // namespace sg
 
 // An open IVF index: its arrays in HBM, the default execution context of sg_search, and the
-// tuning of its kernels.
+// tuning of its kernels. The arrays are read-only after open, so any number of contexts search
+// them at once; `mu` serialises only the users of the default context.
 struct sg_index {
   sg::DevIndex ix;
   sg::Ctx def;  // the context of sg_search / sg_search_device
-  sg::Config cfg;
   std::mutex mu;
+  sg::Config cfg;  // guarded by cfg_mu; calls read it through sg::index_config
+  mutable std::mutex cfg_mu;
   int sms = 148;
-  bool timing_on = false;
+  std::atomic<bool> timing_on{false};
+};
+
+// A search context (ivf::Scratch, src/ivf.rs:497-513): one thread's scratch, stream and captured
+// graphs over a shared index, so that threads searching one index overlap on the GPU.
+struct sg_context {
+  sg_index* h = nullptr;
+  sg::Ctx ctx;
+  std::mutex mu;  // a context serves one call at a time
 };
 
 // filter::Filter (src/filter.rs:18-25) resident on its index's device.
@@ -312,12 +352,13 @@ struct sg_filter {
 namespace sg {
 // Execution-context entry points (sieve_gpu.cu) for the serving loop: grow c's scratch for a
 // batch, launch the whole pipeline on the queries already staged in c.ws (no host sync), run one
-// query synchronously (host queries, device allow bitset), and the scratch bytes of a batch.
-int ctx_prepare(sg_index* h, Ctx& c, uint32_t nq, const sg_params& p);
-int ctx_launch(sg_index* h, Ctx& c, uint32_t nq, const sg_params& p, bool have_q256);
-int ctx_search_one(sg_index* h, Ctx& c, const float* q768, const float* q256, const sg_params& p,
-                   const uint64_t* d_allow, uint64_t allow_words, float* out_sc, uint32_t* out_id,
-                   uint32_t* out_n);
-uint64_t ctx_bytes(const sg_index* h, const sg_params& p, uint32_t nq);
+// query synchronously (host queries, device allow bitset), and the scratch bytes of a batch. A
+// batch passes the same config snapshot to each.
+int ctx_prepare(sg_index* h, const Config& cfg, Ctx& c, uint32_t nq, const sg_params& p);
+int ctx_launch(sg_index* h, const Config& cfg, Ctx& c, uint32_t nq, const sg_params& p, bool have_q256);
+int ctx_search_one(sg_index* h, const Config& cfg, Ctx& c, const float* q768, const float* q256,
+                   const sg_params& p, const uint64_t* d_allow, uint64_t allow_words, float* out_sc,
+                   uint32_t* out_id, uint32_t* out_n);
+uint64_t ctx_bytes(const sg_index* h, const Config& cfg, const sg_params& p, uint32_t nq);
 void free_ctx(Ctx& c);
 }  // namespace sg

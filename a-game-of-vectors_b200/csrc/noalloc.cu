@@ -13,6 +13,11 @@
 // where the GPU can reach host memory. So, once per device and with that device current, the
 // first call on the device asks cudaGetSymbolAddress for the real device address and keeps it;
 // that first call should therefore come before any stream capture begins on the caller's side.
+//
+// Failures on the device (a bounded tensor-core wait that ran out, a work queue or candidate
+// buffer that overflowed) cannot be returned from an asynchronous call: a last one-thread kernel
+// turns them into the count SG_COUNT_FAILED in *d_out_count, which the caller checks with its
+// results.
 #include <mutex>
 #include <string>
 
@@ -88,6 +93,15 @@ void carve_workspace(Carve& c, sg::Workspace& w, const sg::DevIndex& x, uint32_t
   w.ln = c.take<uint32_t>(1);
 }
 
+// Runs after the rerank on the call's stream: a device-side failure of any earlier stage (the
+// status word's overflow or timeout bit, or the candidate buffer's overflow flag) replaces the
+// result count with SG_COUNT_FAILED.
+__global__ void k_noalloc_status(const uint32_t* __restrict__ counters, const uint8_t* __restrict__ overflow,
+                                 uint32_t* __restrict__ out_n) {
+  if (threadIdx.x == 0 && ((counters[2] & (sg::kStatusOverflow | sg::kStatusTimeout)) || overflow[0]))
+    out_n[0] = SG_COUNT_FAILED;
+}
+
 }  // namespace
 
 extern "C" int sg_search_noalloc(sg_index* h, const float* d_q768, const float* d_q256,
@@ -99,18 +113,21 @@ extern "C" int sg_search_noalloc(sg_index* h, const float* d_q768, const float* 
   int rc = sg::index_check_params(h, params);
   if (rc) return rc;
   const sg::DevIndex& x = *sg::index_arrays(h);
-  const sg::Config& cfg = *sg::index_config(h);
+  const sg::Config cfg = sg::index_config(h);  // one snapshot: sg_set_tuning may run concurrently
   const sg_params& p = *params;
   cudaError_t e = cudaSetDevice(x.device);
   if (e != cudaSuccess) return sg::fail(SG_ERR_DEVICE, std::string("cudaSetDevice: ") + cudaGetErrorString(e));
   unsigned char* base = nullptr;
   if ((rc = scratch_address(x.device, &base))) return rc;
 
-  // Sizes of one query's buffers: the exact work-item and candidate-buffer bounds of sg_search.
+  // Sizes of one query's buffers: the exact work-item and candidate-buffer bounds sg_search uses
+  // for one query. A slot is appended at most once, so the probed clusters' slots bound the
+  // candidate buffer; the chunk scan keeps at most cand per chunk, so chunks x cand does too.
   const uint32_t P = p.nprobe < x.k ? p.nprobe : x.k;
   const uint32_t cand = p.cand > 0 ? p.cand : 1;
   const uint64_t items = x.h_chunks_desc_prefix[P];
-  const uint64_t cbuf = (items * cand + 3) & ~3ull;
+  const uint64_t slots = x.h_slots_desc_prefix[P];
+  const uint64_t cbuf = ((items * cand < slots ? items * cand : slots) + 3) & ~3ull;
   Carve sizing{nullptr};
   sg::Workspace w;
   carve_workspace(sizing, w, x, P, cand, items, (uint32_t)cbuf, d_q256 == nullptr);
@@ -139,18 +156,20 @@ extern "C" int sg_search_noalloc(sg_index* h, const float* d_q768, const float* 
     return sg::fail(SG_ERR_DEVICE, std::string("cudaMemsetAsync: ") + cudaGetErrorString(e));
   if (!d_q256) sg::launch_prefix(w, 1, st);
   sg::launch_prep(x, w, 1, st);
-  if ((e = sg::launch_route_scores(x, w, 1, x.route_precision, st)) != cudaSuccess)
+  if ((e = sg::launch_route_scores(x, w, 1, cfg.route_precision, st)) != cudaSuccess)
     return sg::fail(SG_ERR_DEVICE, std::string("sg_search_noalloc routing: ") + cudaGetErrorString(e));
-  sg::launch_route_select(x, w, 1, p, x.route_precision, cfg.small_chunk_blocks, cfg.seed_blocks,
+  // one query runs with the small-batch shapes, as sg_search runs it
+  sg::launch_route_select(x, w, 1, p, cfg.route_precision, cfg.small_chunk_blocks, cfg.small_seed_blocks,
                           true, st);
   if (p.cand > 0) {
     sg::launch_scan(x, w, 1, p, d_allow_bits, allow_words, sg::index_sms(h), cfg.small_chunk_blocks,
-                    cfg.seed_blocks, cfg.scan_ctas_per_sm, st);
+                    cfg.small_seed_blocks, cfg.scan_ctas_per_sm, st);
     sg::launch_cut(x, w, 1, p, st);
   } else if ((e = cudaMemsetAsync(w.cn, 0, sizeof(uint32_t), st)) != cudaSuccess) {
     return sg::fail(SG_ERR_DEVICE, std::string("cudaMemsetAsync: ") + cudaGetErrorString(e));
   }
   sg::launch_rerank(x, w, 1, p, st, nullptr, nullptr);
+  k_noalloc_status<<<1, 32, 0, st>>>(w.counters, w.overflow, w.out_n);
   if ((e = cudaGetLastError()) != cudaSuccess)
     return sg::fail(SG_ERR_DEVICE, std::string("sg_search_noalloc launch: ") + cudaGetErrorString(e));
   return SG_OK;

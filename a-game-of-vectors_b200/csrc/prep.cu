@@ -37,8 +37,9 @@ __global__ void __launch_bounds__(256) k_prep(const float* __restrict__ q256,
     for (int o = 16; o > 0; o >>= 1) s = __fadd_rn(s, __shfl_xor_sync(0xFFFFFFFFu, s, o));
     if (t == 0) qnorm[q] = sqrtf(s);
   }
-  // Rotation::apply: three rounds of sign flip + FWHT, then the d^-1.5 scale.
-  for (int r = 0; r < 3; r++) {
+  // Rotation::apply: three rounds of sign flip + FWHT, then the d^-1.5 scale. Global sign codes
+  // (no rotation) take the LUT of the prefix itself (src/ivf.rs:701).
+  for (int r = 0; signs && r < 3; r++) {
     v[t] = __fmul_rn(v[t], signs[r * SG_PDIM + t]);
     __syncthreads();
     for (int h = 1; h < SG_PDIM; h *= 2) {
@@ -52,7 +53,7 @@ __global__ void __launch_bounds__(256) k_prep(const float* __restrict__ q256,
       __syncthreads();
     }
   }
-  v[t] = __fmul_rn(v[t], rot_norm);
+  if (signs) v[t] = __fmul_rn(v[t], rot_norm);
   __syncthreads();
   // Lut::new: entry (g, c) sums q[4g + j] over the set bits j of c, ascending, from -0.0.
   for (int e = t; e < SG_GROUPS * 16; e += blockDim.x) {
@@ -84,6 +85,11 @@ __global__ void __launch_bounds__(256) k_prep(const float* __restrict__ q256,
     for (int i = 0; i < SG_PDIM; i++) sum = __fadd_rn(sum, v[i]);
     float a = __fdiv_rn(2.0f, scale);
     float b = __fsub_rn(__fmul_rn(2.0f, bias), sum);
+    // global sign codes rank by the LUT score itself: est = 0 + 1 * (1 * s + 0) = s exactly
+    if (!signs) {
+      a = 1.0f;
+      b = 0.0f;
+    }
     qp[q] = make_float4(scale, bias, a, b);
     s_scale = scale;
   }

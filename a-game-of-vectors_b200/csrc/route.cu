@@ -452,6 +452,25 @@ __global__ void __launch_bounds__(1024) k_route_expand(SelectArgs a,
   emit_probes(a, keys, m, q, tmp);
 }
 
+// Index::candidates over a caller's probe list (src/ivf.rs:647-681): query q's probes
+// given_cl/given_sc [q * P + r], r < given_n[q], in the given order (their admission order),
+// become the probe list, seed and scan items exactly as a routed list would.
+__global__ void __launch_bounds__(256) k_route_given(SelectArgs a, const float* __restrict__ given_sc,
+                                                     const uint32_t* __restrict__ given_cl,
+                                                     const uint32_t* __restrict__ given_n) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  uint64_t* keys = reinterpret_cast<uint64_t*>(smem_raw);  // [P]
+  __shared__ uint32_t tmp[32];
+  const uint32_t q = blockIdx.x;
+  const uint32_t m = min(given_n[q], a.P);
+  for (uint32_t r = threadIdx.x; r < m; r += blockDim.x) {
+    const uint32_t c = given_cl[(size_t)q * a.P + r];
+    keys[r] = rank_key(given_sc[(size_t)q * a.P + r], c < a.K ? c : 0u);
+  }
+  __syncthreads();
+  emit_probes(a, keys, m, q, tmp);
+}
+
 cudaError_t launch_route_scores(const DevIndex& ix, Workspace& w, uint32_t nq, int precision,
                                 cudaStream_t st) {
   if (nq == 0 || ix.k == 0) return cudaSuccess;
@@ -505,6 +524,36 @@ void launch_route_select(const DevIndex& ix, Workspace& w, uint32_t nq, const sg
     return cudaFuncSetAttribute(k_route_select, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   });
   k_route_select<<<nq, 256, smem, st>>>(a);
+}
+
+void launch_route_given(const DevIndex& ix, Workspace& w, uint32_t nq, const sg_params& p, uint32_t chunk_blocks,
+                        uint32_t seed_blocks, bool alu_ranks, const float* given_sc, const uint32_t* given_cl,
+                        const uint32_t* given_n, cudaStream_t st) {
+  SelectArgs a;
+  memset(&a, 0, sizeof a);
+  a.block_off = ix.block_off;
+  a.K = ix.k;
+  a.P = p.nprobe < ix.k ? p.nprobe : ix.k;
+  a.p = p;
+  a.chunk_blocks = chunk_blocks;
+  a.seed_blocks = seed_blocks;
+  a.alu_ranks = alu_ranks ? 1u : 0u;
+  a.seed_items = w.seed_items;
+  a.probe_sc = w.probe_sc;
+  a.probe_cl = w.probe_cl;
+  a.probe_off = w.probe_off;
+  a.probe_n = w.probe_n;
+  a.scanned = w.scanned;
+  a.items = w.items;
+  a.item_cap = w.item_cap;
+  a.counters = w.counters;
+  static PerDeviceOnce attr;
+  attr([] {
+    return cudaFuncSetAttribute(k_route_given, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)(4096 * sizeof(uint64_t)));
+  });
+  k_route_given<<<nq, 256, (size_t)std::max<uint32_t>(a.P, 1) * sizeof(uint64_t), st>>>(a, given_sc, given_cl,
+                                                                                      given_n);
 }
 
 void launch_route_expand(const DevIndex& ix, Workspace& w, uint32_t nq, const sg_params& p,

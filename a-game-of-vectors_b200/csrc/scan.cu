@@ -47,6 +47,9 @@ struct ScanArgs {
   uint64_t allow_words;
   const uint64_t* const* allow_q;  // per-query allow bitsets (null entries: no filter), or null
   const uint64_t* allow_wq;
+  // global sign codes: estimates are the LUT scores (centroid score 0), the admission key is the
+  // row (ties by row, src/ivf.rs:700-717), and a chunk keeps every slot tied at its cut
+  uint32_t global;
 };
 
 SG_DEV uint4 ldg_nc(const uint4* p) {
@@ -118,7 +121,7 @@ SG_DEV void set_seg(const ScanArgs& a, Segs& S, uint32_t i, uint32_t q, uint32_t
   S.b0[i] = b0;
   S.cl[i] = (int32_t)a.clen[c] - (int32_t)((b0 - cb0) * SG_BLOCK);
   S.kb[i] = a.probe_off[(size_t)q * a.P + r] + (b0 - cb0) * SG_BLOCK;
-  S.cent[i] = a.probe_sc[(size_t)q * a.P + r];
+  S.cent[i] = a.global ? 0.0f : a.probe_sc[(size_t)q * a.P + r];
 }
 
 // One CTA: score every segment's blocks, then admit the best `cand` eligible slots at or above
@@ -218,7 +221,7 @@ SG_DEV void scan_segments(const ScanArgs& a, uint32_t q, const Segs& S, uint32_t
     bool sel;
     if (!cut) sel = k != 0u;
     else if (k > T) sel = true;
-    else sel = (k == T) && (tr++ < need);
+    else sel = (k == T) && (a.global || tr++ < need);
     if (sel) {
       selmask |= 1ull << (i - i0);
       nsel++;
@@ -240,7 +243,8 @@ SG_DEV void scan_segments(const ScanArgs& a, uint32_t q, const Segs& S, uint32_t
         const uint32_t gb = i / SG_BLOCK, sg = seg_of(S, gb);
         const uint32_t rel = (gb - S.start[sg]) * SG_BLOCK + (i % SG_BLOCK);
         a.cbuf_est[qbase + pos] = __float_as_uint(unord(s_key[kx(i)]));
-        a.cbuf_info[qbase + pos] = make_uint2(S.kb[sg] + rel, S.b0[sg] * SG_BLOCK + rel);
+        const uint32_t slot = S.b0[sg] * SG_BLOCK + rel;
+        a.cbuf_info[qbase + pos] = make_uint2(a.global ? a.ids[slot] : S.kb[sg] + rel, slot);
       } else {
         a.overflow[q] = 1;
       }
@@ -331,6 +335,7 @@ void launch_scan(const DevIndex& ix, Workspace& w, uint32_t nq, const sg_params&
   a.allow_words = allow_words;
   a.allow_q = w.per_query_allow ? w.allow_q : nullptr;
   a.allow_wq = w.allow_wq;
+  a.global = ix.global;
   static PerDeviceOnce attr;
   attr([] {
     cudaError_t e = cudaFuncSetAttribute(k_scan_seed, cudaFuncAttributeMaxDynamicSharedMemorySize,

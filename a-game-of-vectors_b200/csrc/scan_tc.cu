@@ -528,17 +528,29 @@ int launch_scan_tc(const DevIndex& ix, Workspace& w, uint32_t nq, const sg_param
     // a later round's ALU pass starts where this one's queue ended
     cudaMemcpyAsync(w.counters + 1, w.counters, 4, cudaMemcpyDeviceToDevice, st);
   };
+  // one tensor-core round: the bound pass with its exact recheck (default), or the exact one-hot
+  // contraction (SIEVE_GPU_TC=2, kept for comparison)
+  const bool bound = cfg.tc != 2;
+  auto tc_round = [&]() {
+    if (bound) return launch_scan_tcf(ix, w, nq, P, allow, allow_words, sms, st);
+    k_scan_tc<false><<<sms, kTcThreads, tc_smem_bytes(), st>>>(a);
+    return 1;
+  };
+  if (bound) {
+    launch_filter_prep(w, nq, st);
+    launches++;
+  }
   if (split > 1 && split < P) {
     launch_invert(ix, w, nq, P, kTcQG, 1, split, st, tmin, chunk_blocks);
     alu_pass();
-    k_scan_tc<false><<<sms, kTcThreads, tc_smem_bytes(), st>>>(a);
+    launches += tc_round();
     k_raise_thr<<<nq, 1024, 0, st>>>(w.cbuf_est, w.cbuf_per_q, w.ccount, w.overflow, p.cand, w.thr);
-    launches += 7;
+    launches += 6;
   }
   launch_invert(ix, w, nq, P, kTcQG, split > 1 && split < P ? split : 1, P, st, tmin, chunk_blocks);
   alu_pass();
-  k_scan_tc<false><<<sms, kTcThreads, tc_smem_bytes(), st>>>(a);
-  return launches + 6;
+  launches += tc_round();
+  return launches + 5;
 }
 
 // Raw scores of nq query tables against nblocks blocks (slot-major codes already on the device);

@@ -1,0 +1,511 @@
+// scan_tcf.cu — the batched scan's admission pass on the 5th-generation tensor cores: a rigorous
+// upper bound of every (slot, query) estimate from a 256-wide binary dot product, and the exact
+// LUT score only for the pairs the bound cannot reject.
+//
+// The exact score of a slot is s = sum_g T_g[n_g] over its 64 nibbles (src/lut.rs:58-60,
+// :116-126), with T_g the query's u8 tables (src/lut.rs:33-55). T_g is, up to its per-entry
+// rounding, linear in the four bits of the nibble: T_g[c] ~ T_g[0] + sum_{j in c} (T_g[1<<j] -
+// T_g[0]). So for per-query integer weights w (s8, one per prefix dimension, from the singleton
+// entries of the table, halved when they do not fit) and gamma in {1, 2}:
+//   s = sum_g T_g[n_g] = gamma * D + sum_g (T_g[n_g] - gamma * L_g[n_g]),  D = sum_{k: bit k} w_k,
+// where L_g[c] = sum_{j in c} w_{4g+j}. Each group's residual lies in [rlo_g, rhi_g], its minimum
+// and maximum over the 16 nibbles, computed exactly from the tables. Hence
+//   gamma * D + R_lo <= s <= gamma * D + R_hi,   R_lo = sum_g rlo_g, R_hi = sum_g rhi_g,
+// all integers below 2^24, exact in f32. D is an exact s32 tensor-core product of the slot's 256
+// code bits (u8 0/1, A in tensor memory) and the query's weights (s8, B in shared memory):
+// tcgen05.mma.kind::i8 with K = 256, 8 instructions per 128-slot tile, where the exact one-hot
+// contraction needs K = 1024 (32 instructions).
+//
+// The estimate est = cent + mul * (a * s + b), rounded operation by operation (src/rabitq.rs:
+// 127-130), is non-decreasing in s for mul >= 0 (a > 0) and non-increasing for mul < 0, and IEEE
+// rounding is monotone. So the same expression evaluated at s_ub = gamma * D + R_hi (mul >= 0) or
+// at gamma * D + R_lo (mul < 0) is an upper bound of the exact estimate, and a pair whose bound
+// misses the query's admission threshold cannot be admitted. Pairs that pass reserve their entry
+// in the query's candidate buffer (estimate field holding the probe's centroid score), and
+// k_tc_recheck replaces it with the exact estimate from the exact LUT score. An entry whose exact
+// estimate is below the threshold stays in the buffer with that estimate: the threshold is the
+// cand-th estimate of entries already buffered, so such an entry is never among the best cand
+// the cut keeps. Results are bit-identical to the exact scan.
+//
+// Warp roles of the persistent CTA (one per SM), as in the one-hot kernel of scan_tc.cu: a
+// loader warp fills two item slots (B weights and per-query constants); four producer warps
+// expand their slots' code bits into u8 A rows in tensor memory (one 64-column stage per tile,
+// four stages); one MMA warp issues each tile's 8 MMAs from an elected lane into one of four
+// accumulators; eight epilogue warps bound every (slot, query) pair and reserve buffer entries.
+// Every mbarrier wait is bounded: a wait that runs out raises kStatusTimeout, every role stops,
+// and the CTA frees its tensor memory and returns.
+#include <climits>
+
+#include "common.cuh"
+#include "internal.hpp"
+#include "tcgen05.cuh"
+
+namespace sg {
+
+constexpr int kFQG = 64;            // queries per work item (MMA N, padded to a multiple of 16)
+constexpr int kFStages = 4;         // A stages: one tile (128 slots x 256 K bytes = 64 columns) each
+constexpr uint32_t kFCols = 512;    // TMEM columns: 4 x 64 (A) + 4 x 64 (D)
+constexpr uint32_t kFDCol = 256;    // first D column
+constexpr int kFDBufs = 4;          // accumulators
+constexpr int kFProducers = 4;      // warps 0-3 build A
+constexpr int kFEpi = 4;            // warps 4-11 bound the pairs
+constexpr int kFEpiWarps = 8;
+constexpr int kFMma = 12;           // warp 12 issues the MMAs
+constexpr int kFLoader = 13;        // warp 13 loads work items
+constexpr int kFThreads = 14 * 32;
+constexpr int kFBBytes = kFQG * SG_PDIM;  // B of one item slot: 64 queries x 256 s8 weights
+
+// ---- per-query weights and residual bounds --------------------------------------------------
+// One CTA of 64 threads per query; thread g owns group g (prefix dimensions 4g..4g+3).
+__global__ void __launch_bounds__(64) k_filter_prep(const uint8_t* __restrict__ tables,
+                                                    uint32_t* __restrict__ w8, float4* __restrict__ fq) {
+  __shared__ int s_hi[2], s_lo[2];
+  const uint32_t q = blockIdx.x, g = threadIdx.x;
+  const uint4 row = reinterpret_cast<const uint4*>(tables + (size_t)q * SG_GROUPS * 16)[g];
+  int t[16];
+  const uint32_t wd[4] = {row.x, row.y, row.z, row.w};
+#pragma unroll
+  for (int c = 0; c < 16; c++) t[c] = (int)((wd[c >> 2] >> (8 * (c & 3))) & 0xFFu);
+  int w[4];
+  bool big = false;
+#pragma unroll
+  for (int j = 0; j < 4; j++) {
+    w[j] = t[1 << j] - t[0];
+    big |= w[j] > 127 || w[j] < -127;
+  }
+  const int gam = __syncthreads_or(big) ? 2 : 1;
+#pragma unroll
+  for (int j = 0; j < 4; j++) w[j] /= gam;  // |w| <= 127 (truncation: any integer keeps the bound)
+  int rhi = INT_MIN, rlo = INT_MAX;
+#pragma unroll
+  for (int c = 0; c < 16; c++) {
+    const int L = ((c & 1) ? w[0] : 0) + ((c & 2) ? w[1] : 0) + ((c & 4) ? w[2] : 0) + ((c & 8) ? w[3] : 0);
+    const int v = t[c] - gam * L;
+    rhi = max(rhi, v);
+    rlo = min(rlo, v);
+  }
+  w8[(size_t)q * SG_GROUPS + g] = (uint32_t)(uint8_t)(int8_t)w[0] | ((uint32_t)(uint8_t)(int8_t)w[1] << 8) |
+                                  ((uint32_t)(uint8_t)(int8_t)w[2] << 16) | ((uint32_t)(uint8_t)(int8_t)w[3] << 24);
+  rhi = warp_sum_i(rhi);
+  rlo = warp_sum_i(rlo);
+  if ((g & 31) == 0) {
+    s_hi[g >> 5] = rhi;
+    s_lo[g >> 5] = rlo;
+  }
+  __syncthreads();
+  if (g == 0) fq[q] = make_float4((float)gam, (float)(s_hi[0] + s_hi[1]), (float)(s_lo[0] + s_lo[1]), 0.0f);
+}
+
+// Instruction descriptor of kind::i8: u8 A, s8 B, both K-major, s32 accumulators, M = 128.
+SG_DEV uint32_t idesc_u8s8(uint32_t n) { return (2u << 4) | (1u << 10) | ((n >> 3) << 17) | ((128u >> 4) << 24); }
+
+// The four bits of a nibble as four bytes (bit j at byte j): the terms of the product are at
+// disjoint bit positions, so the multiply is four shifted ORs.
+SG_DEV uint32_t bits_to_bytes(uint32_t nib) { return (nib * 0x00204081u) & 0x01010101u; }
+
+struct TcfArgs {
+  const uint4* codes;  // [nslots * 2] slot-major codes
+  const float* mul;
+  const uint32_t* ids;
+  const uint32_t* block_off;
+  const uint32_t* clen;
+  const uint32_t* w8;   // [nq * 64] s8 weights, 4 per word
+  const float4* fq;     // [nq] (gamma, R_hi, R_lo, -)
+  const float4* qp;     // [nq] (scale, bias, a, b)
+  const float* probe_sc;
+  const uint32_t* probe_off;
+  uint32_t P;
+  const uint32_t* inv_off;
+  const uint32_t* inv_list;
+  const uint2* gitems;
+  uint32_t* counters;  // [2] status, [4] items, [5] next item
+  uint32_t* thr;
+  uint32_t* ccount;
+  uint32_t* cbuf_est;
+  uint2* cbuf_info;
+  uint32_t cap;
+  uint8_t* overflow;
+  const uint64_t* allow;
+  uint64_t allow_words;
+  const uint64_t* const* allow_q;
+  const uint64_t* allow_wq;
+  uint32_t global;  // global sign codes: centroid score 0, admission key = row
+};
+
+__global__ void __launch_bounds__(kFThreads, 1) k_scan_tcf(TcfArgs a) {
+  extern __shared__ __align__(1024) uint8_t smem[];  // B of the two item slots
+  __shared__ __align__(8) uint64_t bar_afull[kFStages], bar_aempty[kFStages], bar_dfull[kFDBufs],
+      bar_dempty[kFDBufs], bar_ifull[2], bar_iempty[2];
+  __shared__ uint32_t s_tmem;
+  __shared__ int s_abort;
+  __shared__ uint32_t s_meta[2][8];  // b0, nb, cl, ng, -, end
+  __shared__ float4 s_qc[2][kFQG];   // cent, a, b, threshold key (as bits)
+  __shared__ float4 s_qf[2][kFQG];   // gamma, R_hi, R_lo, -
+  __shared__ uint2 s_qk[2][kFQG];    // candidate order base, query
+  __shared__ uint2 s_cb[kFEpiWarps][2][32];  // per column: reserved base, admitted lanes
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  volatile int* abort_flag = &s_abort;
+
+  if (warp == kFMma) {
+    tc_alloc(&s_tmem, kFCols);
+    tc_relinquish();
+  }
+  if (tid == 0) {
+    for (int i = 0; i < kFStages; i++) {
+      mbar_init(&bar_afull[i], kFProducers);
+      mbar_init(&bar_aempty[i], 1);
+    }
+    for (int i = 0; i < kFDBufs; i++) {
+      mbar_init(&bar_dfull[i], 1);
+      mbar_init(&bar_dempty[i], 4);  // the two epilogue warps of each lane quarter, per parity
+    }
+    for (int i = 0; i < 2; i++) {
+      mbar_init(&bar_ifull[i], 1);
+      mbar_init(&bar_iempty[i], kFProducers + kFEpiWarps + 1);
+    }
+    s_abort = 0;
+    fence_mbar_init();
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = s_tmem;
+  const uint32_t bs_base = smem_addr(smem);
+  uint32_t* status = a.counters + 2;
+
+  if (warp == kFLoader) {
+    // ---- work items into the two item slots ------------------------------------------------
+    const uint32_t nitems = a.counters[4];
+    for (uint32_t it = 0;; it++) {
+      const uint32_t slot = it & 1, use = it >> 1;
+      if (!mbar_wait(&bar_iempty[slot], (use & 1) ^ 1, abort_flag)) break;
+      uint32_t item = 0;
+      if (lane == 0) item = atomicAdd(a.counters + 5, 1u);
+      item = __shfl_sync(0xFFFFFFFFu, item, 0);
+      if (item >= nitems) {
+        if (lane == 0) {
+          s_meta[slot][5] = 1;
+          mbar_arrive(&bar_ifull[slot]);
+        }
+        break;
+      }
+      const uint2 gi = a.gitems[item];
+      const uint32_t c = gi.x;
+      const uint32_t l0 = a.inv_off[c] + gi.y * kFQG;
+      const uint32_t ng = min((uint32_t)kFQG, a.inv_off[c + 1] - l0);
+      const uint32_t b0 = a.block_off[c], nb = a.block_off[c + 1] - b0, cl = a.clen[c];
+      const uint32_t N = (ng + 15) & ~15u;
+      uint8_t* B = smem + slot * kFBBytes;
+      if (nb > 0) {
+        // query n's 16-byte K chunk g at (n/8)*2048 + g*128 + (n%8)*16 (K-major core matrices)
+#pragma unroll 4
+        for (uint32_t e = lane; e < N * 16; e += 32) {
+          const uint32_t r = e & 7, g = (e >> 3) & 15, n = (e >> 7) * 8 + r;
+          uint4 v = make_uint4(0, 0, 0, 0);
+          if (n < ng) {
+            const uint32_t q = a.inv_list[l0 + n] >> 12;
+            v = reinterpret_cast<const uint4*>(a.w8 + (size_t)q * SG_GROUPS)[g];
+          }
+          *reinterpret_cast<uint4*>(B + (n >> 3) * 2048 + g * 128 + r * 16) = v;
+        }
+      }
+      for (uint32_t qi = lane; qi < ng; qi += 32) {
+        const uint32_t ent = a.inv_list[l0 + qi];
+        const uint32_t q = ent >> 12, r = ent & 0xFFFu;
+        const float4 p = a.qp[q];
+        const float cent = a.global ? 0.0f : a.probe_sc[(size_t)q * a.P + r];
+        const uint32_t thr = *(volatile const uint32_t*)(a.thr + q);
+        s_qc[slot][qi] = make_float4(cent, p.z, p.w, __uint_as_float(thr));
+        s_qf[slot][qi] = a.fq[q];
+        s_qk[slot][qi] = make_uint2(a.probe_off[(size_t)q * a.P + r], q);
+      }
+      if (lane == 0) {
+        s_meta[slot][0] = b0;
+        s_meta[slot][1] = nb;
+        s_meta[slot][2] = cl;
+        s_meta[slot][3] = ng;
+        s_meta[slot][5] = 0;
+      }
+      fence_proxy_async_smem();
+      __syncwarp();
+      if (lane == 0) mbar_arrive(&bar_ifull[slot]);
+    }
+  } else {
+    // ---- consumers: items in order, tiles numbered across items ------------------------------
+    uint32_t ts = 0;  // tiles of earlier items
+    for (uint32_t it = 0;; it++) {
+      const uint32_t slot = it & 1, use = it >> 1;
+      if (!mbar_wait(&bar_ifull[slot], use & 1, abort_flag)) break;
+      if (s_meta[slot][5]) break;
+      const uint32_t b0 = s_meta[slot][0], nb = s_meta[slot][1], cl = s_meta[slot][2], ng = s_meta[slot][3];
+      const uint32_t N = (ng + 15) & ~15u, ntiles = (nb + 3) >> 2;
+      bool ok = true;
+      if (warp < kFProducers) {
+        // A: the code bits of block 4t + warp of the tile as u8 0/1, slot = lane, K = 256
+        const uint32_t qd = warp;
+        const uint32_t lane_base = (32u * qd) << 16;
+        auto codes_of = [&](uint32_t t, uint4& lo, uint4& hi) {
+          const uint32_t bl = 4 * t + qd;
+          lo = hi = make_uint4(0, 0, 0, 0);
+          if (t < ntiles && bl < nb) {
+            const uint64_t gs = (uint64_t)(b0 + bl) * SG_BLOCK + lane;
+            lo = a.codes[2 * gs];
+            hi = a.codes[2 * gs + 1];
+          }
+        };
+        uint4 lo, hi, nlo, nhi;
+        codes_of(0, lo, hi);
+        for (uint32_t t = 0; t < ntiles; t++) {
+          codes_of(t + 1, nlo, nhi);
+          const uint32_t ds = ts + t, st = ds & (kFStages - 1), su = ds / kFStages;
+          if (!mbar_wait(&bar_aempty[st], (su & 1) ^ 1, abort_flag)) {
+            ok = false;
+            break;
+          }
+          // column c holds prefix dimensions 4c..4c+3: nibble c of the code (word c/8)
+          uint32_t r[32];
+          const uint32_t wl[4] = {lo.x, lo.y, lo.z, lo.w}, wh[4] = {hi.x, hi.y, hi.z, hi.w};
+#pragma unroll
+          for (int c = 0; c < 32; c++) r[c] = bits_to_bytes((wl[c >> 3] >> (4 * (c & 7))) & 15u);
+          tc_st32(tmem + lane_base + st * 64, r);
+#pragma unroll
+          for (int c = 0; c < 32; c++) r[c] = bits_to_bytes((wh[c >> 3] >> (4 * (c & 7))) & 15u);
+          tc_st32(tmem + lane_base + st * 64 + 32, r);
+          tc_wait_st();
+          tc_fence_before();
+          __syncwarp();
+          if (lane == 0) mbar_arrive(&bar_afull[st]);
+          lo = nlo;
+          hi = nhi;
+        }
+        if (lane == 0) mbar_arrive(&bar_iempty[slot]);
+      } else if (warp == kFMma) {
+        const uint32_t idesc = idesc_u8s8(N);
+        // K step kk starts 256 B (two core matrices) further on: 16 in the 16-byte address field
+        const uint64_t bdesc = smem_desc(bs_base + slot * kFBBytes, 128, 2048);
+        for (uint32_t t = 0; t < ntiles && ok; t++) {
+          const uint32_t ds = ts + t, dbuf = ds & (kFDBufs - 1), duse = ds / kFDBufs;
+          const uint32_t st = ds & (kFStages - 1), su = ds / kFStages;
+          if (!mbar_wait(&bar_dempty[dbuf], (duse & 1) ^ 1, abort_flag)) break;
+          if (!mbar_wait(&bar_afull[st], su & 1, abort_flag)) break;
+          tc_fence_after();
+#pragma unroll
+          for (uint32_t kk = 0; kk < 8; kk++)  // K bytes 32kk.. = prefix dimensions 32kk..32kk+31
+            tc_mma_i8_elect(tmem + kFDCol + dbuf * kFQG, tmem + st * 64 + kk * 8, bdesc + (uint64_t)(kk * 16),
+                            idesc, kk != 0);
+          tc_commit_elect(&bar_aempty[st]);
+          tc_commit_elect(&bar_dfull[dbuf]);
+          __syncwarp();
+        }
+        if (lane == 0) mbar_arrive(&bar_iempty[slot]);
+      } else {
+        // ---- epilogue: slot (4t + qd)*32 + lane of the tiles of this warp's parity ----------
+        const uint32_t ew = warp - kFEpi, qd = ew & 3, par = ew >> 2;
+        const uint32_t lane_base = (32u * qd) << 16;
+        const uint32_t ncc = (N + 31) >> 5;
+        uint2* cb = &s_cb[ew][0][0];
+        const uint32_t lt = (1u << lane) - 1u;
+        // A chunk's entries are written one chunk later, so the atomic that reserves their room
+        // is in flight meanwhile: p_* is the pending chunk (its column ballots in buffer p_buf,
+        // its reservation in p_base).
+        bool p_on = false;
+        uint32_t p_adm = 0, p_base = 0, p_loc = 0, p_gslot = 0, p_c0 = 0, p_buf = 0;
+        auto flush = [&]() {
+          if (!p_on) return;  // warp-uniform
+          uint2* cbp = cb + p_buf * 32;
+          cbp[lane].x = p_base;
+          __syncwarp();
+          for (uint32_t r = p_adm; r; r &= r - 1) {
+            const uint32_t j = __ffs(r) - 1;
+            const uint2 bc = cbp[j];
+            const uint2 qk = s_qk[slot][p_c0 + j];
+            const uint32_t pos = bc.x + (uint32_t)__popc(bc.y & lt);
+            if (pos < a.cap) {
+              // the probe's centroid score; k_tc_recheck turns it into the exact estimate
+              a.cbuf_est[(size_t)qk.y * a.cap + pos] = __float_as_uint(s_qc[slot][p_c0 + j].x);
+              a.cbuf_info[(size_t)qk.y * a.cap + pos] =
+                  make_uint2(a.global ? a.ids[p_gslot] : qk.x + p_loc, p_gslot);
+            } else {
+              a.overflow[qk.y] = 1;
+            }
+          }
+          __syncwarp();
+          p_on = false;
+        };
+        auto tile_mul = [&](uint32_t t) {
+          const uint32_t bl = 4 * t + qd;
+          if (t >= ntiles || bl >= nb || bl * SG_BLOCK + lane >= cl) return 0.0f;
+          return a.mul[(b0 + bl) * SG_BLOCK + lane];
+        };
+        const uint32_t t0 = ((ts & 1) == par) ? 0 : 1;  // first tile of this warp's parity
+        float mv = tile_mul(t0);
+        for (uint32_t t = t0; t < ntiles; t += 2) {
+          const uint32_t ds = ts + t, dbuf = ds & (kFDBufs - 1), duse = ds / kFDBufs;
+          const uint32_t bl = 4 * t + qd;
+          const uint32_t loc = bl * SG_BLOCK + lane;
+          const bool lane_ok = bl < nb && loc < cl;
+          const uint32_t gslot = (b0 + bl) * SG_BLOCK + lane;
+          const float nmv = tile_mul(t + 2);
+          // the residual bound that gives an upper bound of the estimate for this slot's mul
+          const bool neg = mv < 0.0f;
+          const bool always = !isfinite(mv);  // no monotone bound: recheck every column
+          if (!mbar_wait(&bar_dfull[dbuf], duse & 1, abort_flag)) break;
+          tc_fence_after();
+          for (uint32_t cc = 0; cc < ncc; cc++) {
+            uint32_t v[32];
+            tc_ld32(tmem + lane_base + kFDCol + dbuf * kFQG + 32 * cc, v);
+            tc_wait_ld();
+            // 1. every column's bound of the estimate (the exact estimate's operations at the
+            //    bound of the score) against the query's admission key
+            const uint32_t cbuf = p_on ? (p_buf ^ 1) : 0;
+            const uint32_t ncol = min(32u, ng - 32 * cc);
+            uint32_t adm = 0;
+#pragma unroll
+            for (int j = 0; j < 32; j++) {
+              const float4 qc = s_qc[slot][32 * cc + j];
+              const float4 qf = s_qf[slot][32 * cc + j];
+              const float sb = __fadd_rn(__fmul_rn(qf.x, (float)(int)v[j]), neg ? qf.z : qf.y);
+              const float est = __fadd_rn(qc.x, __fmul_rn(mv, __fadd_rn(__fmul_rn(qc.y, sb), qc.z)));
+              adm |= (always || ord(est) >= __float_as_uint(qc.w) ? 1u : 0u) << j;
+            }
+            adm &= lane_ok ? (ncol == 32 ? 0xFFFFFFFFu : (1u << ncol) - 1u) : 0u;
+            if (adm && (a.allow || a.allow_q)) {  // allowlist filters (View::hidden)
+              const uint32_t id = a.ids[gslot];
+              for (uint32_t r = adm; r; r &= r - 1) {
+                const uint32_t j = __ffs(r) - 1;
+                const uint32_t q = s_qk[slot][32 * cc + j].y;
+                const uint64_t* al = a.allow_q ? a.allow_q[q] : a.allow;
+                const uint64_t aw = a.allow_q ? a.allow_wq[q] : a.allow_words;
+                if (al && !allowed(al, aw, id)) adm &= ~(1u << j);
+              }
+            }
+            if (!__any_sync(0xFFFFFFFFu, adm != 0)) continue;
+            // 2. the 32 x 32 bit matrix (lane = slot, bit = column) transposed across the warp:
+            //    lane j then holds column j's admitted lanes and reserves their room with one atomic
+            uint32_t col = adm;
+#pragma unroll
+            for (int w = 16; w >= 1; w >>= 1) {
+              const uint32_t lo = w == 16 ? 0x0000FFFFu : w == 8 ? 0x00FF00FFu : w == 4 ? 0x0F0F0F0Fu
+                                  : w == 2 ? 0x33333333u : 0x55555555u;
+              const uint32_t y = __shfl_xor_sync(0xFFFFFFFFu, col, w);
+              col = (lane & w) ? ((col & ~lo) | ((y & ~lo) >> w)) : ((col & lo) | ((y & lo) << w));
+            }
+            uint32_t base = 0;
+            if (col) base = atomicAdd(a.ccount + s_qk[slot][32 * cc + lane].y, (uint32_t)__popc(col));
+            cb[cbuf * 32 + lane] = make_uint2(0, col);
+            // 3. the previous pending chunk's entries, then this chunk becomes the pending one
+            flush();
+            p_on = true;
+            p_adm = adm;
+            p_base = base;
+            p_loc = loc;
+            p_gslot = gslot;
+            p_c0 = 32 * cc;
+            p_buf = cbuf;
+          }
+          tc_fence_before();
+          __syncwarp();
+          if (lane == 0) mbar_arrive(&bar_dempty[dbuf]);
+          mv = nmv;
+        }
+        flush();
+        if (lane == 0) mbar_arrive(&bar_iempty[slot]);
+      }
+      ts += ntiles;
+      if (*abort_flag) break;
+    }
+  }
+  if (tid == 0 && *abort_flag) atomicOr(status, kStatusTimeout);
+  tc_fence_before();
+  __syncthreads();
+  if (warp == kFMma) {
+    tc_fence_after();
+    tc_dealloc(tmem, kFCols);
+  }
+}
+
+// The exact estimates of the entries the bound admitted: one CTA per query, its u8 tables in
+// shared memory, the 64 nibble lookups of each entry's slot (src/lut.rs:116-126) and the
+// estimate in the reference's operation order (src/rabitq.rs:127-130).
+__global__ void __launch_bounds__(256) k_tc_recheck(const uint8_t* __restrict__ tables, const float4* __restrict__ qp,
+                                                    const uint4* __restrict__ codes, const float* __restrict__ mul,
+                                                    const uint32_t* __restrict__ tc_start,
+                                                    const uint32_t* __restrict__ ccount, uint32_t cap,
+                                                    uint64_t nslots, uint32_t* __restrict__ cbuf_est,
+                                                    const uint2* __restrict__ cbuf_info) {
+  __shared__ __align__(16) uint8_t T[SG_GROUPS * 16];
+  const uint32_t q = blockIdx.x;
+  const uint32_t lo = tc_start[q], hi = min(ccount[q], cap);
+  if (lo >= hi) return;  // uniform over the CTA
+  reinterpret_cast<uint32_t*>(T)[threadIdx.x] =
+      reinterpret_cast<const uint32_t*>(tables + (size_t)q * SG_GROUPS * 16)[threadIdx.x];
+  __syncthreads();
+  const float4 p = qp[q];
+  uint32_t* E = cbuf_est + (size_t)q * cap;
+  const uint2* I = cbuf_info + (size_t)q * cap;
+  for (uint32_t i = lo + threadIdx.x; i < hi; i += blockDim.x) {
+    const uint32_t gs = I[i].y;
+    if (gs >= nslots) continue;  // only an aborted bound pass leaves an entry unwritten
+    const uint4 c0 = codes[2 * (size_t)gs], c1 = codes[2 * (size_t)gs + 1];
+    const uint32_t wd[8] = {c0.x, c0.y, c0.z, c0.w, c1.x, c1.y, c1.z, c1.w};
+    uint32_t s = 0;
+#pragma unroll
+    for (int k = 0; k < 8; k++)
+#pragma unroll
+      for (int j = 0; j < 8; j++) s += T[(8 * k + j) * 16 + ((wd[k] >> (4 * j)) & 15u)];
+    const float cent = __uint_as_float(E[i]);
+    E[i] = __float_as_uint(__fadd_rn(cent, __fmul_rn(mul[gs], __fadd_rn(__fmul_rn(p.z, (float)s), p.w))));
+  }
+}
+
+static int tcf_smem_bytes() { return 2 * kFBBytes; }
+
+// The tensor-core admission pass over the (cluster, query group) items launch_invert made:
+// weights and residual bounds per query, the bound pass, then the exact estimates of what it
+// admitted. Returns the kernels launched.
+int launch_scan_tcf(const DevIndex& ix, Workspace& w, uint32_t nq, uint32_t P, const uint64_t* allow,
+                    uint64_t allow_words, int sms, cudaStream_t st) {
+  static PerDeviceOnce attr;
+  attr([] {
+    return cudaFuncSetAttribute(k_scan_tcf, cudaFuncAttributeMaxDynamicSharedMemorySize, tcf_smem_bytes());
+  });
+  TcfArgs a{};
+  a.codes = reinterpret_cast<const uint4*>(ix.blocks_tc);
+  a.mul = ix.mul;
+  a.ids = ix.ids;
+  a.block_off = ix.block_off;
+  a.clen = ix.clen;
+  a.w8 = w.w8;
+  a.fq = w.fq;
+  a.qp = w.qp;
+  a.probe_sc = w.probe_sc;
+  a.probe_off = w.probe_off;
+  a.P = P;
+  a.inv_off = w.inv_off;
+  a.inv_list = w.inv_list;
+  a.gitems = w.gitems;
+  a.counters = w.counters;
+  a.thr = w.thr;
+  a.ccount = w.ccount;
+  a.cbuf_est = w.cbuf_est;
+  a.cbuf_info = w.cbuf_info;
+  a.cap = w.cbuf_per_q;
+  a.overflow = w.overflow;
+  a.allow = allow;
+  a.allow_words = allow_words;
+  a.allow_q = w.per_query_allow ? w.allow_q : nullptr;
+  a.allow_wq = w.allow_wq;
+  a.global = ix.global;
+  // entries from tc_start[q] on are the bound pass's (earlier ones are exact already)
+  cudaMemcpyAsync(w.tc_start, w.ccount, (size_t)nq * 4, cudaMemcpyDeviceToDevice, st);
+  k_scan_tcf<<<sms, kFThreads, tcf_smem_bytes(), st>>>(a);
+  k_tc_recheck<<<nq, 256, 0, st>>>(w.tables, w.qp, reinterpret_cast<const uint4*>(ix.blocks_tc), ix.mul,
+                                   w.tc_start, w.ccount, w.cbuf_per_q, ix.nslots, w.cbuf_est, w.cbuf_info);
+  return 2;
+}
+
+void launch_filter_prep(Workspace& w, uint32_t nq, cudaStream_t st) {
+  k_filter_prep<<<nq, 64, 0, st>>>(w.tables, w.w8, w.fq);
+}
+
+}  // namespace sg

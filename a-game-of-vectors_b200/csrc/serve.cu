@@ -67,6 +67,7 @@ struct Slot {
   uint64_t* h_allow_w = nullptr;
   std::vector<std::shared_ptr<Req>> batch;
   sg_params p;
+  sg::Config cfg;      // the index's tuning when the batch was formed (prepare, launch and retries)
   uint32_t limit = 0;  // largest batch of these params that fits the slot's scratch share
   bool have_q256 = false;
   bool busy = false;
@@ -147,7 +148,7 @@ int launch_batch(sg_server* srv, Slot& s) {
   int rc;
   // scratch for the largest batch these params may form, so later batches reuse it without
   // reallocating (a cudaFree would wait for the other contexts' batches)
-  if ((rc = sg::ctx_prepare(h, s.ctx, std::max(n, s.limit), p))) return rc;
+  if ((rc = sg::ctx_prepare(h, s.cfg, s.ctx, std::max(n, s.limit), p))) return rc;
   sg::Workspace& w = s.ctx.ws;
   if (n > w.allow_q_cap) {
     if (w.allow_q) cudaFree(w.allow_q);
@@ -168,7 +169,7 @@ int launch_batch(sg_server* srv, Slot& s) {
     SV_CK(cudaMemcpyAsync(w.allow_wq, s.h_allow_w, (size_t)n * 8, cudaMemcpyHostToDevice, st));
   }
   w.per_query_allow = any_filter;
-  rc = sg::ctx_launch(h, s.ctx, n, p, s.have_q256);
+  rc = sg::ctx_launch(h, s.cfg, s.ctx, n, p, s.have_q256);
   w.per_query_allow = false;
   if (rc) return rc;
   const uint32_t k = p.k;
@@ -207,8 +208,9 @@ void complete_batch(sg_server* srv, Slot& s, int launch_rc) {
       continue;
     }
     if (s.h_ovf[i]) {
-      r.status = sg::ctx_search_one(srv->h, s.ctx, r.q768.data(), r.have_q256 ? r.q256.data() : nullptr,
-                                    s.p, r.filter ? r.filter->allow : nullptr,
+      r.status = sg::ctx_search_one(srv->h, s.cfg, s.ctx, r.q768.data(),
+                                    r.have_q256 ? r.q256.data() : nullptr, s.p,
+                                    r.filter ? r.filter->allow : nullptr,
                                     r.filter ? r.filter->words : 0, r.sc.data(), r.id.data(), &r.n);
       r.retried = 1;
       retried++;
@@ -245,8 +247,9 @@ void form_batch(sg_server* srv, Slot& s) {
   const bool hq = pend.front()->have_q256;
   const uint64_t budget = srv->cfg.scratch_bytes / std::max<uint32_t>(srv->cfg.contexts, 1);
   uint32_t limit = std::min<uint32_t>(srv->cfg.max_batch, s.cap);
+  s.cfg = sg::index_config(srv->h);
   // the largest batch whose scratch fits this slot's share (one query always goes)
-  while (limit > 1 && sg::ctx_bytes(srv->h, p, limit) > budget) limit = (limit + 1) / 2;
+  while (limit > 1 && sg::ctx_bytes(srv->h, s.cfg, p, limit) > budget) limit = (limit + 1) / 2;
   std::deque<std::shared_ptr<Req>> rest;
   while (!pend.empty()) {
     auto r = pend.front();
@@ -362,7 +365,8 @@ int sg_server_submit(sg_server* srv, const float* q768, const float* q256, const
     std::lock_guard<std::mutex> g(srv->mu);
     if (srv->stopping) return fail(SG_ERR_INVALID, "server is stopping");
     const uint64_t budget = srv->cfg.scratch_bytes / std::max<uint32_t>(srv->cfg.contexts, 1);
-    if (srv->pending.size() >= srv->cfg.max_pending || sg::ctx_bytes(srv->h, *params, 1) > budget) {
+    if (srv->pending.size() >= srv->cfg.max_pending ||
+        sg::ctx_bytes(srv->h, sg::index_config(srv->h), *params, 1) > budget) {
       srv->st.rejected++;
       return fail(SG_ERR_ADMISSION, "no queue slot or scratch for this request");
     }

@@ -91,6 +91,7 @@ void free_index(sg::DevIndex& x) {
   dfree(x.rerank);
   dfree(x.norm256);
   dfree(x.qscale);
+  dfree(x.codes);
 }
 
 void free_ws(sg::Workspace& w) {
@@ -102,6 +103,9 @@ void free_ws(sg::Workspace& w) {
   dfree(w.q768);
   dfree(w.q256);
   dfree(w.q16);
+  dfree(w.w8);
+  dfree(w.fq);
+  dfree(w.tc_start);
   dfree(w.tables);
   dfree(w.qp);
   dfree(w.qnorm);
@@ -150,9 +154,8 @@ int build_index(const sg_ivf_arrays* a, int device, sg_index** out) {
   if (a->k == 0 || !a->centroids || !a->block_off)
     return fail(SG_ERR_INVALID, "index needs centroids and block_off");
   if (!a->ids || !a->blocks) return fail(SG_ERR_INVALID, "index needs ids.u32 and blocks.bin");
-  if (!a->factors || !a->rotation)
-    return fail(SG_ERR_UNSUPPORTED,
-                "only RaBitQ indexes (rotation.f32 + factors.f32) run on the GPU path");
+  // without rotation.f32 + factors.f32 the slots hold global sign codes (src/ivf.rs:700-717)
+  const bool global = !a->factors || !a->rotation;
   if (!a->rerank || !a->quant_scale)
     return fail(SG_ERR_INVALID, "corpus needs rerank.i8 and quant.f32");
   const uint32_t K = a->k;
@@ -172,6 +175,7 @@ int build_index(const sg_ivf_arrays* a, int device, sg_index** out) {
   x.n = a->n;
   x.nblocks = nblocks;
   x.nslots = nblocks * SG_BLOCK;
+  x.global = global;
   // cluster lengths: PAD may only fill the tail of a cluster's last block (src/ivf.rs:378-380)
   x.h_block_off.assign(a->block_off, a->block_off + K + 1);
   x.h_clen.resize(K);
@@ -219,11 +223,12 @@ int build_index(const sg_ivf_arrays* a, int device, sg_index** out) {
     nmax = std::max(nmax, (float)sqrt(s));
   }
   x.cent_norm_max = nmax * 1.0001f;
-  // factors.f32 [mul, err] per slot -> two planes
+  // factors.f32 [mul, err] per slot -> two planes; global sign codes: the score itself is the
+  // ranking estimate (mul 1) and carries no bound (err +inf)
   std::vector<float> mul(x.nslots), err(x.nslots);
   for (uint64_t s = 0; s < x.nslots; s++) {
-    mul[s] = a->factors[2 * s];
-    err[s] = a->factors[2 * s + 1];
+    mul[s] = global ? 1.0f : a->factors[2 * s];
+    err[s] = global ? INFINITY : a->factors[2 * s + 1];
   }
   // per-cluster range of mul over the real slots: the MMA scan turns it into an integer floor
   // on the LUT score below which no slot of the cluster can reach a query's threshold
@@ -251,7 +256,8 @@ int build_index(const sg_ivf_arrays* a, int device, sg_index** out) {
       (rc = upload(&x.blocks, a->blocks, (size_t)nblocks * SG_BLOCK_BYTES)) ||
       (rc = upload(&x.mul, mul.data(), mul.size())) || (rc = upload(&x.err, err.data(), err.size())) ||
       (rc = upload(&x.mul_rng, mrng.data(), mrng.size())) ||
-      (rc = upload(&x.ids, a->ids, x.nslots)) || (rc = upload(&x.rot, a->rotation, 3 * SG_PDIM)) ||
+      (rc = upload(&x.ids, a->ids, x.nslots)) ||
+      (!global && (rc = upload(&x.rot, a->rotation, 3 * SG_PDIM))) ||
       (rc = upload(&x.rerank, a->rerank, (size_t)a->n * SG_DIM)) ||
       (rc = upload(&x.qscale, a->quant_scale, SG_DIM))) {
     free_index(x);
@@ -281,7 +287,8 @@ int build_index(const sg_ivf_arrays* a, int device, sg_index** out) {
     free_index(x);
     return rc ? rc : fail(SG_ERR_DEVICE, "transcode of the code blocks failed");
   }
-  if (a->norm256 && (rc = upload(&x.norm256, a->norm256, a->n))) {
+  if ((a->norm256 && (rc = upload(&x.norm256, a->norm256, a->n))) ||
+      (a->codes && (rc = upload(&x.codes, a->codes, (size_t)a->n * SG_CODE_BYTES)))) {
     free_index(x);
     return rc;
   }
@@ -319,12 +326,14 @@ int build_index(const sg_ivf_arrays* a, int device, sg_index** out) {
 struct RoutePlan {
   const uint32_t* per_cluster = nullptr;  // device [k]; set for Expand
   uint64_t target = 0;
+  bool given = false;  // the probe lists are staged in ws.probe_sc / probe_cl / probe_n
   bool expand() const { return per_cluster != nullptr; }
 };
 
 // The device addresses a captured pipeline bakes in; when any moves, captured graphs are stale.
 uint64_t ws_signature(const sg::Workspace& w) {
   const void* ptrs[] = {w.q768, w.q256, w.tables, w.qp, w.qnorm, w.wq, w.winv, w.wq256, w.winv256,
+                        w.w8, w.fq, w.tc_start,
                         w.scores, w.probe_sc, w.probe_cl, w.probe_off, w.probe_n, w.scanned,
                         w.items, w.seed_items, w.counters, w.inv_cnt, w.inv_fill, w.inv_off,
                         w.inv_list, w.gitems, w.thr, w.ccount, w.cbuf_est, w.cbuf_info,
@@ -370,10 +379,12 @@ int ensure_ws_impl(sg_index* h, sg::Ctx& c, uint32_t nq, const sg_params& p, uin
   if (nq > w.nq_cap) {
     uint32_t n = std::max(nq, w.nq_cap * 2);
     dfree(w.q768); dfree(w.q256); dfree(w.q16); dfree(w.tables); dfree(w.qp); dfree(w.qnorm); dfree(w.wq);
+    dfree(w.w8); dfree(w.fq); dfree(w.tc_start);
     dfree(w.winv); dfree(w.wq256); dfree(w.winv256); dfree(w.probe_n); dfree(w.scanned); dfree(w.seed_items);
     dfree(w.thr); dfree(w.ccount); dfree(w.overflow); dfree(w.cn); dfree(w.ln); dfree(w.out_n);
     if ((rc = dalloc(&w.q768, (size_t)n * SG_DIM)) || (rc = dalloc(&w.q256, (size_t)n * SG_PDIM)) ||
-        (rc = dalloc(&w.q16, (size_t)n * SG_PDIM)) ||
+        (rc = dalloc(&w.q16, (size_t)n * SG_PDIM)) || (rc = dalloc(&w.w8, (size_t)n * SG_GROUPS)) ||
+        (rc = dalloc(&w.fq, n)) || (rc = dalloc(&w.tc_start, n)) ||
         (rc = dalloc(&w.tables, (size_t)n * SG_GROUPS * 16)) || (rc = dalloc(&w.qp, n)) ||
         (rc = dalloc(&w.qnorm, n)) || (rc = dalloc(&w.wq, (size_t)n * SG_DIM)) ||
         (rc = dalloc(&w.winv, n)) || (rc = dalloc(&w.wq256, (size_t)n * SG_PDIM)) ||
@@ -464,24 +475,26 @@ int check_params(const sg_index* h, const sg_params* p) {
 
 // Does a call of nq queries run the tensor-core scan? (It pays off once enough queries share each
 // probed cluster; SIEVE_GPU_MMA forces it off (0) or on (2).)
-bool use_mma(const sg_index* h, uint32_t nq, uint32_t P) {
+bool use_mma(const sg_index* h, const sg::Config& cfg, uint32_t nq, uint32_t P) {
   const sg::DevIndex& x = h->ix;
-  if (!(h->cfg.tc ? x.blocks_tc : x.blocks_mma) || P <= 1 || P > 4096)
+  if (!(cfg.tc ? x.blocks_tc : x.blocks_mma) || P <= 1 || P > 4096)
     return false;  // inverted lists keep 12-bit ranks
-  if (h->cfg.mma == 2) return true;
-  if (h->cfg.mma != 1 || nq < 64) return false;
+  if (x.global && cfg.tc != 1) return false;  // only the bound pass ranks global codes
+  if (cfg.mma == 2) return true;
+  if (cfg.mma != 1 || nq < 64) return false;
   // tcgen05: the batch splits per cluster on the device (few queries: ALU, many: tensor cores),
   // so the inverted path pays off once some cluster can gather tc_min_queries queries
-  if (h->cfg.tc) return (uint64_t)nq * (P - 1) >= (uint64_t)h->cfg.tc_min_queries * 16;
-  return (uint64_t)nq * (P - 1) >= (uint64_t)h->cfg.mma_min_queries_per_cluster * x.k;
+  if (cfg.tc) return (uint64_t)nq * (P - 1) >= (uint64_t)cfg.tc_min_queries * 16;
+  return (uint64_t)nq * (P - 1) >= (uint64_t)cfg.mma_min_queries_per_cluster * x.k;
 }
 
 // Exact per-query candidate-buffer bound. A slot is appended at most once, so the probed
 // clusters' slots bound it; the ALU scan also cuts every chunk to `cand`, so chunks x cand does.
-uint32_t full_cap(const sg_index* h, const sg_params& p, uint32_t nq) {
+uint32_t full_cap(const sg_index* h, const sg::Config& cfg, const sg_params& p, uint32_t nq) {
   const uint32_t P = std::min<uint32_t>(p.nprobe, h->ix.k);
   uint64_t b = h->ix.h_slots_desc_prefix[P];
-  if (!use_mma(h, nq, P))
+  // (a global-code chunk keeps every slot tied with its cand-th score, so only the slots bound it)
+  if (!use_mma(h, cfg, nq, P) && !h->ix.global)
     b = std::min<uint64_t>(b, (uint64_t)h->ix.h_chunks_desc_prefix[P] * std::max<uint32_t>(p.cand, 1));
   return (uint32_t)std::min<uint64_t>(std::max<uint64_t>(b, 1), 0x7FFFFFFFull);
 }
@@ -489,11 +502,12 @@ uint32_t full_cap(const sg_index* h, const sg_params& p, uint32_t nq) {
 // Soft per-query buffer for batches: at least 16 x cand entries, and up to the index's
 // candidate-buffer budget (a quarter of the device memory free at open, 8 to 32 GiB) shared by
 // the batch. A query that fills it is re-run (see search_impl) with the exact bound.
-uint32_t batch_cap(const sg_index* h, const sg_params& p, uint32_t nq, bool soft_always = false) {
-  uint32_t full = full_cap(h, p, nq);
-  if (h->cfg.soft_cap) return std::min(full, h->cfg.soft_cap);
+uint32_t batch_cap(const sg_index* h, const sg::Config& cfg, const sg_params& p, uint32_t nq,
+                   bool soft_always = false) {
+  uint32_t full = full_cap(h, cfg, p, nq);
+  if (cfg.soft_cap) return std::min(full, cfg.soft_cap);
   if (nq <= 8 && !soft_always) return full;
-  uint64_t budget = h->cfg.cbuf_budget / (sizeof(uint4) * (uint64_t)nq);
+  uint64_t budget = cfg.cbuf_budget / (sizeof(uint4) * (uint64_t)nq);
   uint64_t soft = std::max<uint64_t>(16ull * std::max<uint32_t>(p.cand, 1), budget);
   return (uint32_t)std::min<uint64_t>(full, soft);
 }
@@ -502,8 +516,8 @@ enum Stage { kToCandidates = 1, kToSearch = 2 };
 
 // Runs the pipeline on queries already in ws.q768 / ws.q256 (have_q256 = false: derive it).
 // With `timed`, events ev[0..7] bracket the stages (see collect_stats).
-int run_pipeline(sg_index* h, sg::Ctx& c, uint32_t nq, const sg_params& p, bool have_q256,
-                 const uint64_t* d_allow, uint64_t allow_words, Stage stage, bool timed,
+int run_pipeline(sg_index* h, const sg::Config& cfg, sg::Ctx& c, uint32_t nq, const sg_params& p,
+                 bool have_q256, const uint64_t* d_allow, uint64_t allow_words, Stage stage, bool timed,
                  const RoutePlan& rp = RoutePlan()) {
   sg::Workspace& w = c.ws;
   sg::DevIndex& x = h->ix;
@@ -520,31 +534,32 @@ int run_pipeline(sg_index* h, sg::Ctx& c, uint32_t nq, const sg_params& p, bool 
   }
   sg::launch_prep(x, w, nq, st);
   if (timed) CK(cudaEventRecord(w.ev[1], st));
-  const int route_prec = rp.expand() ? SG_ROUTE_FP32 : x.route_precision;
-  CK(sg::launch_route_scores(x, w, nq, route_prec, st));
+  const int route_prec = rp.expand() ? SG_ROUTE_FP32 : cfg.route_precision;
+  if (!rp.given) CK(sg::launch_route_scores(x, w, nq, route_prec, st));
   if (timed) CK(cudaEventRecord(w.ev[2], st));
   // Few queries leave most SMs to the chunked pass: a short seed (one CTA per query scans it
   // alone) and short chunks keep the GPU busy.
-  const bool small = nq < h->cfg.small_batch;
-  const uint32_t cb = small ? h->cfg.small_chunk_blocks : h->cfg.chunk_blocks;
-  const uint32_t sb = small ? h->cfg.small_seed_blocks : h->cfg.seed_blocks;
+  const bool small = nq < cfg.small_batch;
+  const uint32_t cb = small ? cfg.small_chunk_blocks : cfg.chunk_blocks;
+  const uint32_t sb = small ? cfg.small_seed_blocks : cfg.seed_blocks;
   // The tensor-core scan pays off once enough queries share each probed cluster.
   const uint32_t P = std::min<uint32_t>(p.nprobe, x.k);
-  const bool mma = !rp.expand() && use_mma(h, nq, P);
+  const bool mma = !rp.expand() && use_mma(h, cfg, nq, P);
   if (rp.expand())
     sg::launch_route_expand(x, w, nq, p, cb, sb, rp.per_cluster, rp.target, st);
+  else if (rp.given)
+    sg::launch_route_given(x, w, nq, p, cb, sb, !mma, w.probe_sc, w.probe_cl, w.probe_n, st);
   else
-    sg::launch_route_select(x, w, nq, p, x.route_precision, cb, sb, !mma, st);
+    sg::launch_route_select(x, w, nq, p, cfg.route_precision, cb, sb, !mma, st);
   if (timed) CK(cudaEventRecord(w.ev[3], st));
   launches += route_prec == SG_ROUTE_BF16 ? 4 : 3;  // prep, routing (BF16: + the bf16 queries), select
   if (p.cand > 0) {
-    sg::launch_scan(x, w, nq, p, d_allow, allow_words, h->sms, 0, sb,
-                    h->cfg.scan_ctas_per_sm, st);
+    sg::launch_scan(x, w, nq, p, d_allow, allow_words, h->sms, 0, sb, cfg.scan_ctas_per_sm, st);
     if (timed) CK(cudaEventRecord(w.ev[9], st));
-    if (mma && h->cfg.tc) {  // ALU chunks and tcgen05 tiles, split per cluster
-      launches += sg::launch_scan_tc(x, w, nq, p, d_allow, allow_words, h->sms, h->cfg, cb, st);
+    if (mma && cfg.tc) {  // ALU chunks and tcgen05 tiles, split per cluster
+      launches += sg::launch_scan_tc(x, w, nq, p, d_allow, allow_words, h->sms, cfg, cb, st);
     } else {
-      sg::launch_scan(x, w, nq, p, d_allow, allow_words, h->sms, cb, 0, h->cfg.scan_ctas_per_sm, st);
+      sg::launch_scan(x, w, nq, p, d_allow, allow_words, h->sms, cb, 0, cfg.scan_ctas_per_sm, st);
       if (mma) launches += sg::launch_scan_mma(x, w, nq, p, d_allow, allow_words, h->sms, st);
     }
     if (timed) CK(cudaEventRecord(w.ev[4], st));
@@ -579,10 +594,10 @@ void collect_stats(sg::Workspace& w, const sg_params& p) {
 // Runs the search pipeline on c's stream: directly, or, for a call shape seen before and with
 // graphs on, by replaying the CUDA graph captured for it (the second time a shape occurs; the
 // first run of each kernel also sets its shared-memory attributes outside any capture).
-int launch_pipeline(sg_index* h, sg::Ctx& c, uint32_t nq, const sg_params& p, bool have_q256,
-                    const uint64_t* d_allow, uint64_t allow_words, bool timed) {
-  if (!h->cfg.graphs || timed)
-    return run_pipeline(h, c, nq, p, have_q256, d_allow, allow_words, kToSearch, timed);
+int launch_pipeline(sg_index* h, const sg::Config& cfg, sg::Ctx& c, uint32_t nq, const sg_params& p,
+                    bool have_q256, const uint64_t* d_allow, uint64_t allow_words, bool timed) {
+  if (!cfg.graphs || timed)
+    return run_pipeline(h, cfg, c, nq, p, have_q256, d_allow, allow_words, kToSearch, timed);
   sg::GraphKey key;
   memset(&key, 0, sizeof key);
   key.nq = nq;
@@ -591,13 +606,13 @@ int launch_pipeline(sg_index* h, sg::Ctx& c, uint32_t nq, const sg_params& p, bo
   key.allow = d_allow;
   key.allow_words = allow_words;
   key.gen = c.gen;
-  key.cfg_gen = h->cfg.gen;
+  key.cfg_gen = cfg.gen;
   for (auto& g : c.graphs)
     if (g.key.same(key)) {
       if (!g.exec) {  // seen once before: capture it now
         cudaGraph_t graph = nullptr;
         CK(cudaStreamBeginCapture(c.stream, cudaStreamCaptureModeThreadLocal));
-        int rc = run_pipeline(h, c, nq, p, have_q256, d_allow, allow_words, kToSearch, false);
+        int rc = run_pipeline(h, cfg, c, nq, p, have_q256, d_allow, allow_words, kToSearch, false);
         cudaError_t e = cudaStreamEndCapture(c.stream, &graph);
         if (rc) {
           if (graph) cudaGraphDestroy(graph);
@@ -623,7 +638,7 @@ int launch_pipeline(sg_index* h, sg::Ctx& c, uint32_t nq, const sg_params& p, bo
     c.graphs.erase(c.graphs.begin());
   }
   c.graphs.push_back({key, nullptr, 0});
-  return run_pipeline(h, c, nq, p, have_q256, d_allow, allow_words, kToSearch, false);
+  return run_pipeline(h, cfg, c, nq, p, have_q256, d_allow, allow_words, kToSearch, false);
 }
 
 int stage_inputs(sg::Ctx& c, uint32_t nq, const float* q768, const float* q256, bool device) {
@@ -656,9 +671,9 @@ int stage_allow(sg::Ctx& c, const uint64_t* allow, uint64_t words, bool device,
 }
 
 // Full search of nq queries with inputs staged; copies results out (kind: D2H or D2D).
-int search_impl(sg_index* h, sg::Ctx& c, uint32_t nq, const float* q768, const float* q256,
-                const sg_params& user_p, const uint64_t* allow, uint64_t allow_words, float* out_sc,
-                uint32_t* out_id, uint32_t* out_n, sg_timing* t, bool device,
+int search_impl(sg_index* h, const sg::Config& cfg, sg::Ctx& c, uint32_t nq, const float* q768,
+                const float* q256, const sg_params& user_p, const uint64_t* allow, uint64_t allow_words,
+                float* out_sc, uint32_t* out_id, uint32_t* out_n, sg_timing* t, bool device,
                 bool allow_dev = false, const RoutePlan& rp = RoutePlan()) {
   int rc;
   if ((rc = check_params(h, &user_p))) return rc;
@@ -672,16 +687,16 @@ int search_impl(sg_index* h, sg::Ctx& c, uint32_t nq, const float* q768, const f
     p.has_margin = 0;
     p.has_budget = 0;
   }
-  uint32_t cap = batch_cap(h, p, nq, rp.expand());
+  uint32_t cap = batch_cap(h, cfg, p, nq, rp.expand());
   if ((rc = ensure_ws(h, c, nq, p, cap))) return rc;
   if ((rc = stage_inputs(c, nq, q768, q256, device))) return rc;
   const uint64_t* d_allow;
   if ((rc = stage_allow(c, allow, allow_words, allow_dev, &d_allow))) return rc;
-  const bool timed_run = t != nullptr || h->timing_on;
+  const bool timed_run = t != nullptr || cfg.timing;
   if (rp.expand())
-    rc = run_pipeline(h, c, nq, p, q256 != nullptr, d_allow, allow_words, kToSearch, timed_run, rp);
+    rc = run_pipeline(h, cfg, c, nq, p, q256 != nullptr, d_allow, allow_words, kToSearch, timed_run, rp);
   else
-    rc = launch_pipeline(h, c, nq, p, q256 != nullptr, d_allow, allow_words, timed_run);
+    rc = launch_pipeline(h, cfg, c, nq, p, q256 != nullptr, d_allow, allow_words, timed_run);
   if (rc) return rc;
   sg::Workspace& w = c.ws;
   std::vector<uint8_t> ovf(nq);
@@ -710,7 +725,7 @@ int search_impl(sg_index* h, sg::Ctx& c, uint32_t nq, const float* q768, const f
   CK(cudaStreamSynchronize(c.stream));
   if (status & sg::kStatusOverflow) return fail(SG_ERR_INVALID, "work queue overflow");
   if (status & sg::kStatusTimeout) return fail(SG_ERR_DEVICE, "a tensor-core wait ran out (routing GEMM or scan)");
-  const bool timed = t != nullptr || h->timing_on;
+  const bool timed = timed_run;
   if (timed) {
     collect_stats(w, p);
     uint64_t sc = 0, pr = 0, rr = 0, bu = 0;
@@ -742,10 +757,10 @@ int search_impl(sg_index* h, sg::Ctx& c, uint32_t nq, const float* q768, const f
     if (ovf[i]) redo.push_back(i);
   if (!redo.empty()) {
     uint32_t per = (uint32_t)redo.size();
-    uint32_t fcap = full_cap(h, p, per);
-    while (per > 1 && (uint64_t)per * fcap * sizeof(uint4) > h->cfg.cbuf_budget) {
+    uint32_t fcap = full_cap(h, cfg, p, per);
+    while (per > 1 && (uint64_t)per * fcap * sizeof(uint4) > cfg.cbuf_budget) {
       per = (per + 1) / 2;
-      fcap = full_cap(h, p, per);
+      fcap = full_cap(h, cfg, p, per);
     }
     std::vector<float> hq768, hq256;
     std::vector<float> osc((size_t)per * std::max<uint32_t>(k, 1));
@@ -761,7 +776,7 @@ int search_impl(sg_index* h, sg::Ctx& c, uint32_t nq, const float* q768, const f
           CK(cudaMemcpyAsync(w.q256 + (size_t)j * SG_PDIM, q256 + (size_t)i * SG_PDIM, SG_PDIM * 4, ik, c.stream));
       }
       if ((rc = stage_allow(c, allow, allow_words, allow_dev, &d_allow))) return rc;
-      if ((rc = run_pipeline(h, c, m, p, q256 != nullptr, d_allow, allow_words, kToSearch, false,
+      if ((rc = run_pipeline(h, cfg, c, m, p, q256 != nullptr, d_allow, allow_words, kToSearch, false,
                              rp)))
         return rc;
       std::vector<uint8_t> o1(m);
@@ -789,9 +804,9 @@ int search_impl(sg_index* h, sg::Ctx& c, uint32_t nq, const float* q768, const f
 
 // filter::search Plan::Brute (src/filter.rs:95-105): exact int8 scores of every allowed row, in
 // query batches whose score matrix stays under 1 GiB.
-int brute_impl(sg_index* h, sg::Ctx& c, const sg_filter* f, uint32_t nq, const float* q768,
-               const float* q256, const sg_params& p, float* out_sc, uint32_t* out_id,
-               uint32_t* out_n, sg_timing* t) {
+int brute_impl(sg_index* h, const sg::Config& cfg, sg::Ctx& c, const sg_filter* f, uint32_t nq,
+               const float* q768, const float* q256, const sg_params& p, float* out_sc,
+               uint32_t* out_id, uint32_t* out_n, sg_timing* t) {
   int rc;
   if ((rc = check_params(h, &p))) return rc;
   if (nq == 0) return SG_OK;
@@ -808,7 +823,7 @@ int brute_impl(sg_index* h, sg::Ctx& c, const sg_filter* f, uint32_t nq, const f
     if ((rc = dalloc(&w.brute, (size_t)per * R))) return rc;
     w.brute_cap = (uint64_t)per * R;
   }
-  const bool timed = t != nullptr || h->timing_on;
+  const bool timed = t != nullptr || cfg.timing;
   if (timed && !w.events) {
     for (auto& e : w.ev) CK(cudaEventCreate(&e));
     w.events = true;
@@ -876,26 +891,33 @@ bool read_file(const std::string& path, std::vector<char>& out, bool optional, i
 namespace sg {
 // Read-only views of an open index for entry points that live in other translation units.
 const DevIndex* index_arrays(const sg_index* h) { return &h->ix; }
-const Config* index_config(const sg_index* h) { return &h->cfg; }
+Config index_config(const sg_index* h) {
+  std::lock_guard<std::mutex> g(h->cfg_mu);
+  Config c = h->cfg;
+  c.timing = h->timing_on.load(std::memory_order_relaxed);
+  return c;
+}
 int index_sms(const sg_index* h) { return h->sms; }
 int index_check_params(const sg_index* h, const sg_params* p) { return check_params(h, p); }
 
 // ---- execution-context entry points for the serving loop (serve.cu) -------------------------
-int ctx_prepare(sg_index* h, Ctx& c, uint32_t nq, const sg_params& p) {
+int ctx_prepare(sg_index* h, const Config& cfg, Ctx& c, uint32_t nq, const sg_params& p) {
   int rc;
   if ((rc = check_params(h, &p))) return rc;
   CK(cudaSetDevice(h->ix.device));
-  return ensure_ws(h, c, nq, p, batch_cap(h, p, nq));
+  return ensure_ws(h, c, nq, p, batch_cap(h, cfg, p, nq));
 }
 
-int ctx_launch(sg_index* h, Ctx& c, uint32_t nq, const sg_params& p, bool have_q256) {
-  return run_pipeline(h, c, nq, p, have_q256, nullptr, 0, kToSearch, false);
+int ctx_launch(sg_index* h, const Config& cfg, Ctx& c, uint32_t nq, const sg_params& p, bool have_q256) {
+  return run_pipeline(h, cfg, c, nq, p, have_q256, nullptr, 0, kToSearch, false);
 }
 
-int ctx_search_one(sg_index* h, Ctx& c, const float* q768, const float* q256, const sg_params& p,
-                   const uint64_t* d_allow, uint64_t allow_words, float* out_sc, uint32_t* out_id,
-                   uint32_t* out_n) {
-  return search_impl(h, c, 1, q768, q256, p, d_allow, allow_words, out_sc, out_id, out_n, nullptr,
+int ctx_search_one(sg_index* h, const Config& cfg, Ctx& c, const float* q768, const float* q256,
+                   const sg_params& p, const uint64_t* d_allow, uint64_t allow_words, float* out_sc,
+                   uint32_t* out_id, uint32_t* out_n) {
+  Config one = cfg;
+  one.timing = false;
+  return search_impl(h, one, c, 1, q768, q256, p, d_allow, allow_words, out_sc, out_id, out_n, nullptr,
                      false, true);
 }
 
@@ -903,14 +925,16 @@ void free_ctx(Ctx& c) {
   if (c.stream) cudaStreamSynchronize(c.stream);
   drop_graphs(c);
   free_ws(c.ws);
+  if (c.order_ev) cudaEventDestroy(c.order_ev);
+  c.order_ev = nullptr;
   if (c.stream) cudaStreamDestroy(c.stream);
   c.stream = nullptr;
 }
 
 // Device scratch of a batch of nq queries with params p (the workspace ensure_ws grows to).
-uint64_t ctx_bytes(const sg_index* h, const sg_params& p, uint32_t nq) {
+uint64_t ctx_bytes(const sg_index* h, const Config& cfg, const sg_params& p, uint32_t nq) {
   const uint64_t P = std::min<uint32_t>(p.nprobe, h->ix.k);
-  const uint64_t cap = batch_cap(h, p, nq);
+  const uint64_t cap = batch_cap(h, cfg, p, nq);
   const uint64_t per_q = SG_DIM * 4 * 2 + SG_PDIM * 5 + 1024 + 64 + (uint64_t)h->ix.k * 4 + P * 16 +
                          cap * 12 + (uint64_t)std::max<uint32_t>(p.cand, 1) * 20 +
                          (uint64_t)std::max<uint32_t>(p.k, 1) * 8 + 64;
@@ -937,7 +961,7 @@ int sg_open_ivf(const char* ingest_dir, const char* index_dir, int device, sg_in
   if (!ingest_dir || !index_dir || !out) return fail(SG_ERR_INVALID, "null argument");
   try {
     std::string I(ingest_dir), X(index_dir);
-    std::vector<char> cent, boff, ids, blocks, fac, rot, sig, t2c, t2n, rer, n256, qs;
+    std::vector<char> cent, boff, ids, blocks, fac, rot, sig, t2c, t2n, rer, n256, qs, codes;
     int rc = SG_OK;
     if (!read_file(X + "/centroids.f32", cent, false, &rc) ||
         !read_file(X + "/block_off.u64", boff, false, &rc) ||
@@ -947,6 +971,7 @@ int sg_open_ivf(const char* ingest_dir, const char* index_dir, int device, sg_in
         !read_file(I + "/norm256.f32", n256, false, &rc) ||
         !read_file(I + "/quant.f32", qs, false, &rc))
       return rc;
+    bool has_codes = read_file(I + "/codes.bin", codes, true, &rc);
     bool has_rot = read_file(X + "/rotation.f32", rot, true, &rc);
     bool has_fac = read_file(X + "/factors.f32", fac, true, &rc);
     bool has_t2 = read_file(X + "/tier2.bin", t2c, true, &rc) &&
@@ -985,6 +1010,10 @@ int sg_open_ivf(const char* ingest_dir, const char* index_dir, int device, sg_in
     }
     a.rerank = (const int8_t*)rer.data();
     a.norm256 = (const float*)n256.data();
+    if (has_codes) {
+      if (codes.size() != a.n * SG_CODE_BYTES) return fail(SG_ERR_INVALID, "codes.bin size");
+      a.codes = (const uint8_t*)codes.data();
+    }
     a.quant_scale = (const float*)qs.data();
     return build_index(&a, device, out);
   } catch (const std::exception& e) {
@@ -1018,18 +1047,17 @@ int sg_set_route_precision(sg_index* h, int precision) {
   if (!h) return fail(SG_ERR_INVALID, "null index");
   if (precision != SG_ROUTE_FP32 && precision != SG_ROUTE_BF16)
     return fail(SG_ERR_INVALID, "precision must be SG_ROUTE_FP32 or SG_ROUTE_BF16");
-  std::lock_guard<std::mutex> lk(h->mu);
-  if (h->ix.route_precision != precision) {
-    h->ix.route_precision = precision;
-    drop_graphs(h->def);  // captured pipelines launch the other routing kernel
-    h->def.gen++;
+  std::lock_guard<std::mutex> lk(h->cfg_mu);
+  if (h->cfg.route_precision != precision) {
+    h->cfg.route_precision = precision;
+    h->cfg.gen++;  // captured pipelines launch the other routing kernel: their keys go stale
   }
   return SG_OK;
 }
 
 int sg_set_timing(sg_index* h, int on) {
   if (!h) return fail(SG_ERR_INVALID, "null index");
-  h->timing_on = on != 0;
+  h->timing_on.store(on != 0, std::memory_order_relaxed);
   return SG_OK;
 }
 
@@ -1044,9 +1072,28 @@ int sg_search(sg_index* h, uint32_t nq, const float* q768, const float* q256,
               float* out_scores, uint32_t* out_ids, uint32_t* out_counts, sg_timing* timing) {
   if (!h || !params) return fail(SG_ERR_INVALID, "null argument");
   std::lock_guard<std::mutex> g(h->mu);
-  return search_impl(h, h->def, nq, q768, q256, *params, allow_bits, allow_words, out_scores, out_ids,
-                     out_counts, timing, false);
+  return search_impl(h, sg::index_config(h), h->def, nq, q768, q256, *params, allow_bits, allow_words,
+                     out_scores, out_ids, out_counts, timing, false);
 }
+
+}  // extern "C"
+
+namespace {
+// sg_search_device on context c: c's stream waits for the caller's stream (one reusable event),
+// and the call returns after the results are in the caller's device buffers.
+int search_device_on(sg_index* h, sg::Ctx& c, uint32_t nq, const float* d_q768, const float* d_q256,
+                     const sg_params* params, const uint64_t* d_allow_bits, uint64_t allow_words,
+                     float* d_out_scores, uint32_t* d_out_ids, uint32_t* d_out_counts, void* stream) {
+  CK(cudaSetDevice(h->ix.device));
+  if (!c.order_ev) CK(cudaEventCreateWithFlags(&c.order_ev, cudaEventDisableTiming));
+  CK(cudaEventRecord(c.order_ev, (cudaStream_t)stream));
+  CK(cudaStreamWaitEvent(c.stream, c.order_ev, 0));
+  return search_impl(h, sg::index_config(h), c, nq, d_q768, d_q256, *params, d_allow_bits, allow_words,
+                     d_out_scores, d_out_ids, d_out_counts, nullptr, true);
+}
+}  // namespace
+
+extern "C" {
 
 int sg_search_device(sg_index* h, uint32_t nq, const float* d_q768, const float* d_q256,
                      const sg_params* params, const uint64_t* d_allow_bits, uint64_t allow_words,
@@ -1054,16 +1101,68 @@ int sg_search_device(sg_index* h, uint32_t nq, const float* d_q768, const float*
                      void* stream) {
   if (!h || !params) return fail(SG_ERR_INVALID, "null argument");
   std::lock_guard<std::mutex> g(h->mu);
-  cudaStream_t user = (cudaStream_t)stream;
-  // order the index stream after the caller's stream, and the caller's after the results
-  cudaEvent_t ev;
-  CK(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
-  CK(cudaEventRecord(ev, user));
-  CK(cudaStreamWaitEvent(h->def.stream, ev, 0));
-  int rc = search_impl(h, h->def, nq, d_q768, d_q256, *params, d_allow_bits, allow_words, d_out_scores,
-                       d_out_ids, d_out_counts, nullptr, true);
-  cudaEventDestroy(ev);
-  return rc;
+  return search_device_on(h, h->def, nq, d_q768, d_q256, params, d_allow_bits, allow_words, d_out_scores,
+                          d_out_ids, d_out_counts, stream);
+}
+
+int sg_context_open(sg_index* h, sg_context** out) {
+  if (!h || !out) return fail(SG_ERR_INVALID, "null argument");
+  *out = nullptr;
+  try {
+    std::unique_ptr<sg_context> c(new sg_context());
+    c->h = h;
+    CK(cudaSetDevice(h->ix.device));
+    CK(cudaStreamCreateWithFlags(&c->ctx.stream, cudaStreamNonBlocking));
+    *out = c.release();
+    return SG_OK;
+  } catch (const std::exception& e) {
+    return fail(SG_ERR_OOM, std::string("host allocation: ") + e.what());
+  }
+}
+
+int sg_context_close(sg_context* c) {
+  if (!c) return SG_OK;
+  {
+    std::lock_guard<std::mutex> g(c->mu);
+    cudaSetDevice(c->h->ix.device);
+    sg::free_ctx(c->ctx);
+  }
+  delete c;
+  return SG_OK;
+}
+
+int sg_search_ctx(sg_context* c, uint32_t nq, const float* q768, const float* q256,
+                  const sg_params* params, const uint64_t* allow_bits, uint64_t allow_words,
+                  float* out_scores, uint32_t* out_ids, uint32_t* out_counts, sg_timing* timing) {
+  if (!c || !params) return fail(SG_ERR_INVALID, "null argument");
+  std::lock_guard<std::mutex> g(c->mu);
+  try {
+    return search_impl(c->h, sg::index_config(c->h), c->ctx, nq, q768, q256, *params, allow_bits,
+                       allow_words, out_scores, out_ids, out_counts, timing, false);
+  } catch (const std::exception& e) {
+    return fail(SG_ERR_OOM, std::string("host allocation: ") + e.what());
+  }
+}
+
+int sg_search_device_ctx(sg_context* c, uint32_t nq, const float* d_q768, const float* d_q256,
+                         const sg_params* params, const uint64_t* d_allow_bits, uint64_t allow_words,
+                         float* d_out_scores, uint32_t* d_out_ids, uint32_t* d_out_counts,
+                         void* stream) {
+  if (!c || !params) return fail(SG_ERR_INVALID, "null argument");
+  std::lock_guard<std::mutex> g(c->mu);
+  try {
+    return search_device_on(c->h, c->ctx, nq, d_q768, d_q256, params, d_allow_bits, allow_words,
+                            d_out_scores, d_out_ids, d_out_counts, stream);
+  } catch (const std::exception& e) {
+    return fail(SG_ERR_OOM, std::string("host allocation: ") + e.what());
+  }
+}
+
+int sg_context_last_stats(sg_context* c, sg_stats* out) {
+  if (!c || !out) return fail(SG_ERR_INVALID, "null argument");
+  std::lock_guard<std::mutex> g(c->mu);
+  *out = c->ctx.ws.last;
+  return SG_OK;
 }
 
 int sg_route(sg_index* h, uint32_t nq, const float* q256, const sg_params* params,
@@ -1080,9 +1179,10 @@ int sg_route(sg_index* h, uint32_t nq, const float* q256, const sg_params* param
   cudaStream_t st = h->def.stream;
   CK(cudaMemsetAsync(w.counters, 0, 32, st));
   sg::launch_prep(h->ix, w, nq, st);
-  CK(sg::launch_route_scores(h->ix, w, nq, h->ix.route_precision, st));
-  sg::launch_route_select(h->ix, w, nq, *params, h->ix.route_precision, h->cfg.chunk_blocks,
-                          h->cfg.seed_blocks, true, st);
+  const sg::Config cfg = sg::index_config(h);
+  CK(sg::launch_route_scores(h->ix, w, nq, cfg.route_precision, st));
+  sg::launch_route_select(h->ix, w, nq, *params, cfg.route_precision, cfg.chunk_blocks, cfg.seed_blocks,
+                          true, st);
   CK(cudaGetLastError());
   const uint32_t P = std::min<uint32_t>(params->nprobe, h->ix.k);
   if (P) {
@@ -1113,7 +1213,7 @@ int sg_route_scores(sg_index* h, uint32_t nq, const float* q256, float* out_scor
   sg::Workspace& w = h->def.ws;
   cudaStream_t st = h->def.stream;
   CK(cudaMemsetAsync(w.counters, 0, 32, st));
-  CK(sg::launch_route_scores(h->ix, w, nq, h->ix.route_precision, st));
+  CK(sg::launch_route_scores(h->ix, w, nq, sg::index_config(h).route_precision, st));
   CK(cudaGetLastError());
   uint32_t status = 0;
   CK(cudaMemcpyAsync(out_scores, w.scores, (size_t)nq * h->ix.k * 4, cudaMemcpyDeviceToHost, st));
@@ -1133,14 +1233,15 @@ int sg_candidates(sg_index* h, uint32_t nq, const float* q256, const sg_params* 
   if (nq == 0) return SG_OK;
   CK(cudaSetDevice(h->ix.device));
   const sg_params& p = *params;
-  uint32_t cap = full_cap(h, p, 1);
+  const sg::Config cfg = sg::index_config(h);
+  uint32_t cap = full_cap(h, cfg, p, 1);
   for (uint32_t q0 = 0; q0 < nq; q0++) {
     // one query at a time with the exact buffer bound: this entry point is for parity checks
     if ((rc = ensure_ws(h, h->def, 1, p, cap))) return rc;
     if ((rc = stage_inputs(h->def, 1, nullptr, q256 + (size_t)q0 * SG_PDIM, false))) return rc;
     const uint64_t* d_allow;
     if ((rc = stage_allow(h->def, allow_bits, allow_words, false, &d_allow))) return rc;
-    if ((rc = run_pipeline(h, h->def, 1, p, true, d_allow, allow_words, kToCandidates, false))) return rc;
+    if ((rc = run_pipeline(h, cfg, h->def, 1, p, true, d_allow, allow_words, kToCandidates, false))) return rc;
     sg::Workspace& w = h->def.ws;
     const uint32_t c = std::max<uint32_t>(p.cand, 1);
     if (p.cand) {
@@ -1175,6 +1276,144 @@ int sg_candidates(sg_index* h, uint32_t nq, const float* q256, const sg_params* 
     }
   }
   return SG_OK;
+}
+
+int sg_candidates_probes(sg_index* h, uint32_t nq, const float* q256, const float* probe_scores,
+                         const uint32_t* probe_clusters, const uint32_t* probe_counts, const sg_params* params,
+                         const uint64_t* allow_bits, uint64_t allow_words, float* out_est, uint32_t* out_ids,
+                         float* out_err, uint32_t* out_counts) {
+  if (!h || !params || (nq && (!q256 || !probe_counts || !out_counts)))
+    return fail(SG_ERR_INVALID, "null argument");
+  int rc;
+  if ((rc = check_params(h, params))) return rc;
+  if (nq == 0) return SG_OK;
+  const sg_params& p = *params;
+  const uint32_t P = std::min<uint32_t>(p.nprobe, h->ix.k);
+  for (uint32_t q = 0; q < nq; q++) {
+    if (probe_counts[q] > P) return fail(SG_ERR_INVALID, "a probe list is longer than min(nprobe, k)");
+    for (uint32_t r = 0; r < probe_counts[q]; r++)
+      if (probe_clusters[(size_t)q * P + r] >= h->ix.k) return fail(SG_ERR_INVALID, "probe cluster >= k");
+  }
+  if (P && (!probe_scores || !probe_clusters)) return fail(SG_ERR_INVALID, "null probe list");
+  if (p.cand && (!out_est || !out_ids || !out_err)) return fail(SG_ERR_INVALID, "null output");
+  std::lock_guard<std::mutex> g(h->mu);
+  try {
+    CK(cudaSetDevice(h->ix.device));
+    const sg::Config cfg = sg::index_config(h);
+    sg::Ctx& c = h->def;
+    sg::Workspace& w = c.ws;
+    const uint32_t cw = std::max<uint32_t>(p.cand, 1);
+    RoutePlan rp;
+    rp.given = true;
+    // queries [q0, q0 + m) with per-query buffers of `cap` entries; their overflow flags in ovf
+    auto run = [&](uint32_t q0, uint32_t m, uint32_t cap, uint8_t* ovf) -> int {
+      int rc2;
+      if ((rc2 = ensure_ws(h, c, m, p, cap))) return rc2;
+      if ((rc2 = stage_inputs(c, m, nullptr, q256 + (size_t)q0 * SG_PDIM, false))) return rc2;
+      if (P) {
+        CK(cudaMemcpyAsync(w.probe_sc, probe_scores + (size_t)q0 * P, (size_t)m * P * 4, cudaMemcpyHostToDevice, c.stream));
+        CK(cudaMemcpyAsync(w.probe_cl, probe_clusters + (size_t)q0 * P, (size_t)m * P * 4, cudaMemcpyHostToDevice,
+                           c.stream));
+      }
+      CK(cudaMemcpyAsync(w.probe_n, probe_counts + q0, (size_t)m * 4, cudaMemcpyHostToDevice, c.stream));
+      const uint64_t* d_allow;
+      if ((rc2 = stage_allow(c, allow_bits, allow_words, false, &d_allow))) return rc2;
+      if ((rc2 = run_pipeline(h, cfg, c, m, p, true, d_allow, allow_words, kToCandidates, false, rp))) return rc2;
+      if (p.cand) {
+        CK(cudaMemcpyAsync(out_est + (size_t)q0 * cw, w.cest, (size_t)m * cw * 4, cudaMemcpyDeviceToHost, c.stream));
+        CK(cudaMemcpyAsync(out_ids + (size_t)q0 * cw, w.cid, (size_t)m * cw * 4, cudaMemcpyDeviceToHost, c.stream));
+        CK(cudaMemcpyAsync(out_err + (size_t)q0 * cw, w.cerr, (size_t)m * cw * 4, cudaMemcpyDeviceToHost, c.stream));
+      }
+      CK(cudaMemcpyAsync(out_counts + q0, w.cn, (size_t)m * 4, cudaMemcpyDeviceToHost, c.stream));
+      CK(cudaMemcpyAsync(ovf, w.overflow, m, cudaMemcpyDeviceToHost, c.stream));
+      uint32_t status = 0;
+      CK(cudaMemcpyAsync(&status, w.counters + 2, 4, cudaMemcpyDeviceToHost, c.stream));
+      CK(cudaStreamSynchronize(c.stream));
+      if (status & sg::kStatusOverflow) return fail(SG_ERR_INVALID, "work queue overflow");
+      if (status & sg::kStatusTimeout) return fail(SG_ERR_DEVICE, "a tensor-core wait ran out (scan)");
+      return SG_OK;
+    };
+    std::vector<uint8_t> ovf(nq);
+    if ((rc = run(0, nq, batch_cap(h, cfg, p, nq), ovf.data()))) return rc;
+    // a query whose buffer filled up runs again alone with its exact bound
+    for (uint32_t q = 0; q < nq; q++) {
+      if (!ovf[q]) continue;
+      uint8_t o1 = 0;
+      if ((rc = run(q, 1, full_cap(h, cfg, p, 1), &o1))) return rc;
+      if (o1) return fail(SG_ERR_INVALID, "candidate buffer overflow at the exact bound");
+    }
+    // the device lists are unordered; Index::candidates returns them in row order
+    for (uint32_t q = 0; q < nq && p.cand; q++) {
+      const uint32_t n = out_counts[q];
+      float* e = out_est + (size_t)q * cw;
+      uint32_t* id = out_ids + (size_t)q * cw;
+      float* er = out_err + (size_t)q * cw;
+      std::vector<uint32_t> ord(n);
+      for (uint32_t i = 0; i < n; i++) ord[i] = i;
+      std::sort(ord.begin(), ord.end(), [&](uint32_t x, uint32_t y) { return id[x] < id[y]; });
+      std::vector<float> e2(n), er2(n);
+      std::vector<uint32_t> id2(n);
+      for (uint32_t i = 0; i < n; i++) {
+        e2[i] = e[ord[i]];
+        id2[i] = id[ord[i]];
+        er2[i] = er[ord[i]];
+      }
+      std::copy(e2.begin(), e2.end(), e);
+      std::copy(id2.begin(), id2.end(), id);
+      std::copy(er2.begin(), er2.end(), er);
+    }
+    return SG_OK;
+  } catch (const std::exception& e) {
+    return fail(SG_ERR_OOM, std::string("host allocation: ") + e.what());
+  }
+}
+
+int sg_rerank(sg_index* h, uint32_t nq, const float* q768, const float* q256, const float* cand_est,
+              const uint32_t* cand_ids, const float* cand_err, const uint32_t* cand_counts, uint32_t cand_stride,
+              const sg_params* params, float* out_scores, uint32_t* out_ids, uint32_t* out_counts) {
+  if (!h || !params || (nq && (!q768 || !cand_counts || !out_counts))) return fail(SG_ERR_INVALID, "null argument");
+  sg_params p = *params;
+  p.cand = cand_stride;
+  int rc;
+  if ((rc = check_params(h, &p))) return rc;
+  if (nq == 0) return SG_OK;
+  if (cand_stride && (!cand_est || !cand_ids)) return fail(SG_ERR_INVALID, "null candidate list");
+  if (p.k && (!out_scores || !out_ids)) return fail(SG_ERR_INVALID, "null output");
+  for (uint32_t q = 0; q < nq; q++) {
+    if (cand_counts[q] > cand_stride) return fail(SG_ERR_INVALID, "a candidate list is longer than its stride");
+    for (uint32_t i = 0; i < cand_counts[q]; i++)
+      if (cand_ids[(size_t)q * cand_stride + i] >= h->ix.n) return fail(SG_ERR_INVALID, "candidate row >= n");
+  }
+  std::lock_guard<std::mutex> g(h->mu);
+  try {
+    CK(cudaSetDevice(h->ix.device));
+    sg::Ctx& c = h->def;
+    sg::Workspace& w = c.ws;
+    if ((rc = ensure_ws(h, c, nq, p, 1))) return rc;
+    if ((rc = stage_inputs(c, nq, q768, q256, false))) return rc;
+    cudaStream_t st = c.stream;
+    if (!q256) sg::launch_prefix(w, nq, st);
+    sg::launch_prep(h->ix, w, nq, st);
+    const size_t nc = (size_t)nq * cand_stride;
+    if (nc) {
+      CK(cudaMemcpyAsync(w.cest, cand_est, nc * 4, cudaMemcpyHostToDevice, st));
+      CK(cudaMemcpyAsync(w.cid, cand_ids, nc * 4, cudaMemcpyHostToDevice, st));
+      if (cand_err) CK(cudaMemcpyAsync(w.cerr, cand_err, nc * 4, cudaMemcpyHostToDevice, st));
+      else CK(cudaMemsetAsync(w.cerr, 0, nc * 4, st));
+    }
+    CK(cudaMemcpyAsync(w.cn, cand_counts, (size_t)nq * 4, cudaMemcpyHostToDevice, st));
+    sg::launch_rerank(h->ix, w, nq, p, st, nullptr, nullptr);
+    CK(cudaGetLastError());
+    if (p.k) {
+      CK(cudaMemcpyAsync(out_scores, w.out_sc, (size_t)nq * p.k * 4, cudaMemcpyDeviceToHost, st));
+      CK(cudaMemcpyAsync(out_ids, w.out_id, (size_t)nq * p.k * 4, cudaMemcpyDeviceToHost, st));
+    }
+    CK(cudaMemcpyAsync(out_counts, w.out_n, (size_t)nq * 4, cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    return SG_OK;
+  } catch (const std::exception& e) {
+    return fail(SG_ERR_OOM, std::string("host allocation: ") + e.what());
+  }
 }
 
 int sg_filter_new(sg_index* h, const uint64_t* allow_bits, uint64_t allow_words, sg_filter** out) {
@@ -1255,21 +1494,59 @@ int sg_filter_search(sg_index* h, const sg_filter* f, int plan, uint64_t expand_
   const int resolved = sg_plan_resolve(plan, f->nrows, h->ix.n);
   if (plan == SG_PLAN_AUTO && resolved == SG_PLAN_EXPAND) expand_target = SG_EXPAND_TARGET;
   std::lock_guard<std::mutex> g(h->mu);
+  const sg::Config cfg = sg::index_config(h);
   try {
     if (resolved == SG_PLAN_BRUTE)
-      return brute_impl(h, h->def, f, nq, q768, q256, *params, out_scores, out_ids, out_counts, timing);
+      return brute_impl(h, cfg, h->def, f, nq, q768, q256, *params, out_scores, out_ids, out_counts, timing);
     if (resolved == SG_PLAN_POST)
-      return search_impl(h, h->def, nq, q768, q256, *params, f->allow, f->words, out_scores, out_ids,
+      return search_impl(h, cfg, h->def, nq, q768, q256, *params, f->allow, f->words, out_scores, out_ids,
                          out_counts, timing, false, true);
     if (h->ix.k > sg::kExpandMaxK)
       return fail(SG_ERR_UNSUPPORTED, "plan Expand needs k <= 16384 clusters");
     RoutePlan rp;
     rp.per_cluster = f->per_cluster;
     rp.target = expand_target;
-    return search_impl(h, h->def, nq, q768, q256, *params, f->allow, f->words, out_scores, out_ids,
+    return search_impl(h, cfg, h->def, nq, q768, q256, *params, f->allow, f->words, out_scores, out_ids,
                        out_counts, timing, false, true, rp);
   } catch (const std::exception& e) {
     return fail(SG_ERR_OOM, e.what());
+  }
+}
+
+int sg_flat_hamming(sg_index* h, uint32_t nq, const float* q768, const float* q256, uint32_t cand,
+                    uint32_t k, float* out_scores, uint32_t* out_ids, uint32_t* out_counts) {
+  if (!h || (nq && (!q768 || !out_counts || (k && (!out_scores || !out_ids)))))
+    return fail(SG_ERR_INVALID, "null argument");
+  if (!h->ix.codes) return fail(SG_ERR_UNSUPPORTED, "the flat Hamming baseline needs codes.bin");
+  if (cand > sg::kMaxCand || k > sg::kMaxCand) return fail(SG_ERR_INVALID, "cand and k must be <= 4096");
+  if (nq == 0) return SG_OK;
+  if (k == 0 || cand == 0) {
+    memset(out_counts, 0, (size_t)nq * 4);
+    return SG_OK;
+  }
+  std::lock_guard<std::mutex> g(h->mu);
+  try {
+    CK(cudaSetDevice(h->ix.device));
+    sg_params p;
+    memset(&p, 0, sizeof p);
+    p.nprobe = 1;
+    p.cand = cand;
+    p.k = k;
+    int rc;
+    if ((rc = ensure_ws(h, h->def, nq, p, 1))) return rc;
+    if ((rc = stage_inputs(h->def, nq, q768, q256, false))) return rc;
+    sg::Workspace& w = h->def.ws;
+    cudaStream_t st = h->def.stream;
+    if (!q256) sg::launch_prefix(w, nq, st);
+    sg::launch_flat_hamming(h->ix, w, nq, cand, k, st);
+    CK(cudaGetLastError());
+    CK(cudaMemcpyAsync(out_scores, w.out_sc, (size_t)nq * k * 4, cudaMemcpyDeviceToHost, st));
+    CK(cudaMemcpyAsync(out_ids, w.out_id, (size_t)nq * k * 4, cudaMemcpyDeviceToHost, st));
+    CK(cudaMemcpyAsync(out_counts, w.out_n, (size_t)nq * 4, cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    return SG_OK;
+  } catch (const std::exception& e) {
+    return fail(SG_ERR_OOM, std::string("host allocation: ") + e.what());
   }
 }
 
@@ -1331,16 +1608,18 @@ int sg_lut_scan(uint32_t groups, const uint8_t* tables, const uint8_t* blocks, u
 
 int sg_get_tuning(const sg_index* h, sg_tuning* out) {
   if (!h || !out) return fail(SG_ERR_INVALID, "null argument");
-  out->tc_min_queries = h->cfg.tc_min_queries;
-  out->chunk_blocks = h->cfg.chunk_blocks;
-  out->scan_ctas_per_sm = h->cfg.scan_ctas_per_sm;
-  out->seed_blocks = h->cfg.seed_blocks;
-  out->tc_split = h->cfg.tc_split;
+  const sg::Config cfg = sg::index_config(h);
+  out->tc_min_queries = cfg.tc_min_queries;
+  out->chunk_blocks = cfg.chunk_blocks;
+  out->scan_ctas_per_sm = cfg.scan_ctas_per_sm;
+  out->seed_blocks = cfg.seed_blocks;
+  out->tc_split = cfg.tc_split;
   return SG_OK;
 }
 
 int sg_set_tuning(sg_index* h, const sg_tuning* t) {
   if (!h || !t) return fail(SG_ERR_INVALID, "null argument");
+  std::lock_guard<std::mutex> g(h->cfg_mu);
   // chunks of at least the small-batch chunk keep the work-queue capacity bound valid
   if (t->chunk_blocks < h->cfg.small_chunk_blocks || t->chunk_blocks > sg::kMaxChunkBlocks)
     return fail(SG_ERR_INVALID, "chunk_blocks must lie in [small chunk, 512]");
@@ -1349,7 +1628,6 @@ int sg_set_tuning(sg_index* h, const sg_tuning* t) {
   if (t->scan_ctas_per_sm < 1 || t->scan_ctas_per_sm > 2) return fail(SG_ERR_INVALID, "scan_ctas_per_sm: 1 or 2");
   if (t->tc_min_queries == 0) return fail(SG_ERR_INVALID, "tc_min_queries must be >= 1");
   if (t->tc_split > 4096) return fail(SG_ERR_INVALID, "tc_split must be <= 4096");
-  std::lock_guard<std::mutex> g(h->mu);
   h->cfg.tc_min_queries = t->tc_min_queries;
   h->cfg.chunk_blocks = t->chunk_blocks;
   h->cfg.scan_ctas_per_sm = t->scan_ctas_per_sm;
@@ -1365,7 +1643,8 @@ int sg_set_tuning(sg_index* h, const sg_tuning* t) {
 int sg_autotune(sg_index* h, uint32_t nq, const float* d_q768, const float* d_q256, const sg_params* params,
                 uint32_t reps, sg_tuning* out, float* out_ms) {
   if (!h || !params || !d_q768 || nq == 0) return fail(SG_ERR_INVALID, "null argument or empty batch");
-  if (nq < h->cfg.small_batch) return fail(SG_ERR_INVALID, "the autotuner tunes batches of >= 64 queries");
+  if (nq < sg::index_config(h).small_batch)
+    return fail(SG_ERR_INVALID, "the autotuner tunes batches of >= 64 queries");
   int rc;
   if ((rc = check_params(h, params))) return rc;
   CK(cudaSetDevice(h->ix.device));
@@ -1381,10 +1660,10 @@ int sg_autotune(sg_index* h, uint32_t nq, const float* d_q768, const float* d_q2
     float best = INFINITY;
     for (uint32_t r = 0; r < reps + 1; r++) {  // the first run warms the workspace
       std::lock_guard<std::mutex> g(h->mu);
-      const bool was = h->timing_on;
-      h->timing_on = true;
-      int rc2 = search_impl(h, h->def, nq, d_q768, d_q256, *params, nullptr, 0, osc, oid, on, nullptr, true);
-      h->timing_on = was;
+      sg::Config cfg = sg::index_config(h);
+      cfg.timing = true;
+      int rc2 = search_impl(h, cfg, h->def, nq, d_q768, d_q256, *params, nullptr, 0, osc, oid, on, nullptr,
+                            true);
       if (rc2) return rc2;
       if (r > 0) best = std::min(best, h->def.ws.last.ms_total);
     }
@@ -1397,7 +1676,7 @@ int sg_autotune(sg_index* h, uint32_t nq, const float* d_q768, const float* d_q2
   if ((rc = time_batch(&base_ms))) goto done;
   cur = base_ms;
   {
-    const uint32_t tmins[] = {2, 3, 4, 6, 8, 12, 16, 24, 32, 0xFFFFFFFFu};
+    const uint32_t tmins[] = {1, 2, 3, 4, 6, 8, 12, 16, 24, 32, 0xFFFFFFFFu};
     const uint32_t chunks[] = {64, 128, 256, 512};
     const uint32_t seeds[] = {128, 256, 512};
     const uint32_t ctas[] = {1, 2};
@@ -1407,7 +1686,7 @@ int sg_autotune(sg_index* h, uint32_t nq, const float* d_q768, const float* d_q2
       uint32_t best_v = keep;
       for (size_t i = 0; i < nv; i++) {
         if (vals[i] == keep) continue;
-        if (field == &t.chunk_blocks && vals[i] < h->cfg.small_chunk_blocks) continue;
+        if (field == &t.chunk_blocks && vals[i] < sg::index_config(h).small_chunk_blocks) continue;
         *field = vals[i];
         int rc2 = sg_set_tuning(h, &t);
         if (rc2) return rc2;

@@ -95,6 +95,7 @@ class SgIvfArrays(ctypes.Structure):
         ("rerank", c_void_p),
         ("norm256", c_void_p),
         ("quant_scale", c_void_p),
+        ("codes", c_void_p),
     ]
 
 
@@ -112,6 +113,7 @@ ARRAY_FIELDS = {
     "rerank": np.int8,
     "norm256": np.float32,
     "quant_scale": np.float32,
+    "codes": np.uint8,
 }
 
 
@@ -124,15 +126,16 @@ def ptr(a: np.ndarray | None) -> c_void_p | None:
     return c_void_p(a.ctypes.data)
 
 
-def make_arrays(arrays: dict) -> tuple[SgIvfArrays, list]:
+def make_arrays(arrays: dict, codes: bool = False) -> tuple[SgIvfArrays, list]:
     """Fills an SgIvfArrays from a dict of numpy arrays; returns it with the arrays it points
-    into (the caller keeps them alive while the struct is used)."""
+    into (the caller keeps them alive while the struct is used). The rows' global sign codes
+    (codes.bin) are passed only with codes=True: only the flat Hamming baseline reads them."""
     keep = []
     st = SgIvfArrays()
     st.n = int(arrays["n"])
     st.k = int(arrays["k"])
     for name, dt in ARRAY_FIELDS.items():
-        a = arrays.get(name)
+        a = arrays.get(name) if (name != "codes" or codes) else None
         if a is not None:
             a = np.ascontiguousarray(a, dtype=dt)
             keep.append(a)
@@ -247,10 +250,18 @@ EXPORTS = [
     "sg_last_stats",
     "sg_search",
     "sg_search_device",
+    "sg_context_open",
+    "sg_context_close",
+    "sg_search_ctx",
+    "sg_search_device_ctx",
+    "sg_context_last_stats",
     "sg_search_noalloc",
+    "sg_flat_hamming",
     "sg_route",
     "sg_route_scores",
     "sg_candidates",
+    "sg_candidates_probes",
+    "sg_rerank",
     "sg_filter_new",
     "sg_filter_info",
     "sg_filter_free",

@@ -214,8 +214,10 @@ def rabitq_encode(xr: torch.Tensor, cr: torch.Tensor):
 # ---- build (src/ivf.rs:268-395) ------------------------------------------------------------------
 def build_ivf(corpus: dict, k: int, sample_n: int = 262144, iters: int = 10,
               balance: float | None = None, soar_lambda: float | None = 1.0,
-              device: str = "cpu", chunk: int = 131072) -> dict:
-    """Trains and packs a RaBitQ IVF index over corpus arrays; returns host numpy arrays."""
+              device: str = "cpu", chunk: int = 131072, rabitq: bool = True) -> dict:
+    """Trains and packs an IVF index over corpus arrays; returns host numpy arrays. With
+    rabitq=False every slot holds its row's global sign code (codes.bin) and the index has no
+    rotation.f32 / factors.f32, as ivf::build(.., rabitq: false) writes (src/ivf.rs:366-372)."""
     dev = torch.device(device)
     n = int(corpus["n"])
     rer = corpus["rerank"]
@@ -260,9 +262,14 @@ def build_ivf(corpus: dict, k: int, sample_n: int = 262144, iters: int = 10,
                 pairs = [(prim, rows), (sec, rows)]
             else:
                 pairs = [(prim, rows)]
-        xr = rotate(signs, x)
+        xr = rotate(signs, x) if rabitq else None
+        gcode = None if rabitq else torch.as_tensor(corpus["codes"][s:e], device=dev)
         for c, r in pairs:
-            code, mul, err = rabitq_encode(xr, cents_rot[c])
+            if rabitq:
+                code, mul, err = rabitq_encode(xr, cents_rot[c])
+            else:
+                code = gcode
+                mul = err = torch.zeros(e - s, device=dev)
             slot_cluster.append(c)
             slot_row.append(r)
             slot_code.append(code)
@@ -302,8 +309,8 @@ def build_ivf(corpus: dict, k: int, sample_n: int = 262144, iters: int = 10,
         "block_off": block_off.cpu().numpy().astype(np.uint64),
         "ids": ids.cpu().numpy().astype(np.uint32),
         "blocks": blocks.cpu().numpy().reshape(-1),
-        "factors": factors.cpu().numpy().reshape(-1),
-        "rotation": signs.cpu().numpy(),
+        "factors": factors.cpu().numpy().reshape(-1) if rabitq else None,
+        "rotation": signs.cpu().numpy() if rabitq else None,
         "tier2_sigma": sigma.cpu().numpy(),
         "tier2_codes": t2_codes,
         "tier2_norm": t2_norm,

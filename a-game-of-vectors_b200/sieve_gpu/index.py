@@ -161,8 +161,10 @@ class Index:
         return cls(h, device)
 
     @classmethod
-    def from_arrays(cls, arrays: dict, device: int = 0) -> "Index":
-        st, keep = make_arrays(arrays)
+    def from_arrays(cls, arrays: dict, device: int = 0, codes: bool = False) -> "Index":
+        """Uploads the arrays; codes=True also uploads the rows' sign codes (codes.bin) for
+        flat_hamming."""
+        st, keep = make_arrays(arrays, codes=codes)
         h = c_void_p()
         check(lib().sg_open_ivf_arrays(byref(st), c_int(device), byref(h)))
         del keep
@@ -256,6 +258,19 @@ class Index:
                                      c_void_p(d_out_scores), c_void_p(d_out_ids), c_void_p(d_out_counts),
                                      c_void_p(stream)))
 
+    # flat_hamming_rerank of the search binary (src/bin/search.rs:251-269)
+    def flat_hamming(self, q768, q256=None, cand: int = 1000, k: int = 100):
+        """The flat Hamming baseline: (scores [nq, k], ids [nq, k], counts [nq]), best first."""
+        q768 = np.ascontiguousarray(q768, np.float32).reshape(-1, _abi.DIM)
+        nq = q768.shape[0]
+        q2 = None if q256 is None else _f32(q256, nq, _abi.PDIM)
+        sc = np.zeros((nq, max(k, 1)), np.float32)
+        ids = np.zeros((nq, max(k, 1)), np.uint32)
+        cnt = np.zeros(nq, np.uint32)
+        check(lib().sg_flat_hamming(self._h, c_uint32(nq), ptr(q768), ptr(q2), c_uint32(cand), c_uint32(k),
+                                    ptr(sc), ptr(ids), ptr(cnt)))
+        return sc[:, :k], ids[:, :k], cnt
+
     # Index::route (src/ivf.rs:589-613)
     def route(self, q256, params: Params):
         q = np.ascontiguousarray(q256, np.float32).reshape(-1, _abi.PDIM)
@@ -293,6 +308,59 @@ class Index:
                                   ptr(cnt)))
         return [(est[i, : cnt[i]], ids[i, : cnt[i]], err[i, : cnt[i]]) for i in range(nq)]
 
+    # Index::candidates over given probe lists (src/ivf.rs:647-729), a shard's phase 1
+    def candidates_probes(self, q256, probes, params: Params, allow=None):
+        """probes: per query (centroid scores, clusters) in scan order. Returns per query
+        (estimates, rows, error widths) in row order."""
+        q = np.ascontiguousarray(q256, np.float32).reshape(-1, _abi.PDIM)
+        nq = q.shape[0]
+        P = max(min(params.nprobe, self.k), 1)
+        ps = np.zeros((nq, P), np.float32)
+        pc = np.zeros((nq, P), np.uint32)
+        pn = np.zeros(nq, np.uint32)
+        for i, (sc, cl) in enumerate(probes):
+            pn[i] = len(cl)
+            ps[i, : len(cl)] = sc
+            pc[i, : len(cl)] = cl
+        c = max(params.cand, 1)
+        est = np.zeros((nq, c), np.float32)
+        ids = np.zeros((nq, c), np.uint32)
+        err = np.zeros((nq, c), np.float32)
+        cnt = np.zeros(nq, np.uint32)
+        al = None if allow is None else np.ascontiguousarray(allow, np.uint64)
+        p = params.to_c()
+        check(lib().sg_candidates_probes(self._h, c_uint32(nq), ptr(q), ptr(ps), ptr(pc), ptr(pn), byref(p),
+                                         ptr(al), c_uint64(0 if al is None else al.size), ptr(est), ptr(ids),
+                                         ptr(err), ptr(cnt)))
+        return [(est[i, : cnt[i]], ids[i, : cnt[i]], err[i, : cnt[i]]) for i in range(nq)]
+
+    # Index::rerank of given candidates (src/ivf.rs:734-815), a shard's phase 2
+    def rerank(self, q768, q256, cands, params: Params):
+        """cands: per query (estimates, rows, error widths or None). Returns (scores [nq, k],
+        ids [nq, k], counts [nq]) best first."""
+        q768 = np.ascontiguousarray(q768, np.float32).reshape(-1, _abi.DIM)
+        nq = q768.shape[0]
+        q2 = None if q256 is None else _f32(q256, nq, _abi.PDIM)
+        stride = max([len(c[1]) for c in cands] + [1])
+        est = np.zeros((nq, stride), np.float32)
+        ids = np.zeros((nq, stride), np.uint32)
+        err = np.zeros((nq, stride), np.float32)
+        cn = np.zeros(nq, np.uint32)
+        for i, (e, r, w) in enumerate(cands):
+            cn[i] = len(r)
+            est[i, : len(r)] = e
+            ids[i, : len(r)] = r
+            if w is not None:
+                err[i, : len(r)] = w
+        p = params.to_c()
+        k = max(p.k, 1)
+        sc = np.zeros((nq, k), np.float32)
+        oid = np.zeros((nq, k), np.uint32)
+        cnt = np.zeros(nq, np.uint32)
+        check(lib().sg_rerank(self._h, c_uint32(nq), ptr(q768), ptr(q2), ptr(est), ptr(ids), ptr(err), ptr(cn),
+                              c_uint32(stride), byref(p), ptr(sc), ptr(oid), ptr(cnt)))
+        return sc[:, : p.k], oid[:, : p.k], cnt
+
     # rabitq::Query::new (src/rabitq.rs:119-125)
     def query_prep(self, q256):
         q = np.ascontiguousarray(q256, np.float32).reshape(-1, _abi.PDIM)
@@ -301,6 +369,69 @@ class Index:
         sc, bi, a, b = (np.zeros(nq, np.float32) for _ in range(4))
         check(lib().sg_query_prep(self._h, c_uint32(nq), ptr(q), ptr(tables), ptr(sc), ptr(bi), ptr(a), ptr(b)))
         return tables, sc, bi, a, b
+
+
+class Context:
+    """ivf::Scratch (src/ivf.rs:497-513) on the GPU: one thread's stream, device scratch and captured
+    graphs over a shared Index. Threads that each search through their own Context run at once
+    (sg_search on the Index itself serialises its callers); a Context serves one call at a time."""
+
+    def __init__(self, index: Index):
+        self.index = index
+        self._c = c_void_p()
+        check(lib().sg_context_open(index._h, byref(self._c)))
+
+    def close(self) -> None:
+        if self._c:
+            check(lib().sg_context_close(self._c))
+            self._c = None
+
+    def __enter__(self) -> "Context":
+        return self
+
+    def __exit__(self, *exc) -> None:
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # Index::search(&self, &Corpus, q768, q256, &Params, &mut Scratch, &mut Timing), batched
+    def search_batch(self, q768, q256=None, params: Params | None = None, allow=None,
+                     timing: Timing | None = None):
+        """Returns (scores [nq, k], ids [nq, k], counts [nq]) best first per query."""
+        q768 = np.ascontiguousarray(q768, np.float32).reshape(-1, _abi.DIM)
+        nq = q768.shape[0]
+        q2 = None if q256 is None else _f32(q256, nq, _abi.PDIM)
+        p = params.to_c()
+        k = max(p.k, 1)
+        sc = np.zeros((nq, k), np.float32)
+        ids = np.zeros((nq, k), np.uint32)
+        cnt = np.zeros(nq, np.uint32)
+        al = None if allow is None else np.ascontiguousarray(allow, np.uint64)
+        t = SgTiming()
+        check(lib().sg_search_ctx(self._c, c_uint32(nq), ptr(q768), ptr(q2), byref(p), ptr(al),
+                                  c_uint64(0 if al is None else al.size), ptr(sc), ptr(ids), ptr(cnt),
+                                  byref(t)))
+        if timing is not None:
+            timing.add(t)
+        return sc[:, : p.k], ids[:, : p.k], cnt
+
+    def search_device(self, nq: int, d_q768: int, d_q256: int | None, params: Params,
+                      d_out_scores: int, d_out_ids: int, d_out_counts: int, stream: int = 0) -> None:
+        """sg_search_device_ctx over raw device pointers."""
+        p = params.to_c()
+        check(lib().sg_search_device_ctx(self._c, c_uint32(nq), c_void_p(d_q768),
+                                         c_void_p(d_q256) if d_q256 else None, byref(p), None, c_uint64(0),
+                                         c_void_p(d_out_scores), c_void_p(d_out_ids), c_void_p(d_out_counts),
+                                         c_void_p(stream)))
+
+    def last_stats(self) -> dict:
+        st = SgStats()
+        check(lib().sg_context_last_stats(self._c, byref(st)))
+        return {name: getattr(st, name) for name, _ in SgStats._fields_ if not name.startswith("reserved")}
 
 
 def lut_scan(tables: np.ndarray, blocks: np.ndarray) -> np.ndarray:

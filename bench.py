@@ -157,6 +157,44 @@ def build_workload(name: str, device: str, rows: int | None, nq_pool: int, n_eva
     return w, arrays, queries, gt, {"ingest_s": round(t_ingest, 1), "build_s": round(t_build, 1)}
 
 
+def prefix256(q768: np.ndarray) -> np.ndarray:
+    """quant::prefix (src/quant.rs:17-20) of each row: the first 256 dims renormalised."""
+    p = q768[:, :256].astype(np.float32)
+    return (p / np.sqrt((p * p).sum(1, keepdims=True))).astype(np.float32)
+
+
+def probe_stats(index, q768: np.ndarray, params, batch: int) -> tuple[dict, list]:
+    """Probe counts of the queries (Index::route with the search's own margin, budget and cap)
+    and, per `batch`-query window, the distinct clusters the window probes."""
+    routes = index.route(prefix256(q768), params)
+    counts = np.array([len(c) for _, c in routes])
+    stats = {"min": int(counts.min()), "median": float(np.median(counts)), "max": int(counts.max()),
+             "mean": float(counts.mean())}
+    return stats, [c for _, c in routes]
+
+
+def distinct_slots(routes: list, lo: int, batch: int, slots_per_cluster: np.ndarray) -> int:
+    """Slots of the distinct clusters queries [lo, lo + batch) probe: what a batch must read at
+    least once."""
+    cl = np.unique(np.concatenate(routes[lo:lo + batch]))
+    return int(slots_per_cluster[cl].sum())
+
+
+def parity_check(gpu_ids, gpu_sc, gpu_cnt, cpu: dict) -> dict:
+    """Per query, the GPU's (score, row) list against the CPU leg's, bit for bit. A query whose
+    lists differ is counted as tied, not mismatched, when a cut on its oracle path was tied (the
+    reference leaves the survivors of a tie unspecified)."""
+    m = min(len(gpu_cnt), len(cpu["cnt"]))
+    same = np.array([int(gpu_cnt[i]) == int(cpu["cnt"][i])
+                     and np.array_equal(gpu_ids[i, :gpu_cnt[i]], cpu["ids"][i, :cpu["cnt"][i]])
+                     and np.array_equal(gpu_sc[i, :gpu_cnt[i]], cpu["sc"][i, :cpu["cnt"][i]])
+                     for i in range(m)], dtype=bool)
+    tied = cpu["tied"][:m]
+    return {"queries": int(m), "mismatched": int((~same & ~tied).sum()),
+            "tied_boundary": int(tied.sum()), "tied_and_differing": int((~same & tied).sum()),
+            "rule": "bit-exact (score, row) lists; canonical ties (score desc, row asc)"}
+
+
 def recall10(ids: np.ndarray, cnt: np.ndarray, gt: np.ndarray) -> float:
     r = []
     for i in range(gt.shape[0]):
@@ -213,10 +251,11 @@ def cpu_reference(arrays, q768_host: np.ndarray, params, seconds: float, threads
     n = int(max(probe, seconds / max(per_q, 1e-9)))
     sel = np.arange(n) % q768_host.shape[0]
     t = time.perf_counter()
-    s, o, c, scanned = oi.search_batch(q768_host[sel], q256[sel], p, threads=threads)
+    s, o, c, scanned, tied = oi.search_batch(q768_host[sel], q256[sel], p, threads=threads, tied=True)
     dt = time.perf_counter() - t
     k = min(n, q768_host.shape[0])
-    return {"qps": n / dt, "queries": n, "seconds": dt, "ids": o[:k], "cnt": c[:k]}
+    return {"qps": n / dt, "queries": n, "seconds": dt, "ids": o[:k], "cnt": c[:k], "sc": s[:k],
+            "tied": tied[:k]}
 
 
 def serve_load(index, arrays, queries_host: np.ndarray, params, rates, seconds: float, seed: int = 7,
@@ -298,10 +337,10 @@ def serve_load(index, arrays, queries_host: np.ndarray, params, rates, seconds: 
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=200)
-    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="c2", choices=sorted(WORKLOADS))
+    ap.add_argument("--workload", default="c3", choices=sorted(WORKLOADS))
     ap.add_argument("--rows", type=int, default=None, help="override the corpus size (smoke runs)")
     ap.add_argument("--config", default=None, help="search config nprobe:cand:rerank[:...]")
     ap.add_argument("--batch", type=int, default=4096)
@@ -309,8 +348,9 @@ def main():
     ap.add_argument("--eval", type=int, default=1000, help="queries with exact ground truth")
     ap.add_argument("--plain", type=int, default=512, help="queries timed one per launch")
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
-    ap.add_argument("--serve", default="20000,50000,70000,85000",
-                    help="Poisson arrival rates (queries/s) for the serving loop; empty: skip")
+    ap.add_argument("--serve", default=None,
+                    help="Poisson arrival rates (queries/s) for the serving loop (default: the "
+                         "workload's); empty: skip")
     ap.add_argument("--serve-seconds", type=float, default=2.0)
     ap.add_argument("--no-tune", action="store_true", help="keep the default shapes (no autotuner)")
     args = ap.parse_args()
@@ -340,9 +380,11 @@ def main():
     label, params = parse_config(config, w["k"])
     params.k = 10
     threads = os.cpu_count() or 1
+    # the workload and search as stated; build times and tuning are outcomes, reported apart
     cfg = {"workload": f"{args.workload}: {w['n']} x 768, {w['centers']} centres, {w['k']} clusters",
            "search": config, "batch": args.batch, "route": args.route, "queries_pool": nq_pool,
-           "l2": "inputs larger than L2 (index and per-batch scan far above 126 MB)", **build_info}
+           "l2": "inputs larger than L2 (index and per-batch scan far above 126 MB)"}
+    metric = "QPS at R@10>=0.90 (p50/p99 ms, scan GB/s vs HBM peak)"
 
     if args.impl == "reference":
         q_host = queries.cpu().numpy()
@@ -354,13 +396,17 @@ def main():
             if i >= args.warmup:
                 times.append(res["qps"])
         qps = float(np.mean(times))
-        rec = recall10(res["ids"][: gt.shape[0]], res["cnt"][: gt.shape[0]], gt[: res["ids"].shape[0]])
-        line = {"metric": "QPS at R@10>=0.90 (p50/p99 ms, scan GB/s vs HBM peak)", "impl": "reference",
+        m = min(res["ids"].shape[0], gt.shape[0])
+        rec = recall10(res["ids"][:m], res["cnt"][:m], gt[:m])
+        line = {"metric": metric, "impl": "reference",
                 "value": qps, "unit": "queries/s", "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-                "dtype": "f32/u8/i8", "data": "synthetic", "config": cfg, "recall_at_10": rec,
+                "dtype": "u8 LUT / f32 estimate / i8 rerank", "data": "synthetic", "config": cfg,
+                "recall_at_10": rec, "build": build_info,
                 "cpu_baseline": {"value": qps, "unit": "queries/s", "cores": threads, "kind": "port",
-                                 "sample": f"{res['queries']} queries per step on {threads} threads"},
+                                 "sample": f"{res['queries']} queries per step on {threads} threads "
+                                           f"(the reference's portable path restated in C, "
+                                           f"-march=native, OpenMP over queries)"},
                 "e2e": {"value": qps, "unit": "queries/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
         print(json.dumps(line), flush=True)
         return finish(world)
@@ -369,31 +415,42 @@ def main():
     index.set_route_precision(args.route == "bf16")
     index.set_timing(True)
     q768 = queries.to(dev).contiguous()
+    q_pool_host = queries.cpu().numpy()
     B = args.batch
     out_sc = torch.empty((B, params.k), dtype=torch.float32, device=dev)
     out_id = torch.empty((B, params.k), dtype=torch.int32, device=dev)
     out_n = torch.empty((B,), dtype=torch.int32, device=dev)
     stream = torch.cuda.current_stream()
 
-    # recall on the ground-truth queries
-    ev = q768[: args.eval].cpu().numpy()
-    sc, ids, cnt = index.search_batch(ev, None, params)
-    rec = recall10(ids, cnt, gt)
-    rec_i8 = recall10(ids, cnt, int8_truth(arrays, q768[: args.eval]))
-    log(f"{label}: recall@10 {rec:.4f} (float truth), {rec_i8:.4f} (int8 truth)")
+    # recall on the ground-truth queries, against float truth and against exact int8 truth; the
+    # ceiling is exact int8 brute force (the rerank's own arithmetic over every row) scored
+    # against float truth: no candidate list can do better than the rows' own quantisation
+    ev = q_pool_host[: args.eval]
+    ev_sc, ev_ids, ev_cnt = index.search_batch(ev, None, params)
+    rec = recall10(ev_ids, ev_cnt, gt)
+    t8 = int8_truth(arrays, q768[: args.eval])
+    rec_i8 = recall10(ev_ids, ev_cnt, t8)
+    ceiling = recall10(t8, np.full(t8.shape[0], 10), gt)
+    probes, routes = probe_stats(index, q_pool_host, params, B)
+    slots_pc = np.diff(np.asarray(arrays["block_off"], np.int64)) * 32
+    log(f"{label}: recall@10 {rec:.4f} (float truth), {rec_i8:.4f} (int8 truth), int8 ceiling "
+        f"{ceiling:.4f}; probes {probes}")
+
+    def window(i):
+        return (i * B) % (nq_pool - B + 1)
 
     def step(i):
-        lo = (i * B) % (nq_pool - B + 1)
-        index.search_device(B, q768[lo].data_ptr(), None, params, out_sc.data_ptr(), out_id.data_ptr(),
-                            out_n.data_ptr(), stream.cuda_stream)
+        index.search_device(B, q768[window(i)].data_ptr(), None, params, out_sc.data_ptr(),
+                            out_id.data_ptr(), out_n.data_ptr(), stream.cuda_stream)
 
     # the autotuner picks the batched path's shapes on this batch size (untimed; results are
     # identical under every shape)
+    tuning = None
     if B >= 64 and not args.no_tune:
         index.set_timing(False)
-        cfg["tuning"] = index.autotune(B, q768[nq_pool - B].data_ptr(), params, reps=2)
+        tuning = index.autotune(B, q768[nq_pool - B].data_ptr(), params, reps=2)
         index.set_timing(True)
-        log(f"autotune: {cfg['tuning']}")
+        log(f"autotune: {tuning}")
     for i in range(args.warmup):
         step(i)
     torch.cuda.synchronize()
@@ -414,10 +471,16 @@ def main():
     total_ms = max_over_ranks(float(np.sum(step_ms)), world, dev)
     qps = world * args.steps * B / (total_ms / 1e3)
 
-    # the scan kernel: algorithmic bytes over its event-timed duration, per launch
+    # The scan stage's roofline. Algorithmic bytes of one batch: every distinct cluster its queries
+    # probe, read once (32 B code + 8 B factors per slot), plus the row id of every entry admitted
+    # to a candidate buffer (4 B); over the stage's CUDA-event time on the library's stream.
     scan_ms = np.array([s["ms_scan"] for s in stats])
     scanned = np.array([s["scanned"] for s in stats], dtype=np.float64)
-    achieved = float(np.mean(scanned * SCAN_BYTES_PER_SLOT / (scan_ms / 1e3)) / 1e9)
+    dslots = np.array([distinct_slots(routes, window(args.warmup + i), B, slots_pc)
+                       for i in range(args.steps)], dtype=np.float64)
+    buffered = np.array([s["buffered"] for s in stats], dtype=np.float64)
+    alg_bytes = dslots * SCAN_BYTES_PER_SLOT + buffered * 4
+    achieved = float(np.mean(alg_bytes / (scan_ms / 1e3)) / 1e9)
     peaks = measured_peaks()
     peak = peaks.get("hbm_gbs", 6650.0)
     traffic = None
@@ -429,8 +492,8 @@ def main():
                 and t.get("batch") == args.batch and not args.rows):
             traffic = float(t["dram_bytes_per_slot"]) * float(np.mean(scanned))
     stage = {k: round(float(np.mean([s[k] for s in stats])), 4)
-             for k in ("ms_prep", "ms_route_gemm", "ms_route_select", "ms_scan", "ms_cut", "ms_rerank",
-                       "ms_tier2", "ms_total")}
+             for k in ("ms_prep", "ms_route_gemm", "ms_route_select", "ms_seed", "ms_scan", "ms_cut",
+                       "ms_rerank", "ms_tier2", "ms_total")}
 
     # one query per launch (timing off: repeated call shapes replay their captured CUDA graph)
     index.set_timing(False)
@@ -453,7 +516,7 @@ def main():
     host_pool = queries.cpu()
     e2e_s = []
     for i in range(args.warmup + args.steps):
-        lo = (i * B) % (nq_pool - B + 1)
+        lo = window(i)
         qh.copy_(host_pool[lo:lo + B])
         t = time.perf_counter()
         index.search_into(qh.numpy(), params, osc.numpy(), oid.numpy().view(np.uint32), ocn.numpy().view(np.uint32))
@@ -462,25 +525,32 @@ def main():
     e2e_qps = replica_qps(args.steps * B, float(np.sum(e2e_s)), world, dev)
 
     serving = None
-    if args.serve:
-        rates = [float(x) for x in args.serve.split(",") if x]
-        serving = serve_load(index, arrays, queries.cpu().numpy(), params, rates, args.serve_seconds)
+    rates = args.serve if args.serve is not None else wl.get("serve", "")
+    if rates:
+        rates = [float(x) for x in rates.split(",") if x]
+        serving = serve_load(index, arrays, q_pool_host, params, rates, args.serve_seconds)
 
-    cpu = None
+    cpu, parity = None, None
     if rank == 0 and world == 1 and args.cpu_seconds > 0:
-        r = cpu_reference(arrays, queries[: max(args.eval, 256)].cpu().numpy(), params, args.cpu_seconds,
-                          threads)
+        r = cpu_reference(arrays, q_pool_host[: max(args.eval, 256)], params, args.cpu_seconds, threads)
         cpu = {"value": r["qps"], "unit": "queries/s", "cores": threads, "kind": "port",
                "sample": f"{r['queries']} queries of the same workload, {r['seconds']:.1f} s, "
                          f"OpenMP over queries, oracle built -march=native"}
+        parity = parity_check(ev_ids, ev_sc, ev_cnt, r)
+        log(f"parity against the CPU leg: {parity}")
     line = {
-        "metric": "QPS at R@10>=0.90 (p50/p99 ms, scan GB/s vs HBM peak)",
+        "metric": metric,
         "value": qps, "unit": "queries/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": total_ms / args.steps, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "u8 LUT / f32 estimate / i8 rerank", "data": "synthetic",
         "config": cfg, "recall_at_10": rec, "recall_at_10_int8_truth": rec_i8,
+        "recall_ceiling_int8": ceiling,
         "recall_note": "float truth = exact FP32 top-10 over the unit 768-d vectors; int8 truth = "
-                       "exact top-10 of the int8 rerank score over every row",
+                       "exact top-10 of the int8 rerank score over every row; ceiling = that int8 "
+                       "top-10 scored against float truth (the best any candidate list can reach "
+                       "with the corpus's int8 rows)",
+        "probes": probes,
+        "parity": parity,
         "p50_ms": float(np.percentile(step_ms, 50)), "p99_ms": float(np.percentile(step_ms, 99)),
         "latency_note": "batched form: every query of a batch completes with its batch",
         "plain": {"qps": float(1e3 / np.mean(plain_ms)), "p50_ms": float(np.percentile(plain_ms, 50)),
@@ -491,20 +561,25 @@ def main():
                         "Python client, 10% filtered, after 0.5 s of unmeasured warm-up at the same "
                         "rate; latency = sg_server_submit to results on the host, on the library's clock",
         "scanned_per_query": float(np.mean(scanned) / B),
+        "distinct_probed_slots_per_step": float(np.mean(dslots)),
         "retried_queries_per_step": float(np.mean([s["retried"] for s in stats])),
         "roofline": {"bound": "hbm", "kernel": "k_scan_seed + k_scan + k_scan_tc (the scan stage)",
                      "achieved": achieved, "peak": peak,
                      "unit": "GB/s", "frac": achieved / peak,
                      "peak_source": "MEASURED_PEAKS.json hbm_gbs" if "hbm_gbs" in peaks else "fallback",
-                     "traffic": traffic, "bytes_per_slot": SCAN_BYTES_PER_SLOT,
-                     "note": "algorithmic bytes = scanned (query, slot) pairs x 40 B; a batch reads each "
-                             "probed cluster from HBM about once for all its queries, so the algorithmic "
-                             "rate can exceed the copy bandwidth while DRAM traffic (ncu) stays ~3 B/pair"},
+                     "traffic": traffic,
+                     "traffic_frac": (traffic / (float(np.mean(scan_ms)) / 1e3) / 1e9 / peak) if traffic else None,
+                     "bytes": "distinct probed slots x 40 B (32 B code + 8 B factors) + buffered entries "
+                              "x 4 B (row ids), per batch",
+                     "note": "a batch reads each probed cluster once for all its queries; traffic = ncu "
+                             "dram bytes of the scan kernels per batch (profiles/scan_traffic.json)"},
         "cpu_baseline": cpu,
         "e2e": {"value": e2e_qps, "unit": "queries/s", "h2d_bytes_per_step": B * 768 * 4,
                 "d2h_bytes_per_step": B * params.k * 8 + B * 4},
         "gpu_launches": int(sum(s["launches"] for s in stats)),
         "clocks": clocks.summary(),
+        "build": build_info,
+        "tuning": tuning,
     }
     if rank == 0:
         print(json.dumps(line), flush=True)
@@ -553,8 +628,8 @@ def main_bigann(args, rank: int, world: int, local: int, dev: str):
     cfg = {"workload": f"c4: {wl['n']} x 100 int8 (1B shape cut to {wl['n']} rows), "
                        f"{wl['centers']} centres, {wl['k1']}x{wl['k2']} leaves, {wl['bits']}-bit refine",
            "search": config, "batch": args.batch, "queries_pool": nq_pool,
-           "l2": "inputs larger than L2 (records and base far above 126 MB)",
-           "ingest_s": round(t_ingest, 1), "build_s": round(t_build, 1)}
+           "l2": "inputs larger than L2 (records and base far above 126 MB)"}
+    build_info = {"ingest_s": round(t_ingest, 1), "build_s": round(t_build, 1)}
     metric = "QPS at R@10>=0.90 (p50/p99 ms, scan GB/s vs HBM peak)"
     qh_all = queries.cpu().numpy()
 
@@ -585,7 +660,7 @@ def main_bigann(args, rank: int, world: int, local: int, dev: str):
         line = {"metric": metric, "impl": "reference", "value": qps, "unit": "queries/s", "n_gpus": world,
                 "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
                 "vs_baseline": None, "dtype": "i8/u8/f32", "data": "synthetic", "config": cfg,
-                "recall_at_10": rec, "recall_at_10_strict": rec_strict,
+                "recall_at_10": rec, "recall_at_10_strict": rec_strict, "build": build_info,
                 "cpu_baseline": {"value": qps, "unit": "queries/s", "cores": threads, "kind": "port",
                                  "sample": f"{res['queries']} queries per step on {threads} threads"},
                 "e2e": {"value": qps, "unit": "queries/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
@@ -683,6 +758,7 @@ def main_bigann(args, rank: int, world: int, local: int, dev: str):
                 "d2h_bytes_per_step": B * k * 8 + B * 4},
         "gpu_launches": 6 * args.steps * -(-B // min(65535, (1 << 28) // max(int(arrays["k"]), 1))),
         "clocks": clocks.summary(),
+        "build": build_info,
     }
     if rank == 0:
         print(json.dumps(line), flush=True)

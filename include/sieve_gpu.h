@@ -44,6 +44,8 @@ extern "C" {
 #define SG_BLOCK_BYTES 1024 /* GROUPS * 16                                                    */
 #define SG_TIER2_BYTES 64   /* 2-bit middle tier code (src/tier2.rs:7)                        */
 #define SG_PAD 0xFFFFFFFFu  /* id of a padding slot                                           */
+#define SG_COUNT_FAILED 0xFFFFFFFFu /* a device-written result count: the call failed on the GPU
+                                       (see sg_search_noalloc)                                  */
 
 /* ---- ivf::Rerank (src/ivf.rs:425-439) --------------------------------------------------- */
 typedef enum {
@@ -116,8 +118,10 @@ typedef struct sg_index sg_index;
 
 /* Host arrays of an IVF index plus its corpus, laid out exactly as the reference's files
  * (src/ivf.rs:75-90 Corpus::open, src/ivf.rs:553-578 Index::open). Optional members may be
- * NULL: tier2_* (no 2-bit tier), rotation/factors (global sign-code index, unsupported here),
- * norm256 (no prefix rerank). */
+ * NULL: tier2_* (no 2-bit tier), rotation/factors (both NULL: a global sign-code index, whose
+ * slots hold their rows' sign codes, ranked by the u16 LUT score of the unrotated prefix with
+ * ties by row and no error bound, src/ivf.rs:700-717), norm256 (no prefix rerank), codes (no
+ * flat Hamming baseline). */
 typedef struct {
   uint64_t n;                 /* corpus rows                                                   */
   uint32_t k;                 /* clusters                                                      */
@@ -133,6 +137,8 @@ typedef struct {
   const int8_t* rerank;       /* rerank.i8       [n * 768]                                     */
   const float* norm256;       /* norm256.f32     [n]                                           */
   const float* quant_scale;   /* quant.f32       [768]                                         */
+  const uint8_t* codes;       /* codes.bin       [n * 32] global sign codes of the rows
+                                 (nullable: only sg_flat_hamming reads them)                 */
 } sg_ivf_arrays;
 
 /* ---- bigann: L2 search over int8 rows (src/bigann.rs) ---------------------------------- */
@@ -218,6 +224,30 @@ int sg_search_device(sg_index* index, uint32_t nq, const float* d_q768, const fl
                      uint64_t allow_words, float* d_out_scores, uint32_t* d_out_ids,
                      uint32_t* d_out_counts, void* stream);
 
+/* ---- search contexts: ivf::Scratch (src/ivf.rs:497-513) --------------------------------- */
+/* The reference shares one Index across rayon workers, each with its own Scratch
+ * (src/bin/search.rs:312-323). A context is that per-thread state on the GPU: its own stream,
+ * device scratch and captured CUDA graphs over a shared index. sg_search / sg_search_device use
+ * the index's default context and serialise their callers; threads that search through contexts
+ * of their own run concurrently and overlap on the device. A context serves one call at a time
+ * and must be closed before its index. */
+typedef struct sg_context sg_context;
+int sg_context_open(sg_index* index, sg_context** out);
+int sg_context_close(sg_context* ctx);
+/* ivf::Index::search(&self, &Corpus, q768, q256, &Params, &mut Scratch, &mut Timing)
+ * (src/ivf.rs:621-623) for nq queries on the context's scratch; arguments as sg_search. */
+int sg_search_ctx(sg_context* ctx, uint32_t nq, const float* q768, const float* q256,
+                  const sg_params* params, const uint64_t* allow_bits, uint64_t allow_words,
+                  float* out_scores, uint32_t* out_ids, uint32_t* out_counts, sg_timing* timing);
+/* The same with device pointers, ordered after `stream` (cudaStream_t); returns once the results
+ * are in the output buffers. */
+int sg_search_device_ctx(sg_context* ctx, uint32_t nq, const float* d_q768, const float* d_q256,
+                         const sg_params* params, const uint64_t* d_allow_bits, uint64_t allow_words,
+                         float* d_out_scores, uint32_t* d_out_ids, uint32_t* d_out_counts,
+                         void* stream);
+/* Stage times and counters of the context's last search (timing on: sg_set_timing). */
+int sg_context_last_stats(sg_context* ctx, sg_stats* out);
+
 /* No counterpart in the reference. One query through the same path as sg_search, for callers
  * that must not allocate device memory while serving: a latency-critical serving thread (cudaFree
  * synchronises the device, cudaMalloc can wait behind running kernels) or a host whose device
@@ -225,13 +255,25 @@ int sg_search_device(sg_index* index, uint32_t nq, const float* d_q768, const fl
  * every GPU loading the library holds until exit; the call allocates nothing (no cudaMalloc,
  * cudaFree or allocating library routine). Params whose buffers exceed 32 MiB are rejected with
  * SG_ERR_INVALID. Pointers are device pointers (d_q256 nullable); results (k scores, k ids, one
- * count) are written on `stream` asynchronously, as sg_search orders them. The first call on a
- * device looks up the array's device address (once per device, that device current), so make it
- * before any stream capture. Calls share the array: calls that overlap on the GPU race. */
+ * count) are written on `stream` asynchronously, as sg_search orders them. A failure on the
+ * device (a bounded tensor-core wait that ran out, an overflowed buffer) cannot be returned by
+ * the asynchronous call: *d_out_count then reads SG_COUNT_FAILED and the results are void. The
+ * first call on a device looks up the array's device address (once per device, that device
+ * current), so make it before any stream capture. Calls share the array: calls that overlap on
+ * the GPU race. */
 int sg_search_noalloc(sg_index* index, const float* d_q768, const float* d_q256,
                       const sg_params* params, const uint64_t* d_allow_bits, uint64_t allow_words,
                       float* d_out_scores, uint32_t* d_out_ids, uint32_t* d_out_count,
                       void* stream);
+
+/* The flat Hamming baseline of the reference's search binary (flat_hamming_rerank,
+ * src/bin/search.rs:251-269): no index; each query's sign code (of q256, NULL: derived from q768)
+ * against every row's code (codes.bin) by 256 - Hamming distance (lut::hamming,
+ * src/lut.rs:156-165), the best `cand` rows by (score desc, row asc), reranked by the float-weight
+ * int8 dot quant::dot_i8 (src/quant.rs:72-84) into the top k, best first. Needs the index opened
+ * with codes (SG_ERR_UNSUPPORTED otherwise); cand, k <= 4096. out_* [nq * k], out_counts [nq]. */
+int sg_flat_hamming(sg_index* index, uint32_t nq, const float* q768, const float* q256, uint32_t cand,
+                    uint32_t k, float* out_scores, uint32_t* out_ids, uint32_t* out_counts);
 
 /* ivf::Index::route (src/ivf.rs:589-613): the probe list of each query, best first, as
  * (centroid score, cluster). out_scores/out_clusters [nq * params.nprobe], out_counts [nq]. */
@@ -251,6 +293,24 @@ int sg_route_scores(sg_index* index, uint32_t nq, const float* q256, float* out_
 int sg_candidates(sg_index* index, uint32_t nq, const float* q256, const sg_params* params,
                   const uint64_t* allow_bits, uint64_t allow_words, float* out_est,
                   uint32_t* out_ids, float* out_err, uint32_t* out_counts);
+
+/* ivf::Index::candidates over the caller's probe lists (src/ivf.rs:647-729), as a shard server
+ * runs it on the clusters it owns (src/shard.rs:189-191): query q's probes are probe_scores /
+ * probe_clusters [q * P + r], r < probe_counts[q] <= P = min(params.nprobe, k), in scan order
+ * (their order is the admission order). Outputs as sg_candidates (row order). */
+int sg_candidates_probes(sg_index* index, uint32_t nq, const float* q256, const float* probe_scores,
+                         const uint32_t* probe_clusters, const uint32_t* probe_counts, const sg_params* params,
+                         const uint64_t* allow_bits, uint64_t allow_words, float* out_est, uint32_t* out_ids,
+                         float* out_err, uint32_t* out_counts);
+
+/* ivf::Index::rerank (src/ivf.rs:734-815) of the caller's candidates, as a shard server runs
+ * phase 2 of the two-phase merge (src/shard.rs:192-195): query q's (estimate, row, error)
+ * triples cand_* [q * cand_stride + i], i < cand_counts[q] (cand_err nullable: widths 0), are
+ * pruned (params.has_prune) and reranked by params.rerank_kind into the top params.k; params.cand
+ * is ignored (cand_stride <= 4096 takes its place). Outputs as sg_search. */
+int sg_rerank(sg_index* index, uint32_t nq, const float* q768, const float* q256, const float* cand_est,
+              const uint32_t* cand_ids, const float* cand_err, const uint32_t* cand_counts, uint32_t cand_stride,
+              const sg_params* params, float* out_scores, uint32_t* out_ids, uint32_t* out_counts);
 
 /* ---- filters: filter::Filter / Plan / search (src/filter.rs) ---------------------------- */
 /* filter::Plan (src/filter.rs:42-53). */

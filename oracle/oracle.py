@@ -69,6 +69,9 @@ def lib(native: bool = False) -> ctypes.CDLL:
     L.or_rerank.restype = c_uint32
     L.or_search.restype = c_uint32
     L.or_search_batch.restype = c_uint64
+    L.or_flat_hamming.restype = c_uint32
+    L.or_tie_rule.restype = c_int
+    L.or_last_tied.restype = c_int
     L.or_plan_resolve.restype = c_int
     L.or_filter_search.restype = c_uint32
     L.or_recall_at.restype = c_double
@@ -283,11 +286,16 @@ def tier2_score(tables, code, norm) -> float:
     return lib().or_tier2_score(P(f32(tables)), P(np.ascontiguousarray(code, np.uint8)), float(norm))
 
 
-def topk(scores, ids, k: int):
-    """TopK::new(k), push in order, into_sorted (src/topk.rs)."""
+def topk(scores, ids, k: int, tied: bool = False):
+    """TopK::new(k), push in order, into_sorted (src/topk.rs) under the current tie rule; with
+    tied=True also whether the cut at the k-th place was tied."""
     scores, ids = f32(scores), np.ascontiguousarray(ids, np.uint32)
     os_, oi = np.zeros(max(k, 1), np.float32), np.zeros(max(k, 1), np.uint32)
-    m = lib().or_topk(P(scores), P(ids), c_uint64(scores.size), c_uint32(k), P(os_), P(oi))
+    L = lib()
+    L.or_clear_tied()
+    m = L.or_topk(P(scores), P(ids), c_uint64(scores.size), c_uint32(k), P(os_), P(oi))
+    if tied:
+        return os_[:m], oi[:m], bool(L.or_last_tied())
     return os_[:m], oi[:m]
 
 
@@ -315,11 +323,21 @@ def plan_resolve(plan: int, allowed_rows: int, n: int) -> int:
 
 
 # ---- the query path over an index ------------------------------------------------------------
+TIE_CANONICAL, TIE_REFERENCE = 0, 1
+
+
+def set_tie_rule(rule: int, native: bool = False) -> None:
+    """The tie rule of every TopK (sieve_oracle.h): TIE_CANONICAL keeps the k best by (score desc,
+    id asc); TIE_REFERENCE restates src/topk.rs's `<=` rejection and select-by-score cut."""
+    lib(native).or_set_tie_rule(c_int(rule))
+
+
 class OracleIndex:
     """ivf::Index + ivf::Corpus over in-memory arrays (the same dict the GPU index opens)."""
 
     def __init__(self, arrays: dict, native: bool = False):
         self.st, self._keep = make_arrays(arrays)
+        self._arrays = arrays
         self.k = int(arrays["k"])
         self.n = int(arrays["n"])
         self.L = lib(native)
@@ -362,19 +380,34 @@ class OracleIndex:
                              P(s), P(o), ctypes.byref(t))
         return s[:m], o[:m], t
 
-    def search_batch(self, q768, q256, p: SgParams, allow=None, threads: int = 1):
+    def search_batch(self, q768, q256, p: SgParams, allow=None, threads: int = 1, tied: bool = False):
+        """(scores, ids, counts, scanned) of many queries; with tied=True also a per-query flag
+        that some TopK on its path cut a tie at its k-th place."""
         q768, q256 = f32(q768), f32(q256)
         nq = q768.shape[0]
         k = max(p.k, 1)
         s = np.zeros((nq, k), np.float32)
         o = np.zeros((nq, k), np.uint32)
         cnt = np.zeros(nq, np.uint32)
+        tie = np.zeros(nq, np.uint8)
         al = None if allow is None else np.ascontiguousarray(allow, np.uint64)
         scanned = self.L.or_search_batch(ctypes.byref(self.st), c_uint32(nq), P(q768), P(q256),
                                          ctypes.byref(p), None if al is None else P(al),
                                          c_uint64(0 if al is None else al.size), c_int(threads),
-                                         P(s), P(o), P(cnt))
+                                         P(s), P(o), P(cnt), P(tie))
+        if tied:
+            return s, o, cnt, scanned, tie.astype(bool)
         return s, o, cnt, scanned
+
+    def flat_hamming(self, codes, q768, q256, cand: int, k: int):
+        """The search binary's flat Hamming baseline (src/bin/search.rs:251-269) over codes.bin."""
+        codes = np.ascontiguousarray(codes, np.uint8)
+        s, o = np.zeros(max(k, 1), np.float32), np.zeros(max(k, 1), np.uint32)
+        a = self._arrays
+        m = self.L.or_flat_hamming(P(codes), c_uint64(codes.size // 32), P(np.ascontiguousarray(a["rerank"])),
+                                   P(f32(a["quant_scale"])), P(f32(q768)), P(f32(q256)), c_uint32(cand),
+                                   c_uint32(k), P(s), P(o))
+        return s[:m], o[:m]
 
     def filter_per_cluster(self, allow) -> np.ndarray:
         al = np.ascontiguousarray(allow, np.uint64)

@@ -344,13 +344,30 @@ float or_tier2_score(const float* tables, const uint8_t* code, float norm) {
   return (acc[0] + acc[1] + acc[2] + acc[3]) / norm;
 }
 
-/* ---- TopK: src/topk.rs:4-62 (canonical total order, see header) ------------------------ */
+/* ---- TopK: src/topk.rs:4-62 (two tie rules, see header) -------------------------------- */
 typedef struct {
   float s;
   uint32_t id;
 } item;
 
-static inline int better(item a, item b) { return a.s > b.s || (a.s == b.s && a.id < b.id); }
+/* OR_TIE_CANONICAL keeps the k best by (score desc, id asc). OR_TIE_REFERENCE restates the
+ * reference's own mechanics: a push is rejected when score <= threshold (src/topk.rs:28-31), a
+ * full buffer is cut with a selection by score alone (select_nth_unstable_by, src/topk.rs:38-44)
+ * and the threshold becomes the k-th score; only the final sort orders (score desc, id asc)
+ * (src/topk.rs:57-61). Which of several equal scores the selection keeps is unspecified in
+ * Rust; this selection is a median-of-three Hoare quickselect, so the two rules can differ only
+ * on a query whose boundary is tied, which every TopK records (see `tied` below). */
+static int g_tie_rule = OR_TIE_CANONICAL;
+void or_set_tie_rule(int rule) { g_tie_rule = rule == OR_TIE_REFERENCE ? OR_TIE_REFERENCE : OR_TIE_CANONICAL; }
+int or_tie_rule(void) { return g_tie_rule; }
+
+/* Set when any TopK of the current query (on this thread) cut a tie at its k-th place. */
+static _Thread_local int g_tied = 0;
+
+static inline int better(item a, item b) {
+  if (g_tie_rule == OR_TIE_REFERENCE) return a.s > b.s;
+  return a.s > b.s || (a.s == b.s && a.id < b.id);
+}
 
 static void select_nth(item* v, int64_t n, int64_t kth) {
   int64_t lo = 0, hi = n - 1;
@@ -378,19 +395,14 @@ static void select_nth(item* v, int64_t n, int64_t kth) {
   }
 }
 
-static int cmp_item(const void* x, const void* y) {
-  item a = *(const item*)x, b = *(const item*)y;
-  if (better(a, b)) return -1;
-  if (better(b, a)) return 1;
-  return 0;
-}
-
 typedef struct {
   uint32_t k;
   item* items;
   uint32_t len;
   int has_thr;
   item thr;
+  int has_out;  /* some item was rejected or cut off; out_s is the best such score */
+  float out_s;
 } topk;
 
 static void topk_init(topk* t, uint32_t k) {
@@ -398,6 +410,12 @@ static void topk_init(topk* t, uint32_t k) {
   t->items = (item*)malloc(sizeof(item) * 2 * t->k);
   t->len = 0;
   t->has_thr = 0;
+  t->has_out = 0;
+}
+
+static inline void topk_left_out(topk* t, float s) {
+  if (!t->has_out || s > t->out_s) t->out_s = s;
+  t->has_out = 1;
 }
 
 static void topk_free(topk* t) { free(t->items); }
@@ -405,6 +423,7 @@ static void topk_free(topk* t) { free(t->items); }
 static void topk_compact(topk* t) {
   if (t->len > t->k) {
     select_nth(t->items, t->len, t->k - 1);
+    for (uint32_t i = t->k; i < t->len; i++) topk_left_out(t, t->items[i].s);
     t->len = t->k;
     /* the k-th best (worst kept) becomes the admission threshold */
     item w = t->items[0];
@@ -415,12 +434,15 @@ static void topk_compact(topk* t) {
   }
 }
 
-/* Would a push of (s, id) enter? Equivalent to the reference's `score <= threshold` rejection
- * for the push orders the query path uses (ids rising with push order). */
-static inline int topk_admits(const topk* t, float s, uint32_t id) {
+/* Would a push of (s, id) enter? The canonical rule's order agrees with the reference's
+ * `score <= threshold` rejection for the push orders the query path uses (ids rising with push
+ * order); the reference rule is that rejection itself. A rejected item is recorded as left out. */
+static inline int topk_admits(topk* t, float s, uint32_t id) {
   if (!t->has_thr) return 1;
   item x = {s, id};
-  return better(x, t->thr);
+  if (better(x, t->thr)) return 1;
+  topk_left_out(t, s);
+  return 0;
 }
 
 static inline void topk_push(topk* t, float s, uint32_t id) {
@@ -431,10 +453,19 @@ static inline void topk_push(topk* t, float s, uint32_t id) {
   if (t->len >= 2 * t->k) topk_compact(t);
 }
 
+static int cmp_item_final(const void* x, const void* y) {
+  item a = *(const item*)x, b = *(const item*)y;
+  if (a.s != b.s) return a.s > b.s ? -1 : 1;
+  return a.id < b.id ? -1 : (a.id > b.id);
+}
+
+/* into_sorted (src/topk.rs:57-61): the kept items by (score desc, id asc). A left-out item whose
+ * score equals the k-th kept score means the cut at the k-th place was tied. */
 static uint32_t topk_sorted(topk* t) {
   topk_compact(t);
-  qsort(t->items, t->len, sizeof(item), cmp_item);
+  qsort(t->items, t->len, sizeof(item), cmp_item_final);
   if (t->len > t->k) t->len = t->k;
+  if (t->has_out && t->len == t->k && t->items[t->len - 1].s == t->out_s) g_tied = 1;
   return t->len;
 }
 
@@ -544,10 +575,72 @@ static int cmp_dedup(const void* x, const void* y) {
   return a->order < b->order ? -1 : (a->order > b->order);
 }
 
+/* Index::candidates over global sign codes (the `None` branch, src/ivf.rs:700-717): Lut::new on
+ * the unrotated prefix, TopK(cand) of the u16 LUT scores keyed by corpus row, then estimates
+ * lut.to_float(score) and an infinite error width (pruning keeps every such candidate). */
+static uint32_t candidates_global(const sg_ivf_arrays* ix, const float* q256,
+                                  const uint32_t* probe_clusters, uint32_t nprobe, const sg_params* p,
+                                  const uint64_t* allow, uint64_t allow_words, float* out_est,
+                                  uint32_t* out_ids, float* out_err, uint64_t* scanned) {
+  uint8_t tables[SG_GROUPS * 16];
+  float scale, bias;
+  or_lut_new(q256, SG_GROUPS, tables, &scale, &bias);
+  topk cand;
+  topk_init(&cand, p->cand);
+  uint16_t* scores = NULL;
+  size_t scores_cap = 0;
+  uint64_t nscanned = 0;
+  for (uint32_t pi = 0; pi < nprobe; pi++) {
+    uint32_t c = probe_clusters[pi];
+    uint64_t b0 = ix->block_off[c], b1 = ix->block_off[c + 1];
+    size_t ns = (size_t)(b1 - b0) * SG_BLOCK;
+    if (ns > scores_cap) {
+      scores_cap = ns;
+      scores = (uint16_t*)realloc(scores, sizeof(uint16_t) * ns);
+    }
+    or_scan(tables, SG_GROUPS, ix->blocks + b0 * SG_BLOCK_BYTES, b1 - b0, scores);
+    nscanned += ns;
+    const uint32_t* ids = ix->ids + b0 * SG_BLOCK;
+    for (size_t j = 0; j < ns; j++) {
+      uint32_t id = ids[j];
+      if (id == SG_PAD) continue;
+      if (allow && !allowed(allow, allow_words, id)) continue;
+      float sc = (float)scores[j];
+      if (!topk_admits(&cand, sc, id)) continue;
+      topk_push(&cand, sc, id);
+    }
+  }
+  uint32_t m = topk_sorted(&cand);
+  cand3* v = (cand3*)malloc(sizeof(cand3) * (m ? m : 1));
+  for (uint32_t i = 0; i < m; i++) {
+    v[i].est = or_lut_to_float(scale, bias, (uint16_t)cand.items[i].s);
+    v[i].id = cand.items[i].id;
+    v[i].err = INFINITY;
+    v[i].order = i;
+  }
+  qsort(v, m, sizeof(cand3), cmp_dedup);
+  uint32_t w = 0;
+  for (uint32_t i = 0; i < m; i++) {
+    if (w > 0 && v[i].id == out_ids[w - 1]) continue;
+    out_est[w] = v[i].est;
+    out_ids[w] = v[i].id;
+    out_err[w] = v[i].err;
+    w++;
+  }
+  if (scanned) *scanned += nscanned;
+  free(v);
+  free(scores);
+  topk_free(&cand);
+  return w;
+}
+
 uint32_t or_candidates(const sg_ivf_arrays* ix, const float* q256, const float* probe_scores,
                        const uint32_t* probe_clusters, uint32_t nprobe, const sg_params* p,
                        const uint64_t* allow, uint64_t allow_words, float* out_est,
                        uint32_t* out_ids, float* out_err, uint64_t* scanned) {
+  if (!ix->rotation || !ix->factors)
+    return candidates_global(ix, q256, probe_clusters, nprobe, p, allow, allow_words, out_est, out_ids,
+                             out_err, scanned);
   uint8_t tables[SG_GROUPS * 16];
   float scale, bias, a, b;
   or_query_new(ix->rotation, SG_PDIM, q256, tables, &scale, &bias, &a, &b);
@@ -574,10 +667,10 @@ uint32_t or_candidates(const sg_ivf_arrays* ix, const float* q256, const float* 
     const uint32_t* ids = ix->ids + b0 * SG_BLOCK;
     for (size_t j = 0; j < ns; j++) {
       float est = or_estimate(a, b, cent, f[2 * j], scores[j]);
-      if (!topk_admits(&cand, est, (uint32_t)meta_len)) continue;
       uint32_t id = ids[j];
       if (id == SG_PAD) continue;
       if (allow && !allowed(allow, allow_words, id)) continue;
+      if (!topk_admits(&cand, est, (uint32_t)meta_len)) continue;
       topk_push(&cand, est, (uint32_t)meta_len);
       if (meta_len == meta_cap) {
         meta_cap *= 2;
@@ -772,23 +865,63 @@ uint32_t or_search(const sg_ivf_arrays* ix, const float* q768, const float* q256
   return k;
 }
 
+/* The flat Hamming baseline of the search binary (src/bin/search.rs:251-269): the query's sign code
+ * against every corpus code (hamming, src/lut.rs:156-165), TopK(cand) of PDIM - distance keyed by
+ * row, then the rows' float-weight int8 dot (quant::dot_i8 with Int8Quantizer::query_weights)
+ * into TopK(k), best first. */
+uint32_t or_flat_hamming(const uint8_t* codes, uint64_t n, const int8_t* rerank, const float* quant_scale,
+                         const float* q768, const float* q256, uint32_t cand, uint32_t k, float* out_scores,
+                         uint32_t* out_ids) {
+  uint8_t qc[SG_CODE_BYTES];
+  or_sign_code(q256, qc);
+  topk top;
+  topk_init(&top, cand);
+  for (uint64_t i = 0; i < n; i++) {
+    float s = (float)(uint16_t)(SG_PDIM - or_hamming(qc, codes + i * SG_CODE_BYTES, SG_CODE_BYTES));
+    if (topk_admits(&top, s, (uint32_t)i)) topk_push(&top, s, (uint32_t)i);
+  }
+  uint32_t m = cand ? topk_sorted(&top) : 0;
+  float w[SG_DIM];
+  or_int8_query_weights(quant_scale, q768, SG_DIM, w);
+  topk out;
+  topk_init(&out, k);
+  for (uint32_t j = 0; j < m; j++) {
+    uint32_t id = top.items[j].id;
+    float s = or_dot_i8(w, rerank + (uint64_t)id * SG_DIM, SG_DIM);
+    if (topk_admits(&out, s, id)) topk_push(&out, s, id);
+  }
+  uint32_t r = k ? topk_sorted(&out) : 0;
+  for (uint32_t j = 0; j < r; j++) {
+    out_scores[j] = out.items[j].s;
+    out_ids[j] = out.items[j].id;
+  }
+  topk_free(&top);
+  topk_free(&out);
+  return r;
+}
+
 uint64_t or_search_batch(const sg_ivf_arrays* ix, uint32_t nq, const float* q768,
                          const float* q256, const sg_params* p, const uint64_t* allow,
                          uint64_t allow_words, int threads, float* out_scores,
-                         uint32_t* out_ids, uint32_t* out_counts) {
+                         uint32_t* out_ids, uint32_t* out_counts, uint8_t* out_tied) {
   uint64_t scanned = 0;
   if (threads < 1) threads = 1;
 #pragma omp parallel for schedule(dynamic, 4) num_threads(threads) reduction(+ : scanned)
   for (int64_t i = 0; i < (int64_t)nq; i++) {
     sg_timing t;
     memset(&t, 0, sizeof t);
+    g_tied = 0;
     out_counts[i] =
         or_search(ix, q768 + (uint64_t)i * SG_DIM, q256 + (uint64_t)i * SG_PDIM, p, allow,
                   allow_words, out_scores + (uint64_t)i * p->k, out_ids + (uint64_t)i * p->k, &t);
+    if (out_tied) out_tied[i] = (uint8_t)g_tied;
     scanned += t.scanned;
   }
   return scanned;
 }
+
+int or_last_tied(void) { return g_tied; }
+void or_clear_tied(void) { g_tied = 0; }
 
 /* ---- filter.rs: src/filter.rs:27-110 ----------------------------------------------------- */
 void or_filter_per_cluster(const sg_ivf_arrays* ix, const uint64_t* allow, uint64_t words,

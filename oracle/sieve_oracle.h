@@ -25,9 +25,13 @@
  *
  * Tie order. TopK (src/topk.rs) rejects a push whose score is <= the threshold and compacts
  * with select_nth_unstable, so which of several *equal* scores survives at the k-th place is
- * unspecified in the reference. This oracle keeps the k best under the total order
- * (score desc, id asc), which agrees with the reference whenever the survivors are the
- * earlier-pushed of the tied items (the reference's `<=` rejection already prefers them).
+ * unspecified in the reference. The oracle has two rules (or_set_tie_rule): the canonical one
+ * (the default) keeps the k best under the total order (score desc, id asc), which agrees with
+ * the reference whenever the survivors are the earlier-pushed of the tied items (the reference's
+ * `<=` rejection already prefers them); the reference rule restates TopK's own mechanics
+ * (`<=` rejection, a selection by score alone, the k-th score as threshold). Every TopK records
+ * whether its k-th place was tied (an item left out with the k-th kept score); or_search_batch
+ * reports it per query, so parity runs can tell tied queries from mismatches.
  *
  * Parity pin: the reference is Rust and cannot be built here (no cargo/rustc, no network) and
  * ships no golden vectors. The oracle is pinned by ports of the reference's own unit and
@@ -100,12 +104,24 @@ uint32_t or_rerank(const sg_ivf_arrays* ix, const float* q768, const float* q256
 uint32_t or_search(const sg_ivf_arrays* ix, const float* q768, const float* q256,
                    const sg_params* p, const uint64_t* allow, uint64_t allow_words,
                    float* out_scores, uint32_t* out_ids, sg_timing* t);
+/* The flat Hamming baseline (src/bin/search.rs:251-269) over codes.bin [n * 32]: out_* [k]. */
+uint32_t or_flat_hamming(const uint8_t* codes, uint64_t n, const int8_t* rerank, const float* quant_scale,
+                         const float* q768, const float* q256, uint32_t cand, uint32_t k, float* out_scores,
+                         uint32_t* out_ids);
 /* Many queries over `threads` OpenMP threads (the rayon par_iter of src/bin/search.rs:312-323).
  * out_* are [nq * p->k]; returns the total slots scanned. */
 uint64_t or_search_batch(const sg_ivf_arrays* ix, uint32_t nq, const float* q768,
                          const float* q256, const sg_params* p, const uint64_t* allow,
                          uint64_t allow_words, int threads, float* out_scores,
-                         uint32_t* out_ids, uint32_t* out_counts);
+                         uint32_t* out_ids, uint32_t* out_counts, uint8_t* out_tied);
+/* Tie rules of every TopK (process-wide; set it before a batch, not during one). */
+#define OR_TIE_CANONICAL 0
+#define OR_TIE_REFERENCE 1
+void or_set_tie_rule(int rule);
+int or_tie_rule(void);
+/* Whether a TopK on this thread cut a tie since the last or_clear_tied (or batch query). */
+int or_last_tied(void);
+void or_clear_tied(void);
 
 /* filter.rs: allowed slots per cluster, the Auto plan, and filter::search. */
 void or_filter_per_cluster(const sg_ivf_arrays* ix, const uint64_t* allow, uint64_t words,

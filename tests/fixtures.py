@@ -5,6 +5,8 @@ INDEX_B: 30,000 rows with 400 exact duplicates, 8 clusters — clusters span sev
          and the duplicates make exactly tied estimates and tied int8 scores.
 INDEX_C: 12,000 rows, 300 clusters, 150 queries — several routing GEMM tiles on both axes.
 INDEX_D: 16,384 rows, 4096 clusters, 4096 queries — the routing GEMM at full size.
+INDEX_G: 6,000 rows, 16 clusters, built without RaBitQ: global sign codes, no rotation/factors;
+         96 queries (16 copies of rows) so the batched path runs.
 Queries come from the same mixtures (sigma 0.35) plus copies of corpus rows (self-matches).
 """
 from __future__ import annotations
@@ -80,6 +82,21 @@ def index_d():
     arrays = {**corpus, **ix}
     q768 = mix.queries(4096, sigma=0.35).numpy().astype(np.float32)
     return arrays, q768, prefixes(q768), mix
+
+
+@functools.lru_cache(maxsize=None)
+def index_g():
+    """ivf::build with rabitq: false (src/ivf.rs:366-372): every slot holds its row's global sign
+    code; the index has no rotation.f32 / factors.f32 (the ablation of src/ivf.rs:700-717)."""
+    torch.manual_seed(4)
+    mix = synth.Mixture(n=6000, n_centers=24, seed=17)
+    corpus = builder.ingest(mix)
+    ix = builder.build_ivf(corpus, k=16, sample_n=6000, iters=4, rabitq=False)
+    arrays = {**corpus, **ix}
+    q = mix.queries(80, sigma=0.35).numpy()
+    rows = mix.rows(50, 16).numpy()  # self-match queries: every slot of their row ties
+    q768 = np.concatenate([q, rows]).astype(np.float32)
+    return arrays, q768, prefixes(q768)
 
 
 @functools.lru_cache(maxsize=None)

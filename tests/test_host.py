@@ -42,7 +42,7 @@ def test_abi_struct_layouts():
     assert ctypes_size(_abi.SgParams) == 56
     assert ctypes_size(_abi.SgTiming) == 72
     assert ctypes_size(_abi.SgStats) == 8 * 4 + 8 + 4 * 8 + 8
-    assert ctypes_size(_abi.SgIvfArrays) == 8 + 8 + 12 * 8
+    assert ctypes_size(_abi.SgIvfArrays) == 8 + 8 + 13 * 8
 
 
 def ctypes_size(t):
