@@ -64,11 +64,8 @@ struct DevIndex {
   uint32_t* block_off = nullptr;     // [k+1] first block of each cluster
   uint32_t* clen = nullptr;          // [k] real (non-PAD) slots of each cluster
   uint8_t* blocks = nullptr;         // [nblocks*1024] nibble-transposed codes (blocks.bin)
-  uint32_t* blocks_mma = nullptr;    // [nblocks*256] the same codes in the mma.sync scan's word order
   uint32_t* blocks_tc = nullptr;     // [nslots*8] the same codes slot-major (tcgen05 scan)
   float* mul = nullptr;              // [nslots] factors.f32 [.., 0]
-  float2* mul_rng = nullptr;         // [k] (min, max) of mul over each cluster's real slots;
-                                     // min = -1 where the range bound does not apply
   float* err = nullptr;              // [nslots] factors.f32 [.., 1]
   uint32_t* ids = nullptr;           // [nslots] ids.u32
   float* rot = nullptr;              // [768] rotation.f32 (null for global sign codes)
@@ -200,10 +197,9 @@ struct Config {
   uint32_t scan_ctas_per_sm = 2;
   uint32_t soft_cap = 0;  // per-query buffer override (0: automatic); SIEVE_GPU_SOFT_CAP
   int graphs = 1;         // capture and replay CUDA graphs per call shape (SIEVE_GPU_GRAPHS)
-  uint32_t mma_min_queries_per_cluster = 8;   // use the MMA scan at or above this average
-  int mma = 1;            // SIEVE_GPU_MMA: 0 ALU scan only, 1 automatic, 2 MMA whenever nprobe > 1
-  int tc = 1;             // SIEVE_GPU_TC: 1 the tcgen05 bound scan, 2 the tcgen05 one-hot scan,
-                          // 0 the mma.sync scan (the last two kept for comparison)
+  int mma = 1;            // SIEVE_GPU_MMA: 0 ALU scan only, 1 automatic, 2 tensor cores whenever nprobe > 1
+  int tc = 1;             // SIEVE_GPU_TC: 1 the tcgen05 bound scan, 2 the tcgen05 one-hot scan (kept
+                          // for comparison)
   uint32_t tc_split = 0;  // SIEVE_GPU_TC_SPLIT (> 1): a first tcgen05 round over the ranks below it
   // Clusters probed by fewer queries than this in a batch are scanned by the ALU kernel: a
   // tcgen05 tile costs the same ~32 x 101 cycles per 128 slots for any query count up to 128,
@@ -260,17 +256,12 @@ void launch_route_select(const DevIndex& ix, Workspace& w, uint32_t nq, const sg
 void launch_route_given(const DevIndex& ix, Workspace& w, uint32_t nq, const sg_params& p, uint32_t chunk_blocks,
                         uint32_t seed_blocks, bool alu_ranks, const float* given_sc, const uint32_t* given_cl,
                         const uint32_t* given_n, cudaStream_t st);
-// Inverts the probe lists and runs the tensor-core scan over (cluster, query group) items;
-// returns the kernels launched. Needs the seed pass first (it sets the thresholds).
-int launch_scan_mma(const DevIndex& ix, Workspace& w, uint32_t nq, const sg_params& p,
-                    const uint64_t* allow, uint64_t allow_words, int sms, cudaStream_t st);
-int transcode_mma(const uint8_t* blocks, uint64_t nblocks, uint32_t* out);
 void launch_invert(const DevIndex& ix, Workspace& w, uint32_t nq, uint32_t P, uint32_t qg, uint32_t rlo,
                    uint32_t rhi, cudaStream_t st, uint32_t tmin = 1, uint32_t alu_chunk = 0);
 // The batched pass after the seed (scan_tc.cu): the (query, probe) pairs of clusters probed by
 // fewer than cfg.tc_min_queries queries go to the ALU chunk scan (with the routing kernel's
 // rank-0 chunks), the others to the tcgen05 scan, which has the same admission as
-// launch_scan_mma. With cfg.tc_split > 1 it scans probe ranks [1, split) first, raises every
+// the ALU scan. With cfg.tc_split > 1 it scans probe ranks [1, split) first, raises every
 // query's threshold to the cand-th best estimate its buffer then holds, and scans the rest.
 struct Config;
 int launch_scan_tc(const DevIndex& ix, Workspace& w, uint32_t nq, const sg_params& p,

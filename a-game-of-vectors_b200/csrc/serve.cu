@@ -410,6 +410,58 @@ int sg_server_poll(sg_server* srv, uint64_t ticket, int wait_ms, float* out_scor
   return SG_OK;
 }
 
+int sg_server_replay(sg_server* srv, uint32_t nreq, const uint64_t* arrival_ns, const float* q768,
+                     const uint32_t* which, const sg_params* params, const sg_filter* const* filters,
+                     const int32_t* filter_of, float* out_latency_ms, uint32_t* out_batch,
+                     double* out_wall_s) {
+  if (!srv || !params || (nreq && (!arrival_ns || !q768 || !which || !out_latency_ms)))
+    return fail(SG_ERR_INVALID, "null argument");
+  if (nreq == 0) return SG_OK;
+  std::vector<uint64_t> tickets(nreq, 0);
+  std::vector<std::atomic<uint8_t>> ready(nreq);
+  for (auto& r : ready) r.store(0, std::memory_order_relaxed);
+  std::atomic<int> collect_rc{SG_OK};
+  // the collector waits for each request in submission order; latency is the library's clock
+  // from submit to results on the host
+  std::thread collector([&] {
+    for (uint32_t i = 0; i < nreq; i++) {
+      while (!ready[i].load(std::memory_order_acquire)) std::this_thread::yield();
+      sg_request_info info;
+      const int rc = sg_server_poll(srv, tickets[i], -1, nullptr, nullptr, nullptr, &info);
+      if (rc != SG_OK) {
+        int expect = SG_OK;
+        collect_rc.compare_exchange_strong(expect, rc);
+        out_latency_ms[i] = -1.0f;
+        if (out_batch) out_batch[i] = 0;
+        continue;
+      }
+      out_latency_ms[i] = info.queue_ms + info.service_ms;
+      if (out_batch) out_batch[i] = info.batch;
+    }
+  });
+  // the submitter keeps the open-loop schedule: each request goes at its arrival time, whatever
+  // the state of earlier ones
+  const auto t0 = Clock::now();
+  int rc = SG_OK;
+  for (uint32_t i = 0; i < nreq; i++) {
+    const auto due = t0 + std::chrono::nanoseconds(arrival_ns[i]);
+    while (Clock::now() < due) {
+    }
+    const sg_filter* f = (filters && filter_of && filter_of[i] >= 0) ? filters[filter_of[i]] : nullptr;
+    int r = sg_server_submit(srv, q768 + (size_t)which[i] * SG_DIM, nullptr, params, f, &tickets[i]);
+    if (r != SG_OK) {
+      if (rc == SG_OK) rc = r;
+      // the request is not queued: record it as refused so the collector does not wait on it
+      tickets[i] = 0;
+    }
+    ready[i].store(1, std::memory_order_release);
+  }
+  collector.join();
+  if (out_wall_s) *out_wall_s = std::chrono::duration<double>(Clock::now() - t0).count();
+  if (rc != SG_OK) return rc;
+  return collect_rc.load();
+}
+
 int sg_server_get_stats(sg_server* srv, sg_server_stats* out) {
   if (!srv || !out) return fail(SG_ERR_INVALID, "null argument");
   std::lock_guard<std::mutex> g(srv->mu);

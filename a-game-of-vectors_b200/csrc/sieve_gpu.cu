@@ -78,10 +78,8 @@ void free_index(sg::DevIndex& x) {
   dfree(x.block_off);
   dfree(x.clen);
   dfree(x.blocks);
-  dfree(x.blocks_mma);
   dfree(x.blocks_tc);
   dfree(x.mul);
-  dfree(x.mul_rng);
   dfree(x.err);
   dfree(x.ids);
   dfree(x.rot);
@@ -230,22 +228,6 @@ int build_index(const sg_ivf_arrays* a, int device, sg_index** out) {
     mul[s] = global ? 1.0f : a->factors[2 * s];
     err[s] = global ? INFINITY : a->factors[2 * s + 1];
   }
-  // per-cluster range of mul over the real slots: the MMA scan turns it into an integer floor
-  // on the LUT score below which no slot of the cluster can reach a query's threshold
-  std::vector<float2> mrng(K);
-  for (uint32_t c = 0; c < K; c++) {
-    const uint64_t s0 = a->block_off[c] * SG_BLOCK;
-    float lo = INFINITY, hi = 0.0f;
-    bool ok = true;
-    for (uint64_t s = s0; s < s0 + x.h_clen[c]; s++) {
-      const float m = mul[s];
-      if (!(m >= 0.0f) || !std::isfinite(m)) ok = false;
-      lo = std::min(lo, m);
-      hi = std::max(hi, m);
-    }
-    if (x.h_clen[c] == 0) lo = 0.0f;
-    mrng[c] = ok ? make_float2(lo, hi) : make_float2(-1.0f, -1.0f);
-  }
   x.rot_norm = powf(256.0f, -1.5f);
   int rc;
   if ((rc = upload(&x.cent, a->centroids, (size_t)K * SG_PDIM)) ||
@@ -255,7 +237,6 @@ int build_index(const sg_ivf_arrays* a, int device, sg_index** out) {
       (rc = upload(&x.clen, x.h_clen.data(), x.h_clen.size())) ||
       (rc = upload(&x.blocks, a->blocks, (size_t)nblocks * SG_BLOCK_BYTES)) ||
       (rc = upload(&x.mul, mul.data(), mul.size())) || (rc = upload(&x.err, err.data(), err.size())) ||
-      (rc = upload(&x.mul_rng, mrng.data(), mrng.size())) ||
       (rc = upload(&x.ids, a->ids, x.nslots)) ||
       (!global && (rc = upload(&x.rot, a->rotation, 3 * SG_PDIM))) ||
       (rc = upload(&x.rerank, a->rerank, (size_t)a->n * SG_DIM)) ||
@@ -267,25 +248,18 @@ int build_index(const sg_ivf_arrays* a, int device, sg_index** out) {
     free_index(x);
     return fail(SG_ERR_DEVICE, "cuTensorMapEncodeTiled (the routing GEMM's TMA maps) is unavailable");
   }
-  // the batched tensor-core scan reads its own copy of the codes: slot-major for tcgen05 (the
-  // default), or the mma.sync word order when SIEVE_GPU_TC=0
-  if (const char* tc = getenv("SIEVE_GPU_TC")) h->cfg.tc = atoi(tc);
+  // the batched tensor-core scan reads its own copy of the codes, slot-major
+  if (const char* tc = getenv("SIEVE_GPU_TC")) h->cfg.tc = atoi(tc) == 2 ? 2 : 1;
   if (const char* sp = getenv("SIEVE_GPU_TC_SPLIT")) h->cfg.tc_split = (uint32_t)strtoul(sp, nullptr, 10);
   if (const char* tm = getenv("SIEVE_GPU_TC_MIN")) h->cfg.tc_min_queries = (uint32_t)strtoul(tm, nullptr, 10);
-  if (h->cfg.tc) {
-    if ((rc = dalloc(&x.blocks_tc, (size_t)nblocks * 256))) {
-      free_index(x);
-      return rc;
-    }
-    sg::transcode_tc(x.blocks, nblocks, x.blocks_tc, 0);
-    if (cudaGetLastError() != cudaSuccess || cudaDeviceSynchronize() != cudaSuccess) {
-      free_index(x);
-      return fail(SG_ERR_DEVICE, "transcode of the code blocks failed");
-    }
-  } else if ((rc = dalloc(&x.blocks_mma, (size_t)nblocks * 256)) ||
-             sg::transcode_mma(x.blocks, nblocks, x.blocks_mma) || cudaDeviceSynchronize() != cudaSuccess) {
+  if ((rc = dalloc(&x.blocks_tc, (size_t)nblocks * 256))) {
     free_index(x);
-    return rc ? rc : fail(SG_ERR_DEVICE, "transcode of the code blocks failed");
+    return rc;
+  }
+  sg::transcode_tc(x.blocks, nblocks, x.blocks_tc, 0);
+  if (cudaGetLastError() != cudaSuccess || cudaDeviceSynchronize() != cudaSuccess) {
+    free_index(x);
+    return fail(SG_ERR_DEVICE, "transcode of the code blocks failed");
   }
   if ((a->norm256 && (rc = upload(&x.norm256, a->norm256, a->n))) ||
       (a->codes && (rc = upload(&x.codes, a->codes, (size_t)a->n * SG_CODE_BYTES)))) {
@@ -477,15 +451,13 @@ int check_params(const sg_index* h, const sg_params* p) {
 // probed cluster; SIEVE_GPU_MMA forces it off (0) or on (2).)
 bool use_mma(const sg_index* h, const sg::Config& cfg, uint32_t nq, uint32_t P) {
   const sg::DevIndex& x = h->ix;
-  if (!(cfg.tc ? x.blocks_tc : x.blocks_mma) || P <= 1 || P > 4096)
-    return false;  // inverted lists keep 12-bit ranks
-  if (x.global && cfg.tc != 1) return false;  // only the bound pass ranks global codes
+  if (!x.blocks_tc || P <= 1 || P > 4096) return false;  // inverted lists keep 12-bit ranks
+  if (x.global && cfg.tc != 1) return false;             // only the bound pass ranks global codes
   if (cfg.mma == 2) return true;
   if (cfg.mma != 1 || nq < 64) return false;
-  // tcgen05: the batch splits per cluster on the device (few queries: ALU, many: tensor cores),
-  // so the inverted path pays off once some cluster can gather tc_min_queries queries
-  if (cfg.tc) return (uint64_t)nq * (P - 1) >= (uint64_t)cfg.tc_min_queries * 16;
-  return (uint64_t)nq * (P - 1) >= (uint64_t)cfg.mma_min_queries_per_cluster * x.k;
+  // the batch splits per cluster on the device (few queries: ALU, many: tensor cores), so the
+  // inverted path pays off once some cluster can gather tc_min_queries queries
+  return (uint64_t)nq * (P - 1) >= (uint64_t)cfg.tc_min_queries * 16;
 }
 
 // Exact per-query candidate-buffer bound. A slot is appended at most once, so the probed
@@ -556,12 +528,10 @@ int run_pipeline(sg_index* h, const sg::Config& cfg, sg::Ctx& c, uint32_t nq, co
   if (p.cand > 0) {
     sg::launch_scan(x, w, nq, p, d_allow, allow_words, h->sms, 0, sb, cfg.scan_ctas_per_sm, st);
     if (timed) CK(cudaEventRecord(w.ev[9], st));
-    if (mma && cfg.tc) {  // ALU chunks and tcgen05 tiles, split per cluster
+    if (mma)  // ALU chunks and tcgen05 tiles, split per cluster
       launches += sg::launch_scan_tc(x, w, nq, p, d_allow, allow_words, h->sms, cfg, cb, st);
-    } else {
+    else
       sg::launch_scan(x, w, nq, p, d_allow, allow_words, h->sms, cb, 0, cfg.scan_ctas_per_sm, st);
-      if (mma) launches += sg::launch_scan_mma(x, w, nq, p, d_allow, allow_words, h->sms, st);
-    }
     if (timed) CK(cudaEventRecord(w.ev[4], st));
     sg::launch_cut(x, w, nq, p, st);
     launches += 3;

@@ -271,6 +271,7 @@ EXPORTS = [
     "sg_server_submit",
     "sg_server_poll",
     "sg_server_get_stats",
+    "sg_server_replay",
     "sg_server_stop",
     "sg_open_bigann",
     "sg_open_bigann_arrays",

@@ -79,6 +79,25 @@ class Server:
         m = n.value
         return sc[:m], ids[:m], RequestInfo(info.queue_ms, info.service_ms, info.batch, bool(info.retried))
 
+    def replay(self, arrival_s, q768_pool, which, params: Params, filters=(), filter_of=None):
+        """Open-loop load from a library thread (sg_server_replay): request i goes at arrival_s[i]
+        seconds after the start with query q768_pool[which[i]] and filters[filter_of[i]] (no
+        filter where filter_of[i] < 0). Returns (latency ms per request, batch size per request,
+        wall seconds from the first arrival to the last result)."""
+        n = len(which)
+        arr = np.ascontiguousarray(np.round(np.asarray(arrival_s) * 1e9), np.uint64)
+        pool = np.ascontiguousarray(q768_pool, np.float32).reshape(-1, _abi.DIM)
+        wh = np.ascontiguousarray(which, np.uint32)
+        fs = (c_void_p * max(len(filters), 1))(*[f._h for f in filters])
+        fo = None if filter_of is None else np.ascontiguousarray(filter_of, np.int32)
+        lat = np.zeros(n, np.float32)
+        bat = np.zeros(n, np.uint32)
+        wall = ctypes.c_double()
+        p = params.to_c()
+        check(lib().sg_server_replay(self._h, c_uint32(n), ptr(arr), ptr(pool), ptr(wh), byref(p),
+                                     fs if filters else None, ptr(fo), ptr(lat), ptr(bat), byref(wall)))
+        return lat, bat, wall.value
+
     def stats(self) -> dict:
         st = SgServerStats()
         check(lib().sg_server_get_stats(self._h, byref(st)))

@@ -62,6 +62,21 @@ class Mixture:
             out.append(x[lo:hi])
         return torch.cat(out) if len(out) > 1 else out[0]
 
+    def centres_of(self, start: int, count: int) -> torch.Tensor:
+        """The mixture centre of rows [start, start + count): the first draw of each chunk's
+        generator, so regenerating it alone gives the same centres as rows()."""
+        out = []
+        dev = self.centers.device
+        c0, c1 = start // CHUNK, (start + count - 1) // CHUNK
+        for c in range(c0, c1 + 1):
+            rows = min(CHUNK, self.n - c * CHUNK)
+            g = _gen(dev, (self.seed * 1_000_003 + c) * 31)
+            which = torch.randint(0, self.n_centers, (rows,), generator=g, device=dev)
+            lo = max(start - c * CHUNK, 0)
+            hi = min(start + count - c * CHUNK, rows)
+            out.append(which[lo:hi])
+        return torch.cat(out) if len(out) > 1 else out[0]
+
     def queries(self, nq: int, sigma: float, seed: int = 99) -> torch.Tensor:
         """nq query vectors from the same centres with noise sigma (salted stream)."""
         out = []

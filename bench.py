@@ -37,8 +37,10 @@ import torch  # noqa: E402
 
 WORKLOADS = {
     "c1": dict(n=1_000_000, centers=1024, k=1024, queries=10_000, search="32:1000:full"),
-    "c2": dict(n=18_400_000, centers=16384, k=4096, queries=50_000, search="32:2000:full"),
-    "c3": dict(n=113_500_000, centers=65536, k=16384, queries=100_000, search="128:2000:full:p0.1"),
+    "c2": dict(n=18_400_000, centers=16384, k=4096, queries=50_000, search="64:500:tiered200",
+               serve="5000,20000,50000,100000,150000,200000"),
+    "c3": dict(n=113_500_000, centers=65536, k=16384, queries=100_000, search="128:500:tiered200:p0.3",
+               serve="5000,20000,50000,100000,150000,200000"),
     # billion-scale L2 (bigann): 512 x 256 = 131,072 leaves, 2-bit refinement. The bench default
     # is a 100M-row cut of the 1B shape (--rows sets it): the 1B build does not fit the run's time.
     "c4": dict(n=100_000_000, centers=131072, k1=512, k2=256, bits=2, queries=10_000,
@@ -148,6 +150,7 @@ def build_workload(name: str, device: str, rows: int | None, nq_pool: int, n_eva
     del corpus, index
     torch.cuda.empty_cache()  # the index upload needs the build's cached device memory back
     queries = mix.queries(nq_pool, sigma=0.35).float()
+    arrays["domain"] = domain_ids(mix, w["n"])  # per-row domains of the serving filters
     t1 = time.time()
     gt = builder.ground_truth(mix, queries[:n_eval], k=10)
     torch.cuda.empty_cache()
@@ -258,80 +261,108 @@ def cpu_reference(arrays, q768_host: np.ndarray, params, seconds: float, threads
             "tied": tied[:k]}
 
 
-def serve_load(index, arrays, queries_host: np.ndarray, params, rates, seconds: float, seed: int = 7,
-               warmup_s: float = 0.5):
-    """Open-loop Poisson arrivals into the serving loop (continuous batching): for each rate, the
-    achieved QPS and the p50/p99 latency from submit to results on the host. One request in ten
-    carries a filter (allowlists of 30%, 3% and 0.3% of the rows, seeded). Each rate first runs
-    `warmup_s` of the same arrival process whose requests are not measured: a fresh server sizes
-    its contexts' scratch and captures a CUDA graph per batch shape on first use."""
+N_DOMAINS = 10_000
+GOLDEN = 0x9E3779B97F4A7C15
+
+
+def domain_ids(mix, n: int, seed: int = 23) -> np.ndarray:
+    """Seeded per-row domain ids over 10,000 domains. A row's domain follows its mixture centre
+    (centre mod 10,000) with probability 0.8 and is uniform otherwise, so a domain's rows cluster
+    by topic as a real site's pages do."""
+    out = np.empty(n, np.uint16)
+    rng = np.random.default_rng(seed)
+    for s in range(0, n, 1 << 22):
+        e = min(n, s + (1 << 22))
+        d = (mix.centres_of(s, e - s).cpu().numpy() % N_DOMAINS).astype(np.uint16)
+        flip = rng.random(e - s) < 0.2
+        d[flip] = rng.integers(0, N_DOMAINS, int(flip.sum()))
+        out[s:e] = d
+    return out
+
+
+def domain_allowlist(dom: np.ndarray, selectivity: float) -> np.ndarray:
+    """The search binary's filter allowlists (src/bin/search.rs:598-620): domains in the fixed
+    pseudo-random order of (h * 0x9E3779B97F4A7C15).rotate_left(17), whole domains allowed until
+    they hold `selectivity` of the rows. Returns the allow bitset (u64 words)."""
+    counts = np.bincount(dom, minlength=N_DOMAINS)
+    h = np.arange(N_DOMAINS, dtype=np.uint64)
+    with np.errstate(over="ignore"):
+        x = h * np.uint64(GOLDEN)
+    key = (x << np.uint64(17)) | (x >> np.uint64(47))
+    order = np.argsort(key, kind="stable")
+    want = int(selectivity * dom.size)
+    allowed, rows = np.zeros(N_DOMAINS, bool), 0
+    for d in order:
+        if rows >= want:
+            break
+        allowed[d] = True
+        rows += int(counts[d])
+    mask = allowed[dom]
+    pad = (-mask.size) % 64
+    bits = np.packbits(np.concatenate([mask, np.zeros(pad, bool)]), bitorder="little")
+    return bits.view(np.uint64).copy()
+
+
+def serve_load(index, arrays, queries_host: np.ndarray, params, rates, seconds: float, dom=None,
+               seed: int = 7, warmup_s: float = 0.3):
+    """Open-loop Poisson arrivals into the serving loop (continuous batching), replayed by the
+    library's own submitter thread (sg_server_replay): for each rate, the achieved QPS and the
+    p50/p99 latency from submit to results on the host. One request in ten carries a domain
+    allowlist (whole domains at 0.1%, 1%, 10% and 50% of the rows). Each rate first replays
+    `warmup_s` of the same process unmeasured: a fresh server sizes its contexts' scratch on
+    first use."""
     from sieve_gpu import Server
     from sieve_gpu import filter as F
-    from sieve_gpu.index import allow_bitset
 
-    n = int(arrays["n"])
     rng = np.random.default_rng(seed)
-    sys.setswitchinterval(0.0002)  # the spinning submitter must not starve the collector
-    filters = [F.Filter(allow_bitset(np.nonzero(rng.random(n) < f)[0], n), index) for f in (0.3, 0.03, 0.003)]
+    sels = (0.001, 0.01, 0.1, 0.5)
+    filters = []
+    if dom is not None:
+        filters = [F.Filter(domain_allowlist(dom, s), index) for s in sels]
     out = []
     try:
         for rate in rates:
-            srv = Server(index, max_batch=2048, contexts=3)
-            nwarm = int(rate * warmup_s)
-            wgaps = rng.exponential(1.0 / rate, nwarm)
-            wwhich = rng.integers(0, queries_host.shape[0], nwarm)
-            wfilt = rng.random(nwarm) < 0.1
-            due = time.perf_counter()
-            wt = []
-            for i in range(nwarm):
-                due += wgaps[i]
-                while time.perf_counter() < due:
-                    pass
-                wt.append(srv.submit(queries_host[wwhich[i]], None, params, filters[i % len(filters)] if wfilt[i] else None))
-            for t in wt:
-                srv.poll(t, wait_ms=-1)
-            st0 = srv.stats()
-            nreq = int(rate * seconds)
-            gaps = rng.exponential(1.0 / rate, nreq)
-            which = rng.integers(0, queries_host.shape[0], nreq)
-            filt = rng.random(nreq) < 0.1
-            fsel = rng.integers(0, len(filters), nreq)
-            tickets = [None] * nreq
-            lat = np.zeros(nreq)
-            t_sub = np.zeros(nreq)
-
-            def collector():
-                for i in range(nreq):
-                    while tickets[i] is None:
-                        time.sleep(0)
-                    r = srv.poll(tickets[i], wait_ms=-1)
-                    lat[i] = r[2].queue_ms + r[2].service_ms  # the library's own clock
-
-            th = threading.Thread(target=collector)
-            th.start()
-            t0 = time.perf_counter()
-            due = t0
-            for i in range(nreq):
-                due += gaps[i]
-                while time.perf_counter() < due:
-                    pass
-                t_sub[i] = time.perf_counter()
-                tickets[i] = srv.submit(queries_host[which[i]], None, params,
-                                        filters[fsel[i]] if filt[i] else None)
-            th.join()
-            wall = time.perf_counter() - t0
-            st = srv.stats()
-            srv.stop()
-            out.append({"offered_qps": rate, "achieved_qps": nreq / wall, "p50_ms": float(np.percentile(lat, 50)),
-                        "p99_ms": float(np.percentile(lat, 99)), "requests": nreq,
+            srv = Server(index, max_batch=4096, contexts=3)
+            try:
+                def trace(n):
+                    t = np.cumsum(rng.exponential(1.0 / rate, n))
+                    which = rng.integers(0, queries_host.shape[0], n)
+                    fo = np.where(rng.random(n) < 0.1, rng.integers(0, max(len(filters), 1), n), -1)
+                    return t, which, fo if filters else None
+                t, wh, fo = trace(max(int(rate * warmup_s), 1))
+                srv.replay(t, queries_host, wh, params, filters, fo)
+                st0 = srv.stats()
+                nreq = int(rate * seconds)
+                t, wh, fo = trace(nreq)
+                lat, bat, wall = srv.replay(t, queries_host, wh, params, filters, fo)
+                st = srv.stats()
+            finally:
+                srv.stop()
+            out.append({"offered_qps": rate, "achieved_qps": nreq / wall,
+                        "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
+                        "requests": nreq, "filtered": int((fo >= 0).sum()) if fo is not None else 0,
                         "mean_batch": (st["queries_batched"] - st0["queries_batched"])
                         / max(st["batches"] - st0["batches"], 1),
-                        "retried": st["retried"] - st0["retried"], "warmup_requests": nwarm})
+                        "retried": st["retried"] - st0["retried"]})
             log(f"serve {rate}/s: {out[-1]}")
     finally:
         for f in filters:
             f.close()
     return out
+
+
+def serving_knee(serving, plain_ms) -> dict | None:
+    """The highest offered rate whose p99 stays within 5 ms and whose achieved rate keeps up
+    (>= 95% of offered), and its ratio to the plain one-query-per-launch path."""
+    if not serving:
+        return None
+    ok = [s for s in serving if s["p99_ms"] <= 5.0 and s["achieved_qps"] >= 0.95 * s["offered_qps"]]
+    if not ok:
+        return {"offered_qps": None, "note": "no rate met p99 <= 5 ms"}
+    best = max(ok, key=lambda s: s["achieved_qps"])
+    plain_qps = float(1e3 / np.mean(plain_ms))
+    return {"offered_qps": best["offered_qps"], "achieved_qps": best["achieved_qps"], "p99_ms": best["p99_ms"],
+            "vs_plain": best["achieved_qps"] / plain_qps}
 
 
 def main():
@@ -528,7 +559,8 @@ def main():
     rates = args.serve if args.serve is not None else wl.get("serve", "")
     if rates:
         rates = [float(x) for x in rates.split(",") if x]
-        serving = serve_load(index, arrays, q_pool_host, params, rates, args.serve_seconds)
+        serving = serve_load(index, arrays, q_pool_host, params, rates, args.serve_seconds,
+                             dom=arrays.get("domain"))
 
     cpu, parity = None, None
     if rank == 0 and world == 1 and args.cpu_seconds > 0:
@@ -557,9 +589,13 @@ def main():
                   "p99_ms": float(np.percentile(plain_ms, 99)), "queries": int(plain_ms.size)},
         "stage_ms": stage,
         "serving": serving,
-        "serving_note": "continuous batching (sg_server, 3 contexts): open-loop Poisson arrivals from a "
-                        "Python client, 10% filtered, after 0.5 s of unmeasured warm-up at the same "
-                        "rate; latency = sg_server_submit to results on the host, on the library's clock",
+        "serving_note": "continuous batching (sg_server, 3 contexts, batches up to 4096): open-loop "
+                        "Poisson arrivals replayed by the library's submitter thread "
+                        "(sg_server_replay), 10% of requests on domain allowlists (10,000 seeded "
+                        "domains, whole domains at 0.1/1/10/50% of the rows, Post plan), after 0.3 s "
+                        "of unmeasured warm-up at the same rate; latency = submit to results on the "
+                        "host, on the library's clock",
+        "serving_knee": serving_knee(serving, plain_ms),
         "scanned_per_query": float(np.mean(scanned) / B),
         "distinct_probed_slots_per_step": float(np.mean(dslots)),
         "retried_queries_per_step": float(np.mean([s["retried"] for s in stats])),

@@ -383,6 +383,18 @@ int sg_server_submit(sg_server* server, const float* q768, const float* q256,
 int sg_server_poll(sg_server* server, uint64_t ticket, int wait_ms, float* out_scores,
                    uint32_t* out_ids, uint32_t* out_count, sg_request_info* info);
 int sg_server_get_stats(sg_server* server, sg_server_stats* out);
+/* An open-loop load from a library thread (no counterpart in the reference; its bench replays
+ * queries from rayon workers, src/bin/search.rs:742-748): request i is submitted at arrival_ns[i]
+ * after the call starts, whatever the state of earlier requests, with the query
+ * q768 + which[i] * 768 and the filter filters[filter_of[i]] (none where filter_of is NULL or
+ * filter_of[i] < 0); a second thread collects the results in order. out_latency_ms[i] is the
+ * request's submit-to-results time on the library's clock (-1 if it failed), out_batch[i]
+ * (nullable) the size of its batch, *out_wall_s (nullable) the time from the first arrival to the
+ * last result. Returns the first failure of a submit or a poll. */
+int sg_server_replay(sg_server* server, uint32_t nreq, const uint64_t* arrival_ns, const float* q768,
+                     const uint32_t* which, const sg_params* params, const sg_filter* const* filters,
+                     const int32_t* filter_of, float* out_latency_ms, uint32_t* out_batch,
+                     double* out_wall_s);
 /* Runs every queued request to completion, then stops the dispatcher and frees the contexts. */
 int sg_server_stop(sg_server* server);
 
