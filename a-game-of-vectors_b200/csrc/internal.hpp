@@ -55,7 +55,12 @@ constexpr uint32_t kStatusTimeout = 4u;    // a tensor-core wait ran out (the CT
 // HBM layout of one IVF index (all arrays on the index's device).
 struct DevIndex {
   int device = 0;
-  uint32_t k = 0;
+  uint32_t k = 0;   // clusters: the centroids', plus in a live index one delta list per centroid
+  uint32_t kc = 0;  // centroids (routing scores these)
+  // A live index (sg_live_open): cluster kc + c is cluster c's delta list (rows inserted since the
+  // build, src/live.rs:39-66), scanned right after c's base list; routing expands every probe c
+  // whose delta list holds slots into (c, kc + c) with the same centroid score.
+  bool live = false;
   uint64_t n = 0, nblocks = 0, nslots = 0;
   float* cent = nullptr;             // [k*256] centroids.f32
   float* cent_t = nullptr;           // [256*k] transposed, for the exact routing kernel
@@ -88,6 +93,13 @@ struct DevIndex {
   std::vector<uint64_t> h_slots_desc_prefix;   // prefix sums of per-cluster slot counts, largest first
 };
 
+// Stride of a call's probe arrays: min(nprobe, centroids), doubled in a live index (each probe may
+// be followed by its delta list).
+inline uint32_t probe_stride(const DevIndex& x, uint32_t nprobe) {
+  const uint32_t p = nprobe < x.kc ? nprobe : x.kc;
+  return x.live ? 2 * p : p;
+}
+
 // Device buffers of one batched call, grown on demand and reused.
 struct Workspace {
   uint32_t nq_cap = 0, P_cap = 0, cand_cap = 0, k_cap = 0, r_cap = 0;
@@ -115,6 +127,7 @@ struct Workspace {
   uint4* items = nullptr;        // [item_cap] (query, probe rank, first block, end block)
   uint4* seed_items = nullptr;   // [nq] each query's first rank-0 chunk (the seed)
   uint32_t* counters = nullptr;  // [8]: nitems, next item, status, -, mma groups, next group
+  uint32_t inv_k = 0;            // clusters the per-cluster arrays below are sized for
   uint32_t* inv_cnt = nullptr;   // [k] (query, probe >= 1) pairs per cluster
   uint32_t* inv_fill = nullptr;  // [k]
   uint32_t* inv_off = nullptr;   // [k+1]
@@ -214,6 +227,7 @@ struct Config {
 };
 
 std::string& last_error();
+void set_cluster_bounds(DevIndex& x, uint32_t chunk);
 int fail(int code, const std::string& msg);
 
 // Views of an open index for entry points in other translation units (sieve_gpu.cu defines them).
@@ -352,4 +366,14 @@ int ctx_search_one(sg_index* h, const Config& cfg, Ctx& c, const float* q768, co
                    uint32_t* out_id, uint32_t* out_n);
 uint64_t ctx_bytes(const sg_index* h, const Config& cfg, const sg_params& p, uint32_t nq);
 void free_ctx(Ctx& c);
+// Live indexes (live.cu): make `h` live with room for max_rows inserted rows and block_cap delta
+// blocks (its slot and row arrays are reallocated; the caller holds no other call on h); replace
+// the delta lists (nb_of / clen_of [kc] per cluster, then nblocks blocks of codes, factors and ids
+// in cluster order); search with a device allow bitset.
+int index_make_live(sg_index* h, uint64_t max_rows, uint64_t block_cap);
+int index_set_delta(sg_index* h, const uint32_t* nb_of, const uint32_t* clen_of, const uint8_t* blocks,
+                    const float* mul, const float* err, const uint32_t* ids, uint64_t nblocks);
+int index_search_allow(sg_index* h, uint32_t nq, const float* q768, const float* q256, const sg_params& p,
+                       const uint64_t* d_allow, uint64_t allow_words, float* out_sc, uint32_t* out_id,
+                       uint32_t* out_n);
 }  // namespace sg

@@ -70,7 +70,7 @@ void carve_workspace(Carve& c, sg::Workspace& w, const sg::DevIndex& x, uint32_t
   w.winv = c.take<float>(1);
   w.wq256 = c.take<int8_t>(SG_PDIM);
   w.winv256 = c.take<float>(1);
-  w.scores = c.take<float>(x.k);
+  w.scores = c.take<float>(x.kc);
   w.probe_sc = c.take<float>(P);
   w.probe_cl = c.take<uint32_t>(P);
   w.probe_off = c.take<uint32_t>(P);
@@ -123,7 +123,7 @@ extern "C" int sg_search_noalloc(sg_index* h, const float* d_q768, const float* 
   // Sizes of one query's buffers: the exact work-item and candidate-buffer bounds sg_search uses
   // for one query. A slot is appended at most once, so the probed clusters' slots bound the
   // candidate buffer; the chunk scan keeps at most cand per chunk, so chunks x cand does too.
-  const uint32_t P = p.nprobe < x.k ? p.nprobe : x.k;
+  const uint32_t P = sg::probe_stride(x, p.nprobe);
   const uint32_t cand = p.cand > 0 ? p.cand : 1;
   const uint64_t items = x.h_chunks_desc_prefix[P];
   const uint64_t slots = x.h_slots_desc_prefix[P];

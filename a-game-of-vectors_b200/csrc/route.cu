@@ -213,7 +213,9 @@ struct SelectArgs {
   const uint32_t* block_off;
   uint32_t K;
   float* scores;
-  uint32_t P;  // min(nprobe, K): stride of the probe arrays
+  uint32_t P;        // stride of the probe arrays (probe_stride)
+  uint32_t Pb;       // probes routing selects: min(nprobe, K)
+  uint32_t live_kc;  // a live index's centroid count (delta list of c = cluster kc + c), else 0
   int bf16;
   sg_params p;
   uint32_t chunk_blocks;
@@ -308,13 +310,37 @@ SG_DEV void emit_probes(const SelectArgs& a, const uint64_t* keys, uint32_t m, u
   }
 }
 
+// A live index: every probe c whose delta list holds slots is followed by cluster kc + c with the
+// same centroid score, so the delta list is scanned right after the base list and its slots come
+// after the base list's in admission order (src/ivf.rs:679-684). keys[0..m) hold the probes best
+// first and have room for 2m; returns the expanded count.
+SG_DEV uint32_t expand_delta(const SelectArgs& a, uint64_t* keys, uint32_t m) {
+  __shared__ uint32_t s_m2;
+  if (threadIdx.x == 0) {
+    const uint32_t kc = a.live_kc;
+    auto has_delta = [&](uint32_t c) { return a.block_off[kc + c + 1] > a.block_off[kc + c]; };
+    uint32_t extra = 0;
+    for (uint32_t r = 0; r < m; r++) extra += has_delta(key_id(keys[r]));
+    uint32_t pos = m + extra;
+    for (int r = (int)m - 1; r >= 0; r--) {  // back to front: an entry only moves to a later place
+      const uint64_t k = keys[r];
+      const uint32_t c = key_id(k);
+      if (has_delta(c)) keys[--pos] = rank_key(key_score(k), kc + c);
+      keys[--pos] = k;
+    }
+    s_m2 = m + extra;
+  }
+  __syncthreads();
+  return s_m2;
+}
+
 __global__ void __launch_bounds__(256) k_route_select(SelectArgs a) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   uint64_t* keys = reinterpret_cast<uint64_t*>(smem_raw);  // [kWinCap]
   __shared__ float qv[SG_PDIM];
   __shared__ uint32_t hist[256], tmp[32];
   __shared__ uint32_t s_nw, s_m, s_keep;
-  const uint32_t q = blockIdx.x, P = a.P, K = a.K;
+  const uint32_t q = blockIdx.x, P = a.Pb, K = a.K;
   float* row = a.scores + (size_t)q * K;
   for (int i = threadIdx.x; i < SG_PDIM; i += blockDim.x) qv[i] = a.q256[(size_t)q * SG_PDIM + i];
   if (threadIdx.x == 0) s_nw = 0;
@@ -409,7 +435,8 @@ __global__ void __launch_bounds__(256) k_route_select(SelectArgs a) {
     s_keep = m;
   }
   __syncthreads();
-  emit_probes(a, keys, s_keep, q, tmp);
+  const uint32_t m = a.live_kc ? expand_delta(a, keys, s_keep) : s_keep;
+  emit_probes(a, keys, m, q, tmp);
 }
 
 // filter::search with Plan::Expand (src/filter.rs:79-93): every cluster in route order (exact f32
@@ -473,21 +500,21 @@ __global__ void __launch_bounds__(256) k_route_given(SelectArgs a, const float* 
 
 cudaError_t launch_route_scores(const DevIndex& ix, Workspace& w, uint32_t nq, int precision,
                                 cudaStream_t st) {
-  if (nq == 0 || ix.k == 0) return cudaSuccess;
+  if (nq == 0 || ix.kc == 0) return cudaSuccess;
   if (precision == SG_ROUTE_BF16) {
     static PerDeviceOnce attr;
     attr([] { return cudaFuncSetAttribute(k_route_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, kRtSmem); });
     CUtensorMap map_c, map_q;
-    if (!encode_rows(&map_c, ix.cent_bf16, ix.k, kRtM) || !encode_rows(&map_q, w.q16, nq, kRtN))
+    if (!encode_rows(&map_c, ix.cent_bf16, ix.kc, kRtM) || !encode_rows(&map_q, w.q16, nq, kRtN))
       return cudaErrorInvalidValue;
     const uint32_t n4 = nq * (SG_PDIM / 4);
     k_q_bf16<<<(n4 + 255) / 256, 256, 0, st>>>(reinterpret_cast<const float4*>(w.q256), n4,
                                                reinterpret_cast<uint2*>(w.q16));
-    dim3 grid((ix.k + kRtM - 1) / kRtM, (nq + kRtN - 1) / kRtN);
-    k_route_tc<<<grid, kRtThreads, kRtSmem, st>>>(map_c, map_q, ix.k, nq, w.scores, w.counters + 2);
+    dim3 grid((ix.kc + kRtM - 1) / kRtM, (nq + kRtN - 1) / kRtN);
+    k_route_tc<<<grid, kRtThreads, kRtSmem, st>>>(map_c, map_q, ix.kc, nq, w.scores, w.counters + 2);
   } else {
-    dim3 grid((ix.k + 255) / 256, (nq + kRouteQB - 1) / kRouteQB);
-    k_route_fp32<<<grid, 256, 0, st>>>(w.q256, ix.cent_t, ix.k, nq, w.scores);
+    dim3 grid((ix.kc + 255) / 256, (nq + kRouteQB - 1) / kRouteQB);
+    k_route_fp32<<<grid, 256, 0, st>>>(w.q256, ix.cent_t, ix.kc, nq, w.scores);
   }
   return cudaGetLastError();
 }
@@ -501,9 +528,11 @@ void launch_route_select(const DevIndex& ix, Workspace& w, uint32_t nq, const sg
   a.qnorm = w.qnorm;
   a.cent_norm_max = ix.cent_norm_max;
   a.block_off = ix.block_off;
-  a.K = ix.k;
+  a.K = ix.kc;
   a.scores = w.scores;
-  a.P = p.nprobe < ix.k ? p.nprobe : ix.k;
+  a.P = probe_stride(ix, p.nprobe);
+  a.Pb = p.nprobe < ix.kc ? p.nprobe : ix.kc;
+  a.live_kc = ix.live ? ix.kc : 0;
   a.bf16 = precision == SG_ROUTE_BF16;
   a.p = p;
   a.chunk_blocks = chunk_blocks;
@@ -532,8 +561,10 @@ void launch_route_given(const DevIndex& ix, Workspace& w, uint32_t nq, const sg_
   SelectArgs a;
   memset(&a, 0, sizeof a);
   a.block_off = ix.block_off;
-  a.K = ix.k;
-  a.P = p.nprobe < ix.k ? p.nprobe : ix.k;
+  a.K = ix.kc;
+  a.P = probe_stride(ix, p.nprobe);
+  a.Pb = p.nprobe < ix.kc ? p.nprobe : ix.kc;
+  a.live_kc = ix.live ? ix.kc : 0;
   a.p = p;
   a.chunk_blocks = chunk_blocks;
   a.seed_blocks = seed_blocks;
@@ -566,9 +597,10 @@ void launch_route_expand(const DevIndex& ix, Workspace& w, uint32_t nq, const sg
   a.qnorm = w.qnorm;
   a.cent_norm_max = ix.cent_norm_max;
   a.block_off = ix.block_off;
-  a.K = ix.k;
+  a.K = ix.kc;
   a.scores = w.scores;
-  a.P = ix.k;
+  a.P = ix.kc;
+  a.Pb = ix.kc;
   a.bf16 = 0;
   a.p = p;
   a.chunk_blocks = chunk_blocks;
@@ -583,7 +615,7 @@ void launch_route_expand(const DevIndex& ix, Workspace& w, uint32_t nq, const sg
   a.items = w.items;
   a.item_cap = w.item_cap;
   a.counters = w.counters;
-  const size_t smem = (size_t)next_pow2_host(ix.k) * sizeof(uint64_t);
+  const size_t smem = (size_t)next_pow2_host(ix.kc) * sizeof(uint64_t);
   static PerDeviceOnce attr;
   attr([] {
     return cudaFuncSetAttribute(k_route_expand, cudaFuncAttributeMaxDynamicSharedMemorySize,

@@ -319,7 +319,7 @@ void launch_scan(const DevIndex& ix, Workspace& w, uint32_t nq, const sg_params&
   a.probe_sc = w.probe_sc;
   a.probe_cl = w.probe_cl;
   a.probe_off = w.probe_off;
-  a.P = p.nprobe < ix.k ? p.nprobe : ix.k;
+  a.P = probe_stride(ix, p.nprobe);
   a.items = w.items;
   a.seed_items = w.seed_items;
   a.item_cap = w.item_cap;

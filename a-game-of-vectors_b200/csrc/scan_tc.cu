@@ -492,7 +492,7 @@ __global__ void __launch_bounds__(1024) k_raise_thr(const uint32_t* __restrict__
 
 int launch_scan_tc(const DevIndex& ix, Workspace& w, uint32_t nq, const sg_params& p, const uint64_t* allow,
                    uint64_t allow_words, int sms, const Config& cfg, uint32_t chunk_blocks, cudaStream_t st) {
-  const uint32_t P = p.nprobe < ix.k ? p.nprobe : ix.k;
+  const uint32_t P = probe_stride(ix, p.nprobe);
   const uint32_t split = cfg.tc_split, tmin = std::max<uint32_t>(cfg.tc_min_queries, 1);
   TcArgs a{};
   a.codes = reinterpret_cast<const uint4*>(ix.blocks_tc);

@@ -146,6 +146,34 @@ void free_ws(sg::Workspace& w) {
   w = sg::Workspace();
 }
 
+}  // namespace
+
+namespace sg {
+// Per-cluster chunk and slot counts, largest first, as prefix sums over x.k clusters (from
+// x.h_block_off): the work-queue and candidate-buffer bounds of a call probing P clusters.
+void set_cluster_bounds(DevIndex& x, uint32_t chunk) {
+  const uint32_t K = x.k;
+  std::vector<uint32_t> ch(K);
+  std::vector<uint64_t> sl(K);
+  for (uint32_t c = 0; c < K; c++) {
+    const uint64_t nb = x.h_block_off[c + 1] - x.h_block_off[c];
+    ch[c] = (uint32_t)((nb + chunk - 1) / chunk);
+    sl[c] = nb * SG_BLOCK;
+  }
+  std::sort(ch.begin(), ch.end(), std::greater<uint32_t>());
+  std::sort(sl.begin(), sl.end(), std::greater<uint64_t>());
+  x.h_chunks_desc_prefix.assign(K + 1, 0);
+  x.h_slots_desc_prefix.assign(K + 1, 0);
+  for (uint32_t c = 0; c < K; c++) {
+    x.h_chunks_desc_prefix[c + 1] = x.h_chunks_desc_prefix[c] + ch[c];
+    x.h_slots_desc_prefix[c + 1] = x.h_slots_desc_prefix[c] + sl[c];
+  }
+}
+}  // namespace sg
+
+namespace {
+using sg::set_cluster_bounds;
+
 int build_index(const sg_ivf_arrays* a, int device, sg_index** out) {
   if (!a || !out) return fail(SG_ERR_INVALID, "null argument");
   *out = nullptr;
@@ -170,6 +198,7 @@ int build_index(const sg_ivf_arrays* a, int device, sg_index** out) {
   sg::DevIndex& x = h->ix;
   x.device = device;
   x.k = K;
+  x.kc = K;
   x.n = a->n;
   x.nblocks = nblocks;
   x.nslots = nblocks * SG_BLOCK;
@@ -192,20 +221,7 @@ int build_index(const sg_ivf_arrays* a, int device, sg_index** out) {
   }
   std::vector<uint32_t> boff32(K + 1);
   for (uint32_t c = 0; c <= K; c++) boff32[c] = (uint32_t)a->block_off[c];
-  // per-cluster chunk counts, largest first, for the work-queue capacity bound
-  {
-    std::vector<uint32_t> ch(K);
-    for (uint32_t c = 0; c < K; c++)
-      ch[c] = (boff32[c + 1] - boff32[c] + h->cfg.small_chunk_blocks - 1) / h->cfg.small_chunk_blocks;
-    std::sort(ch.begin(), ch.end(), std::greater<uint32_t>());
-    x.h_chunks_desc_prefix.assign(K + 1, 0);
-    for (uint32_t c = 0; c < K; c++) x.h_chunks_desc_prefix[c + 1] = x.h_chunks_desc_prefix[c] + ch[c];
-    std::vector<uint64_t> sl(K);
-    for (uint32_t c = 0; c < K; c++) sl[c] = (uint64_t)(boff32[c + 1] - boff32[c]) * SG_BLOCK;
-    std::sort(sl.begin(), sl.end(), std::greater<uint64_t>());
-    x.h_slots_desc_prefix.assign(K + 1, 0);
-    for (uint32_t c = 0; c < K; c++) x.h_slots_desc_prefix[c + 1] = x.h_slots_desc_prefix[c] + sl[c];
-  }
+  set_cluster_bounds(x, h->cfg.small_chunk_blocks);
   // centroids: row-major, transposed, BF16; largest norm for the routing error window
   std::vector<float> ct((size_t)K * SG_PDIM);
   std::vector<__nv_bfloat16> cb((size_t)K * SG_PDIM);
@@ -342,7 +358,7 @@ int ensure_ws_impl(sg_index* h, sg::Ctx& c, uint32_t nq, const sg_params& p, uin
   sg::Workspace& w = c.ws;
   cbuf_per_q = (cbuf_per_q + 3) & ~3u;
   const sg::DevIndex& x = h->ix;
-  const uint32_t P = std::min<uint32_t>(p.nprobe, x.k);
+  const uint32_t P = sg::probe_stride(x, p.nprobe);
   const uint32_t cand = std::max<uint32_t>(p.cand, 1);
   const uint32_t k = std::max<uint32_t>(p.k, 1);
   int rc;
@@ -374,10 +390,10 @@ int ensure_ws_impl(sg_index* h, sg::Ctx& c, uint32_t nq, const sg_params& p, uin
     w.cbuf_cap = 0;
   }
   const uint32_t n = w.nq_cap;
-  if ((uint64_t)n * x.k > w.scores_cap) {
+  if ((uint64_t)n * x.kc > w.scores_cap) {
     dfree(w.scores);
-    if ((rc = dalloc(&w.scores, (size_t)n * x.k))) return rc;
-    w.scores_cap = (uint64_t)n * x.k;
+    if ((rc = dalloc(&w.scores, (size_t)n * x.kc))) return rc;
+    w.scores_cap = (uint64_t)n * x.kc;
   }
   if (P > w.P_cap) {
     dfree(w.probe_sc); dfree(w.probe_cl); dfree(w.probe_off);
@@ -407,10 +423,17 @@ int ensure_ws_impl(sg_index* h, sg::Ctx& c, uint32_t nq, const sg_params& p, uin
     w.item_cap = want;
   }
   if (!w.counters && (rc = dalloc(&w.counters, 8))) return rc;
-  if (!w.inv_cnt) {
+  if (!w.inv_cnt || w.inv_k != x.k) {  // a live index has twice the clusters it opened with
+    dfree(w.inv_cnt);
+    dfree(w.inv_fill);
+    dfree(w.inv_off);
+    dfree(w.inv_list);
+    dfree(w.gitems);
+    w.inv_cap = 0;
     if ((rc = dalloc(&w.inv_cnt, x.k)) || (rc = dalloc(&w.inv_fill, x.k)) ||
         (rc = dalloc(&w.inv_off, (size_t)x.k + 1)))
       return rc;
+    w.inv_k = x.k;
   }
   const uint64_t pairs = (uint64_t)nq * P;
   if (pairs > w.inv_cap) {
@@ -436,8 +459,8 @@ int check_params(const sg_index* h, const sg_params* p) {
   if (!p) return fail(SG_ERR_INVALID, "params is null");
   if (p->cand > sg::kMaxCand || p->k > sg::kMaxCand || p->rerank_r > sg::kMaxCand)
     return fail(SG_ERR_INVALID, "cand, k and rerank_r must be <= 4096");
-  if (std::min<uint32_t>(p->nprobe, h->ix.k) > 4096)
-    return fail(SG_ERR_INVALID, "nprobe must be <= 4096");
+  if (sg::probe_stride(h->ix, p->nprobe) > 4096)
+    return fail(SG_ERR_INVALID, h->ix.live ? "nprobe must be <= 2048 in a live index" : "nprobe must be <= 4096");
   if (p->rerank_kind > SG_RERANK_SSD) return fail(SG_ERR_INVALID, "unknown rerank kind");
   if ((p->rerank_kind == SG_RERANK_PREFIX ||
        (p->rerank_kind == SG_RERANK_TIERED && !h->ix.has_t2)) &&
@@ -463,7 +486,7 @@ bool use_mma(const sg_index* h, const sg::Config& cfg, uint32_t nq, uint32_t P) 
 // Exact per-query candidate-buffer bound. A slot is appended at most once, so the probed
 // clusters' slots bound it; the ALU scan also cuts every chunk to `cand`, so chunks x cand does.
 uint32_t full_cap(const sg_index* h, const sg::Config& cfg, const sg_params& p, uint32_t nq) {
-  const uint32_t P = std::min<uint32_t>(p.nprobe, h->ix.k);
+  const uint32_t P = sg::probe_stride(h->ix, p.nprobe);
   uint64_t b = h->ix.h_slots_desc_prefix[P];
   // (a global-code chunk keeps every slot tied with its cand-th score, so only the slots bound it)
   if (!use_mma(h, cfg, nq, P) && !h->ix.global)
@@ -515,7 +538,7 @@ int run_pipeline(sg_index* h, const sg::Config& cfg, sg::Ctx& c, uint32_t nq, co
   const uint32_t cb = small ? cfg.small_chunk_blocks : cfg.chunk_blocks;
   const uint32_t sb = small ? cfg.small_seed_blocks : cfg.seed_blocks;
   // The tensor-core scan pays off once enough queries share each probed cluster.
-  const uint32_t P = std::min<uint32_t>(p.nprobe, x.k);
+  const uint32_t P = sg::probe_stride(x, p.nprobe);
   const bool mma = !rp.expand() && use_mma(h, cfg, nq, P);
   if (rp.expand())
     sg::launch_route_expand(x, w, nq, p, cb, sb, rp.per_cluster, rp.target, st);
@@ -901,9 +924,110 @@ void free_ctx(Ctx& c) {
   c.stream = nullptr;
 }
 
+// ---- live indexes (live.cu) ---------------------------------------------------------------
+// Grows a device array from `have` to `want` elements, keeping its first `have` (device copy).
+template <typename T>
+static int grow(T*& p, size_t have, size_t want) {
+  if (!p) return SG_OK;
+  T* q = nullptr;
+  int rc = dalloc(&q, want);
+  if (rc) return rc;
+  if (have) CK(cudaMemcpy(q, p, have * sizeof(T), cudaMemcpyDeviceToDevice));
+  if (want > have) CK(cudaMemset(q + have, 0, (want - have) * sizeof(T)));
+  dfree(p);
+  p = q;
+  return SG_OK;
+}
+
+int index_make_live(sg_index* h, uint64_t max_rows, uint64_t block_cap) {
+  DevIndex& x = h->ix;
+  if (x.live) return fail(SG_ERR_INVALID, "the index is live already");
+  if (x.global) return fail(SG_ERR_UNSUPPORTED, "live updates need a RaBitQ index (src/live.rs:168)");
+  if (2ull * x.kc > 4096ull * 1024) return fail(SG_ERR_INVALID, "too many clusters for a live index");
+  if ((x.nblocks + block_cap) * SG_BLOCK >= 0xFFFFFFFFull) return fail(SG_ERR_INVALID, "more than 2^32 slots");
+  CK(cudaSetDevice(x.device));
+  CK(cudaDeviceSynchronize());
+  const size_t nb = x.nblocks, nb2 = nb + block_cap, n = x.n, n2 = n + max_rows;
+  int rc;
+  if ((rc = grow(x.blocks, nb * SG_BLOCK_BYTES, nb2 * SG_BLOCK_BYTES)) ||
+      (rc = grow(x.blocks_tc, nb * 256, nb2 * 256)) || (rc = grow(x.mul, nb * SG_BLOCK, nb2 * SG_BLOCK)) ||
+      (rc = grow(x.err, nb * SG_BLOCK, nb2 * SG_BLOCK)) || (rc = grow(x.ids, nb * SG_BLOCK, nb2 * SG_BLOCK)) ||
+      (rc = grow(x.rerank, n * SG_DIM, n2 * SG_DIM)) || (rc = grow(x.norm256, n, n2)) ||
+      (rc = grow(x.t2_codes, n * SG_TIER2_BYTES, n2 * SG_TIER2_BYTES)) || (rc = grow(x.t2_norm, n, n2)) ||
+      (rc = grow(x.codes, n * SG_CODE_BYTES, n2 * SG_CODE_BYTES)))
+    return rc;
+  // clusters kc..2kc-1: the delta lists, empty, after the base blocks
+  const uint32_t kc = x.kc;
+  x.h_block_off.resize(2 * (size_t)kc + 1, x.h_block_off[kc]);
+  x.h_clen.resize(2 * (size_t)kc, 0);
+  std::vector<uint32_t> boff32(2 * (size_t)kc + 1);
+  for (size_t c = 0; c < boff32.size(); c++) boff32[c] = (uint32_t)x.h_block_off[c];
+  dfree(x.block_off);
+  dfree(x.clen);
+  if ((rc = upload(&x.block_off, boff32.data(), boff32.size())) ||
+      (rc = upload(&x.clen, x.h_clen.data(), x.h_clen.size())))
+    return rc;
+  x.k = 2 * kc;
+  x.live = true;
+  x.nslots = nb2 * SG_BLOCK;
+  {
+    std::lock_guard<std::mutex> g(h->cfg_mu);
+    set_cluster_bounds(x, h->cfg.small_chunk_blocks);
+    h->cfg.gen++;
+  }
+  // the default context's workspace is sized for the old cluster count
+  free_ws(h->def.ws);
+  drop_graphs(h->def);
+  h->def.gen++;
+  return SG_OK;
+}
+
+int index_set_delta(sg_index* h, const uint32_t* nb_of, const uint32_t* clen_of, const uint8_t* blocks,
+                    const float* mul, const float* err, const uint32_t* ids, uint64_t nblocks) {
+  DevIndex& x = h->ix;
+  const uint32_t kc = x.kc;
+  const uint64_t b0 = x.nblocks;
+  if (b0 + nblocks > x.nslots / SG_BLOCK) return fail(SG_ERR_OOM, "the live index's delta lists are full");
+  CK(cudaSetDevice(x.device));
+  cudaStream_t st = h->def.stream;
+  CK(cudaStreamSynchronize(st));
+  if (nblocks) {
+    CK(cudaMemcpy(x.blocks + b0 * SG_BLOCK_BYTES, blocks, nblocks * SG_BLOCK_BYTES, cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(x.mul + b0 * SG_BLOCK, mul, nblocks * SG_BLOCK * 4, cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(x.err + b0 * SG_BLOCK, err, nblocks * SG_BLOCK * 4, cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(x.ids + b0 * SG_BLOCK, ids, nblocks * SG_BLOCK * 4, cudaMemcpyHostToDevice));
+    sg::transcode_tc(x.blocks + b0 * SG_BLOCK_BYTES, nblocks, x.blocks_tc + b0 * 256, st);
+    CK(cudaGetLastError());
+  }
+  uint64_t off = b0;
+  for (uint32_t c = 0; c < kc; c++) {
+    x.h_block_off[kc + c] = off;
+    x.h_clen[kc + c] = clen_of[c];
+    off += nb_of[c];
+  }
+  x.h_block_off[2 * (size_t)kc] = off;
+  std::vector<uint32_t> boff32(kc + 1);
+  for (uint32_t c = 0; c <= kc; c++) boff32[c] = (uint32_t)x.h_block_off[kc + c];
+  CK(cudaMemcpyAsync(x.block_off + kc, boff32.data(), (kc + 1) * 4, cudaMemcpyHostToDevice, st));
+  CK(cudaMemcpyAsync(x.clen + kc, x.h_clen.data() + kc, (size_t)kc * 4, cudaMemcpyHostToDevice, st));
+  CK(cudaStreamSynchronize(st));
+  std::lock_guard<std::mutex> g(h->cfg_mu);
+  set_cluster_bounds(x, h->cfg.small_chunk_blocks);
+  h->cfg.gen++;  // captured pipelines baked in the old bounds: their keys go stale
+  return SG_OK;
+}
+
+int index_search_allow(sg_index* h, uint32_t nq, const float* q768, const float* q256, const sg_params& p,
+                       const uint64_t* d_allow, uint64_t allow_words, float* out_sc, uint32_t* out_id,
+                       uint32_t* out_n) {
+  std::lock_guard<std::mutex> g(h->mu);
+  return search_impl(h, index_config(h), h->def, nq, q768, q256, p, d_allow, allow_words, out_sc, out_id, out_n,
+                     nullptr, false, true);
+}
+
 // Device scratch of a batch of nq queries with params p (the workspace ensure_ws grows to).
 uint64_t ctx_bytes(const sg_index* h, const Config& cfg, const sg_params& p, uint32_t nq) {
-  const uint64_t P = std::min<uint32_t>(p.nprobe, h->ix.k);
+  const uint64_t P = sg::probe_stride(h->ix, p.nprobe);
   const uint64_t cap = batch_cap(h, cfg, p, nq);
   const uint64_t per_q = SG_DIM * 4 * 2 + SG_PDIM * 5 + 1024 + 64 + (uint64_t)h->ix.k * 4 + P * 16 +
                          cap * 12 + (uint64_t)std::max<uint32_t>(p.cand, 1) * 20 +
@@ -1006,7 +1130,7 @@ int sg_close(sg_index* h) {
 int sg_index_info(const sg_index* h, uint32_t* k, uint64_t* n, uint64_t* nblocks,
                   uint32_t* has_tier2) {
   if (!h) return fail(SG_ERR_INVALID, "null index");
-  if (k) *k = h->ix.k;
+  if (k) *k = h->ix.kc;
   if (n) *n = h->ix.n;
   if (nblocks) *nblocks = h->ix.nblocks;
   if (has_tier2) *has_tier2 = h->ix.has_t2;
@@ -1186,7 +1310,7 @@ int sg_route_scores(sg_index* h, uint32_t nq, const float* q256, float* out_scor
   CK(sg::launch_route_scores(h->ix, w, nq, sg::index_config(h).route_precision, st));
   CK(cudaGetLastError());
   uint32_t status = 0;
-  CK(cudaMemcpyAsync(out_scores, w.scores, (size_t)nq * h->ix.k * 4, cudaMemcpyDeviceToHost, st));
+  CK(cudaMemcpyAsync(out_scores, w.scores, (size_t)nq * h->ix.kc * 4, cudaMemcpyDeviceToHost, st));
   CK(cudaMemcpyAsync(&status, w.counters + 2, 4, cudaMemcpyDeviceToHost, st));
   CK(cudaStreamSynchronize(st));
   if (status & sg::kStatusTimeout) return fail(SG_ERR_DEVICE, "routing GEMM: a tensor-core wait ran out");
@@ -1258,7 +1382,8 @@ int sg_candidates_probes(sg_index* h, uint32_t nq, const float* q256, const floa
   if ((rc = check_params(h, params))) return rc;
   if (nq == 0) return SG_OK;
   const sg_params& p = *params;
-  const uint32_t P = std::min<uint32_t>(p.nprobe, h->ix.k);
+  if (h->ix.live) return fail(SG_ERR_UNSUPPORTED, "probe lists of a live index come from its own routing");
+  const uint32_t P = sg::probe_stride(h->ix, p.nprobe);
   for (uint32_t q = 0; q < nq; q++) {
     if (probe_counts[q] > P) return fail(SG_ERR_INVALID, "a probe list is longer than min(nprobe, k)");
     for (uint32_t r = 0; r < probe_counts[q]; r++)

@@ -262,6 +262,12 @@ EXPORTS = [
     "sg_candidates",
     "sg_candidates_probes",
     "sg_rerank",
+    "sg_live_open",
+    "sg_live_close",
+    "sg_live_insert",
+    "sg_live_delete",
+    "sg_live_search",
+    "sg_live_info",
     "sg_filter_new",
     "sg_filter_info",
     "sg_filter_free",

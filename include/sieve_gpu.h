@@ -312,6 +312,31 @@ int sg_rerank(sg_index* index, uint32_t nq, const float* q768, const float* q256
               const uint32_t* cand_ids, const float* cand_err, const uint32_t* cand_counts, uint32_t cand_stride,
               const sg_params* params, float* out_scores, uint32_t* out_ids, uint32_t* out_counts);
 
+/* ---- live updates: ivf live layer (src/live.rs) ------------------------------------------ */
+/* Inserts, deletes and upserts over an open index without a rebuild (Live, src/live.rs:1-17):
+ * an inserted row is encoded on the device as Live::apply_insert encodes it (src/live.rs:318-350)
+ * and its slots join per-centroid delta lists in the base block layout, scanned right after each
+ * probed cluster's base list (src/ivf.rs:682-684); a delete tombstones the row (View::hidden,
+ * src/ivf.rs:474-483). Results carry external ids: a corpus row's is its row, an inserted row's
+ * the id it was inserted under; inserting a live id replaces it. The write-ahead log, its replay
+ * and compaction are host file I/O and not part of this path. */
+typedef struct sg_live sg_live;
+/* Live::open (src/live.rs:167-209) over a RaBitQ index: its row and slot arrays grow on the
+ * device to hold max_rows inserted rows (the old arrays are copied, so the device briefly holds
+ * both). soar_lambda < 0: inserts take no SOAR secondary (the index was built without SOAR).
+ * Search a live index through sg_live_search only; close the live handle before the index. */
+int sg_live_open(sg_index* index, uint64_t max_rows, float soar_lambda, sg_live** out);
+int sg_live_close(sg_live* live);
+/* Live::insert (src/live.rs:274-292): m unit 768-d vectors vecs [m * 768] under ext_ids [m]. */
+int sg_live_insert(sg_live* live, uint32_t m, const uint32_t* ext_ids, const float* vecs);
+/* Live::delete (src/live.rs:295-305): external ids; unknown ones are ignored. */
+int sg_live_delete(sg_live* live, uint32_t m, const uint32_t* ext_ids);
+/* Live::search (src/live.rs:381-385) for nq queries; outputs as sg_search, with external ids. */
+int sg_live_search(sg_live* live, uint32_t nq, const float* q768, const float* q256, const sg_params* params,
+                   float* out_scores, uint32_t* out_ids, uint32_t* out_counts);
+/* Rows inserted, slots in delta lists, rows tombstoned (each nullable). */
+int sg_live_info(sg_live* live, uint64_t* delta_rows, uint64_t* delta_slots, uint64_t* deleted);
+
 /* ---- filters: filter::Filter / Plan / search (src/filter.rs) ---------------------------- */
 /* filter::Plan (src/filter.rs:42-53). */
 typedef enum {

@@ -399,6 +399,20 @@ class OracleIndex:
             return s, o, cnt, scanned, tie.astype(bool)
         return s, o, cnt, scanned
 
+    def live_encode(self, cents_rot, soar: bool, lam: float, v):
+        """Live::apply_insert's encoding of one unit 768-d row (src/live.rs:318-350): (int8 row,
+        prefix norm, (primary, secondary or PAD), codes [2, 32], factors [2, 2], tier-2 code, norm)."""
+        row = np.zeros(768, np.int8)
+        nrm, t2n = c_float(), c_float()
+        pair = np.zeros(2, np.uint32)
+        codes = np.zeros((2, 32), np.uint8)
+        fac = np.zeros((2, 2), np.float32)
+        t2 = np.zeros(64, np.uint8)
+        self.L.or_live_encode(ctypes.byref(self.st), P(f32(cents_rot)), c_int(1 if soar else 0), c_float(lam),
+                              P(f32(v)), P(row), ctypes.byref(nrm), P(pair), P(codes), P(fac), P(t2),
+                              ctypes.byref(t2n))
+        return row, nrm.value, pair, codes, fac, t2, t2n.value
+
     def flat_hamming(self, codes, q768, q256, cand: int, k: int):
         """The search binary's flat Hamming baseline (src/bin/search.rs:251-269) over codes.bin."""
         codes = np.ascontiguousarray(codes, np.uint8)

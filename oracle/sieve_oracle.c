@@ -865,6 +865,86 @@ uint32_t or_search(const sg_ivf_arrays* ix, const float* q768, const float* q256
   return k;
 }
 
+/* Live::apply_insert's encoding of one inserted row (src/live.rs:274-350), as ivf::build encodes
+ * a row: the int8 row (Int8Quantizer::encode), the prefix norm, the normalised prefix of the int8
+ * row, its primary cluster and (with SOAR) its secondary among the 16 nearest (assign_top,
+ * soar_secondary, src/ivf.rs:138-186), the RaBitQ residual code and factors of the rotated
+ * prefix against each rotated centroid (rabitq::encode), and the 2-bit tier code and norm.
+ * pair[1] = PAD without SOAR; its code and factors are then zero. */
+static float dot16(const float* a, const float* b, uint32_t n) { return or_dot_f32(a, b, n); }
+
+static uint32_t soar_secondary(const float* x, const float* cents, const uint32_t* cand, uint32_t nc,
+                               float lambda) {
+  const float* c1 = cents + (uint64_t)cand[0] * SG_PDIM;
+  float x_c1 = dot16(x, c1, SG_PDIM);
+  float r2 = fmaxf(2.0f - 2.0f * x_c1, 1e-12f);
+  float r_x = 1.0f - x_c1;
+  float best = FLT_MAX;
+  uint32_t best_c = cand[1];
+  for (uint32_t i = 1; i < nc; i++) {
+    const float* cv = cents + (uint64_t)cand[i] * SG_PDIM;
+    float x_c = dot16(x, cv, SG_PDIM);
+    float r_c = x_c - dot16(c1, cv, SG_PDIM);
+    float along = r_x - r_c;
+    float loss = (2.0f - 2.0f * x_c) + lambda * along * along / r2;
+    if (loss < best) {
+      best = loss;
+      best_c = cand[i];
+    }
+  }
+  return best_c;
+}
+
+void or_live_encode(const sg_ivf_arrays* ix, const float* cents_rot, int soar, float lambda, const float* v,
+                    int8_t* row, float* norm256, uint32_t* pair, uint8_t* codes, float* factors, uint8_t* t2,
+                    float* t2_norm) {
+  or_int8_encode(ix->quant_scale, v, row);
+  float nn = NEG0;
+  for (int i = 0; i < SG_PDIM; i++) nn += v[i] * v[i];
+  *norm256 = sqrtf(nn);
+  float x[SG_PDIM];
+  for (int i = 0; i < SG_PDIM; i++) x[i] = (float)row[i] / ix->quant_scale[i];
+  or_normalize(x, SG_PDIM);
+  const uint32_t K = ix->k;
+  float* sc = (float*)malloc(sizeof(float) * K);
+  or_gemm_abt(x, ix->centroids, 1, K, SG_PDIM, sc);
+  if (!soar) {
+    uint32_t bj = 0;
+    float bv = -FLT_MAX;
+    for (uint32_t j = 0; j < K; j++)
+      if (sc[j] > bv) {
+        bv = sc[j];
+        bj = j;
+      }
+    pair[0] = bj;
+    pair[1] = SG_PAD;
+  } else {
+    uint32_t cand[16] = {0};
+    uint32_t* ids = (uint32_t*)malloc(sizeof(uint32_t) * K);
+    for (uint32_t j = 0; j < K; j++) ids[j] = j;
+    float top_s[16];
+    uint32_t m = or_topk(sc, ids, K, 16, top_s, cand);
+    free(ids);
+    (void)m;  /* fewer than 16 clusters leave the rest of cand at cluster 0, as assign_top does */
+    pair[0] = cand[0];
+    pair[1] = soar_secondary(x, ix->centroids, cand, 16, lambda);
+  }
+  free(sc);
+  float xr[SG_PDIM];
+  memcpy(xr, x, sizeof xr);
+  or_rotation_apply(ix->rotation, SG_PDIM, xr);
+  for (int h = 0; h < 2; h++) {
+    if (pair[h] == SG_PAD) {
+      memset(codes + h * SG_CODE_BYTES, 0, SG_CODE_BYTES);
+      factors[2 * h] = factors[2 * h + 1] = 0.0f;
+      continue;
+    }
+    or_rabitq_encode(xr, cents_rot + (uint64_t)pair[h] * SG_PDIM, SG_PDIM, codes + h * SG_CODE_BYTES,
+                     factors + 2 * h);
+  }
+  if (ix->tier2_sigma) *t2_norm = or_tier2_encode(ix->tier2_sigma, x, t2);
+}
+
 /* The flat Hamming baseline of the search binary (src/bin/search.rs:251-269): the query's sign code
  * against every corpus code (hamming, src/lut.rs:156-165), TopK(cand) of PDIM - distance keyed by
  * row, then the rows' float-weight int8 dot (quant::dot_i8 with Int8Quantizer::query_weights)

@@ -104,6 +104,13 @@ uint32_t or_rerank(const sg_ivf_arrays* ix, const float* q768, const float* q256
 uint32_t or_search(const sg_ivf_arrays* ix, const float* q768, const float* q256,
                    const sg_params* p, const uint64_t* allow, uint64_t allow_words,
                    float* out_scores, uint32_t* out_ids, sg_timing* t);
+/* Live::apply_insert's encoding of one unit 768-d row v (src/live.rs:274-350); cents_rot are the
+ * index's centroids rotated (Live::open, src/live.rs:171-179). Outputs: row [768], *norm256,
+ * pair [2] (PAD without SOAR), codes [2 * 32], factors [2 * 2], t2 [64] and *t2_norm (when the
+ * index has a 2-bit tier). */
+void or_live_encode(const sg_ivf_arrays* ix, const float* cents_rot, int soar, float lambda, const float* v,
+                    int8_t* row, float* norm256, uint32_t* pair, uint8_t* codes, float* factors, uint8_t* t2,
+                    float* t2_norm);
 /* The flat Hamming baseline (src/bin/search.rs:251-269) over codes.bin [n * 32]: out_* [k]. */
 uint32_t or_flat_hamming(const uint8_t* codes, uint64_t n, const int8_t* rerank, const float* quant_scale,
                          const float* q768, const float* q256, uint32_t cand, uint32_t k, float* out_scores,
