@@ -323,6 +323,34 @@ def plan_resolve(plan: int, allowed_rows: int, n: int) -> int:
 
 
 # ---- the query path over an index ------------------------------------------------------------
+def build_ivf(corpus: dict, k: int, sample_n: int, iters: int, balance: float | None = None,
+              soar_lambda: float | None = 1.0) -> dict:
+    """ivf::build (src/ivf.rs:268-395) with RaBitQ codes, on the corpus's int8 rows: the arrays
+    of the index files (centroids, tier-2 files, block_off, ids, blocks, factors, rotation)."""
+    n = int(corpus["n"])
+    rer = np.ascontiguousarray(corpus["rerank"], np.int8)
+    scale = f32(corpus["quant_scale"])
+    cents = np.zeros((k, 256), np.float32)
+    sigma = np.zeros(256, np.float32)
+    t2 = np.zeros((n, 64), np.uint8)
+    t2n = np.zeros(n, np.float32)
+    boff = np.zeros(k + 1, np.uint64)
+    maxb = (2 * n + 31) // 32 + k
+    ids = np.zeros(maxb * 32, np.uint32)
+    blocks = np.zeros(maxb * 1024, np.uint8)
+    fac = np.zeros(maxb * 64, np.float32)
+    L = lib()
+    L.or_build_ivf.restype = c_uint64
+    nb = L.or_build_ivf(c_uint64(n), P(rer), P(scale), c_uint32(k), c_uint64(sample_n), c_uint32(iters),
+                        c_int(balance is not None), c_float(balance or 0.0), c_int(soar_lambda is not None),
+                        c_float(soar_lambda or 0.0), P(cents), P(sigma), P(t2), P(t2n), P(boff), P(ids),
+                        P(blocks), P(fac), c_uint64(maxb))
+    assert nb <= maxb
+    return {"n": n, "k": k, "centroids": cents, "tier2_sigma": sigma, "tier2_codes": t2, "tier2_norm": t2n,
+            "block_off": boff, "ids": ids[: nb * 32], "blocks": blocks[: nb * 1024], "factors": fac[: nb * 64],
+            "rotation": rotation_signs(11)}
+
+
 TIE_CANONICAL, TIE_REFERENCE = 0, 1
 
 

@@ -865,6 +865,194 @@ uint32_t or_search(const sg_ivf_arrays* ix, const float* q768, const float* q256
   return k;
 }
 
+/* ---- ivf::build: src/ivf.rs:188-395 (the index the query path reads) -------------------- */
+static uint32_t soar_secondary(const float* x, const float* cents, const uint32_t* cand, uint32_t nc,
+                               float lambda);
+
+/* Corpus::prefix_f32 (src/ivf.rs:110-116): the int8 row's prefix over its scale, normalised. */
+static void prefix_f32(const int8_t* rerank, const float* scale, uint64_t i, float* out) {
+  for (int d = 0; d < SG_PDIM; d++) out[d] = (float)rerank[i * SG_DIM + d] / scale[d];
+  or_normalize(out, SG_PDIM);
+}
+
+/* assign (src/ivf.rs:160-162): the first maximum of the sequential f32 dots. */
+static uint32_t assign1(const float* x, const float* cents, uint32_t k) {
+  uint32_t bj = 0;
+  float bv = -FLT_MAX;
+  for (uint32_t j = 0; j < k; j++) {
+    float s;
+    or_gemm_abt(x, cents + (uint64_t)j * SG_PDIM, 1, 1, SG_PDIM, &s);
+    if (s > bv) {
+      bv = s;
+      bj = j;
+    }
+  }
+  return bj;
+}
+
+/* split_large (src/ivf.rs:231-254). The reference orders clusters by size with an unstable sort,
+ * which leaves equal sizes in an unspecified order; here equal sizes keep cluster order. */
+static uint32_t split_large(const float* sample, uint64_t n, const uint32_t* a, const uint64_t* counts,
+                            uint32_t k, float* cents, float r, uint64_t* rng) {
+  float mean = (float)n / (float)k;
+  uint32_t* order = (uint32_t*)malloc(sizeof(uint32_t) * k);
+  for (uint32_t c = 0; c < k; c++) order[c] = c;
+  for (uint32_t i = 1; i < k; i++) { /* stable insertion sort by count desc */
+    uint32_t v = order[i];
+    int32_t j = (int32_t)i - 1;
+    while (j >= 0 && counts[order[j]] < counts[v]) {
+      order[j + 1] = order[j];
+      j--;
+    }
+    order[j + 1] = v;
+  }
+  uint32_t nl = 0;
+  while (nl < k && (float)counts[order[nl]] > r * mean) nl++;
+  uint32_t ns = 0;
+  while (ns < nl && ns < k && (float)counts[order[k - 1 - ns]] < 0.5f * mean) ns++;
+  for (uint32_t t = 0; t < ns; t++) {
+    uint32_t big = order[t], tiny = order[k - 1 - t];
+    uint64_t cnt = 0;
+    for (uint64_t i = 0; i < n; i++) cnt += a[i] == big;
+    uint64_t pick_k = or_rng_below(rng, cnt), seen = 0, pick = 0;
+    for (uint64_t i = 0; i < n; i++)
+      if (a[i] == big && seen++ == pick_k) {
+        pick = i;
+        break;
+      }
+    memcpy(cents + (uint64_t)tiny * SG_PDIM, sample + pick * SG_PDIM, sizeof(float) * SG_PDIM);
+  }
+  free(order);
+  return ns;
+}
+
+/* kmeans (src/ivf.rs:194-225): spherical Lloyd on the sample. */
+static void kmeans(const float* sample, uint64_t n, uint32_t k, uint32_t iters, uint64_t seed, int has_balance,
+                   float balance, float* cents) {
+  uint64_t rng = seed;
+  for (uint32_t c = 0; c < k; c++)
+    memcpy(cents + (uint64_t)c * SG_PDIM, sample + or_rng_below(&rng, n) * SG_PDIM, sizeof(float) * SG_PDIM);
+  uint32_t* a = (uint32_t*)malloc(sizeof(uint32_t) * (n ? n : 1));
+  float* sums = (float*)malloc(sizeof(float) * k * SG_PDIM);
+  uint64_t* counts = (uint64_t*)malloc(sizeof(uint64_t) * k);
+  for (uint32_t it = 0; it < iters; it++) {
+    for (uint64_t i = 0; i < n; i++) a[i] = assign1(sample + i * SG_PDIM, cents, k);
+    memset(sums, 0, sizeof(float) * k * SG_PDIM);
+    memset(counts, 0, sizeof(uint64_t) * k);
+    for (uint64_t i = 0; i < n; i++) {
+      counts[a[i]]++;
+      for (int d = 0; d < SG_PDIM; d++) sums[(uint64_t)a[i] * SG_PDIM + d] += sample[i * SG_PDIM + d];
+    }
+    for (uint32_t c = 0; c < k; c++) {
+      float* dst = cents + (uint64_t)c * SG_PDIM;
+      if (counts[c] == 0) {
+        memcpy(dst, sample + or_rng_below(&rng, n) * SG_PDIM, sizeof(float) * SG_PDIM);
+      } else {
+        memcpy(dst, sums + (uint64_t)c * SG_PDIM, sizeof(float) * SG_PDIM);
+        or_normalize(dst, SG_PDIM);
+      }
+    }
+    if (has_balance && it + 2 < iters) split_large(sample, n, a, counts, k, cents, balance, &rng);
+  }
+  free(a);
+  free(sums);
+  free(counts);
+}
+
+uint64_t or_build_ivf(uint64_t n, const int8_t* rerank, const float* quant_scale, uint32_t k, uint64_t sample_n,
+                      uint32_t iters, int has_balance, float balance, int has_soar, float lambda, float* cents,
+                      float* sigma, uint8_t* t2_codes, float* t2_norm, uint64_t* block_off, uint32_t* ids,
+                      uint8_t* blocks, float* factors, uint64_t max_blocks) {
+  uint64_t rng = 42;
+  if (sample_n > n) sample_n = n;
+  float* sample = (float*)malloc(sizeof(float) * (sample_n ? sample_n : 1) * SG_PDIM);
+  for (uint64_t s = 0; s < sample_n; s++) prefix_f32(rerank, quant_scale, or_rng_below(&rng, n), sample + s * SG_PDIM);
+  kmeans(sample, sample_n, k, iters, 7, has_balance, balance, cents);
+  or_tier2_fit(sample, sample_n, sigma);
+  free(sample);
+  float signs[3 * SG_PDIM];
+  or_rotation_signs(11, SG_PDIM, signs);
+  float* cents_rot = (float*)malloc(sizeof(float) * k * SG_PDIM);
+  memcpy(cents_rot, cents, sizeof(float) * k * SG_PDIM);
+  for (uint32_t c = 0; c < k; c++) or_rotation_apply(signs, SG_PDIM, cents_rot + (uint64_t)c * SG_PDIM);
+  uint64_t* cnt = (uint64_t*)calloc(k, sizeof(uint64_t));
+  uint32_t* pc = (uint32_t*)malloc(sizeof(uint32_t) * 2 * (n ? n : 1));
+  uint8_t* pcode = (uint8_t*)malloc(2 * SG_CODE_BYTES * (n ? n : 1));
+  float* pfac = (float*)malloc(sizeof(float) * 4 * (n ? n : 1));
+  float* sc = (float*)malloc(sizeof(float) * k);
+  uint32_t* cid = (uint32_t*)malloc(sizeof(uint32_t) * k);
+  for (uint32_t j = 0; j < k; j++) cid[j] = j;
+  for (uint64_t i = 0; i < n; i++) {
+    float x[SG_PDIM], xr[SG_PDIM];
+    prefix_f32(rerank, quant_scale, i, x);
+    t2_norm[i] = or_tier2_encode(sigma, x, t2_codes + i * SG_TIER2_BYTES);
+    uint32_t* pair = pc + 2 * i;
+    if (!has_soar) {
+      pair[0] = assign1(x, cents, k);
+      pair[1] = SG_PAD;
+    } else {
+      uint32_t cand[16] = {0};
+      float top[16];
+      or_gemm_abt(x, cents, 1, k, SG_PDIM, sc);
+      or_topk(sc, cid, k, 16, top, cand);
+      pair[0] = cand[0];
+      pair[1] = soar_secondary(x, cents, cand, 16, lambda);
+    }
+    memcpy(xr, x, sizeof xr);
+    or_rotation_apply(signs, SG_PDIM, xr);
+    for (int h = 0; h < 2; h++) {
+      uint8_t* code = pcode + (2 * i + h) * SG_CODE_BYTES;
+      float* f = pfac + 4 * i + 2 * h;
+      memset(code, 0, SG_CODE_BYTES);
+      f[0] = f[1] = 0.0f;
+      if (pair[h] == SG_PAD) continue;
+      or_rabitq_encode(xr, cents_rot + (uint64_t)pair[h] * SG_PDIM, SG_PDIM, code, f);
+      cnt[pair[h]]++;
+    }
+  }
+  uint64_t nb = 0;
+  block_off[0] = 0;
+  for (uint32_t c = 0; c < k; c++) {
+    nb += (cnt[c] + SG_BLOCK - 1) / SG_BLOCK;
+    block_off[c + 1] = nb;
+  }
+  if (nb <= max_blocks) {
+    /* cluster-major write (src/ivf.rs:356-385): members in row order, 32 per block */
+    uint64_t* fill = (uint64_t*)calloc(k, sizeof(uint64_t));
+    for (uint64_t s = 0; s < nb * SG_BLOCK; s++) {
+      ids[s] = SG_PAD;
+      factors[2 * s] = factors[2 * s + 1] = 0.0f;
+    }
+    uint8_t* raw = (uint8_t*)calloc(nb * SG_BLOCK + 1, SG_CODE_BYTES);
+    for (uint64_t i = 0; i < n; i++)
+      for (int h = 0; h < 2; h++) {
+        const uint32_t c = pc[2 * i + h];
+        if (c == SG_PAD) continue;
+        const uint64_t s = block_off[c] * SG_BLOCK + fill[c]++;
+        ids[s] = (uint32_t)i;
+        factors[2 * s] = pfac[4 * i + 2 * h];
+        factors[2 * s + 1] = pfac[4 * i + 2 * h + 1];
+        memcpy(raw + s * SG_CODE_BYTES, pcode + (2 * i + h) * SG_CODE_BYTES, SG_CODE_BYTES);
+      }
+    for (uint32_t c = 0; c < k; c++)
+      for (uint64_t b = block_off[c]; b < block_off[c + 1]; b++) {
+        const uint64_t s0 = b * SG_BLOCK, end = block_off[c] * SG_BLOCK + cnt[c];
+        const uint64_t used = s0 + SG_BLOCK <= end ? SG_BLOCK : end - s0;
+        or_pack_block(raw + s0 * SG_CODE_BYTES, (uint32_t)used, SG_GROUPS, blocks + b * SG_BLOCK_BYTES);
+      }
+    free(raw);
+    free(fill);
+  }
+  free(cents_rot);
+  free(cnt);
+  free(pc);
+  free(pcode);
+  free(pfac);
+  free(sc);
+  free(cid);
+  return nb;
+}
+
 /* Live::apply_insert's encoding of one inserted row (src/live.rs:274-350), as ivf::build encodes
  * a row: the int8 row (Int8Quantizer::encode), the prefix norm, the normalised prefix of the int8
  * row, its primary cluster and (with SOAR) its secondary among the 16 nearest (assign_top,

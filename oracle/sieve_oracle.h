@@ -104,6 +104,14 @@ uint32_t or_rerank(const sg_ivf_arrays* ix, const float* q768, const float* q256
 uint32_t or_search(const sg_ivf_arrays* ix, const float* q768, const float* q256,
                    const sg_params* p, const uint64_t* allow, uint64_t allow_words,
                    float* out_scores, uint32_t* out_ids, sg_timing* t);
+/* ivf::build (src/ivf.rs:268-395) over the corpus's int8 rows: centroids [k * 256], tier2 sigma
+ * [256], codes [n * 64] and norms [n], block_off [k + 1]; with the returned block count <=
+ * max_blocks also ids [nb * 32], blocks [nb * 1024] and factors [nb * 64]. Sample seed 42,
+ * k-means seed 7, rotation seed 11, 16 SOAR candidates, as the reference. */
+uint64_t or_build_ivf(uint64_t n, const int8_t* rerank, const float* quant_scale, uint32_t k, uint64_t sample_n,
+                      uint32_t iters, int has_balance, float balance, int has_soar, float lambda, float* cents,
+                      float* sigma, uint8_t* t2_codes, float* t2_norm, uint64_t* block_off, uint32_t* ids,
+                      uint8_t* blocks, float* factors, uint64_t max_blocks);
 /* Live::apply_insert's encoding of one unit 768-d row v (src/live.rs:274-350); cents_rot are the
  * index's centroids rotated (Live::open, src/live.rs:171-179). Outputs: row [768], *norm256,
  * pair [2] (PAD without SOAR), codes [2 * 32], factors [2 * 2], t2 [64] and *t2_norm (when the
