@@ -1,8 +1,11 @@
 // bigann.cu — the billion-scale L2 query path of bigann::Index (src/bigann.rs:634-747) on one GPU.
 //
 // Rows are int8 x 100; a query q (int8 x 100) ranks rows by s(x) = 2<q,x> - |x|^2. The stages:
-//   route      (src/bigann.rs:660-678): dots <q, c> of every leaf (sequential f32, exact), the
-//              TopK(nprobe) of 2<q,c> - |c|^2, then the margin rule on |q - c|^2.
+//   route      (src/bigann.rs:660-678): the TopK(nprobe) of 2<q,c> - |c|^2 over every leaf, then the
+//              margin rule on |q - c|^2. By default on the tcgen05 tensor cores with an exact FP32
+//              rescoring window (bg_route.cu); params.route_fp32 scores every leaf with the
+//              reference's sequential f32 dot instead (k_bg_scores + k_bg_select). Both give the
+//              same probe lists.
 //   candidates (src/bigann.rs:683-732): 32-group LUT scan of the probed leaves' 128-bit codes,
 //              est = 2 (cent + mul (a s + b)) - |x|^2, a TopK of the best `cand` (or, on a
 //              multi-bit index with refine > 0, a 1-bit shortlist TopK(max(refine, cand)) whose
@@ -19,6 +22,7 @@
 #include <float.h>
 
 #include <algorithm>
+#include <cmath>
 #include <fstream>
 #include <memory>
 #include <mutex>
@@ -693,6 +697,14 @@ struct BgWork {
   float* out_sc = nullptr;
   uint32_t* out_id = nullptr;
   uint32_t* out_n = nullptr;
+  // tcgen05 routing
+  uint64_t tc_nq_cap = 0, sub_cap = 0, ent_cap = 0;
+  __nv_bfloat16* qhl = nullptr;
+  float* lim = nullptr;
+  uint32_t* cnt = nullptr;
+  float* sub_scores = nullptr;
+  uint2* ent = nullptr;
+  uint32_t* status = nullptr;
   cudaEvent_t ev[4] = {};
   bool events = false;
 };
@@ -706,6 +718,10 @@ struct sg_bigann {
   float* leaves = nullptr;    // [k*100]
   float* leaves_t = nullptr;  // [100*k]
   float* leaf_norm = nullptr;
+  __nv_bfloat16* hl = nullptr;  // [k x 208] bf16 hi/lo rows of the leaves (tcgen05 routing)
+  float cmax = 0.0f, cmax2 = 0.0f;
+  bool route_tc = false;        // the tcgen05 routing is available
+  uint64_t route_exact_fallbacks = 0;  // passes in which a query fell back to exact FP32 routing
   uint32_t* block_off = nullptr;
   uint8_t* blocks = nullptr;
   float2* factors = nullptr;
@@ -728,10 +744,11 @@ void bg_free_all(sg_bigann* h) {
   bg_free(w.scores); bg_free(w.probe); bg_free(w.probe_cent); bg_free(w.probe_n); bg_free(w.scanned);
   bg_free(w.cid); bg_free(w.cest); bg_free(w.cnx); bg_free(w.cn); bg_free(w.lsc);
   bg_free(w.out_sc); bg_free(w.out_id); bg_free(w.out_n);
+  bg_free(w.qhl); bg_free(w.lim); bg_free(w.cnt); bg_free(w.sub_scores); bg_free(w.ent); bg_free(w.status);
   if (w.events)
     for (auto& e : w.ev) cudaEventDestroy(e);
   w.events = false;
-  bg_free(h->leaves); bg_free(h->leaves_t); bg_free(h->leaf_norm); bg_free(h->block_off);
+  bg_free(h->leaves); bg_free(h->leaves_t); bg_free(h->leaf_norm); bg_free(h->hl); bg_free(h->block_off);
   bg_free(h->blocks); bg_free(h->factors); bg_free(h->ids); bg_free(h->ext); bg_free(h->rot);
   bg_free(h->base);
   if (h->stream) cudaStreamDestroy(h->stream);
@@ -747,9 +764,18 @@ int bg_check_params(const sg_bigann* h, const sg_bigann_params* p) {
   return SG_OK;
 }
 
-// Queries per pass: the routing scores of a pass ([nq x k] f32) stay under 1 GiB.
-uint32_t bg_pass(const sg_bigann* h, uint32_t nq) {
-  const uint64_t per = std::max<uint64_t>(1, (1ull << 28) / std::max<uint32_t>(h->k, 1));
+bool bg_uses_tc(const sg_bigann* h, const sg_bigann_params& p) { return h->route_tc && !p.route_fp32; }
+
+// Queries per pass: the routing scratch of a pass stays under 1 GiB: [nq x k] f32 scores on the
+// FP32 path; the subset scores and the emitted lists ([nq x ksub] f32 + [nq x cap] 8 B) on the
+// tcgen05 path.
+uint32_t bg_pass(const sg_bigann* h, uint32_t nq, const sg_bigann_params& p) {
+  uint64_t per_query = (uint64_t)std::max<uint32_t>(h->k, 1) * 4;
+  if (bg_uses_tc(h, p)) {
+    const sg::BgRoutePlan pl = sg::bg_route_plan(h->k, std::min<uint32_t>(p.nprobe, h->k));
+    per_query = (pl.subset ? (uint64_t)pl.ksub * 4 : 0) + (uint64_t)pl.cap * 8;
+  }
+  const uint64_t per = std::max<uint64_t>(1, (1ull << 30) / per_query);
   return (uint32_t)std::min<uint64_t>(nq, std::min<uint64_t>(per, 65535ull));  // grid.y
 }
 
@@ -774,7 +800,23 @@ int bg_ensure(sg_bigann* h, uint32_t nq, const sg_bigann_params& p) {
     w.nq_cap = nq;
   }
   const uint64_t n = w.nq_cap;
-  if ((rc = bg_grow(&w.scores, &w.scores_cap, n * h->k))) return rc;
+  if (bg_uses_tc(h, p)) {
+    const sg::BgRoutePlan pl = sg::bg_route_plan(h->k, std::min<uint32_t>(p.nprobe, h->k));
+    if (n > w.tc_nq_cap) {
+      bg_free(w.qhl); bg_free(w.lim); bg_free(w.cnt);
+      w.tc_nq_cap = 0;
+      if ((rc = bg_alloc(&w.qhl, sg::bg_route_tc_hl_elems((uint32_t)n))) || (rc = bg_alloc(&w.lim, n)) ||
+          (rc = bg_alloc(&w.cnt, n)))
+        return rc;
+      w.tc_nq_cap = n;
+    }
+    if ((rc = bg_grow(&w.sub_scores, &w.sub_cap, pl.subset ? n * pl.ksub : 1)) ||
+        (rc = bg_grow(&w.ent, &w.ent_cap, n * pl.cap)))
+      return rc;
+  } else if ((rc = bg_grow(&w.scores, &w.scores_cap, n * h->k))) {
+    return rc;
+  }
+  if (!w.status && (rc = bg_alloc(&w.status, 1))) return rc;
   if (n * P > w.probe_cap) {
     bg_free(w.probe_cent);
     uint64_t cap = w.probe_cap;
@@ -819,11 +861,10 @@ int bg_run(sg_bigann* h, uint32_t nq, const sg_bigann_params& p, BgStage stage, 
   const bool refine = h->bits > 1 && p.refine > 0;
   const uint32_t KC = refine ? std::max(p.refine, p.cand) : p.cand;
   uint32_t L = 0;
+  BG_CK(cudaMemsetAsync(w.status, 0, sizeof(uint32_t), st));
   if (timed) BG_CK(cudaEventRecord(w.ev[0], st));
   sg::k_bg_prep<<<nq, 128, 0, st>>>(w.q, h->rot, h->rot_norm, h->bits, refine ? 1 : 0, w.tables,
                                     w.qp, w.qq, w.rtab, w.roff);
-  dim3 g1((h->k + 255) / 256, (nq + sg::kBgRouteQ - 1) / sg::kBgRouteQ);
-  sg::k_bg_scores<<<g1, 256, 0, st>>>(w.q, nq, h->leaves_t, h->leaf_norm, h->k, w.scores);
   static sg::PerDeviceOnce attr;
   const cudaError_t smem_limits = attr([] {
     cudaError_t e = cudaFuncSetAttribute(sg::k_bg_select, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -837,10 +878,39 @@ int bg_run(sg_bigann* h, uint32_t nq, const sg_bigann_params& p, BgStage stage, 
     return e;
   });
   BG_CK(smem_limits);
-  const size_t sel_smem = (size_t)sg::next_pow2_host(std::max<uint32_t>(P, 1)) * 8;
-  sg::k_bg_select<<<nq, 1024, sel_smem, st>>>(w.scores, h->k, P, p.margin, w.qq, w.q, h->leaves,
-                                              w.probe, w.probe_cent, w.probe_n);
-  L += 3;
+  if (bg_uses_tc(h, p)) {
+    sg::BgRouteTc r;
+    r.K = h->k;
+    r.P = P;
+    r.nq = nq;
+    r.sms = h->sms;
+    r.margin = p.margin;
+    r.cmax = h->cmax;
+    r.cmax2 = h->cmax2;
+    r.q = w.q;
+    r.qhl = w.qhl;
+    r.hl = h->hl;
+    r.leaves = h->leaves;
+    r.ln = h->leaf_norm;
+    r.qq = w.qq;
+    r.sub_scores = w.sub_scores;
+    r.lim = w.lim;
+    r.ent = w.ent;
+    r.cnt = w.cnt;
+    r.probe = w.probe;
+    r.probe_cent = w.probe_cent;
+    r.probe_n = w.probe_n;
+    r.status = w.status;
+    BG_CK(sg::launch_bg_route_tc(r, st));
+    L += 1 + (sg::bg_route_plan(h->k, P).subset ? 5 : 4);
+  } else {
+    dim3 g1((h->k + 255) / 256, (nq + sg::kBgRouteQ - 1) / sg::kBgRouteQ);
+    sg::k_bg_scores<<<g1, 256, 0, st>>>(w.q, nq, h->leaves_t, h->leaf_norm, h->k, w.scores);
+    const size_t sel_smem = (size_t)sg::next_pow2_host(std::max<uint32_t>(P, 1)) * 8;
+    sg::k_bg_select<<<nq, 1024, sel_smem, st>>>(w.scores, h->k, P, p.margin, w.qq, w.q, h->leaves,
+                                                w.probe, w.probe_cent, w.probe_n);
+    L += 3;
+  }
   if (timed) BG_CK(cudaEventRecord(w.ev[1], st));
   if (stage >= kBgCandidates) {
     sg::BgScanArgs a;
@@ -950,6 +1020,26 @@ int bg_build(const sg_bigann_arrays* a, int device, sg_bigann** out) {
     return bail(rc);
   sg::k_bg_leaf_norm<<<(K + 255) / 256, 256>>>(h->leaves, K, h->leaf_norm);
   if (cudaDeviceSynchronize() != cudaSuccess) return bail(fail(SG_ERR_DEVICE, "leaf norms"));
+  // the tcgen05 routing: the bf16 hi/lo leaf matrix and the largest leaf norm (rounded up)
+  {
+    double m2 = 0.0;
+    for (uint32_t c = 0; c < K; c++) {
+      double s2 = 0.0;
+      for (int i = 0; i < SG_BG_DIM; i++) {
+        const double v = a->leaves[(size_t)c * SG_BG_DIM + i];
+        s2 += v * v;
+      }
+      m2 = std::max(m2, s2);
+    }
+    h->cmax2 = (float)(m2 * (1.0 + 1e-6)) ;
+    h->cmax = (float)(std::sqrt(m2) * (1.0 + 1e-6));
+    h->route_tc = sg::route_gemm_ready() && std::isfinite(h->cmax2);
+    if (h->route_tc) {
+      if ((rc = bg_alloc(&h->hl, sg::bg_route_tc_hl_elems(K)))) return bail(rc);
+      if (sg::bg_route_tc_prepare(h->leaves, K, h->hl, 0) || cudaDeviceSynchronize() != cudaSuccess)
+        return bail(fail(SG_ERR_DEVICE, "bf16 leaf matrix"));
+    }
+  }
   if (cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) != cudaSuccess)
     return bail(fail(SG_ERR_DEVICE, "stream"));
   *out = h.release();
@@ -972,6 +1062,15 @@ bool bg_read(const std::string& path, std::vector<char>& out, bool optional, int
   return true;
 }
 
+// After a pass has synchronised: a tensor-core wait that ran out fails the call.
+int bg_check_status(sg_bigann* h) {
+  uint32_t st = 0;
+  BG_CK(cudaMemcpy(&st, h->w.status, sizeof(st), cudaMemcpyDeviceToHost));
+  if (st & sg::kStatusTimeout) return fail(SG_ERR_DEVICE, "bigann routing: a tensor-core pipeline wait timed out");
+  if (st & sg::kStatusWindow) h->route_exact_fallbacks++;
+  return SG_OK;
+}
+
 // Copies results of a pass out and accumulates timing.
 int bg_search_impl(sg_bigann* h, uint32_t nq, const int8_t* q, const sg_bigann_params& p,
                    float* out_sc, uint32_t* out_id, uint32_t* out_n, sg_bigann_timing* t,
@@ -981,7 +1080,7 @@ int bg_search_impl(sg_bigann* h, uint32_t nq, const int8_t* q, const sg_bigann_p
   if (nq == 0) return SG_OK;
   if (!q) return fail(SG_ERR_INVALID, "q is null");
   BG_CK(cudaSetDevice(h->device));
-  const uint32_t per = bg_pass(h, nq);
+  const uint32_t per = bg_pass(h, nq, p);
   if ((rc = bg_ensure(h, per, p))) return rc;
   BgWork& w = h->w;
   const uint32_t K = p.k;
@@ -1007,6 +1106,7 @@ int bg_search_impl(sg_bigann* h, uint32_t nq, const int8_t* q, const sg_bigann_p
       BG_CK(cudaMemcpyAsync(probes.data(), w.probe_n, (size_t)m * 4, cudaMemcpyDeviceToHost, h->stream));
     }
     BG_CK(cudaStreamSynchronize(h->stream));
+    if ((rc = bg_check_status(h))) return rc;
     if (t) {
       float r = 0, s = 0, x = 0;
       BG_CK(cudaEventElapsedTime(&r, w.ev[0], w.ev[1]));
@@ -1124,6 +1224,12 @@ int sg_bigann_info(const sg_bigann* h, uint32_t* k, uint64_t* n, uint64_t* nbloc
   return SG_OK;
 }
 
+int sg_bigann_route_fallbacks(const sg_bigann* h, uint64_t* passes) {
+  if (!h || !passes) return fail(SG_ERR_INVALID, "null argument");
+  *passes = h->route_exact_fallbacks;
+  return SG_OK;
+}
+
 int sg_search_bigann(sg_bigann* h, uint32_t nq, const int8_t* q100, const sg_bigann_params* params,
                      float* out_scores, uint32_t* out_ids, uint32_t* out_counts,
                      sg_bigann_timing* timing) {
@@ -1159,7 +1265,7 @@ int sg_bigann_route(sg_bigann* h, uint32_t nq, const int8_t* q100, const sg_biga
   if ((rc = bg_check_params(h, params))) return rc;
   if (nq == 0) return SG_OK;
   BG_CK(cudaSetDevice(h->device));
-  const uint32_t per = bg_pass(h, nq);
+  const uint32_t per = bg_pass(h, nq, *params);
   if ((rc = bg_ensure(h, per, *params))) return rc;
   BgWork& w = h->w;
   const uint32_t P = std::min<uint32_t>(params->nprobe, h->k);
@@ -1171,6 +1277,7 @@ int sg_bigann_route(sg_bigann* h, uint32_t nq, const int8_t* q100, const sg_biga
     if (P) BG_CK(cudaMemcpyAsync(out_probe + (size_t)q0 * P, w.probe, (size_t)m * P * 4, cudaMemcpyDeviceToHost, h->stream));
     BG_CK(cudaMemcpyAsync(out_counts + q0, w.probe_n, (size_t)m * 4, cudaMemcpyDeviceToHost, h->stream));
     BG_CK(cudaStreamSynchronize(h->stream));
+    if ((rc = bg_check_status(h))) return rc;
   }
   return SG_OK;
 }
@@ -1183,7 +1290,7 @@ int sg_bigann_candidates(sg_bigann* h, uint32_t nq, const int8_t* q100, const sg
   if ((rc = bg_check_params(h, params))) return rc;
   if (nq == 0) return SG_OK;
   BG_CK(cudaSetDevice(h->device));
-  const uint32_t per = bg_pass(h, nq);
+  const uint32_t per = bg_pass(h, nq, *params);
   if ((rc = bg_ensure(h, per, *params))) return rc;
   BgWork& w = h->w;
   const uint32_t C = params->cand;
@@ -1199,6 +1306,7 @@ int sg_bigann_candidates(sg_bigann* h, uint32_t nq, const int8_t* q100, const sg
     }
     BG_CK(cudaMemcpyAsync(out_counts + q0, w.cn, (size_t)m * 4, cudaMemcpyDeviceToHost, h->stream));
     BG_CK(cudaStreamSynchronize(h->stream));
+    if ((rc = bg_check_status(h))) return rc;
   }
   return SG_OK;
 }

@@ -1,6 +1,7 @@
 // internal.hpp — device-resident index, per-call workspace and kernel launchers.
 #pragma once
 
+#include <cuda.h>
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
@@ -244,6 +245,45 @@ void launch_prep(const DevIndex& ix, Workspace& w, uint32_t nq, cudaStream_t st)
 // Looks up the driver's tensor-map encoder the BF16 routing GEMM needs (once per process);
 // false if the driver does not provide it.
 bool route_gemm_ready();
+// A 2-D TMA map over a bf16 matrix of `rows` rows of `cols` elements, `row_bytes` apart (a multiple
+// of 16), whose box is one 16-byte k-chunk (8 elements) of box_rows rows; rows past `rows` read as
+// zeros. False if the encoder is missing or rejects the shape.
+bool encode_bf16_rows(CUtensorMap* m, const void* base, uint64_t cols, uint64_t rows, uint64_t row_bytes,
+                      uint32_t box_rows);
+
+// ---- bigann routing on the tcgen05 tensor cores (bg_route.cu) --------------------------------
+constexpr uint32_t kBgSubStep = 16;  // the threshold subset: every 16th leaf
+struct BgRoutePlan {
+  uint32_t ksub;  // leaves in the subset
+  uint32_t cap;   // emitted entries one query's list holds
+  bool subset;    // false: every leaf is emitted (cap = K)
+};
+BgRoutePlan bg_route_plan(uint32_t K, uint32_t P);
+// Elements of the [rows x 208] bf16 hi/lo matrix, and its fill from the f32 leaves [K x 100].
+size_t bg_route_tc_hl_elems(uint32_t rows);
+int bg_route_tc_prepare(const float* d_leaves, uint32_t K, __nv_bfloat16* d_hl, cudaStream_t st);
+struct BgRouteTc {
+  uint32_t K, P, nq;
+  int sms;
+  float margin, cmax, cmax2;  // cmax: the largest leaf norm, cmax2 its square (rounded up)
+  const int8_t* q;
+  __nv_bfloat16* qhl;  // [nq x 208] scratch
+  const __nv_bfloat16* hl;
+  const float* leaves;
+  const float* ln;
+  const float* qq;     // |q|^2 per query
+  float* sub_scores;   // [nq x ksub]
+  float* lim;          // [nq]
+  uint2* ent;          // [nq x cap]
+  uint32_t* cnt;       // [nq]
+  uint32_t* probe;     // [nq x P]
+  float* probe_cent;   // [nq x P]
+  uint32_t* probe_n;   // [nq]
+  uint32_t* status;    // kStatus* bits
+};
+// Five launches: queries to bf16, the subset GEMM (when the plan has a subset), the thresholds,
+// the filtered GEMM, the per-query select.
+cudaError_t launch_bg_route_tc(const BgRouteTc& r, cudaStream_t st);
 // BF16: two launches (the queries to bf16, then the tcgen05 GEMM); FP32: one. Returns the
 // launch error, or cudaErrorInvalidValue if the GEMM's TMA tensor maps cannot be encoded.
 cudaError_t launch_route_scores(const DevIndex& ix, Workspace& w, uint32_t nq, int precision,

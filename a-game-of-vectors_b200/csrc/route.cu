@@ -174,18 +174,23 @@ static PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
 
 bool route_gemm_ready() { return tensor_map_encoder() != nullptr; }
 
-// A 2-D map over a row-major [rows x 256] bf16 matrix (16-byte aligned) whose box is one 16-byte
-// k-chunk (8 elements) of box_rows rows; rows past `rows` read as zeros.
-static bool encode_rows(CUtensorMap* m, const __nv_bfloat16* base, uint64_t rows, uint32_t box_rows) {
+bool encode_bf16_rows(CUtensorMap* m, const void* base, uint64_t cols, uint64_t rows, uint64_t row_bytes,
+                      uint32_t box_rows) {
   const PFN_cuTensorMapEncodeTiled_v12000 enc = tensor_map_encoder();
-  if (!enc) return false;
-  const cuuint64_t dims[2] = {SG_PDIM, rows};
-  const cuuint64_t strides[1] = {SG_PDIM * sizeof(__nv_bfloat16)};
+  if (!enc || rows == 0 || row_bytes % 16 || box_rows == 0 || box_rows > 256) return false;
+  const cuuint64_t dims[2] = {cols, rows};
+  const cuuint64_t strides[1] = {row_bytes};
   const cuuint32_t box[2] = {8, box_rows};
   const cuuint32_t estr[2] = {1, 1};
-  return enc(m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<__nv_bfloat16*>(base), dims, strides,
-             box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
-             CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+  return enc(m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<void*>(base), dims, strides, box, estr,
+             CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+             CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+// A map over a row-major [rows x 256] bf16 matrix (16-byte aligned) whose box is one 16-byte
+// k-chunk (8 elements) of box_rows rows; rows past `rows` read as zeros.
+static bool encode_rows(CUtensorMap* m, const __nv_bfloat16* base, uint64_t rows, uint32_t box_rows) {
+  return encode_bf16_rows(m, base, SG_PDIM, rows, SG_PDIM * sizeof(__nv_bfloat16), box_rows);
 }
 
 // The reference's sequential FP32 dot of one query with one centroid row.

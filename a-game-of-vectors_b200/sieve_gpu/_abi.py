@@ -151,7 +151,7 @@ class SgBigannParams(ctypes.Structure):
     """sg_bigann_params: bigann::Params."""
 
     _fields_ = [("nprobe", c_uint32), ("cand", c_uint32), ("k", c_uint32), ("refine", c_uint32),
-                ("margin", c_float), ("reserved", c_uint32)]
+                ("margin", c_float), ("route_fp32", c_uint32)]
 
 
 class SgBigannTiming(ctypes.Structure):
@@ -283,6 +283,7 @@ EXPORTS = [
     "sg_open_bigann_arrays",
     "sg_close_bigann",
     "sg_bigann_info",
+    "sg_bigann_route_fallbacks",
     "sg_search_bigann",
     "sg_search_bigann_device",
     "sg_bigann_route",

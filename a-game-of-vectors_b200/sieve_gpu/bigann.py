@@ -25,10 +25,11 @@ class BigannParams:
     k: int = 10
     refine: int = 0
     margin: float = 0.0
+    route_fp32: bool = False  # exact FP32 dots of every leaf instead of the tensor-core routing
 
     def to_c(self) -> SgBigannParams:
         return SgBigannParams(int(self.nprobe), int(self.cand), int(self.k), int(self.refine),
-                              float(self.margin), 0)
+                              float(self.margin), int(bool(self.route_fp32)))
 
 
 def parse_config(cfg: str, k: int = 10) -> BigannParams:
@@ -84,6 +85,13 @@ class BigannIndex:
         check(lib().sg_open_bigann_arrays(byref(st), c_int(device), byref(h)))
         del keep
         return cls(h, device)
+
+    def route_fallbacks(self) -> int:
+        """Passes since open in which a query's tensor-core routing fell back to exact FP32 dots
+        of every leaf (same results, slower)."""
+        n = c_uint64()
+        check(lib().sg_bigann_route_fallbacks(self._h, byref(n)))
+        return n.value
 
     def close(self) -> None:
         if self._h:

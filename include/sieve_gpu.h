@@ -156,7 +156,8 @@ typedef struct {
   uint32_t k;       /* results returned                                                         */
   uint32_t refine;  /* multi-bit index: 1-bit shortlist re-estimated from all planes; 0 = off   */
   float margin;     /* keep leaves with |q-c|^2 <= (1 + margin) |q-c1|^2; 0 = off               */
-  uint32_t reserved;
+  uint32_t route_fp32; /* 0: route on the tensor cores (bf16 hi/lo GEMM, exact FP32 rescoring of a
+                          window: the same probe lists); 1: the exact FP32 dot of every leaf     */
 } sg_bigann_params;
 
 /* bigann::Timing (src/bigann.rs:624-632): device times in nanoseconds. */
@@ -435,6 +436,10 @@ int sg_open_bigann_arrays(const sg_bigann_arrays* a, int device, sg_bigann** out
 int sg_close_bigann(sg_bigann* index);
 int sg_bigann_info(const sg_bigann* index, uint32_t* k, uint64_t* n, uint64_t* nblocks,
                    uint32_t* bits);
+/* Routing passes (since open) in which some query's tensor-core routing fell back to the exact
+ * FP32 dot of every leaf: its emitted list or its rescoring window overflowed. No reference
+ * counterpart; the results are the same either way. */
+int sg_bigann_route_fallbacks(const sg_bigann* index, uint64_t* passes);
 /* bigann::Index::search (src/bigann.rs:653-657) for nq int8 queries q100 [nq * 100]: the top
  * params.k rows by 2<q,x> - |x|^2 as (score, row), best first. out_* [nq * k], out_counts [nq]. */
 int sg_search_bigann(sg_bigann* index, uint32_t nq, const int8_t* q100,

@@ -114,6 +114,21 @@ def bigann_a(bits: int):
 
 
 @functools.lru_cache(maxsize=None)
+def bigann_c():
+    """bigann with many small leaves: 30,000 int8 rows, 64 x 160 = 10,240 leaves (more than the
+    8,192 past which the tensor-core routing takes its threshold from a 1/16 subset of the leaves),
+    duplicate leaves where a top cluster holds fewer rows than 160 (tied route scores); 40 queries
+    from the mixture and 8 copies of leaf centres' nearest base rows."""
+    from sieve_gpu import bigann_builder as BB
+
+    sp = BB.Spacev(30000, 256, seed=13, device="cpu")
+    base = sp.rows(0, 30000)
+    ix = BB.build_bigann(base, 64, 160, bits=1, sample_n=30000, iters=4)
+    q = torch.cat([sp.queries(40), base[5000:5008]]).numpy()
+    return ix, q
+
+
+@functools.lru_cache(maxsize=None)
 def bigann_b():
     """bigann with few, large leaves (2 x 4 of about 5,000 slots): scan steps span whole chunks
     and the shortlist compacts many times inside one leaf."""

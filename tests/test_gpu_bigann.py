@@ -6,7 +6,7 @@ import numpy as np
 import pytest
 
 import oracle as O
-from fixtures import bigann_a, bigann_b
+from fixtures import bigann_a, bigann_b, bigann_c
 from sieve_gpu.bigann import BigannIndex, BigannParams, BigannTiming
 
 pytestmark = pytest.mark.gpu
@@ -32,14 +32,50 @@ def cp(p: BigannParams):
     return p.to_c()
 
 
+@pytest.mark.parametrize("route_fp32", [False, True], ids=["tc", "fp32"])
 @pytest.mark.parametrize("nprobe,margin", [(1, 0.0), (12, 0.0), (40, 0.0), (40, 0.05), (40, 0.3), (10**6, 0.0)])
-def test_route_matches_oracle(env, nprobe, margin):
+def test_route_matches_oracle(env, nprobe, margin, route_fp32):
     g, ob, ix, q = env
-    p = BigannParams(nprobe, 100, 10, 0, margin)
+    p = BigannParams(nprobe, 100, 10, 0, margin, route_fp32)
     got = g.route(q, p)
     for i in range(q.shape[0]):
         want, _, _ = ob.route(q[i], cp(p))
         assert np.array_equal(got[i], want), i
+
+
+@pytest.fixture(scope="module")
+def env_c():
+    ix, q = bigann_c()
+    g = BigannIndex.from_arrays(ix)
+    yield g, O.OracleBigann(ix), ix, q
+    g.close()
+
+
+# 10,240 leaves: nprobe 1..300 take the subset threshold (cap 8,192 or 32 nprobe entries per
+# query); 320 emits every leaf (640 subset leaves < 2 nprobe); 4096 the largest nprobe.
+@pytest.mark.parametrize("route_fp32", [False, True], ids=["tc", "fp32"])
+@pytest.mark.parametrize("nprobe,margin", [(1, 0.0), (64, 0.0), (64, 0.2), (300, 0.0), (320, 0.05), (4096, 0.0)])
+def test_route_many_leaves_matches_oracle(env_c, nprobe, margin, route_fp32):
+    g, ob, ix, q = env_c
+    p = BigannParams(nprobe, 100, 10, 0, margin, route_fp32)
+    before = g.route_fallbacks()
+    got = g.route(q, p)
+    for i in range(q.shape[0]):
+        want, _, _ = ob.route(q[i], cp(p))
+        assert np.array_equal(got[i], want), i
+    if not route_fp32 and nprobe <= 320:
+        # the rescoring windows fit: no query needed the exact fallback
+        assert g.route_fallbacks() == before
+
+
+def test_search_many_leaves_matches_oracle(env_c):
+    g, ob, ix, q = env_c
+    p = BigannParams(64, 200, 10, 0, 0.1)
+    sc, ids, cnt = g.search_batch(q, p)
+    for i in range(q.shape[0]):
+        ws, wo, _ = ob.search(q[i], cp(p))
+        assert np.array_equal(ids[i, : cnt[i]], wo), i
+        assert np.array_equal(sc[i, : cnt[i]], ws), i
 
 
 CASES = [(8, 100, 10, 0), (8, 100, 10, 500), (16, 40, 10, 60), (16, 10, 5, 30), (4, 3, 3, 0),
