@@ -300,34 +300,6 @@ SG_DEV float bg_exact_score(const float* qf, const float* __restrict__ leaves, c
   return __fsub_rn(__fmul_rn(2.0f, d), ln[c]);
 }
 
-// TopK(P) by (score desc, leaf asc) over leaves 0..K-1 with scores from score(i): the winners'
-// rank keys go to keys[0..P) (unordered). Every thread of the block calls it.
-template <typename Score>
-SG_DEV void bg_top_leaves(Score score, uint32_t K, uint32_t P, uint64_t* keys, uint32_t* hist, uint32_t* tmp) {
-  __shared__ uint32_t s_n;
-  auto okey = [&](uint32_t i) { return ord(score(i)); };
-  const uint32_t T = block_select_nth_u32r(okey, K, P, hist, tmp);
-  uint32_t gt = 0, eq = 0;
-  for (uint32_t i = threadIdx.x; i < K; i += blockDim.x) {
-    const uint32_t o = okey(i);
-    gt += o > T;
-    eq += o == T;
-  }
-  const uint32_t n_gt = block_sum(gt, tmp), n_eq = block_sum(eq, tmp);
-  const uint32_t need = P - n_gt;
-  uint32_t Kt = 0;  // among leaves at T, keep those with 0xFFFFFFFF - leaf >= Kt (the lowest `need`)
-  if (n_eq > need)
-    Kt = block_select_nth_u32r([&](uint32_t i) { return okey(i) == T ? 0xFFFFFFFFu - i : 0u; }, K, need, hist, tmp);
-  if (threadIdx.x == 0) s_n = 0;
-  __syncthreads();
-  for (uint32_t i = threadIdx.x; i < K; i += blockDim.x) {
-    const float v = score(i);
-    const uint32_t o = ord(v);
-    if (o > T || (o == T && 0xFFFFFFFFu - i >= Kt)) keys[atomicAdd(&s_n, 1u)] = rank_key(v, i);
-  }
-  __syncthreads();
-}
-
 // Sorts keys[0..P) best first, applies the margin rule on |q - c|^2 = |q|^2 - s (src/bigann.rs:
 // 671-677) and writes the kept leaves with their exact dots <q, c>.
 SG_DEV void bg_emit_probes(uint64_t* keys, uint32_t P, float margin, float Q, const float* qf,
@@ -419,7 +391,7 @@ __global__ void __launch_bounds__(1024) k_bg_select_tc(const uint2* __restrict__
   }
   if (exact_all) {
     if (threadIdx.x == 0) atomicOr(status, kStatusWindow);
-    bg_top_leaves([&](uint32_t i) { return bg_exact_score(qf, leaves, ln, i, nullptr); }, K, P, keys, hist, tmp);
+    block_top_keys([&](uint32_t i) { return bg_exact_score(qf, leaves, ln, i, nullptr); }, K, P, keys, hist, tmp);
   }
   bg_emit_probes(keys, P, margin, qq[q], qf, leaves, ln, q, probe, probe_cent, probe_n);
 }

@@ -360,4 +360,34 @@ SG_DEV uint32_t block_select_nth_u32r(Get get, uint32_t m, uint32_t n, uint32_t*
   return lo + want;
 }
 
+// TopK(P) by (score desc, id asc) over ids 0..K-1 (1 <= P <= K), the scores read through
+// score(i) (several times: min/max, up to three digit passes, a count, the gather): the winners'
+// rank keys go to keys[0..P), unordered. `hist` needs 2048 words and `tmp` 32; every thread of the
+// block calls it.
+template <typename Score>
+SG_DEV void block_top_keys(Score score, uint32_t K, uint32_t P, uint64_t* keys, uint32_t* hist, uint32_t* tmp) {
+  __shared__ uint32_t s_top_n;
+  auto okey = [&](uint32_t i) { return ord(score(i)); };
+  const uint32_t T = block_select_nth_u32r(okey, K, P, hist, tmp);
+  uint32_t gt = 0, eq = 0;
+  for (uint32_t i = threadIdx.x; i < K; i += blockDim.x) {
+    const uint32_t o = okey(i);
+    gt += o > T;
+    eq += o == T;
+  }
+  const uint32_t n_gt = block_sum(gt, tmp), n_eq = block_sum(eq, tmp);
+  const uint32_t need = P - n_gt;  // >= 1: T is the P-th largest
+  uint32_t Kt = 0;  // among ids at T, keep those with 0xFFFFFFFF - id >= Kt (the lowest `need`)
+  if (n_eq > need)
+    Kt = block_select_nth_u32r([&](uint32_t i) { return okey(i) == T ? 0xFFFFFFFFu - i : 0u; }, K, need, hist, tmp);
+  if (threadIdx.x == 0) s_top_n = 0;
+  __syncthreads();
+  for (uint32_t i = threadIdx.x; i < K; i += blockDim.x) {
+    const float v = score(i);
+    const uint32_t o = ord(v);
+    if (o > T || (o == T && 0xFFFFFFFFu - i >= Kt)) keys[atomicAdd(&s_top_n, 1u)] = rank_key(v, i);
+  }
+  __syncthreads();
+}
+
 }  // namespace sg

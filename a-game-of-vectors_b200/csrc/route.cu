@@ -343,7 +343,7 @@ __global__ void __launch_bounds__(256) k_route_select(SelectArgs a) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   uint64_t* keys = reinterpret_cast<uint64_t*>(smem_raw);  // [kWinCap]
   __shared__ float qv[SG_PDIM];
-  __shared__ uint32_t hist[256], tmp[32];
+  __shared__ uint32_t hist[2048], tmp[32];
   __shared__ uint32_t s_nw, s_m, s_keep;
   const uint32_t q = blockIdx.x, P = a.Pb, K = a.K;
   float* row = a.scores + (size_t)q * K;
@@ -361,7 +361,7 @@ __global__ void __launch_bounds__(256) k_route_select(SelectArgs a) {
   bool exact = !a.bf16;
   if (a.bf16) {
     // the P-th largest BF16 score and the window below it
-    const uint32_t kth = block_select_nth_u32([&](uint32_t i) { return ord(row[i]); }, K, P, hist);
+    const uint32_t kth = block_select_nth_u32r([&](uint32_t i) { return ord(row[i]); }, K, P, hist, tmp);
     const float sP = unord(kth);
     float delta = 0.0085f * a.qnorm[q] * a.cent_norm_max;
     float lim = sP - 2.0f * delta;
@@ -400,17 +400,7 @@ __global__ void __launch_bounds__(256) k_route_select(SelectArgs a) {
       exact = true;
     }
   }
-  if (exact) {
-    uint64_t T = block_select_nth_u64([&](uint32_t i) { return rank_key(row[i], i); }, K, P, hist,
-                                      tmp);
-    if (threadIdx.x == 0) s_m = 0;
-    __syncthreads();
-    for (uint32_t c = threadIdx.x; c < K; c += blockDim.x) {
-      uint64_t k = rank_key(row[c], c);
-      if (k >= T) keys[atomicAdd(&s_m, 1u)] = k;
-    }
-    __syncthreads();
-  }
+  if (exact) block_top_keys([&](uint32_t i) { return row[i]; }, K, P, keys, hist, tmp);
   // keys[0..P) hold the winners: sort best first
   uint32_t n2 = next_pow2(P);
   for (uint32_t i = P + threadIdx.x; i < n2; i += blockDim.x) keys[i] = 0;

@@ -35,12 +35,20 @@ for p in (os.path.join(ROOT, "a-game-of-vectors_b200"), os.path.join(ROOT, "orac
 import numpy as np  # noqa: E402
 import torch  # noqa: E402
 
+# `search` is the headline search of a workload: the stated probing with enough candidates that
+# recall reaches the corpus's int8 ceiling (on these mixtures 500 candidates leave most true
+# neighbours behind: ~1,150 near-equidistant rows sit around each centre). `stated` is the
+# workload's search exactly as stated (500 candidates, the 2-bit tier picking 200 int8 rows),
+# measured beside it.
 WORKLOADS = {
-    "c1": dict(n=1_000_000, centers=1024, k=1024, queries=10_000, search="32:1000:full"),
-    "c2": dict(n=18_400_000, centers=16384, k=4096, queries=50_000, search="64:500:tiered200",
-               serve="5000,20000,50000,100000,150000,200000"),
-    "c3": dict(n=113_500_000, centers=65536, k=16384, queries=100_000, search="128:500:tiered200:p0.3",
-               serve="5000,20000,50000,100000,150000,200000"),
+    "c1": dict(n=1_000_000, centers=1024, k=1024, queries=10_000, search="32:1000:full",
+               stated="32:500:full"),
+    "c2": dict(n=18_400_000, centers=16384, k=4096, queries=50_000, search="32:2000:full",
+               stated="32:500:tiered200", serve="5000,20000,50000,100000,150000,200000"),
+    # margin probing: 0.35 gives a median of ~46 probes (cap 128) on this mixture
+    "c3": dict(n=113_500_000, centers=65536, k=16384, queries=100_000, search="128:2000:full:p0.35",
+               stated="128:500:tiered200:p0.35", serve="5000,20000,50000,100000,150000,200000",
+               secondary="c2"),
     # billion-scale L2 (bigann): 512 x 256 = 131,072 leaves, 2-bit refinement. The bench default
     # is a 100M-row cut of the 1B shape (--rows sets it): the 1B build does not fit the run's time.
     "c4": dict(n=100_000_000, centers=131072, k1=512, k2=256, bits=2, queries=10_000,
@@ -196,6 +204,53 @@ def parity_check(gpu_ids, gpu_sc, gpu_cnt, cpu: dict) -> dict:
     return {"queries": int(m), "mismatched": int((~same & ~tied).sum()),
             "tied_boundary": int(tied.sum()), "tied_and_differing": int((~same & tied).sum()),
             "rule": "bit-exact (score, row) lists; canonical ties (score desc, row asc)"}
+
+
+def time_search(index, q768: torch.Tensor, params, batch: int, nq_pool: int, warmup: int, steps: int) -> dict:
+    """Device-timed batches of one search config (inputs resident in HBM, CUDA events on the
+    launching stream): queries/s, ms per batch and the mean stage times."""
+    dev = q768.device
+    out_sc = torch.empty((batch, params.k), dtype=torch.float32, device=dev)
+    out_id = torch.empty((batch, params.k), dtype=torch.int32, device=dev)
+    out_n = torch.empty((batch,), dtype=torch.int32, device=dev)
+    stream = torch.cuda.current_stream()
+    ms, stats = [], []
+    for i in range(warmup + steps):
+        lo = (i * batch) % (nq_pool - batch + 1)
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        index.search_device(batch, q768[lo].data_ptr(), None, params, out_sc.data_ptr(), out_id.data_ptr(),
+                            out_n.data_ptr(), stream.cuda_stream)
+        b.record(stream)
+        b.synchronize()
+        if i >= warmup:
+            ms.append(a.elapsed_time(b))
+            stats.append(index.last_stats())
+    stage = {k: round(float(np.mean([s[k] for s in stats])), 4)
+             for k in ("ms_route_gemm", "ms_route_select", "ms_scan", "ms_cut", "ms_rerank", "ms_tier2", "ms_total")}
+    return {"qps": batch * len(ms) / (float(np.sum(ms)) / 1e3), "ms_per_batch": float(np.mean(ms)),
+            "stage_ms": stage, "batches": len(ms)}
+
+
+def search_line(index, arrays, queries, gt, t8, config: str, nclusters: int, batch: int, nq_pool: int,
+                warmup: int, steps: int) -> dict:
+    """Recall (float and int8 truth), probe counts and device-timed QPS of one search config."""
+    from sieve_gpu import parse_config
+
+    _, p = parse_config(config, nclusters)
+    p.k = 10
+    q_host = queries.cpu().numpy()
+    ev = q_host[: gt.shape[0]]
+    _, ids, cnt = index.search_batch(ev, None, p)
+    probes, _ = probe_stats(index, q_host[:batch], p, batch)
+    index.set_timing(True)
+    t = time_search(index, queries.to(index_device(index)).contiguous(), p, batch, nq_pool, warmup, steps)
+    return {"search": config, "recall_at_10": recall10(ids, cnt, gt), "recall_at_10_int8_truth": recall10(ids, cnt, t8),
+            "probes": probes, **t}
+
+
+def index_device(index) -> str:
+    return f"cuda:{index.device}"
 
 
 def recall10(ids: np.ndarray, cnt: np.ndarray, gt: np.ndarray) -> float:
@@ -384,6 +439,12 @@ def main():
                          "workload's); empty: skip")
     ap.add_argument("--serve-seconds", type=float, default=2.0)
     ap.add_argument("--no-tune", action="store_true", help="keep the default shapes (no autotuner)")
+    ap.add_argument("--stated", default=None,
+                    help="search config measured beside the headline (default: the workload's "
+                         "stated search); empty: skip")
+    ap.add_argument("--secondary", default=None,
+                    help="a second workload measured after the first (its headline and stated "
+                         "searches; default: the workload's, c2 for c3); empty: skip")
     args = ap.parse_args()
 
     rank = int(os.environ.get("RANK", "0"))
@@ -562,6 +623,13 @@ def main():
         serving = serve_load(index, arrays, q_pool_host, params, rates, args.serve_seconds,
                              dom=arrays.get("domain"))
 
+    # the workload's search exactly as stated, beside the headline
+    stated = None
+    stated_cfg = args.stated if args.stated is not None else wl.get("stated", "")
+    if stated_cfg and stated_cfg != config and rank == 0:
+        stated = search_line(index, arrays, queries[:nq_pool], gt, t8, stated_cfg, w["k"], B, nq_pool, 3, 5)
+        log(f"stated {stated_cfg}: {stated}")
+
     cpu, parity = None, None
     if rank == 0 and world == 1 and args.cpu_seconds > 0:
         r = cpu_reference(arrays, q_pool_host[: max(args.eval, 256)], params, args.cpu_seconds, threads)
@@ -599,7 +667,10 @@ def main():
         "scanned_per_query": float(np.mean(scanned) / B),
         "distinct_probed_slots_per_step": float(np.mean(dslots)),
         "retried_queries_per_step": float(np.mean([s["retried"] for s in stats])),
-        "roofline": {"bound": "hbm", "kernel": "k_scan_seed + k_scan + k_scan_tc (the scan stage)",
+        "stated": stated,
+        "roofline": {"bound": "hbm",
+                     "kernel": "the scan stage: k_scan_seed + k_scan (ALU chunks) + k_filter_prep + "
+                               "k_scan_tcf (tcgen05 bound) + k_tc_recheck",
                      "achieved": achieved, "peak": peak,
                      "unit": "GB/s", "frac": achieved / peak,
                      "peak_source": "MEASURED_PEAKS.json hbm_gbs" if "hbm_gbs" in peaks else "fallback",
@@ -617,10 +688,35 @@ def main():
         "build": build_info,
         "tuning": tuning,
     }
+    index.close()
+    sec_name = args.secondary if args.secondary is not None else wl.get("secondary", "")
+    if sec_name and rank == 0 and not args.rows:
+        del arrays
+        torch.cuda.empty_cache()
+        line["secondary"] = secondary_workload(sec_name, dev, local, B, args.route)
     if rank == 0:
         print(json.dumps(line), flush=True)
-    index.close()
     return finish(world)
+
+
+def secondary_workload(name: str, dev: str, local: int, batch: int, route: str) -> dict:
+    """A second workload after the first: its headline and stated searches, device-timed (the
+    autotuner off: the default shapes)."""
+    from sieve_gpu import Index
+
+    wl = WORKLOADS[name]
+    nq_pool = min(max(batch * 2, 1000), wl["queries"])
+    w, arrays, queries, gt, build_info = build_workload(name, dev, None, nq_pool, 1000)
+    index = Index.from_arrays(arrays, device=local)
+    index.set_route_precision(route == "bf16")
+    t8 = int8_truth(arrays, queries[:1000].to(dev))
+    out = {"workload": f"{name}: {w['n']} x 768, {w['centers']} centres, {w['k']} clusters", "batch": batch,
+           "recall_ceiling_int8": recall10(t8, np.full(t8.shape[0], 10), gt), "build": build_info}
+    for key in ("search", "stated"):
+        out[key] = search_line(index, arrays, queries, gt, t8, wl[key], w["k"], batch, nq_pool, 3, 10)
+        log(f"secondary {name} {key}: {out[key]}")
+    index.close()
+    return out
 
 
 # ---- bigann (billion-scale L2 over int8 rows) ----------------------------------------------------
