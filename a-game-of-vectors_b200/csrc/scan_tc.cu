@@ -530,9 +530,10 @@ int launch_scan_tc(const DevIndex& ix, Workspace& w, uint32_t nq, const sg_param
   };
   // one tensor-core round: the bound pass with its exact recheck (default), or the exact one-hot
   // contraction (SIEVE_GPU_TC=2, kept for comparison)
-  const bool bound = cfg.tc != 2;
+  const bool bound = cfg.tc != 2, transposed = cfg.tc == 3;
+  const uint32_t qg = transposed ? kScanTctGroup : kTcQG;
   auto tc_round = [&]() {
-    if (bound) return launch_scan_tcf(ix, w, nq, P, allow, allow_words, sms, st);
+    if (bound) return launch_scan_tcf(ix, w, nq, P, allow, allow_words, sms, transposed, st);
     k_scan_tc<false><<<sms, kTcThreads, tc_smem_bytes(), st>>>(a);
     return 1;
   };
@@ -541,13 +542,13 @@ int launch_scan_tc(const DevIndex& ix, Workspace& w, uint32_t nq, const sg_param
     launches++;
   }
   if (split > 1 && split < P) {
-    launch_invert(ix, w, nq, P, kTcQG, 1, split, st, tmin, chunk_blocks);
+    launch_invert(ix, w, nq, P, qg, 1, split, st, tmin, chunk_blocks);
     alu_pass();
     launches += tc_round();
     k_raise_thr<<<nq, 1024, 0, st>>>(w.cbuf_est, w.cbuf_per_q, w.ccount, w.overflow, p.cand, w.thr);
     launches += 6;
   }
-  launch_invert(ix, w, nq, P, kTcQG, split > 1 && split < P ? split : 1, P, st, tmin, chunk_blocks);
+  launch_invert(ix, w, nq, P, qg, split > 1 && split < P ? split : 1, P, st, tmin, chunk_blocks);
   alu_pass();
   launches += tc_round();
   return launches + 5;

@@ -265,7 +265,7 @@ int build_index(const sg_ivf_arrays* a, int device, sg_index** out) {
     return fail(SG_ERR_DEVICE, "cuTensorMapEncodeTiled (the routing GEMM's TMA maps) is unavailable");
   }
   // the batched tensor-core scan reads its own copy of the codes, slot-major
-  if (const char* tc = getenv("SIEVE_GPU_TC")) h->cfg.tc = atoi(tc) == 2 ? 2 : 1;
+  if (const char* tc = getenv("SIEVE_GPU_TC")) h->cfg.tc = atoi(tc) == 2 ? 2 : atoi(tc) == 3 ? 3 : 1;
   if (const char* sp = getenv("SIEVE_GPU_TC_SPLIT")) h->cfg.tc_split = (uint32_t)strtoul(sp, nullptr, 10);
   if (const char* tm = getenv("SIEVE_GPU_TC_MIN")) h->cfg.tc_min_queries = (uint32_t)strtoul(tm, nullptr, 10);
   if ((rc = dalloc(&x.blocks_tc, (size_t)nblocks * 256))) {
