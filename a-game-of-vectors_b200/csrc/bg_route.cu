@@ -29,10 +29,12 @@
 //      exact FP32 scoring of every leaf in that query's CTA (kStatusWindow is raised).
 //
 // The GEMM kernel is persistent: one CTA per SM walks a contiguous range of (query group, leaf
-// tile) jobs. Warp 0 loads tiles by TMA (no multicast): the query group's B once per group, each
-// 128-leaf A tile into one of two stages. Warp 1 issues the 13 MMAs of a job into one of two TMEM
-// accumulators (M = 128 leaves, N = 64/128/256 queries). Eight epilogue warps read the
-// accumulators (two per TMEM lane quarter, one half of the columns each), so the epilogue of one
+// tile) jobs. Warp 0 loads tiles by TMA (no multicast) in the 128-byte swizzle, one copy per
+// 64-element k-block (four per tile, the last one zero-filled past column 208): the query group's
+// B once per group, each 128-leaf A tile into one of two stages. Warp 1 issues the 13 MMAs of a
+// job into one of two TMEM accumulators (M = 128 leaves, N = 64/128/192 queries). Eight epilogue
+// warps read the accumulators (two per TMEM lane quarter, one half of the columns each) and emit
+// the passing (leaf, score) pairs with one atomic per query and 32 leaves, so the epilogue of one
 // job overlaps the loads and MMAs of the next. Every wait is bounded (2 s); a wait that runs out
 // raises kStatusTimeout and the CTA stops after its copies in flight have landed.
 #include <cuda_bf16.h>
@@ -48,9 +50,9 @@ namespace sg {
 constexpr uint32_t kHlCols = 208;  // [hi 100, 0 x 4, lo 100, 0 x 4]
 constexpr uint32_t kHlLo = 104;    // first column of lo
 constexpr uint32_t kBrM = 128;     // leaves per tile (TMEM lanes)
-constexpr uint32_t kBrRowBytes = kHlCols * 2;
-constexpr uint32_t kBrABytes = kBrM * kBrRowBytes;  // 53,248
-constexpr uint32_t kBrChunks = kHlCols / 8;         // 26 k-chunks of 16 B
+constexpr uint32_t kBrRowBytes = kHlCols * 2;       // 416 B per row in HBM
+constexpr uint32_t kBrAtoms = 4;                    // 64-element k-blocks (the last one 16 real)
+constexpr uint32_t kBrABytes = kBrAtoms * kBrM * 128;  // 64 KB per A stage (128-byte swizzle)
 constexpr uint32_t kBrSteps = kHlCols / 16;         // 13 MMAs of K = 16
 constexpr int kBrProducer = 0, kBrMma = 1, kBrEpi0 = 2, kBrEpiWarps = 8;
 constexpr int kBrThreads = 32 * (kBrEpi0 + kBrEpiWarps);  // 320
@@ -86,7 +88,7 @@ __global__ void k_bg_q_hl(const int8_t* __restrict__ q, uint32_t nq, __nv_bfloat
 struct BrArgs {
   uint32_t K;         // rows of the leaf matrix the map covers
   uint32_t row_step;  // leaf number of matrix row r: r * row_step
-  uint32_t nq, N;     // queries; queries per job (64, 128 or 256)
+  uint32_t nq, N;     // queries; queries per job (64, 128 or 192)
   uint32_t ntiles;    // 128-row tiles of the leaf matrix
   uint64_t njobs;     // ceil(nq / N) * ntiles
   const float* ln;    // |c|^2 per leaf
@@ -118,7 +120,7 @@ __global__ void __launch_bounds__(kBrThreads, 1) k_bg_route_tc(const __grid_cons
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   volatile int* abort_flag = &s_abort;
   const uint64_t j0 = a.njobs * blockIdx.x / gridDim.x, j1 = a.njobs * (blockIdx.x + 1) / gridDim.x;
-  const uint32_t N = a.N, ncols = 2 * N;
+  const uint32_t N = a.N, ncols = N <= 64 ? 128 : N <= 128 ? 256 : 512;  // 2N, rounded to a power of two
 
   if (warp == kBrMma) {
     tc_alloc(&s_tmem, ncols);
@@ -139,7 +141,7 @@ __global__ void __launch_bounds__(kBrThreads, 1) k_bg_route_tc(const __grid_cons
   __syncthreads();
   tc_fence_after();
   const uint32_t tmem = s_tmem;
-  const uint32_t bsm = smem_addr(smem), asm0 = bsm + N * kBrRowBytes;
+  const uint32_t bsm = smem_addr(smem), asm0 = bsm + kBrAtoms * N * 128;
   // one lane waits, the warp follows its verdict (keeps the warp converged for .sync.aligned ops)
   auto wait1 = [&](uint64_t* b, uint32_t par) {
     int r = 0;
@@ -158,15 +160,15 @@ __global__ void __launch_bounds__(kBrThreads, 1) k_bg_route_tc(const __grid_cons
         if (qg != cur_qg) {
           // B is read by every MMA issued so far: wait for the last job's (its commit tracks all)
           if (t > 0 && !mbar_wait(&bar_aempty[(t - 1) & 1], (uint32_t)(((t - 1) >> 1) & 1), abort_flag)) break;
-          mbar_expect_tx(&bar_bfull, N * kBrRowBytes);
-          for (uint32_t c = 0; c < kBrChunks; c++)
-            tma_load_2d(bsm + c * N * 16, &map_q, (int32_t)(8 * c), (int32_t)(qg * N), &bar_bfull);
+          mbar_expect_tx(&bar_bfull, kBrAtoms * N * 128);
+          for (uint32_t kb = 0; kb < kBrAtoms; kb++)
+            tma_load_2d(bsm + kb * N * 128, &map_q, (int32_t)(64 * kb), (int32_t)(qg * N), &bar_bfull);
           cur_qg = qg;
           nb++;
         }
         mbar_expect_tx(&bar_afull[s], kBrABytes);
-        for (uint32_t c = 0; c < kBrChunks; c++)
-          tma_load_2d(asm0 + s * kBrABytes + c * kBrM * 16, &map_l, (int32_t)(8 * c), (int32_t)(tile * kBrM),
+        for (uint32_t kb = 0; kb < kBrAtoms; kb++)
+          tma_load_2d(asm0 + s * kBrABytes + kb * kBrM * 128, &map_l, (int32_t)(64 * kb), (int32_t)(tile * kBrM),
                       &bar_afull[s]);
       }
       // copies in flight land before the CTA leaves (a no-op when every job ran)
@@ -181,7 +183,6 @@ __global__ void __launch_bounds__(kBrThreads, 1) k_bg_route_tc(const __grid_cons
   } else if (warp == kBrMma) {
     // kind::f16: F32 accumulators, BF16 A and B, both K-major, M = 128, N
     const uint32_t idesc = (1u << 4) | (1u << 7) | (1u << 10) | ((N >> 3) << 17) | ((kBrM >> 4) << 24);
-    const uint64_t bd = smem_desc(bsm, N * 16, 128);
     uint32_t cur_qg = 0xFFFFFFFFu, nb = 0;
     uint64_t t = 0;
     for (uint64_t j = j0; j < j1; j++, t++) {
@@ -195,11 +196,12 @@ __global__ void __launch_bounds__(kBrThreads, 1) k_bg_route_tc(const __grid_cons
       if (!wait1(&bar_dempty[s], (u & 1) ^ 1)) break;
       if (!wait1(&bar_afull[s], u & 1)) break;
       tc_fence_after();
-      const uint64_t ad = smem_desc(asm0 + s * kBrABytes, kBrM * 16, 128);
-      // K step k covers k-chunks 2k and 2k + 1: the starts move 2 chunks (2 * rows * 16 B)
+      const uint32_t as = asm0 + s * kBrABytes;
+      // K step k: k-block k/4 (rows * 128 B further on), then 32 B into its rows
 #pragma unroll
       for (uint32_t k = 0; k < kBrSteps; k++)
-        tc_mma_bf16_ss_elect(tmem + s * N, ad + 2 * k * kBrM, bd + 2 * k * N, idesc, k != 0);
+        tc_mma_bf16_ss_elect(tmem + s * N, smem_desc_sw128(as + (k >> 2) * (kBrM * 128) + (k & 3) * 32),
+                             smem_desc_sw128(bsm + (k >> 2) * (N * 128) + (k & 3) * 32), idesc, k != 0);
       tc_commit_elect(&bar_aempty[s]);
       tc_commit_elect(&bar_dfull[s]);
       __syncwarp();
@@ -228,22 +230,35 @@ __global__ void __launch_bounds__(kBrThreads, 1) k_bg_route_tc(const __grid_cons
             if (valid && q0 + jj < a.nq)
               a.scores[(size_t)(q0 + jj) * a.K + row] = __fsub_rn(__fmul_rn(2.0f, __uint_as_float(r[jj])), lnc);
         } else {
-          const float my_lim = q0 + lane < a.nq ? a.lim[q0 + lane] : 0.0f;
+          // 1. every column's passing leaves as a ballot; lane j keeps column j's
+          const bool q_on = q0 + lane < a.nq;
+          const float my_lim = q_on ? a.lim[q0 + lane] : 0.0f;
+          uint32_t mine = 0;
 #pragma unroll
           for (uint32_t jj = 0; jj < 32; jj++) {
             const float v = __fsub_rn(__fmul_rn(2.0f, __uint_as_float(r[jj])), lnc);
+            r[jj] = __float_as_uint(v);
             const float lj = __shfl_sync(0xFFFFFFFFu, my_lim, jj);
-            const bool pass = valid && q0 + jj < a.nq && v >= lj;
-            const uint32_t m = __ballot_sync(0xFFFFFFFFu, pass);
-            if (m) {
-              const uint32_t q = q0 + jj;
-              uint32_t base = 0;
-              if (lane == 0) base = atomicAdd(a.cnt + q, (uint32_t)__popc(m));
-              base = __shfl_sync(0xFFFFFFFFu, base, 0);
-              if (pass) {
-                const uint32_t idx = base + (uint32_t)__popc(m & ((1u << lane) - 1u));
-                if (idx < a.cap) a.ent[(size_t)q * a.cap + idx] = make_uint2(leaf, __float_as_uint(v));
-              }
+            const uint32_t m = __ballot_sync(0xFFFFFFFFu, valid && v >= lj);
+            if (lane == jj) mine = m;
+          }
+          if (!q_on) mine = 0;
+          // 2. one atomic per column with entries, all columns at once (lane j for query q0 + j)
+          uint32_t base = 0;
+          if (mine) base = atomicAdd(a.cnt + q0 + lane, (uint32_t)__popc(mine));
+          // 3. the entries, column by column over the columns that have any
+          const uint32_t lt = (1u << lane) - 1u;
+          for (uint32_t cols = __ballot_sync(0xFFFFFFFFu, mine != 0); cols; cols &= cols - 1) {
+            const uint32_t jj = __ffs(cols) - 1;
+            const uint32_t m = __shfl_sync(0xFFFFFFFFu, mine, jj);
+            const uint32_t b = __shfl_sync(0xFFFFFFFFu, base, jj);
+            float v = 0.0f;
+#pragma unroll
+            for (uint32_t k = 0; k < 32; k++)
+              if (k == jj) v = __uint_as_float(r[k]);
+            if ((m >> lane) & 1u) {
+              const uint32_t idx = b + (uint32_t)__popc(m & lt);
+              if (idx < a.cap) a.ent[(size_t)(q0 + jj) * a.cap + idx] = make_uint2(leaf, __float_as_uint(v));
             }
           }
         }
@@ -420,11 +435,13 @@ BgRoutePlan bg_route_plan(uint32_t K, uint32_t P) {
   return pl;
 }
 
-static uint32_t queries_per_job(uint32_t nq) { return nq <= 64 ? 64 : nq <= 128 ? 128 : 256; }
+// Queries per job: B (4 x N x 128 B) and the two A stages (2 x 64 KB) fit in shared memory up to
+// N = 192.
+static uint32_t queries_per_job(uint32_t nq) { return nq <= 64 ? 64 : nq <= 128 ? 128 : 192; }
 
 cudaError_t launch_bg_route_tc(const BgRouteTc& r, cudaStream_t st) {
   static PerDeviceOnce attr;
-  const int gemm_smem_max = (int)(256 * kBrRowBytes + 2 * kBrABytes);
+  const int gemm_smem_max = (int)(kBrAtoms * 192 * 128 + 2 * kBrABytes);
   attr([&] {
     cudaError_t e = cudaFuncSetAttribute(k_bg_route_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, gemm_smem_max);
     if (e == cudaSuccess)
@@ -437,11 +454,11 @@ cudaError_t launch_bg_route_tc(const BgRouteTc& r, cudaStream_t st) {
   const uint64_t nel = (uint64_t)nq * kHlCols;
   k_bg_q_hl<<<(unsigned)((nel + 255) / 256), 256, 0, st>>>(r.q, nq, r.qhl);
   CUtensorMap map_q, map_full, map_sub;
-  if (!encode_bf16_rows(&map_q, r.qhl, kHlCols, nq, kBrRowBytes, N) ||
-      !encode_bf16_rows(&map_full, r.hl, kHlCols, r.K, kBrRowBytes, kBrM) ||
-      (pl.subset && !encode_bf16_rows(&map_sub, r.hl, kHlCols, pl.ksub, (uint64_t)kBgSubStep * kBrRowBytes, kBrM)))
+  if (!encode_bf16_rows(&map_q, r.qhl, kHlCols, nq, kBrRowBytes, N, true) ||
+      !encode_bf16_rows(&map_full, r.hl, kHlCols, r.K, kBrRowBytes, kBrM, true) ||
+      (pl.subset && !encode_bf16_rows(&map_sub, r.hl, kHlCols, pl.ksub, (uint64_t)kBgSubStep * kBrRowBytes, kBrM, true)))
     return cudaErrorInvalidValue;
-  const size_t smem = (size_t)N * kBrRowBytes + 2 * kBrABytes;
+  const size_t smem = (size_t)kBrAtoms * N * 128 + 2 * kBrABytes;
   const uint32_t nqg = (nq + N - 1) / N;
   BrArgs a{};
   a.nq = nq;

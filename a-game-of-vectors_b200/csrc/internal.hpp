@@ -248,10 +248,11 @@ void launch_prep(const DevIndex& ix, Workspace& w, uint32_t nq, cudaStream_t st)
 // false if the driver does not provide it.
 bool route_gemm_ready();
 // A 2-D TMA map over a bf16 matrix of `rows` rows of `cols` elements, `row_bytes` apart (a multiple
-// of 16), whose box is one 16-byte k-chunk (8 elements) of box_rows rows; rows past `rows` read as
-// zeros. False if the encoder is missing or rejects the shape.
+// of 16), whose box is one k-chunk of box_rows rows: 16 bytes (8 elements) without swizzle, or
+// 128 bytes (64 elements) in the 128-byte swizzle (sw128); rows and columns past the matrix read
+// as zeros. False if the encoder is missing or rejects the shape.
 bool encode_bf16_rows(CUtensorMap* m, const void* base, uint64_t cols, uint64_t rows, uint64_t row_bytes,
-                      uint32_t box_rows);
+                      uint32_t box_rows, bool sw128);
 
 // ---- bigann routing on the tcgen05 tensor cores (bg_route.cu) --------------------------------
 constexpr uint32_t kBgSubStep = 16;  // the threshold subset: every 16th leaf

@@ -56,15 +56,15 @@ __global__ void __launch_bounds__(256) k_route_fp32(const float* __restrict__ q2
 
 // ---- BF16 GEMM on the tcgen05 tensor cores: 128 centroids x 64 queries per CTA --------------
 // D[centroid][query] = sum_k c_bf16[k] * bf16(q[k]) in FP32 tensor memory (M = 128 TMEM lanes,
-// N = 64 columns). Both operands come into shared memory by TMA as K-major core matrices without
-// swizzle (8 rows x 16 B = 8 bf16 each): one tiled copy per 16-byte k-chunk c brings that chunk
-// of all the tile's rows, row after row, to c * rows * 16 B. So the core matrices of a chunk
-// are 128 B apart along the rows (SBO) and the chunks rows * 16 B apart along K (LBO). The
-// copies bypass the load/store pipe, which register-staged loads of this layout saturate (each
-// warp-wide load touches 8 rows). One elected lane issues the 16 MMAs (K = 16 each). All warps
-// then read the accumulators with tcgen05.ld: warp w takes TMEM lanes 32*(w&3).. (the tile's
-// centroids) and columns 32*(w>>2).. (queries), and stores each query's 32 centroid scores as
-// one coalesced 128 B row segment. Rows past K or nq come in as zeros (the maps' bounds).
+// N = 64 columns). Both operands come into shared memory by TMA in the 128-byte-swizzled K-major
+// layout: one tiled copy per 64-element (128 B) k-block brings that block of all the tile's rows,
+// 128 B per row, to kb * rows * 128 B, each row's 16-byte chunks permuted by the row index
+// (chunk j of row r at j ^ (r & 7)), 8-row groups 1024 B apart (SBO). The MMA descriptors carry the
+// same swizzle mode, and an MMA's K step (16 elements, 32 B) moves the start 32 B within the
+// 128-byte row. One elected lane issues the 16 MMAs (K = 16 each). All warps then read the
+// accumulators with tcgen05.ld: warp w takes TMEM lanes 32*(w&3).. (the tile's centroids) and
+// columns 32*(w>>2).. (queries), and stores each query's 32 centroid scores as one coalesced
+// 128 B row segment. Rows past K or nq come in as zeros (the maps' bounds).
 constexpr int kRtM = 128, kRtN = 64, kRtThreads = 256;
 constexpr uint32_t kRtCols = 64;  // TMEM columns: the f32 accumulators
 constexpr int kRtABytes = kRtM * SG_PDIM * 2, kRtBBytes = kRtN * SG_PDIM * 2;
@@ -112,9 +112,9 @@ __global__ void __launch_bounds__(kRtThreads) k_route_tc(const __grid_constant__
     const uint32_t a = smem_addr(smem), b = a + kRtABytes;
     if (lane == 0) {
       mbar_expect_tx(&bar_load, kRtABytes + kRtBBytes);
-      for (int c = 0; c < SG_PDIM / 8; c++) {
-        tma_load_2d(a + c * (kRtM * 16), &map_c, 8 * c, (int32_t)m0, &bar_load);
-        tma_load_2d(b + c * (kRtN * 16), &map_q, 8 * c, (int32_t)q0, &bar_load);
+      for (int kb = 0; kb < SG_PDIM / 64; kb++) {
+        tma_load_2d(a + kb * (kRtM * 128), &map_c, 64 * kb, (int32_t)m0, &bar_load);
+        tma_load_2d(b + kb * (kRtN * 128), &map_q, 64 * kb, (int32_t)q0, &bar_load);
       }
     }
     __syncwarp();
@@ -123,11 +123,11 @@ __global__ void __launch_bounds__(kRtThreads) k_route_tc(const __grid_constant__
       // kind::f16 instruction descriptor: F32 accumulators, BF16 A and B, both K-major
       const uint32_t idesc = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(kRtN >> 3) << 17) |
                              ((uint32_t)(kRtM >> 4) << 24);
-      const uint64_t ad = smem_desc(a, kRtM * 16, 128), bd = smem_desc(b, kRtN * 16, 128);
-      // K step s covers k-chunks 2s and 2s + 1: the start moves two chunks (2 * rows * 16 B)
+      // K step s: k-block s/4 (rows * 128 B further on), then 32 B into its rows
 #pragma unroll
       for (uint32_t s = 0; s < SG_PDIM / 16; s++)
-        tc_mma_bf16_ss_elect(tmem, ad + 2 * s * kRtM, bd + 2 * s * kRtN, idesc, s != 0);
+        tc_mma_bf16_ss_elect(tmem, smem_desc_sw128(a + (s >> 2) * (kRtM * 128) + (s & 3) * 32),
+                             smem_desc_sw128(b + (s >> 2) * (kRtN * 128) + (s & 3) * 32), idesc, s != 0);
       tc_commit_elect(&bar_done);
     }
     __syncwarp();
@@ -175,22 +175,22 @@ static PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
 bool route_gemm_ready() { return tensor_map_encoder() != nullptr; }
 
 bool encode_bf16_rows(CUtensorMap* m, const void* base, uint64_t cols, uint64_t rows, uint64_t row_bytes,
-                      uint32_t box_rows) {
+                      uint32_t box_rows, bool sw128) {
   const PFN_cuTensorMapEncodeTiled_v12000 enc = tensor_map_encoder();
   if (!enc || rows == 0 || row_bytes % 16 || box_rows == 0 || box_rows > 256) return false;
   const cuuint64_t dims[2] = {cols, rows};
   const cuuint64_t strides[1] = {row_bytes};
-  const cuuint32_t box[2] = {8, box_rows};
+  const cuuint32_t box[2] = {sw128 ? 64u : 8u, box_rows};
   const cuuint32_t estr[2] = {1, 1};
   return enc(m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<void*>(base), dims, strides, box, estr,
-             CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
-             CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+             CU_TENSOR_MAP_INTERLEAVE_NONE, sw128 ? CU_TENSOR_MAP_SWIZZLE_128B : CU_TENSOR_MAP_SWIZZLE_NONE,
+             CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
-// A map over a row-major [rows x 256] bf16 matrix (16-byte aligned) whose box is one 16-byte
-// k-chunk (8 elements) of box_rows rows; rows past `rows` read as zeros.
+// A map over a row-major [rows x 256] bf16 matrix (16-byte aligned) whose box is one 128-byte
+// k-block (64 elements) of box_rows rows in the 128-byte swizzle; rows past `rows` read as zeros.
 static bool encode_rows(CUtensorMap* m, const __nv_bfloat16* base, uint64_t rows, uint32_t box_rows) {
-  return encode_bf16_rows(m, base, SG_PDIM, rows, SG_PDIM * sizeof(__nv_bfloat16), box_rows);
+  return encode_bf16_rows(m, base, SG_PDIM, rows, SG_PDIM * sizeof(__nv_bfloat16), box_rows, true);
 }
 
 // The reference's sequential FP32 dot of one query with one centroid row.

@@ -113,6 +113,15 @@ SG_DEV uint64_t smem_desc(uint32_t saddr, uint32_t lbo, uint32_t sbo) {
          ((uint64_t)((sbo >> 4) & 0x3FFFu) << 32) | (1ull << 46);
 }
 
+// Shared-memory matrix descriptor, K-major in the 128-byte swizzle (the layout a TMA copy with
+// CU_TENSOR_MAP_SWIZZLE_128B writes): rows of 128 B, 8-row groups 1024 B apart (SBO), the
+// leading offset unused (1), layout type 2. The 1024-byte group must be 1024-byte aligned; the
+// start may sit 32/64/96 B into its rows (an MMA's K step inside the 128-byte row).
+SG_DEV uint64_t smem_desc_sw128(uint32_t saddr) {
+  return (uint64_t)((saddr >> 4) & 0x3FFFu) | (1ull << 16) | ((uint64_t)(1024 >> 4) << 32) | (1ull << 46) |
+         (2ull << 61);
+}
+
 // D[tmem] (+)= A[smem descriptor] x B[smem descriptor], bf16 x bf16 -> f32 with the shape of the
 // instruction descriptor, issued by one elected lane of a converged warp.
 SG_DEV void tc_mma_bf16_ss_elect(uint32_t d_tmem, uint64_t a_desc, uint64_t b_desc, uint32_t idesc,
