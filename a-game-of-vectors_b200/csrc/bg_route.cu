@@ -56,7 +56,8 @@ constexpr uint32_t kBrABytes = kBrAtoms * kBrM * 128;  // 64 KB per A stage (128
 constexpr uint32_t kBrSteps = kHlCols / 16;         // 13 MMAs of K = 16
 constexpr int kBrProducer = 0, kBrMma = 1, kBrEpi0 = 2, kBrEpiWarps = 8;
 constexpr int kBrThreads = 32 * (kBrEpi0 + kBrEpiWarps);  // 320
-constexpr uint32_t kBrWin = 8192;  // rescoring window of one query (u64 keys in shared memory)
+constexpr uint32_t kBrWin = 4096;  // rescoring window of one query (u64 keys in shared memory)
+constexpr uint32_t kBrSelThreads = 256;
 
 // The [K x 208] bf16 hi/lo matrix of the leaves, one element per thread.
 __global__ void k_bg_leaf_hl(const float* __restrict__ leaves, uint32_t K, __nv_bfloat16* __restrict__ hl) {
@@ -348,8 +349,8 @@ SG_DEV void bg_emit_probes(uint64_t* keys, uint32_t P, float margin, float Q, co
   }
 }
 
-// Step 5 of the header: one CTA (1024 threads) per query.
-__global__ void __launch_bounds__(1024) k_bg_select_tc(const uint2* __restrict__ ent, const uint32_t* __restrict__ cnt,
+// Step 5 of the header: one CTA (256 threads) per query.
+__global__ void __launch_bounds__(kBrSelThreads) k_bg_select_tc(const uint2* __restrict__ ent, const uint32_t* __restrict__ cnt,
                                                        uint32_t cap, uint32_t K, uint32_t P, float margin,
                                                        const float* __restrict__ qq, float cmax, float cmax2,
                                                        const int8_t* __restrict__ qin, const float* __restrict__ leaves,
@@ -394,7 +395,7 @@ __global__ void __launch_bounds__(1024) k_bg_select_tc(const uint2* __restrict__
       }
       __syncthreads();
       const uint64_t T2 = block_select_nth_u64([&](uint32_t i) { return keys[i]; }, nw, P, hist, tmp);
-      uint64_t mine[kBrWin / 1024];
+      uint64_t mine[kBrWin / kBrSelThreads];
       uint32_t nm = 0;
       for (uint32_t i = threadIdx.x; i < nw; i += blockDim.x)
         if (keys[i] >= T2) mine[nm++] = keys[i];
@@ -485,7 +486,7 @@ cudaError_t launch_bg_route_tc(const BgRouteTc& r, cudaStream_t st) {
   a.cap = pl.cap;
   a.cnt = r.cnt;
   k_bg_route_tc<<<(unsigned)std::min<uint64_t>(a.njobs, (uint64_t)r.sms), kBrThreads, smem, st>>>(map_full, map_q, a);
-  k_bg_select_tc<<<nq, 1024, kBrWin * sizeof(uint64_t), st>>>(r.ent, r.cnt, pl.cap, r.K, r.P, r.margin, r.qq, r.cmax,
+  k_bg_select_tc<<<nq, kBrSelThreads, kBrWin * sizeof(uint64_t), st>>>(r.ent, r.cnt, pl.cap, r.K, r.P, r.margin, r.qq, r.cmax,
                                                                r.cmax2, r.q, r.leaves, r.ln, r.probe, r.probe_cent,
                                                                r.probe_n, r.status);
   return cudaGetLastError();
