@@ -71,6 +71,9 @@ struct DevIndex {
   float cent_norm_max = 0.0f;
   uint32_t* block_off = nullptr;     // [k+1] first block of each cluster
   uint32_t* clen = nullptr;          // [k] real (non-PAD) slots of each cluster
+  float2* mul_rng = nullptr;         // [k] (min, max) of a cluster's mul over its real slots when all
+                                     // are finite and >= 0, else (NaN, NaN): the bound pass's integer
+                                     // prefilter (scan_tcf.cu)
   uint8_t* blocks = nullptr;         // [nblocks*1024] nibble-transposed codes (blocks.bin)
   uint32_t* blocks_tc = nullptr;     // [nslots*8] the same codes slot-major (tcgen05 scan)
   float* mul = nullptr;              // [nslots] factors.f32 [.., 0]
@@ -92,6 +95,7 @@ struct DevIndex {
   uint8_t* codes = nullptr;          // [n*32] codes.bin, when given (the flat Hamming baseline)
   std::vector<uint64_t> h_block_off;
   std::vector<uint32_t> h_clen;
+  std::vector<float2> h_mul_rng;
   std::vector<uint32_t> h_chunks_desc_prefix;  // prefix sums of per-cluster chunk counts, largest first
   std::vector<uint64_t> h_slots_desc_prefix;   // prefix sums of per-cluster slot counts, largest first
 };
@@ -231,6 +235,8 @@ struct Config {
 
 std::string& last_error();
 void set_cluster_bounds(DevIndex& x, uint32_t chunk);
+// (min, max) of mul[0..len) when every value is finite and >= 0, else (NaN, NaN).
+float2 mul_range(const float* mul, uint64_t len);
 int fail(int code, const std::string& msg);
 
 // Views of an open index for entry points in other translation units (sieve_gpu.cu defines them).

@@ -130,7 +130,38 @@ struct TcfArgs {
   const uint64_t* const* allow_q;
   const uint64_t* allow_wq;
   uint32_t global;  // global sign codes: centroid score 0, admission key = row
+  const float2* mul_rng;  // [k] per cluster (min, max) of mul, or NaN: the integer prefilter
 };
+
+// The integer prefilter of the transposed pass. For a query with admission threshold T (an
+// estimate), centroid score cent, estimator constants a > 0, b, residual bound gamma * D + R_hi,
+// and a cluster whose slots all have mul in [m0, m1] with m0 >= 0, returns an integer Df such that
+// every slot with D <= Df has a bound estimate below T: then only pairs with D > Df need the
+// float bound. In exact arithmetic est(D, mul) = cent + mul * X(D) with X(D) = a (gamma D + R) + b
+// increasing in D. Take T' = T - slack, slack above the rounding error of the float bound over
+// |D| <= 256 * 127 (16 roundings of 2^-24 of the magnitudes it adds). If T' > cent, est >= T'
+// needs X(D) > 0 and m1 X(D) >= T' - cent; otherwise X(D) < 0 everywhere below the root and
+// est <= cent + m0 X(D). Either way D >= D* = ((T' - cent) / m - b) / a - R) / gamma with m = m1
+// or m0, so Df = floor(D*) - 1. Returns INT_MIN (no prefilter) where any input is unusable.
+SG_DEV int tct_prefilter(float cent, float a, float b, float gam, float rhi, uint32_t thr_key, float2 mr) {
+  const double m0 = mr.x, m1 = mr.y;
+  if (thr_key == 0u || !(m0 >= 0.0) || !(m1 >= m0) || !isfinite(m1) || !(a > 0.0f) || !(gam > 0.0f) ||
+      !isfinite(cent) || !isfinite(b) || !isfinite(rhi))
+    return INT_MIN;
+  const double T = unord(thr_key);
+  if (!isfinite(T)) return INT_MIN;
+  const double dmax = 256.0 * 127.0;
+  const double mag = fabs((double)cent) + m1 * (fabs((double)a) * ((double)gam * dmax + fabs((double)rhi)) +
+                                                fabs((double)b)) + fabs(T);
+  const double Tl = T - 16.0 * 5.9604644775390625e-08 * mag;
+  const double m = Tl > (double)cent ? m1 : m0;
+  if (!(m > 0.0)) return INT_MIN;
+  const double Ds = (((Tl - (double)cent) / m - (double)b) / (double)a - (double)rhi) / (double)gam;
+  if (!isfinite(Ds)) return INT_MIN;
+  const double Df = floor(Ds) - 1.0;
+  if (Df < -dmax - 1.0) return INT_MIN;
+  return Df > dmax ? (int)dmax : (int)Df;
+}
 
 __global__ void __launch_bounds__(kFThreads, 1) k_scan_tcf(TcfArgs a) {
   extern __shared__ __align__(1024) uint8_t smem[];  // B of the two item slots
@@ -468,6 +499,7 @@ __global__ void __launch_bounds__(kTThreads, 1) k_scan_tct(TcfArgs a) {
   __shared__ float4 s_qc[2][kTM];    // cent, a, b, threshold key (as bits)
   __shared__ float4 s_qf[2][kTM];    // gamma, R_hi, R_lo, -
   __shared__ uint2 s_qk[2][kTM];     // candidate order base, query
+  __shared__ int s_qd[2][kTM];       // the integer prefilter: only D > s_qd needs the float bound
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   volatile int* abort_flag = &s_abort;
 
@@ -546,9 +578,11 @@ __global__ void __launch_bounds__(kTThreads, 1) k_scan_tct(TcfArgs a) {
         const float4 p = a.qp[q];
         const float cent = a.global ? 0.0f : a.probe_sc[(size_t)q * a.P + r];
         const uint32_t thr = *(volatile const uint32_t*)(a.thr + q);
+        const float4 f = a.fq[q];
         s_qc[slot][qi] = make_float4(cent, p.z, p.w, __uint_as_float(thr));
-        s_qf[slot][qi] = a.fq[q];
+        s_qf[slot][qi] = f;
         s_qk[slot][qi] = make_uint2(a.probe_off[(size_t)q * a.P + r], q);
+        s_qd[slot][qi] = tct_prefilter(cent, p.z, p.w, f.x, f.y, thr, a.mul_rng[c]);
       }
       if (lane == 0) {
         s_meta[slot][0] = b0;
@@ -629,10 +663,12 @@ __global__ void __launch_bounds__(kTThreads, 1) k_scan_tct(TcfArgs a) {
         const bool lane_on = n < ng;
         float4 qc = make_float4(0, 0, 0, 0), qf = qc;
         uint2 qk = make_uint2(0, 0);
+        int dq = INT_MAX;  // a lane without a query passes nothing
         if (lane_on) {
           qc = s_qc[slot][n];
           qf = s_qf[slot][n];
           qk = s_qk[slot][n];
+          dq = s_qd[slot][n];
         }
         const uint32_t thr = __float_as_uint(qc.w);
         for (uint32_t t = 0; t < ntiles; t++) {
@@ -650,20 +686,30 @@ __global__ void __launch_bounds__(kTThreads, 1) k_scan_tct(TcfArgs a) {
             tc_ld32(tmem + ((32u * qd) << 16) + dbuf * kTN + col0, v);
             tc_wait_ld();
             if (!on || bl >= nb) continue;  // warp-uniform
-            const uint32_t gbase = (b0 + bl) * SG_BLOCK;
-            const float my_mul = bl * SG_BLOCK + lane < cl ? a.mul[gbase + lane] : 0.0f;
-            const uint32_t nvalid = min(32u, cl > bl * SG_BLOCK ? cl - bl * SG_BLOCK : 0u);
-            uint32_t adm = 0;
+            // 1. the integer prefilter: columns whose product could reach the threshold
+            uint32_t cand = 0;
 #pragma unroll
-            for (int j = 0; j < 32; j++) {
-              const float mv = __shfl_sync(0xFFFFFFFFu, my_mul, j);
+            for (int j = 0; j < 32; j++) cand |= ((int)v[j] > dq ? 1u : 0u) << j;
+            const uint32_t nvalid = min(32u, cl > bl * SG_BLOCK ? cl - bl * SG_BLOCK : 0u);
+            cand &= nvalid == 32 ? 0xFFFFFFFFu : (1u << nvalid) - 1u;
+            if (!cand) continue;
+            // 2. the float bound of those pairs (the exact estimate's operations at the bound of
+            //    the score) against the query's admission key
+            const uint32_t gbase = (b0 + bl) * SG_BLOCK;
+            uint32_t adm = 0;
+            for (uint32_t r = cand; r; r &= r - 1) {
+              const uint32_t j = __ffs(r) - 1;
+              const float mv = a.mul[gbase + j];
               const bool neg = mv < 0.0f;
               const bool always = !isfinite(mv);  // no monotone bound: recheck the pair
-              const float sb = __fadd_rn(__fmul_rn(qf.x, (float)(int)v[j]), neg ? qf.z : qf.y);
+              int dv = 0;
+#pragma unroll
+              for (int k = 0; k < 32; k++)
+                if (k == (int)j) dv = (int)v[k];
+              const float sb = __fadd_rn(__fmul_rn(qf.x, (float)dv), neg ? qf.z : qf.y);
               const float est = __fadd_rn(qc.x, __fmul_rn(mv, __fadd_rn(__fmul_rn(qc.y, sb), qc.z)));
-              adm |= (always || ord(est) >= thr ? 1u : 0u) << j;
+              if (always || ord(est) >= thr) adm |= 1u << j;
             }
-            adm &= (lane_on ? (nvalid == 32 ? 0xFFFFFFFFu : (1u << nvalid) - 1u) : 0u);
             if (adm && (a.allow || a.allow_q)) {  // allowlist filters (View::hidden)
               const uint64_t* al = a.allow_q ? a.allow_q[qk.y] : a.allow;
               const uint64_t aw = a.allow_q ? a.allow_wq[qk.y] : a.allow_words;
@@ -784,6 +830,7 @@ int launch_scan_tcf(const DevIndex& ix, Workspace& w, uint32_t nq, uint32_t P, c
   a.allow_q = w.per_query_allow ? w.allow_q : nullptr;
   a.allow_wq = w.allow_wq;
   a.global = ix.global;
+  a.mul_rng = ix.mul_rng;
   // entries from tc_start[q] on are the bound pass's (earlier ones are exact already)
   cudaMemcpyAsync(w.tc_start, w.ccount, (size_t)nq * 4, cudaMemcpyDeviceToDevice, st);
   if (transposed) k_scan_tct<<<sms, kTThreads, kTSmem, st>>>(a);
