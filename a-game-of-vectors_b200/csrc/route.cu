@@ -240,10 +240,20 @@ struct SelectArgs {
   uint32_t* counters;
 };
 
-// Writes query q's probe list (keys[0..m) sorted best first: probe ranks 0..m-1), the admission
-// offset of each probe's first slot, its seed descriptor and its ALU scan items. All threads of
-// the block call it.
-SG_DEV void emit_probes(const SelectArgs& a, const uint64_t* keys, uint32_t m, uint32_t q,
+// Blocks of each probe, nbs[r] for keys[0..m), read in parallel (the seed and the budget then walk
+// them in shared memory). All threads of the block call it.
+SG_DEV void probe_blocks(const SelectArgs& a, const uint64_t* keys, uint32_t m, uint32_t* nbs) {
+  for (uint32_t r = threadIdx.x; r < m; r += blockDim.x) {
+    const uint32_t c = key_id(keys[r]);
+    nbs[r] = a.block_off[c + 1] - a.block_off[c];
+  }
+  __syncthreads();
+}
+
+// Writes query q's probe list (keys[0..m) sorted best first: probe ranks 0..m-1, nbs[r] their
+// blocks), the admission offset of each probe's first slot, its seed descriptor and its ALU scan
+// items. All threads of the block call it.
+SG_DEV void emit_probes(const SelectArgs& a, const uint64_t* keys, const uint32_t* nbs, uint32_t m, uint32_t q,
                         uint32_t* tmp) {
   const uint32_t P = a.P;
   // probe list, admission offsets and chunk counts (block scans over probe ranks)
@@ -257,8 +267,7 @@ SG_DEV void emit_probes(const SelectArgs& a, const uint64_t* keys, uint32_t m, u
   if (threadIdx.x == 0) {
     uint32_t used = 0, rs = 0, partial = 0;
     for (uint32_t r = 0; r < m && r < kMaxSegs; r++) {
-      const uint32_t c = key_id(keys[r]);
-      const uint32_t nb = a.block_off[c + 1] - a.block_off[c];
+      const uint32_t nb = nbs[r];
       if (r == 0 && nb > a.seed_blocks) {
         rs = 1;
         partial = a.seed_blocks;
@@ -280,8 +289,7 @@ SG_DEV void emit_probes(const SelectArgs& a, const uint64_t* keys, uint32_t m, u
   };
   uint32_t slots = 0, chunks = 0;
   for (uint32_t r = r0; r < r1; r++) {
-    uint32_t c = key_id(keys[r]);
-    uint32_t nb = a.block_off[c + 1] - a.block_off[c];
+    const uint32_t nb = nbs[r];
     slots += nb * SG_BLOCK;
     chunks += nchunks(r, nb);
   }
@@ -345,7 +353,8 @@ SG_DEV uint32_t expand_delta(const SelectArgs& a, uint64_t* keys, uint32_t m) {
 __global__ void __launch_bounds__(256) k_route_select(SelectArgs a) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   uint64_t* keys = reinterpret_cast<uint64_t*>(smem_raw);  // [kWinCap]
-  uint32_t* okeys = reinterpret_cast<uint32_t*>(smem_raw + kWinCap * sizeof(uint64_t));  // [K] if staged
+  uint32_t* nbs = reinterpret_cast<uint32_t*>(smem_raw + kWinCap * sizeof(uint64_t));     // [kWinCap]
+  uint32_t* okeys = nbs + kWinCap;  // [K] if staged
   __shared__ float qv[SG_PDIM];
   __shared__ uint32_t hist[2048], tmp[32];
   __shared__ uint32_t s_nw, s_m, s_keep;
@@ -420,6 +429,7 @@ __global__ void __launch_bounds__(256) k_route_select(SelectArgs a) {
   for (uint32_t i = P + threadIdx.x; i < n2; i += blockDim.x) keys[i] = 0;
   __syncthreads();
   block_bitonic_sort_desc(keys, n2);
+  if (a.p.has_budget) probe_blocks(a, keys, P, nbs);
   // margin (prefix of the sorted list) and budget
   if (threadIdx.x == 0) {
     uint32_t m = P;
@@ -433,8 +443,7 @@ __global__ void __launch_bounds__(256) k_route_select(SelectArgs a) {
       uint64_t used = 0;
       uint32_t keep = 0;
       for (uint32_t i = 0; i < m; i++) {
-        uint32_t c = key_id(keys[i]);
-        used += (uint64_t)(a.block_off[c + 1] - a.block_off[c]) * SG_BLOCK;
+        used += (uint64_t)nbs[i] * SG_BLOCK;
         if (used <= a.p.budget) keep++;
         else break;
       }
@@ -445,7 +454,8 @@ __global__ void __launch_bounds__(256) k_route_select(SelectArgs a) {
   }
   __syncthreads();
   const uint32_t m = a.live_kc ? expand_delta(a, keys, s_keep) : s_keep;
-  emit_probes(a, keys, m, q, tmp);
+  probe_blocks(a, keys, m, nbs);
+  emit_probes(a, keys, nbs, m, q, tmp);
 }
 
 // filter::search with Plan::Expand (src/filter.rs:79-93): every cluster in route order (exact f32
@@ -485,7 +495,9 @@ __global__ void __launch_bounds__(1024) k_route_expand(SelectArgs a,
     before += per_cluster[key_id(keys[i])];
   }
   const uint32_t m = block_sum(take, tmp);
-  emit_probes(a, keys, m, q, tmp);
+  uint32_t* nbs = reinterpret_cast<uint32_t*>(keys + next_pow2(K));  // [next_pow2(K)]
+  probe_blocks(a, keys, m, nbs);
+  emit_probes(a, keys, nbs, m, q, tmp);
 }
 
 // Index::candidates over a caller's probe list (src/ivf.rs:647-681): query q's probes
@@ -496,6 +508,7 @@ __global__ void __launch_bounds__(256) k_route_given(SelectArgs a, const float* 
                                                      const uint32_t* __restrict__ given_n) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   uint64_t* keys = reinterpret_cast<uint64_t*>(smem_raw);  // [P]
+  uint32_t* nbs = reinterpret_cast<uint32_t*>(keys + (a.P > 0 ? a.P : 1));  // [P]
   __shared__ uint32_t tmp[32];
   const uint32_t q = blockIdx.x;
   const uint32_t m = min(given_n[q], a.P);
@@ -504,7 +517,8 @@ __global__ void __launch_bounds__(256) k_route_given(SelectArgs a, const float* 
     keys[r] = rank_key(given_sc[(size_t)q * a.P + r], c < a.K ? c : 0u);
   }
   __syncthreads();
-  emit_probes(a, keys, m, q, tmp);
+  probe_blocks(a, keys, m, nbs);
+  emit_probes(a, keys, nbs, m, q, tmp);
 }
 
 cudaError_t launch_route_scores(const DevIndex& ix, Workspace& w, uint32_t nq, int precision,
@@ -559,9 +573,10 @@ void launch_route_select(const DevIndex& ix, Workspace& w, uint32_t nq, const sg
   static PerDeviceOnce attr;
   attr([&] {
     return cudaFuncSetAttribute(k_route_select, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                (int)(kWinCap * sizeof(uint64_t) + kRouteStageK * sizeof(uint32_t)));
+                                (int)(kWinCap * (sizeof(uint64_t) + sizeof(uint32_t)) + kRouteStageK * sizeof(uint32_t)));
   });
-  const size_t smem = kWinCap * sizeof(uint64_t) + (ix.kc <= kRouteStageK ? ix.kc * sizeof(uint32_t) : 0);
+  const size_t smem = kWinCap * (sizeof(uint64_t) + sizeof(uint32_t)) +
+                      (ix.kc <= kRouteStageK ? ix.kc * sizeof(uint32_t) : 0);
   k_route_select<<<nq, 256, smem, st>>>(a);
 }
 
@@ -591,10 +606,10 @@ void launch_route_given(const DevIndex& ix, Workspace& w, uint32_t nq, const sg_
   static PerDeviceOnce attr;
   attr([] {
     return cudaFuncSetAttribute(k_route_given, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                (int)(4096 * sizeof(uint64_t)));
+                                (int)(2 * 4096 * (sizeof(uint64_t) + sizeof(uint32_t))));
   });
-  k_route_given<<<nq, 256, (size_t)std::max<uint32_t>(a.P, 1) * sizeof(uint64_t), st>>>(a, given_sc, given_cl,
-                                                                                      given_n);
+  k_route_given<<<nq, 256, (size_t)std::max<uint32_t>(a.P, 1) * (sizeof(uint64_t) + sizeof(uint32_t)), st>>>(
+      a, given_sc, given_cl, given_n);
 }
 
 void launch_route_expand(const DevIndex& ix, Workspace& w, uint32_t nq, const sg_params& p,
@@ -625,11 +640,11 @@ void launch_route_expand(const DevIndex& ix, Workspace& w, uint32_t nq, const sg
   a.items = w.items;
   a.item_cap = w.item_cap;
   a.counters = w.counters;
-  const size_t smem = (size_t)next_pow2_host(ix.kc) * sizeof(uint64_t);
+  const size_t smem = (size_t)next_pow2_host(ix.kc) * (sizeof(uint64_t) + sizeof(uint32_t));
   static PerDeviceOnce attr;
   attr([] {
     return cudaFuncSetAttribute(k_route_expand, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                (int)(kExpandMaxK * sizeof(uint64_t)));
+                                (int)(kExpandMaxK * (sizeof(uint64_t) + sizeof(uint32_t))));
   });
   k_route_expand<<<nq, 1024, smem, st>>>(a, per_cluster, target);
 }
