@@ -46,8 +46,6 @@ constexpr uint32_t kSeedBlocks = 512;    // block budget of each query's seed (i
 constexpr uint32_t kMaxSegs = 64;        // probes one seed can cover
 // Largest cand / k / r the select kernels sort in shared memory.
 constexpr uint32_t kMaxCand = 4096;
-// Queries per work item of the transposed bound scan (its MMA M).
-constexpr uint32_t kScanTctGroup = 128;
 // Most clusters the filter plan Expand sorts per query in shared memory (128 KB of keys).
 constexpr uint32_t kExpandMaxK = 16384;
 // Status bits a kernel raises in Workspace::status.
@@ -71,9 +69,6 @@ struct DevIndex {
   float cent_norm_max = 0.0f;
   uint32_t* block_off = nullptr;     // [k+1] first block of each cluster
   uint32_t* clen = nullptr;          // [k] real (non-PAD) slots of each cluster
-  float2* mul_rng = nullptr;         // [k] (min, max) of a cluster's mul over its real slots when all
-                                     // are finite and >= 0, else (NaN, NaN): the bound pass's integer
-                                     // prefilter (scan_tcf.cu)
   uint8_t* blocks = nullptr;         // [nblocks*1024] nibble-transposed codes (blocks.bin)
   uint32_t* blocks_tc = nullptr;     // [nslots*8] the same codes slot-major (tcgen05 scan)
   float* mul = nullptr;              // [nslots] factors.f32 [.., 0]
@@ -95,7 +90,6 @@ struct DevIndex {
   uint8_t* codes = nullptr;          // [n*32] codes.bin, when given (the flat Hamming baseline)
   std::vector<uint64_t> h_block_off;
   std::vector<uint32_t> h_clen;
-  std::vector<float2> h_mul_rng;
   std::vector<uint32_t> h_chunks_desc_prefix;  // prefix sums of per-cluster chunk counts, largest first
   std::vector<uint64_t> h_slots_desc_prefix;   // prefix sums of per-cluster slot counts, largest first
 };
@@ -218,8 +212,8 @@ struct Config {
   uint32_t soft_cap = 0;  // per-query buffer override (0: automatic); SIEVE_GPU_SOFT_CAP
   int graphs = 1;         // capture and replay CUDA graphs per call shape (SIEVE_GPU_GRAPHS)
   int mma = 1;            // SIEVE_GPU_MMA: 0 ALU scan only, 1 automatic, 2 tensor cores whenever nprobe > 1
-  int tc = 1;             // SIEVE_GPU_TC: 1 the tcgen05 bound scan, 3 the same with slots on the MMA's N
-                          // axis, 2 the tcgen05 one-hot scan (kept for comparison)
+  int tc = 1;             // SIEVE_GPU_TC: 1 the tcgen05 bound scan, 2 the tcgen05 one-hot scan (kept
+                          // for comparison)
   uint32_t tc_split = 0;  // SIEVE_GPU_TC_SPLIT (> 1): a first tcgen05 round over the ranks below it
   // Clusters probed by fewer queries than this in a batch are scanned by the ALU kernel: a
   // tcgen05 tile costs the same ~32 x 101 cycles per 128 slots for any query count up to 128,
@@ -235,8 +229,6 @@ struct Config {
 
 std::string& last_error();
 void set_cluster_bounds(DevIndex& x, uint32_t chunk);
-// (min, max) of mul[0..len) when every value is finite and >= 0, else (NaN, NaN).
-float2 mul_range(const float* mul, uint64_t len);
 int fail(int code, const std::string& msg);
 
 // Views of an open index for entry points in other translation units (sieve_gpu.cu defines them).
@@ -335,7 +327,7 @@ int launch_scan_tc(const DevIndex& ix, Workspace& w, uint32_t nq, const sg_param
 // admitted (returns the kernels launched).
 void launch_filter_prep(Workspace& w, uint32_t nq, cudaStream_t st);
 int launch_scan_tcf(const DevIndex& ix, Workspace& w, uint32_t nq, uint32_t P, const uint64_t* allow,
-                    uint64_t allow_words, int sms, bool transposed, cudaStream_t st);
+                    uint64_t allow_words, int sms, cudaStream_t st);
 // Launch errors of these two are left for the caller's cudaGetLastError.
 void transcode_tc(const uint8_t* blocks, uint64_t nblocks, uint32_t* out, cudaStream_t st);
 void launch_lut_scan_tc(uint32_t nq, const uint8_t* tables, const uint32_t* codes, uint64_t nblocks,

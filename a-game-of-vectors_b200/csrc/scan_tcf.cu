@@ -130,38 +130,8 @@ struct TcfArgs {
   const uint64_t* const* allow_q;
   const uint64_t* allow_wq;
   uint32_t global;  // global sign codes: centroid score 0, admission key = row
-  const float2* mul_rng;  // [k] per cluster (min, max) of mul, or NaN: the integer prefilter
 };
 
-// The integer prefilter of the transposed pass. For a query with admission threshold T (an
-// estimate), centroid score cent, estimator constants a > 0, b, residual bound gamma * D + R_hi,
-// and a cluster whose slots all have mul in [m0, m1] with m0 >= 0, returns an integer Df such that
-// every slot with D <= Df has a bound estimate below T: then only pairs with D > Df need the
-// float bound. In exact arithmetic est(D, mul) = cent + mul * X(D) with X(D) = a (gamma D + R) + b
-// increasing in D. Take T' = T - slack, slack above the rounding error of the float bound over
-// |D| <= 256 * 127 (16 roundings of 2^-24 of the magnitudes it adds). If T' > cent, est >= T'
-// needs X(D) > 0 and m1 X(D) >= T' - cent; otherwise X(D) < 0 everywhere below the root and
-// est <= cent + m0 X(D). Either way D >= D* = ((T' - cent) / m - b) / a - R) / gamma with m = m1
-// or m0, so Df = floor(D*) - 1. Returns INT_MIN (no prefilter) where any input is unusable.
-SG_DEV int tct_prefilter(float cent, float a, float b, float gam, float rhi, uint32_t thr_key, float2 mr) {
-  const double m0 = mr.x, m1 = mr.y;
-  if (thr_key == 0u || !(m0 >= 0.0) || !(m1 >= m0) || !isfinite(m1) || !(a > 0.0f) || !(gam > 0.0f) ||
-      !isfinite(cent) || !isfinite(b) || !isfinite(rhi))
-    return INT_MIN;
-  const double T = unord(thr_key);
-  if (!isfinite(T)) return INT_MIN;
-  const double dmax = 256.0 * 127.0;
-  const double mag = fabs((double)cent) + m1 * (fabs((double)a) * ((double)gam * dmax + fabs((double)rhi)) +
-                                                fabs((double)b)) + fabs(T);
-  const double Tl = T - 16.0 * 5.9604644775390625e-08 * mag;
-  const double m = Tl > (double)cent ? m1 : m0;
-  if (!(m > 0.0)) return INT_MIN;
-  const double Ds = (((Tl - (double)cent) / m - (double)b) / (double)a - (double)rhi) / (double)gam;
-  if (!isfinite(Ds)) return INT_MIN;
-  const double Df = floor(Ds) - 1.0;
-  if (Df < -dmax - 1.0) return INT_MIN;
-  return Df > dmax ? (int)dmax : (int)Df;
-}
 
 __global__ void __launch_bounds__(kFThreads, 1) k_scan_tcf(TcfArgs a) {
   extern __shared__ __align__(1024) uint8_t smem[];  // B of the two item slots
@@ -455,306 +425,6 @@ __global__ void __launch_bounds__(kFThreads, 1) k_scan_tcf(TcfArgs a) {
   }
 }
 
-// ---- the same bound with slots on the MMA's N axis ---------------------------------------------
-// kind::i8 costs the same per instruction for every N up to 256 (M = 128, K = 32), so a tile of
-// 128 slots against a group of ~16 queries uses a sixteenth of it. Here the product is turned
-// around: D[query][slot] = sum_k w[query][k] * bit[slot][k], with the group's weights as A (s8,
-// M = 128 queries, K-major in shared memory, loaded once per item) and the code bits of 256 slots
-// as B (u8 0/1, N = 256, K-major in shared memory, built by the producers per tile). A tile costs
-// 8 instructions for 256 slots whatever the group's size (up to 128 queries). In tensor memory
-// lane = query and column = slot, so each epilogue lane bounds one query's pairs with that query's
-// constants in registers, and reserves its admitted entries with one atomic per 32 slots.
-constexpr int kTM = 128;             // queries per work item (MMA M)
-constexpr int kTN = 256;             // slots per tile (MMA N): 8 blocks
-constexpr int kTStages = 2;          // B stages
-constexpr int kTBBytes = kTN * SG_PDIM;  // 64 KB: 256 slots x 256 u8 bits
-constexpr int kTABytes = kTM * SG_PDIM;  // 32 KB: 128 queries x 256 s8 weights
-constexpr uint32_t kTCols = 512;     // TMEM: 2 accumulators x 256 columns
-constexpr int kTDBufs = 2;
-constexpr int kTProducers = 4;       // warps 0-3 build B
-constexpr int kTEpi = 4;             // warps 4-19 bound the pairs (4 per lane quarter)
-constexpr int kTEpiWarps = 16;
-constexpr int kTMma = 20;            // warp 20 issues the MMAs
-constexpr int kTLoader = 21;         // warp 21 loads work items
-constexpr int kTThreads = 22 * 32;
-constexpr int kTSmem = 2 * kTABytes + kTStages * kTBBytes;  // 192 KB
-
-// kind::i8 with s8 A (weights) and u8 B (code bits), s32 accumulators, M = 128, N = 256.
-constexpr uint32_t kTIdesc = (2u << 4) | (1u << 7) | ((uint32_t)(kTN >> 3) << 17) | ((uint32_t)(kTM >> 4) << 24);
-
-SG_DEV void tc_mma_i8_ss_elect(uint32_t d_tmem, uint64_t a_desc, uint64_t b_desc, uint32_t idesc, uint32_t accumulate) {
-  asm volatile(
-      "{\n.reg .pred p, e;\nsetp.ne.b32 p, %4, 0;\nelect.sync _|e, 0xffffffff;\n"
-      "@e tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, {%5, %5, %5, %5}, p;\n}\n" ::"r"(d_tmem),
-      "l"(a_desc), "l"(b_desc), "r"(idesc), "r"(accumulate), "r"(0u));
-}
-
-__global__ void __launch_bounds__(kTThreads, 1) k_scan_tct(TcfArgs a) {
-  extern __shared__ __align__(1024) uint8_t smem[];  // A of the two item slots, then the B stages
-  __shared__ __align__(8) uint64_t bar_bfull[kTStages], bar_bempty[kTStages], bar_dfull[kTDBufs],
-      bar_dempty[kTDBufs], bar_ifull[2], bar_iempty[2];
-  __shared__ uint32_t s_tmem;
-  __shared__ int s_abort;
-  __shared__ uint32_t s_meta[2][8];  // b0, nb, cl, ng, -, end
-  __shared__ float4 s_qc[2][kTM];    // cent, a, b, threshold key (as bits)
-  __shared__ float4 s_qf[2][kTM];    // gamma, R_hi, R_lo, -
-  __shared__ uint2 s_qk[2][kTM];     // candidate order base, query
-  __shared__ int s_qd[2][kTM];       // the integer prefilter: only D > s_qd needs the float bound
-  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-  volatile int* abort_flag = &s_abort;
-
-  if (warp == kTMma) {
-    tc_alloc(&s_tmem, kTCols);
-    tc_relinquish();
-  }
-  if (tid == 0) {
-    for (int i = 0; i < kTStages; i++) {
-      mbar_init(&bar_bfull[i], kTProducers);
-      mbar_init(&bar_bempty[i], 1);
-    }
-    for (int i = 0; i < kTDBufs; i++) {
-      mbar_init(&bar_dfull[i], 1);
-      mbar_init(&bar_dempty[i], kTEpiWarps);
-    }
-    for (int i = 0; i < 2; i++) {
-      mbar_init(&bar_ifull[i], 1);
-      mbar_init(&bar_iempty[i], kTProducers + kTEpiWarps + 1);
-    }
-    s_abort = 0;
-    fence_mbar_init();
-  }
-  tc_fence_before();
-  __syncthreads();
-  tc_fence_after();
-  const uint32_t tmem = s_tmem;
-  const uint32_t a_base = smem_addr(smem), b_base = a_base + 2 * kTABytes;
-  uint32_t* status = a.counters + 2;
-  // one lane waits, the warp follows its verdict (the warp stays converged for .sync.aligned ops)
-  auto wait1 = [&](uint64_t* b, uint32_t par) {
-    int r = 0;
-    if (lane == 0) r = mbar_wait(b, par, abort_flag) ? 1 : 0;
-    return __shfl_sync(0xFFFFFFFFu, r, 0) != 0;
-  };
-
-  if (warp == kTLoader) {
-    // ---- work items into the two item slots: A (weights) and the per-query constants --------
-    const uint32_t nitems = a.counters[4];
-    for (uint32_t it = 0;; it++) {
-      const uint32_t slot = it & 1, use = it >> 1;
-      if (!wait1(&bar_iempty[slot], (use & 1) ^ 1)) break;
-      uint32_t item = 0;
-      if (lane == 0) item = atomicAdd(a.counters + 5, 1u);
-      item = __shfl_sync(0xFFFFFFFFu, item, 0);
-      if (item >= nitems) {
-        if (lane == 0) {
-          s_meta[slot][5] = 1;
-          mbar_arrive(&bar_ifull[slot]);
-        }
-        break;
-      }
-      const uint2 gi = a.gitems[item];
-      const uint32_t c = gi.x;
-      const uint32_t l0 = a.inv_off[c] + gi.y * kTM;
-      const uint32_t ng = min((uint32_t)kTM, a.inv_off[c + 1] - l0);
-      const uint32_t b0 = a.block_off[c], nb = a.block_off[c + 1] - b0, cl = a.clen[c];
-      const uint32_t rows = (ng + 7) & ~7u;  // rows past ng are never read back
-      uint8_t* A = smem + slot * kTABytes;
-      if (nb > 0) {
-        // query n's 16-byte K chunk g at (n/8)*2048 + g*128 + (n%8)*16 (K-major core matrices)
-#pragma unroll 4
-        for (uint32_t e = lane; e < rows * 16; e += 32) {
-          const uint32_t r = e & 7, g = (e >> 3) & 15, n = (e >> 7) * 8 + r;
-          uint4 v = make_uint4(0, 0, 0, 0);
-          if (n < ng) {
-            const uint32_t q = a.inv_list[l0 + n] >> 12;
-            v = reinterpret_cast<const uint4*>(a.w8 + (size_t)q * SG_GROUPS)[g];
-          }
-          *reinterpret_cast<uint4*>(A + (n >> 3) * 2048 + g * 128 + r * 16) = v;
-        }
-      }
-      for (uint32_t qi = lane; qi < ng; qi += 32) {
-        const uint32_t ent = a.inv_list[l0 + qi];
-        const uint32_t q = ent >> 12, r = ent & 0xFFFu;
-        const float4 p = a.qp[q];
-        const float cent = a.global ? 0.0f : a.probe_sc[(size_t)q * a.P + r];
-        const uint32_t thr = *(volatile const uint32_t*)(a.thr + q);
-        const float4 f = a.fq[q];
-        s_qc[slot][qi] = make_float4(cent, p.z, p.w, __uint_as_float(thr));
-        s_qf[slot][qi] = f;
-        s_qk[slot][qi] = make_uint2(a.probe_off[(size_t)q * a.P + r], q);
-        s_qd[slot][qi] = tct_prefilter(cent, p.z, p.w, f.x, f.y, thr, a.mul_rng[c]);
-      }
-      if (lane == 0) {
-        s_meta[slot][0] = b0;
-        s_meta[slot][1] = nb;
-        s_meta[slot][2] = cl;
-        s_meta[slot][3] = ng;
-        s_meta[slot][5] = 0;
-      }
-      fence_proxy_async_smem();
-      __syncwarp();
-      if (lane == 0) mbar_arrive(&bar_ifull[slot]);
-    }
-  } else if (warp < kTProducers || warp == kTMma || (warp >= kTEpi && warp < kTEpi + kTEpiWarps)) {
-    // ---- consumers: items in order, tiles numbered across items ------------------------------
-    uint32_t ts = 0;  // tiles of earlier items
-    for (uint32_t it = 0;; it++) {
-      const uint32_t slot = it & 1, use = it >> 1;
-      if (!wait1(&bar_ifull[slot], use & 1)) break;
-      if (s_meta[slot][5]) break;
-      const uint32_t b0 = s_meta[slot][0], nb = s_meta[slot][1], cl = s_meta[slot][2], ng = s_meta[slot][3];
-      const uint32_t ntiles = (nb + 7) >> 3;
-      bool ok = true;
-      if (warp < kTProducers) {
-        // B: the code bits of blocks 8t + 2w and 8t + 2w + 1 as u8 0/1, slot = 32 i + lane
-        for (uint32_t t = 0; t < ntiles && ok; t++) {
-          const uint32_t ds = ts + t, st = ds % kTStages, su = ds / kTStages;
-          if (!wait1(&bar_bempty[st], (su & 1) ^ 1)) {
-            ok = false;
-            break;
-          }
-          uint8_t* B = smem + 2 * kTABytes + st * kTBBytes;
-#pragma unroll
-          for (uint32_t i = 0; i < 2; i++) {
-            const uint32_t bl = 8 * t + 2 * warp + i;
-            if (bl >= nb) continue;  // columns past the cluster are never read back
-            const uint64_t gs = (uint64_t)(b0 + bl) * SG_BLOCK + lane;
-            const uint4 lo = a.codes[2 * gs], hi = a.codes[2 * gs + 1];
-            const uint32_t wd[8] = {lo.x, lo.y, lo.z, lo.w, hi.x, hi.y, hi.z, hi.w};
-            const uint32_t sl = 32 * (2 * warp + i) + lane;  // the slot's row of the tile
-            uint8_t* row = B + (sl >> 3) * 2048 + (sl & 7) * 16;
-            // K chunk g = prefix dimensions 16g..16g+15 = nibbles 4g..4g+3 (word g/2)
-#pragma unroll
-            for (uint32_t g = 0; g < 16; g++) {
-              const uint32_t w = wd[g >> 1] >> (16 * (g & 1));
-              *reinterpret_cast<uint4*>(row + g * 128) =
-                  make_uint4(bits_to_bytes(w & 15u), bits_to_bytes((w >> 4) & 15u), bits_to_bytes((w >> 8) & 15u),
-                             bits_to_bytes((w >> 12) & 15u));
-            }
-          }
-          fence_proxy_async_smem();
-          __syncwarp();
-          if (lane == 0) mbar_arrive(&bar_bfull[st]);
-        }
-        if (lane == 0) mbar_arrive(&bar_iempty[slot]);
-      } else if (warp == kTMma) {
-        const uint64_t adesc = smem_desc(a_base + slot * kTABytes, 128, 2048);
-        for (uint32_t t = 0; t < ntiles && ok; t++) {
-          const uint32_t ds = ts + t, dbuf = ds % kTDBufs, duse = ds / kTDBufs;
-          const uint32_t st = ds % kTStages, su = ds / kTStages;
-          if (!wait1(&bar_dempty[dbuf], (duse & 1) ^ 1)) break;
-          if (!wait1(&bar_bfull[st], su & 1)) break;
-          tc_fence_after();
-          const uint64_t bdesc = smem_desc(b_base + st * kTBBytes, 128, 2048);
-#pragma unroll
-          for (uint32_t kk = 0; kk < 8; kk++)  // K bytes 32kk.. = prefix dimensions 32kk..32kk+31
-            tc_mma_i8_ss_elect(tmem + dbuf * kTN, adesc + (uint64_t)(kk * 16), bdesc + (uint64_t)(kk * 16), kTIdesc,
-                               kk != 0);
-          tc_commit_elect(&bar_bempty[st]);
-          tc_commit_elect(&bar_dfull[dbuf]);
-          __syncwarp();
-        }
-        if (lane == 0) mbar_arrive(&bar_iempty[slot]);
-      } else {
-        // ---- epilogue: lane = query 32 qd + lane, columns 64 cq .. 64 cq + 63 of each tile ---
-        const uint32_t ew = warp - kTEpi, qd = ew & 3, cq = ew >> 2;
-        const uint32_t n = 32 * qd + lane;
-        const bool on = 32 * qd < ng;  // warp-uniform: this quarter holds queries
-        const bool lane_on = n < ng;
-        float4 qc = make_float4(0, 0, 0, 0), qf = qc;
-        uint2 qk = make_uint2(0, 0);
-        int dq = INT_MAX;  // a lane without a query passes nothing
-        if (lane_on) {
-          qc = s_qc[slot][n];
-          qf = s_qf[slot][n];
-          qk = s_qk[slot][n];
-          dq = s_qd[slot][n];
-        }
-        const uint32_t thr = __float_as_uint(qc.w);
-        for (uint32_t t = 0; t < ntiles; t++) {
-          const uint32_t ds = ts + t, dbuf = ds % kTDBufs, duse = ds / kTDBufs;
-          if (!wait1(&bar_dfull[dbuf], duse & 1)) {
-            ok = false;
-            break;
-          }
-          tc_fence_after();
-#pragma unroll 1
-          for (uint32_t cc = 0; cc < 2; cc++) {
-            const uint32_t col0 = 64 * cq + 32 * cc;
-            const uint32_t bl = 8 * t + (col0 >> 5);  // the chunk's 32 columns are one block
-            uint32_t v[32];
-            tc_ld32(tmem + ((32u * qd) << 16) + dbuf * kTN + col0, v);
-            tc_wait_ld();
-            if (!on || bl >= nb) continue;  // warp-uniform
-            // 1. the integer prefilter: columns whose product could reach the threshold
-            uint32_t cand = 0;
-#pragma unroll
-            for (int j = 0; j < 32; j++) cand |= ((int)v[j] > dq ? 1u : 0u) << j;
-            const uint32_t nvalid = min(32u, cl > bl * SG_BLOCK ? cl - bl * SG_BLOCK : 0u);
-            cand &= nvalid == 32 ? 0xFFFFFFFFu : (1u << nvalid) - 1u;
-            if (!cand) continue;
-            // 2. the float bound of those pairs (the exact estimate's operations at the bound of
-            //    the score) against the query's admission key
-            const uint32_t gbase = (b0 + bl) * SG_BLOCK;
-            uint32_t adm = 0;
-            for (uint32_t r = cand; r; r &= r - 1) {
-              const uint32_t j = __ffs(r) - 1;
-              const float mv = a.mul[gbase + j];
-              const bool neg = mv < 0.0f;
-              const bool always = !isfinite(mv);  // no monotone bound: recheck the pair
-              int dv = 0;
-#pragma unroll
-              for (int k = 0; k < 32; k++)
-                if (k == (int)j) dv = (int)v[k];
-              const float sb = __fadd_rn(__fmul_rn(qf.x, (float)dv), neg ? qf.z : qf.y);
-              const float est = __fadd_rn(qc.x, __fmul_rn(mv, __fadd_rn(__fmul_rn(qc.y, sb), qc.z)));
-              if (always || ord(est) >= thr) adm |= 1u << j;
-            }
-            if (adm && (a.allow || a.allow_q)) {  // allowlist filters (View::hidden)
-              const uint64_t* al = a.allow_q ? a.allow_q[qk.y] : a.allow;
-              const uint64_t aw = a.allow_q ? a.allow_wq[qk.y] : a.allow_words;
-              if (al)
-                for (uint32_t r = adm; r; r &= r - 1) {
-                  const uint32_t j = __ffs(r) - 1;
-                  if (!allowed(al, aw, a.ids[gbase + j])) adm &= ~(1u << j);
-                }
-            }
-            if (adm) {
-              const uint32_t base = atomicAdd(a.ccount + qk.y, (uint32_t)__popc(adm));
-              uint32_t k = 0;
-              for (uint32_t r = adm; r; r &= r - 1, k++) {
-                const uint32_t j = __ffs(r) - 1;
-                const uint32_t pos = base + k;
-                if (pos < a.cap) {
-                  // the probe's centroid score; k_tc_recheck turns it into the exact estimate
-                  a.cbuf_est[(size_t)qk.y * a.cap + pos] = __float_as_uint(qc.x);
-                  a.cbuf_info[(size_t)qk.y * a.cap + pos] =
-                      make_uint2(a.global ? a.ids[gbase + j] : qk.x + bl * SG_BLOCK + j, gbase + j);
-                } else {
-                  a.overflow[qk.y] = 1;
-                }
-              }
-            }
-          }
-          tc_fence_before();
-          __syncwarp();
-          if (lane == 0) mbar_arrive(&bar_dempty[dbuf]);
-        }
-        if (lane == 0) mbar_arrive(&bar_iempty[slot]);
-      }
-      ts += ntiles;
-      if (*abort_flag) break;
-    }
-  }
-  if (tid == 0 && *abort_flag) atomicOr(status, kStatusTimeout);
-  tc_fence_before();
-  __syncthreads();
-  if (warp == kTMma) {
-    tc_fence_after();
-    tc_dealloc(tmem, kTCols);
-  }
-}
-
 // The exact estimates of the entries the bound admitted: one CTA per query, its u8 tables in
 // shared memory, the 64 nibble lookups of each entry's slot (src/lut.rs:116-126) and the
 // estimate in the reference's operation order (src/rabitq.rs:127-130).
@@ -790,18 +460,15 @@ __global__ void __launch_bounds__(256) k_tc_recheck(const uint8_t* __restrict__ 
 }
 
 static int tcf_smem_bytes() { return 2 * kFBBytes; }
-static_assert(kTM == kScanTctGroup, "work items of the transposed pass hold kTM queries");
 
 // The tensor-core admission pass over the (cluster, query group) items launch_invert made:
 // weights and residual bounds per query, the bound pass, then the exact estimates of what it
 // admitted. Returns the kernels launched.
 int launch_scan_tcf(const DevIndex& ix, Workspace& w, uint32_t nq, uint32_t P, const uint64_t* allow,
-                    uint64_t allow_words, int sms, bool transposed, cudaStream_t st) {
+                    uint64_t allow_words, int sms, cudaStream_t st) {
   static PerDeviceOnce attr;
   attr([] {
-    cudaError_t e = cudaFuncSetAttribute(k_scan_tcf, cudaFuncAttributeMaxDynamicSharedMemorySize, tcf_smem_bytes());
-    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_scan_tct, cudaFuncAttributeMaxDynamicSharedMemorySize, kTSmem);
-    return e;
+    return cudaFuncSetAttribute(k_scan_tcf, cudaFuncAttributeMaxDynamicSharedMemorySize, tcf_smem_bytes());
   });
   TcfArgs a{};
   a.codes = reinterpret_cast<const uint4*>(ix.blocks_tc);
@@ -830,11 +497,9 @@ int launch_scan_tcf(const DevIndex& ix, Workspace& w, uint32_t nq, uint32_t P, c
   a.allow_q = w.per_query_allow ? w.allow_q : nullptr;
   a.allow_wq = w.allow_wq;
   a.global = ix.global;
-  a.mul_rng = ix.mul_rng;
   // entries from tc_start[q] on are the bound pass's (earlier ones are exact already)
   cudaMemcpyAsync(w.tc_start, w.ccount, (size_t)nq * 4, cudaMemcpyDeviceToDevice, st);
-  if (transposed) k_scan_tct<<<sms, kTThreads, kTSmem, st>>>(a);
-  else k_scan_tcf<<<sms, kFThreads, tcf_smem_bytes(), st>>>(a);
+  k_scan_tcf<<<sms, kFThreads, tcf_smem_bytes(), st>>>(a);
   k_tc_recheck<<<nq, 256, 0, st>>>(w.tables, w.qp, reinterpret_cast<const uint4*>(ix.blocks_tc), ix.mul,
                                    w.tc_start, w.ccount, w.cbuf_per_q, ix.nslots, w.cbuf_est, w.cbuf_info);
   return 2;

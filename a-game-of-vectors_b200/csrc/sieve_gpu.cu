@@ -77,7 +77,6 @@ void free_index(sg::DevIndex& x) {
   dfree(x.cent_bf16);
   dfree(x.block_off);
   dfree(x.clen);
-  dfree(x.mul_rng);
   dfree(x.blocks);
   dfree(x.blocks_tc);
   dfree(x.mul);
@@ -152,17 +151,6 @@ void free_ws(sg::Workspace& w) {
 namespace sg {
 // Per-cluster chunk and slot counts, largest first, as prefix sums over x.k clusters (from
 // x.h_block_off): the work-queue and candidate-buffer bounds of a call probing P clusters.
-float2 mul_range(const float* mul, uint64_t len) {
-  float lo = INFINITY, hi = -INFINITY;
-  for (uint64_t i = 0; i < len; i++) {
-    const float m = mul[i];
-    if (!(m >= 0.0f) || !std::isfinite(m)) return make_float2(NAN, NAN);
-    lo = std::min(lo, m);
-    hi = std::max(hi, m);
-  }
-  return len ? make_float2(lo, hi) : make_float2(NAN, NAN);
-}
-
 void set_cluster_bounds(DevIndex& x, uint32_t chunk) {
   const uint32_t K = x.k;
   std::vector<uint32_t> ch(K);
@@ -256,9 +244,6 @@ int build_index(const sg_ivf_arrays* a, int device, sg_index** out) {
     mul[s] = global ? 1.0f : a->factors[2 * s];
     err[s] = global ? INFINITY : a->factors[2 * s + 1];
   }
-  x.h_mul_rng.resize(K);
-  for (uint32_t c = 0; c < K; c++)
-    x.h_mul_rng[c] = sg::mul_range(mul.data() + a->block_off[c] * SG_BLOCK, x.h_clen[c]);
   x.rot_norm = powf(256.0f, -1.5f);
   int rc;
   if ((rc = upload(&x.cent, a->centroids, (size_t)K * SG_PDIM)) ||
@@ -266,7 +251,6 @@ int build_index(const sg_ivf_arrays* a, int device, sg_index** out) {
       (rc = upload(&x.cent_bf16, cb.data(), cb.size())) ||
       (rc = upload(&x.block_off, boff32.data(), boff32.size())) ||
       (rc = upload(&x.clen, x.h_clen.data(), x.h_clen.size())) ||
-      (rc = upload(&x.mul_rng, x.h_mul_rng.data(), x.h_mul_rng.size())) ||
       (rc = upload(&x.blocks, a->blocks, (size_t)nblocks * SG_BLOCK_BYTES)) ||
       (rc = upload(&x.mul, mul.data(), mul.size())) || (rc = upload(&x.err, err.data(), err.size())) ||
       (rc = upload(&x.ids, a->ids, x.nslots)) ||
@@ -281,7 +265,7 @@ int build_index(const sg_ivf_arrays* a, int device, sg_index** out) {
     return fail(SG_ERR_DEVICE, "cuTensorMapEncodeTiled (the routing GEMM's TMA maps) is unavailable");
   }
   // the batched tensor-core scan reads its own copy of the codes, slot-major
-  if (const char* tc = getenv("SIEVE_GPU_TC")) h->cfg.tc = atoi(tc) == 2 ? 2 : atoi(tc) == 3 ? 3 : 1;
+  if (const char* tc = getenv("SIEVE_GPU_TC")) h->cfg.tc = atoi(tc) == 2 ? 2 : 1;
   if (const char* sp = getenv("SIEVE_GPU_TC_SPLIT")) h->cfg.tc_split = (uint32_t)strtoul(sp, nullptr, 10);
   if (const char* tm = getenv("SIEVE_GPU_TC_MIN")) h->cfg.tc_min_queries = (uint32_t)strtoul(tm, nullptr, 10);
   if ((rc = dalloc(&x.blocks_tc, (size_t)nblocks * 256))) {
@@ -976,15 +960,12 @@ int index_make_live(sg_index* h, uint64_t max_rows, uint64_t block_cap) {
   const uint32_t kc = x.kc;
   x.h_block_off.resize(2 * (size_t)kc + 1, x.h_block_off[kc]);
   x.h_clen.resize(2 * (size_t)kc, 0);
-  x.h_mul_rng.resize(2 * (size_t)kc, make_float2(NAN, NAN));
   std::vector<uint32_t> boff32(2 * (size_t)kc + 1);
   for (size_t c = 0; c < boff32.size(); c++) boff32[c] = (uint32_t)x.h_block_off[c];
   dfree(x.block_off);
   dfree(x.clen);
-  dfree(x.mul_rng);
   if ((rc = upload(&x.block_off, boff32.data(), boff32.size())) ||
-      (rc = upload(&x.clen, x.h_clen.data(), x.h_clen.size())) ||
-      (rc = upload(&x.mul_rng, x.h_mul_rng.data(), x.h_mul_rng.size())))
+      (rc = upload(&x.clen, x.h_clen.data(), x.h_clen.size())))
     return rc;
   x.k = 2 * kc;
   x.live = true;
@@ -1022,7 +1003,6 @@ int index_set_delta(sg_index* h, const uint32_t* nb_of, const uint32_t* clen_of,
   for (uint32_t c = 0; c < kc; c++) {
     x.h_block_off[kc + c] = off;
     x.h_clen[kc + c] = clen_of[c];
-    x.h_mul_rng[kc + c] = sg::mul_range(mul + (off - b0) * SG_BLOCK, clen_of[c]);
     off += nb_of[c];
   }
   x.h_block_off[2 * (size_t)kc] = off;
@@ -1030,8 +1010,6 @@ int index_set_delta(sg_index* h, const uint32_t* nb_of, const uint32_t* clen_of,
   for (uint32_t c = 0; c <= kc; c++) boff32[c] = (uint32_t)x.h_block_off[kc + c];
   CK(cudaMemcpyAsync(x.block_off + kc, boff32.data(), (kc + 1) * 4, cudaMemcpyHostToDevice, st));
   CK(cudaMemcpyAsync(x.clen + kc, x.h_clen.data() + kc, (size_t)kc * 4, cudaMemcpyHostToDevice, st));
-  CK(cudaMemcpyAsync(x.mul_rng + kc, x.h_mul_rng.data() + kc, (size_t)kc * sizeof(float2), cudaMemcpyHostToDevice,
-                     st));
   CK(cudaStreamSynchronize(st));
   std::lock_guard<std::mutex> g(h->cfg_mu);
   set_cluster_bounds(x, h->cfg.small_chunk_blocks);
