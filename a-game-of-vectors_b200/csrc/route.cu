@@ -209,9 +209,6 @@ SG_DEV float exact_dot(const float* __restrict__ q, const float* __restrict__ c)
 }
 
 constexpr uint32_t kWinCap = 4096;
-// Up to this many centroids, k_route_select copies a query's scores into shared memory once (as
-// ordered keys) and runs the select's passes there instead of re-reading global memory.
-constexpr uint32_t kRouteStageK = 16384;
 
 struct SelectArgs {
   const float* q256;
@@ -353,23 +350,16 @@ SG_DEV uint32_t expand_delta(const SelectArgs& a, uint64_t* keys, uint32_t m) {
 __global__ void __launch_bounds__(256) k_route_select(SelectArgs a) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   uint64_t* keys = reinterpret_cast<uint64_t*>(smem_raw);  // [kWinCap]
-  uint32_t* nbs = reinterpret_cast<uint32_t*>(smem_raw + kWinCap * sizeof(uint64_t));     // [kWinCap]
-  uint32_t* okeys = nbs + kWinCap;  // [K] if staged
+  uint32_t* nbs = reinterpret_cast<uint32_t*>(smem_raw + kWinCap * sizeof(uint64_t));  // [kWinCap]
   __shared__ float qv[SG_PDIM];
   __shared__ uint32_t hist[2048], tmp[32];
   __shared__ uint32_t s_nw, s_m, s_keep;
   const uint32_t q = blockIdx.x, P = a.Pb, K = a.K;
   float* row = a.scores + (size_t)q * K;
-  const bool staged = K <= kRouteStageK;
   for (int i = threadIdx.x; i < SG_PDIM; i += blockDim.x) qv[i] = a.q256[(size_t)q * SG_PDIM + i];
-  if (staged) {
-#pragma unroll 8
-    for (uint32_t i = threadIdx.x; i < K; i += blockDim.x) okeys[i] = ord(row[i]);
-  }
   if (threadIdx.x == 0) s_nw = 0;
   __syncthreads();
-  // the ordered key of centroid i's score (ord maps -0.0 to +0.0, as every rank key does)
-  auto okey = [&](uint32_t i) { return staged ? okeys[i] : ord(row[i]); };
+  auto okey = [&](uint32_t i) { return ord(row[i]); };
   if (P == 0) {
     if (threadIdx.x == 0) {
       a.probe_n[q] = 0;
@@ -386,7 +376,7 @@ __global__ void __launch_bounds__(256) k_route_select(SelectArgs a) {
     float delta = 0.0085f * a.qnorm[q] * a.cent_norm_max;
     float lim = sP - 2.0f * delta;
     for (uint32_t c = threadIdx.x; c < K; c += blockDim.x)
-      if (unord(okey(c)) >= lim) {
+      if (row[c] >= lim) {
         uint32_t slot = atomicAdd(&s_nw, 1u);
         if (slot < kWinCap) keys[slot] = c;
       }
@@ -414,16 +404,12 @@ __global__ void __launch_bounds__(256) k_route_select(SelectArgs a) {
     } else {
       // window too wide for the buffer (or degenerate): score every centroid exactly
       if (threadIdx.x == 0) atomicOr(&a.counters[2], kStatusWindow);
-      for (uint32_t c = threadIdx.x; c < K; c += blockDim.x) {
-        const float v = exact_dot(qv, a.cent + (size_t)c * SG_PDIM);
-        if (staged) okeys[c] = ord(v);
-        else row[c] = v;
-      }
+      for (uint32_t c = threadIdx.x; c < K; c += blockDim.x) row[c] = exact_dot(qv, a.cent + (size_t)c * SG_PDIM);
       __syncthreads();
       exact = true;
     }
   }
-  if (exact) block_top_keys([&](uint32_t i) { return unord(okey(i)); }, K, P, keys, hist, tmp);
+  if (exact) block_top_keys([&](uint32_t i) { return row[i]; }, K, P, keys, hist, tmp);
   // keys[0..P) hold the winners: sort best first
   uint32_t n2 = next_pow2(P);
   for (uint32_t i = P + threadIdx.x; i < n2; i += blockDim.x) keys[i] = 0;
@@ -573,10 +559,9 @@ void launch_route_select(const DevIndex& ix, Workspace& w, uint32_t nq, const sg
   static PerDeviceOnce attr;
   attr([&] {
     return cudaFuncSetAttribute(k_route_select, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                (int)(kWinCap * (sizeof(uint64_t) + sizeof(uint32_t)) + kRouteStageK * sizeof(uint32_t)));
+                                (int)(kWinCap * (sizeof(uint64_t) + sizeof(uint32_t))));
   });
-  const size_t smem = kWinCap * (sizeof(uint64_t) + sizeof(uint32_t)) +
-                      (ix.kc <= kRouteStageK ? ix.kc * sizeof(uint32_t) : 0);
+  const size_t smem = kWinCap * (sizeof(uint64_t) + sizeof(uint32_t));
   k_route_select<<<nq, 256, smem, st>>>(a);
 }
 
