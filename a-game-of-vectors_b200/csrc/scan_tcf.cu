@@ -42,18 +42,22 @@
 
 namespace sg {
 
-constexpr int kFQG = 64;            // queries per work item (MMA N, padded to a multiple of 16)
+// Queries per work item (MMA N, padded to a multiple of 16): QG = 64 with four accumulators, or
+// QG = 128 with two (an MMA costs the same for any N up to 256, so a cluster probed by up to 128
+// queries of the batch is read once instead of twice).
 constexpr int kFStages = 4;         // A stages: one tile (128 slots x 256 K bytes = 64 columns) each
-constexpr uint32_t kFCols = 512;    // TMEM columns: 4 x 64 (A) + 4 x 64 (D)
+constexpr uint32_t kFCols = 512;    // TMEM columns: 4 x 64 (A) + 256 (D)
 constexpr uint32_t kFDCol = 256;    // first D column
-constexpr int kFDBufs = 4;          // accumulators
+template <int QG>
+__host__ __device__ constexpr int fdbufs() { return QG == 64 ? 4 : 2; }  // accumulators: 256 TMEM columns in all
 constexpr int kFProducers = 4;      // warps 0-3 build A
 constexpr int kFEpi = 4;            // warps 4-11 bound the pairs
 constexpr int kFEpiWarps = 8;
 constexpr int kFMma = 12;           // warp 12 issues the MMAs
 constexpr int kFLoader = 13;        // warp 13 loads work items
 constexpr int kFThreads = 14 * 32;
-constexpr int kFBBytes = kFQG * SG_PDIM;  // B of one item slot: 64 queries x 256 s8 weights
+template <int QG>
+__host__ __device__ constexpr int fbbytes() { return QG * SG_PDIM; }  // B of one item slot: QG queries x 256 s8 weights
 
 // ---- per-query weights and residual bounds --------------------------------------------------
 // One CTA of 64 threads per query; thread g owns group g (prefix dimensions 4g..4g+3).
@@ -133,7 +137,9 @@ struct TcfArgs {
 };
 
 
+template <int QG>
 __global__ void __launch_bounds__(kFThreads, 1) k_scan_tcf(TcfArgs a) {
+  constexpr int kFQG = QG, kFDBufs = fdbufs<QG>(), kFBBytes = fbbytes<QG>();
   extern __shared__ __align__(1024) uint8_t smem[];  // B of the two item slots
   __shared__ __align__(8) uint64_t bar_afull[kFStages], bar_aempty[kFStages], bar_dfull[kFDBufs],
       bar_dempty[kFDBufs], bar_ifull[2], bar_iempty[2];
@@ -425,9 +431,12 @@ __global__ void __launch_bounds__(kFThreads, 1) k_scan_tcf(TcfArgs a) {
   }
 }
 
-// The exact estimates of the entries the bound admitted: one CTA per query, its u8 tables in
-// shared memory, the 64 nibble lookups of each entry's slot (src/lut.rs:116-126) and the
-// estimate in the reference's operation order (src/rabitq.rs:127-130).
+// The exact estimates of the entries the bound admitted: kRecheckSplit CTAs per query (the
+// entries of one query can number hundreds of thousands, so one CTA per query left a long tail),
+// each with the query's u8 tables in shared memory; per entry the 64 nibble lookups of its slot
+// (src/lut.rs:116-126) and the estimate in the reference's operation order (src/rabitq.rs:127-130).
+// A thread takes two entries at a time so their loads are in flight together.
+constexpr uint32_t kRecheckSplit = 8;
 __global__ void __launch_bounds__(256) k_tc_recheck(const uint8_t* __restrict__ tables, const float4* __restrict__ qp,
                                                     const uint4* __restrict__ codes, const float* __restrict__ mul,
                                                     const uint32_t* __restrict__ tc_start,
@@ -437,38 +446,66 @@ __global__ void __launch_bounds__(256) k_tc_recheck(const uint8_t* __restrict__ 
   __shared__ __align__(16) uint8_t T[SG_GROUPS * 16];
   const uint32_t q = blockIdx.x;
   const uint32_t lo = tc_start[q], hi = min(ccount[q], cap);
-  if (lo >= hi) return;  // uniform over the CTA
+  const uint32_t first = lo + blockIdx.y * blockDim.x + threadIdx.x, stride = gridDim.y * blockDim.x;
+  if (lo + blockIdx.y * blockDim.x >= hi) return;  // uniform over the CTA
   reinterpret_cast<uint32_t*>(T)[threadIdx.x] =
       reinterpret_cast<const uint32_t*>(tables + (size_t)q * SG_GROUPS * 16)[threadIdx.x];
   __syncthreads();
   const float4 p = qp[q];
   uint32_t* E = cbuf_est + (size_t)q * cap;
   const uint2* I = cbuf_info + (size_t)q * cap;
-  for (uint32_t i = lo + threadIdx.x; i < hi; i += blockDim.x) {
-    const uint32_t gs = I[i].y;
-    if (gs >= nslots) continue;  // only an aborted bound pass leaves an entry unwritten
-    const uint4 c0 = codes[2 * (size_t)gs], c1 = codes[2 * (size_t)gs + 1];
+  auto score = [&](const uint4& c0, const uint4& c1) {
     const uint32_t wd[8] = {c0.x, c0.y, c0.z, c0.w, c1.x, c1.y, c1.z, c1.w};
     uint32_t s = 0;
 #pragma unroll
     for (int k = 0; k < 8; k++)
 #pragma unroll
       for (int j = 0; j < 8; j++) s += T[(8 * k + j) * 16 + ((wd[k] >> (4 * j)) & 15u)];
-    const float cent = __uint_as_float(E[i]);
-    E[i] = __float_as_uint(__fadd_rn(cent, __fmul_rn(mul[gs], __fadd_rn(__fmul_rn(p.z, (float)s), p.w))));
+    return s;
+  };
+  auto estimate = [&](float cent, float m, uint32_t s) {
+    return __fadd_rn(cent, __fmul_rn(m, __fadd_rn(__fmul_rn(p.z, (float)s), p.w)));
+  };
+  for (uint32_t i = first; i < hi; i += 2 * stride) {
+    const uint32_t i2 = i + stride;
+    const bool two = i2 < hi;
+    // only an aborted bound pass leaves an entry unwritten (slot >= nslots)
+    const uint32_t gs = I[i].y, gs2 = two ? I[i2].y : 0xFFFFFFFFu;
+    const bool ok = gs < nslots, ok2 = gs2 < nslots;
+    uint4 a0 = make_uint4(0, 0, 0, 0), a1 = a0, b0 = a0, b1 = a0;
+    float m = 0.0f, m2 = 0.0f, ce = 0.0f, ce2 = 0.0f;
+    if (ok) {
+      a0 = codes[2 * (size_t)gs];
+      a1 = codes[2 * (size_t)gs + 1];
+      m = mul[gs];
+      ce = __uint_as_float(E[i]);
+    }
+    if (ok2) {
+      b0 = codes[2 * (size_t)gs2];
+      b1 = codes[2 * (size_t)gs2 + 1];
+      m2 = mul[gs2];
+      ce2 = __uint_as_float(E[i2]);
+    }
+    if (ok) E[i] = __float_as_uint(estimate(ce, m, score(a0, a1)));
+    if (ok2) E[i2] = __float_as_uint(estimate(ce2, m2, score(b0, b1)));
   }
 }
 
-static int tcf_smem_bytes() { return 2 * kFBBytes; }
+template <int QG>
+static int tcf_smem_bytes() { return 2 * fbbytes<QG>(); }
 
 // The tensor-core admission pass over the (cluster, query group) items launch_invert made:
 // weights and residual bounds per query, the bound pass, then the exact estimates of what it
 // admitted. Returns the kernels launched.
 int launch_scan_tcf(const DevIndex& ix, Workspace& w, uint32_t nq, uint32_t P, const uint64_t* allow,
-                    uint64_t allow_words, int sms, cudaStream_t st) {
+                    uint64_t allow_words, int sms, uint32_t qg, cudaStream_t st) {
   static PerDeviceOnce attr;
   attr([] {
-    return cudaFuncSetAttribute(k_scan_tcf, cudaFuncAttributeMaxDynamicSharedMemorySize, tcf_smem_bytes());
+    cudaError_t e = cudaFuncSetAttribute(k_scan_tcf<64>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         tcf_smem_bytes<64>());
+    if (e == cudaSuccess)
+      e = cudaFuncSetAttribute(k_scan_tcf<128>, cudaFuncAttributeMaxDynamicSharedMemorySize, tcf_smem_bytes<128>());
+    return e;
   });
   TcfArgs a{};
   a.codes = reinterpret_cast<const uint4*>(ix.blocks_tc);
@@ -499,8 +536,9 @@ int launch_scan_tcf(const DevIndex& ix, Workspace& w, uint32_t nq, uint32_t P, c
   a.global = ix.global;
   // entries from tc_start[q] on are the bound pass's (earlier ones are exact already)
   cudaMemcpyAsync(w.tc_start, w.ccount, (size_t)nq * 4, cudaMemcpyDeviceToDevice, st);
-  k_scan_tcf<<<sms, kFThreads, tcf_smem_bytes(), st>>>(a);
-  k_tc_recheck<<<nq, 256, 0, st>>>(w.tables, w.qp, reinterpret_cast<const uint4*>(ix.blocks_tc), ix.mul,
+  if (qg == 128) k_scan_tcf<128><<<sms, kFThreads, tcf_smem_bytes<128>(), st>>>(a);
+  else k_scan_tcf<64><<<sms, kFThreads, tcf_smem_bytes<64>(), st>>>(a);
+  k_tc_recheck<<<dim3(nq, kRecheckSplit), 256, 0, st>>>(w.tables, w.qp, reinterpret_cast<const uint4*>(ix.blocks_tc), ix.mul,
                                    w.tc_start, w.ccount, w.cbuf_per_q, ix.nslots, w.cbuf_est, w.cbuf_info);
   return 2;
 }
