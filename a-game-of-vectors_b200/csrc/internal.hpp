@@ -214,7 +214,6 @@ struct Config {
   int mma = 1;            // SIEVE_GPU_MMA: 0 ALU scan only, 1 automatic, 2 tensor cores whenever nprobe > 1
   int tc = 1;             // SIEVE_GPU_TC: 1 the tcgen05 bound scan, 2 the tcgen05 one-hot scan (kept
                           // for comparison)
-  uint32_t tc_group = 64;  // queries per work item of the bound scan: 64 or 128 (SIEVE_GPU_TC_QG)
   uint32_t tc_split = 0;  // SIEVE_GPU_TC_SPLIT (> 1): a first tcgen05 round over the ranks below it
   // Clusters probed by fewer queries than this in a batch are scanned by the ALU kernel: a
   // tcgen05 tile costs the same ~32 x 101 cycles per 128 slots for any query count up to 128,
@@ -328,7 +327,7 @@ int launch_scan_tc(const DevIndex& ix, Workspace& w, uint32_t nq, const sg_param
 // admitted (returns the kernels launched).
 void launch_filter_prep(Workspace& w, uint32_t nq, cudaStream_t st);
 int launch_scan_tcf(const DevIndex& ix, Workspace& w, uint32_t nq, uint32_t P, const uint64_t* allow,
-                    uint64_t allow_words, int sms, uint32_t qg, cudaStream_t st);
+                    uint64_t allow_words, int sms, cudaStream_t st);
 // Launch errors of these two are left for the caller's cudaGetLastError.
 void transcode_tc(const uint8_t* blocks, uint64_t nblocks, uint32_t* out, cudaStream_t st);
 void launch_lut_scan_tc(uint32_t nq, const uint8_t* tables, const uint32_t* codes, uint64_t nblocks,

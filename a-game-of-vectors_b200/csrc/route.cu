@@ -237,20 +237,10 @@ struct SelectArgs {
   uint32_t* counters;
 };
 
-// Blocks of each probe, nbs[r] for keys[0..m), read in parallel (the seed and the budget then walk
-// them in shared memory). All threads of the block call it.
-SG_DEV void probe_blocks(const SelectArgs& a, const uint64_t* keys, uint32_t m, uint32_t* nbs) {
-  for (uint32_t r = threadIdx.x; r < m; r += blockDim.x) {
-    const uint32_t c = key_id(keys[r]);
-    nbs[r] = a.block_off[c + 1] - a.block_off[c];
-  }
-  __syncthreads();
-}
-
-// Writes query q's probe list (keys[0..m) sorted best first: probe ranks 0..m-1, nbs[r] their
-// blocks), the admission offset of each probe's first slot, its seed descriptor and its ALU scan
-// items. All threads of the block call it.
-SG_DEV void emit_probes(const SelectArgs& a, const uint64_t* keys, const uint32_t* nbs, uint32_t m, uint32_t q,
+// Writes query q's probe list (keys[0..m) sorted best first: probe ranks 0..m-1), the admission
+// offset of each probe's first slot, its seed descriptor and its ALU scan items. All threads of
+// the block call it.
+SG_DEV void emit_probes(const SelectArgs& a, const uint64_t* keys, uint32_t m, uint32_t q,
                         uint32_t* tmp) {
   const uint32_t P = a.P;
   // probe list, admission offsets and chunk counts (block scans over probe ranks)
@@ -260,11 +250,17 @@ SG_DEV void emit_probes(const SelectArgs& a, const uint64_t* keys, const uint32_
   // or the first seed_blocks blocks of probe 0 when that cluster alone is larger. It is scanned
   // first, one CTA per query, to set a tight admission threshold; everything else is cut into
   // chunks (or, with alu_ranks off, left to the tensor-core scan).
-  __shared__ uint32_t s_rs, s_partial;
+  __shared__ uint32_t s_rs, s_partial, s_nb[kMaxSegs];
+  // the first probes' block counts, read in parallel (thread 0 then walks them)
+  for (uint32_t r = threadIdx.x; r < m && r < kMaxSegs; r += blockDim.x) {
+    const uint32_t c = key_id(keys[r]);
+    s_nb[r] = a.block_off[c + 1] - a.block_off[c];
+  }
+  __syncthreads();
   if (threadIdx.x == 0) {
     uint32_t used = 0, rs = 0, partial = 0;
     for (uint32_t r = 0; r < m && r < kMaxSegs; r++) {
-      const uint32_t nb = nbs[r];
+      const uint32_t nb = s_nb[r];
       if (r == 0 && nb > a.seed_blocks) {
         rs = 1;
         partial = a.seed_blocks;
@@ -286,7 +282,8 @@ SG_DEV void emit_probes(const SelectArgs& a, const uint64_t* keys, const uint32_
   };
   uint32_t slots = 0, chunks = 0;
   for (uint32_t r = r0; r < r1; r++) {
-    const uint32_t nb = nbs[r];
+    uint32_t c = key_id(keys[r]);
+    uint32_t nb = a.block_off[c + 1] - a.block_off[c];
     slots += nb * SG_BLOCK;
     chunks += nchunks(r, nb);
   }
@@ -350,16 +347,14 @@ SG_DEV uint32_t expand_delta(const SelectArgs& a, uint64_t* keys, uint32_t m) {
 __global__ void __launch_bounds__(256) k_route_select(SelectArgs a) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   uint64_t* keys = reinterpret_cast<uint64_t*>(smem_raw);  // [kWinCap]
-  uint32_t* nbs = reinterpret_cast<uint32_t*>(smem_raw + kWinCap * sizeof(uint64_t));  // [kWinCap]
   __shared__ float qv[SG_PDIM];
-  __shared__ uint32_t hist[2048], tmp[32];
+  __shared__ uint32_t hist[256], tmp[32];
   __shared__ uint32_t s_nw, s_m, s_keep;
   const uint32_t q = blockIdx.x, P = a.Pb, K = a.K;
   float* row = a.scores + (size_t)q * K;
   for (int i = threadIdx.x; i < SG_PDIM; i += blockDim.x) qv[i] = a.q256[(size_t)q * SG_PDIM + i];
   if (threadIdx.x == 0) s_nw = 0;
   __syncthreads();
-  auto okey = [&](uint32_t i) { return ord(row[i]); };
   if (P == 0) {
     if (threadIdx.x == 0) {
       a.probe_n[q] = 0;
@@ -371,7 +366,7 @@ __global__ void __launch_bounds__(256) k_route_select(SelectArgs a) {
   bool exact = !a.bf16;
   if (a.bf16) {
     // the P-th largest BF16 score and the window below it
-    const uint32_t kth = block_select_nth_u32r(okey, K, P, hist, tmp);
+    const uint32_t kth = block_select_nth_u32([&](uint32_t i) { return ord(row[i]); }, K, P, hist);
     const float sP = unord(kth);
     float delta = 0.0085f * a.qnorm[q] * a.cent_norm_max;
     float lim = sP - 2.0f * delta;
@@ -404,18 +399,28 @@ __global__ void __launch_bounds__(256) k_route_select(SelectArgs a) {
     } else {
       // window too wide for the buffer (or degenerate): score every centroid exactly
       if (threadIdx.x == 0) atomicOr(&a.counters[2], kStatusWindow);
-      for (uint32_t c = threadIdx.x; c < K; c += blockDim.x) row[c] = exact_dot(qv, a.cent + (size_t)c * SG_PDIM);
+      for (uint32_t c = threadIdx.x; c < K; c += blockDim.x)
+        row[c] = exact_dot(qv, a.cent + (size_t)c * SG_PDIM);
       __syncthreads();
       exact = true;
     }
   }
-  if (exact) block_top_keys([&](uint32_t i) { return row[i]; }, K, P, keys, hist, tmp);
+  if (exact) {
+    uint64_t T = block_select_nth_u64([&](uint32_t i) { return rank_key(row[i], i); }, K, P, hist,
+                                      tmp);
+    if (threadIdx.x == 0) s_m = 0;
+    __syncthreads();
+    for (uint32_t c = threadIdx.x; c < K; c += blockDim.x) {
+      uint64_t k = rank_key(row[c], c);
+      if (k >= T) keys[atomicAdd(&s_m, 1u)] = k;
+    }
+    __syncthreads();
+  }
   // keys[0..P) hold the winners: sort best first
   uint32_t n2 = next_pow2(P);
   for (uint32_t i = P + threadIdx.x; i < n2; i += blockDim.x) keys[i] = 0;
   __syncthreads();
   block_bitonic_sort_desc(keys, n2);
-  if (a.p.has_budget) probe_blocks(a, keys, P, nbs);
   // margin (prefix of the sorted list) and budget
   if (threadIdx.x == 0) {
     uint32_t m = P;
@@ -429,7 +434,8 @@ __global__ void __launch_bounds__(256) k_route_select(SelectArgs a) {
       uint64_t used = 0;
       uint32_t keep = 0;
       for (uint32_t i = 0; i < m; i++) {
-        used += (uint64_t)nbs[i] * SG_BLOCK;
+        uint32_t c = key_id(keys[i]);
+        used += (uint64_t)(a.block_off[c + 1] - a.block_off[c]) * SG_BLOCK;
         if (used <= a.p.budget) keep++;
         else break;
       }
@@ -440,8 +446,7 @@ __global__ void __launch_bounds__(256) k_route_select(SelectArgs a) {
   }
   __syncthreads();
   const uint32_t m = a.live_kc ? expand_delta(a, keys, s_keep) : s_keep;
-  probe_blocks(a, keys, m, nbs);
-  emit_probes(a, keys, nbs, m, q, tmp);
+  emit_probes(a, keys, m, q, tmp);
 }
 
 // filter::search with Plan::Expand (src/filter.rs:79-93): every cluster in route order (exact f32
@@ -481,9 +486,7 @@ __global__ void __launch_bounds__(1024) k_route_expand(SelectArgs a,
     before += per_cluster[key_id(keys[i])];
   }
   const uint32_t m = block_sum(take, tmp);
-  uint32_t* nbs = reinterpret_cast<uint32_t*>(keys + next_pow2(K));  // [next_pow2(K)]
-  probe_blocks(a, keys, m, nbs);
-  emit_probes(a, keys, nbs, m, q, tmp);
+  emit_probes(a, keys, m, q, tmp);
 }
 
 // Index::candidates over a caller's probe list (src/ivf.rs:647-681): query q's probes
@@ -494,7 +497,6 @@ __global__ void __launch_bounds__(256) k_route_given(SelectArgs a, const float* 
                                                      const uint32_t* __restrict__ given_n) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   uint64_t* keys = reinterpret_cast<uint64_t*>(smem_raw);  // [P]
-  uint32_t* nbs = reinterpret_cast<uint32_t*>(keys + (a.P > 0 ? a.P : 1));  // [P]
   __shared__ uint32_t tmp[32];
   const uint32_t q = blockIdx.x;
   const uint32_t m = min(given_n[q], a.P);
@@ -503,8 +505,7 @@ __global__ void __launch_bounds__(256) k_route_given(SelectArgs a, const float* 
     keys[r] = rank_key(given_sc[(size_t)q * a.P + r], c < a.K ? c : 0u);
   }
   __syncthreads();
-  probe_blocks(a, keys, m, nbs);
-  emit_probes(a, keys, nbs, m, q, tmp);
+  emit_probes(a, keys, m, q, tmp);
 }
 
 cudaError_t launch_route_scores(const DevIndex& ix, Workspace& w, uint32_t nq, int precision,
@@ -557,11 +558,10 @@ void launch_route_select(const DevIndex& ix, Workspace& w, uint32_t nq, const sg
   a.item_cap = w.item_cap;
   a.counters = w.counters;
   static PerDeviceOnce attr;
+  const size_t smem = kWinCap * sizeof(uint64_t);
   attr([&] {
-    return cudaFuncSetAttribute(k_route_select, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                (int)(kWinCap * (sizeof(uint64_t) + sizeof(uint32_t))));
+    return cudaFuncSetAttribute(k_route_select, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   });
-  const size_t smem = kWinCap * (sizeof(uint64_t) + sizeof(uint32_t));
   k_route_select<<<nq, 256, smem, st>>>(a);
 }
 
@@ -591,10 +591,10 @@ void launch_route_given(const DevIndex& ix, Workspace& w, uint32_t nq, const sg_
   static PerDeviceOnce attr;
   attr([] {
     return cudaFuncSetAttribute(k_route_given, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                (int)(2 * 4096 * (sizeof(uint64_t) + sizeof(uint32_t))));
+                                (int)(4096 * sizeof(uint64_t)));
   });
-  k_route_given<<<nq, 256, (size_t)std::max<uint32_t>(a.P, 1) * (sizeof(uint64_t) + sizeof(uint32_t)), st>>>(
-      a, given_sc, given_cl, given_n);
+  k_route_given<<<nq, 256, (size_t)std::max<uint32_t>(a.P, 1) * sizeof(uint64_t), st>>>(a, given_sc, given_cl,
+                                                                                      given_n);
 }
 
 void launch_route_expand(const DevIndex& ix, Workspace& w, uint32_t nq, const sg_params& p,
@@ -625,11 +625,11 @@ void launch_route_expand(const DevIndex& ix, Workspace& w, uint32_t nq, const sg
   a.items = w.items;
   a.item_cap = w.item_cap;
   a.counters = w.counters;
-  const size_t smem = (size_t)next_pow2_host(ix.kc) * (sizeof(uint64_t) + sizeof(uint32_t));
+  const size_t smem = (size_t)next_pow2_host(ix.kc) * sizeof(uint64_t);
   static PerDeviceOnce attr;
   attr([] {
     return cudaFuncSetAttribute(k_route_expand, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                (int)(kExpandMaxK * (sizeof(uint64_t) + sizeof(uint32_t))));
+                                (int)(kExpandMaxK * sizeof(uint64_t)));
   });
   k_route_expand<<<nq, 1024, smem, st>>>(a, per_cluster, target);
 }

@@ -531,9 +531,9 @@ int launch_scan_tc(const DevIndex& ix, Workspace& w, uint32_t nq, const sg_param
   // one tensor-core round: the bound pass with its exact recheck (default), or the exact one-hot
   // contraction (SIEVE_GPU_TC=2, kept for comparison)
   const bool bound = cfg.tc != 2;
-  const uint32_t qg = bound && cfg.tc_group == 128 ? 128u : (uint32_t)kTcQG;
+  const uint32_t qg = kTcQG;
   auto tc_round = [&]() {
-    if (bound) return launch_scan_tcf(ix, w, nq, P, allow, allow_words, sms, qg, st);
+    if (bound) return launch_scan_tcf(ix, w, nq, P, allow, allow_words, sms, st);
     k_scan_tc<false><<<sms, kTcThreads, tc_smem_bytes(), st>>>(a);
     return 1;
   };

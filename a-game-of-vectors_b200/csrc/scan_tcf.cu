@@ -42,22 +42,18 @@
 
 namespace sg {
 
-// Queries per work item (MMA N, padded to a multiple of 16): QG = 64 with four accumulators, or
-// QG = 128 with two (an MMA costs the same for any N up to 256, so a cluster probed by up to 128
-// queries of the batch is read once instead of twice).
+constexpr int kFQG = 64;            // queries per work item (MMA N, padded to a multiple of 16)
 constexpr int kFStages = 4;         // A stages: one tile (128 slots x 256 K bytes = 64 columns) each
-constexpr uint32_t kFCols = 512;    // TMEM columns: 4 x 64 (A) + 256 (D)
+constexpr uint32_t kFCols = 512;    // TMEM columns: 4 x 64 (A) + 4 x 64 (D)
 constexpr uint32_t kFDCol = 256;    // first D column
-template <int QG>
-__host__ __device__ constexpr int fdbufs() { return QG == 64 ? 4 : 2; }  // accumulators: 256 TMEM columns in all
+constexpr int kFDBufs = 4;          // accumulators
 constexpr int kFProducers = 4;      // warps 0-3 build A
 constexpr int kFEpi = 4;            // warps 4-11 bound the pairs
 constexpr int kFEpiWarps = 8;
 constexpr int kFMma = 12;           // warp 12 issues the MMAs
 constexpr int kFLoader = 13;        // warp 13 loads work items
 constexpr int kFThreads = 14 * 32;
-template <int QG>
-__host__ __device__ constexpr int fbbytes() { return QG * SG_PDIM; }  // B of one item slot: QG queries x 256 s8 weights
+constexpr int kFBBytes = kFQG * SG_PDIM;  // B of one item slot: 64 queries x 256 s8 weights
 
 // ---- per-query weights and residual bounds --------------------------------------------------
 // One CTA of 64 threads per query; thread g owns group g (prefix dimensions 4g..4g+3).
@@ -137,9 +133,7 @@ struct TcfArgs {
 };
 
 
-template <int QG>
 __global__ void __launch_bounds__(kFThreads, 1) k_scan_tcf(TcfArgs a) {
-  constexpr int kFQG = QG, kFDBufs = fdbufs<QG>(), kFBBytes = fbbytes<QG>();
   extern __shared__ __align__(1024) uint8_t smem[];  // B of the two item slots
   __shared__ __align__(8) uint64_t bar_afull[kFStages], bar_aempty[kFStages], bar_dfull[kFDBufs],
       bar_dempty[kFDBufs], bar_ifull[2], bar_iempty[2];
@@ -491,21 +485,16 @@ __global__ void __launch_bounds__(256) k_tc_recheck(const uint8_t* __restrict__ 
   }
 }
 
-template <int QG>
-static int tcf_smem_bytes() { return 2 * fbbytes<QG>(); }
+static int tcf_smem_bytes() { return 2 * kFBBytes; }
 
 // The tensor-core admission pass over the (cluster, query group) items launch_invert made:
 // weights and residual bounds per query, the bound pass, then the exact estimates of what it
 // admitted. Returns the kernels launched.
 int launch_scan_tcf(const DevIndex& ix, Workspace& w, uint32_t nq, uint32_t P, const uint64_t* allow,
-                    uint64_t allow_words, int sms, uint32_t qg, cudaStream_t st) {
+                    uint64_t allow_words, int sms, cudaStream_t st) {
   static PerDeviceOnce attr;
   attr([] {
-    cudaError_t e = cudaFuncSetAttribute(k_scan_tcf<64>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         tcf_smem_bytes<64>());
-    if (e == cudaSuccess)
-      e = cudaFuncSetAttribute(k_scan_tcf<128>, cudaFuncAttributeMaxDynamicSharedMemorySize, tcf_smem_bytes<128>());
-    return e;
+    return cudaFuncSetAttribute(k_scan_tcf, cudaFuncAttributeMaxDynamicSharedMemorySize, tcf_smem_bytes());
   });
   TcfArgs a{};
   a.codes = reinterpret_cast<const uint4*>(ix.blocks_tc);
@@ -536,8 +525,7 @@ int launch_scan_tcf(const DevIndex& ix, Workspace& w, uint32_t nq, uint32_t P, c
   a.global = ix.global;
   // entries from tc_start[q] on are the bound pass's (earlier ones are exact already)
   cudaMemcpyAsync(w.tc_start, w.ccount, (size_t)nq * 4, cudaMemcpyDeviceToDevice, st);
-  if (qg == 128) k_scan_tcf<128><<<sms, kFThreads, tcf_smem_bytes<128>(), st>>>(a);
-  else k_scan_tcf<64><<<sms, kFThreads, tcf_smem_bytes<64>(), st>>>(a);
+  k_scan_tcf<<<sms, kFThreads, tcf_smem_bytes(), st>>>(a);
   k_tc_recheck<<<dim3(nq, kRecheckSplit), 256, 0, st>>>(w.tables, w.qp, reinterpret_cast<const uint4*>(ix.blocks_tc), ix.mul,
                                    w.tc_start, w.ccount, w.cbuf_per_q, ix.nslots, w.cbuf_est, w.cbuf_info);
   return 2;

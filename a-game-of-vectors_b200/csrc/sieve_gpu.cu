@@ -268,7 +268,6 @@ int build_index(const sg_ivf_arrays* a, int device, sg_index** out) {
   if (const char* tc = getenv("SIEVE_GPU_TC")) h->cfg.tc = atoi(tc) == 2 ? 2 : 1;
   if (const char* sp = getenv("SIEVE_GPU_TC_SPLIT")) h->cfg.tc_split = (uint32_t)strtoul(sp, nullptr, 10);
   if (const char* tm = getenv("SIEVE_GPU_TC_MIN")) h->cfg.tc_min_queries = (uint32_t)strtoul(tm, nullptr, 10);
-  if (const char* qg = getenv("SIEVE_GPU_TC_QG")) h->cfg.tc_group = strtoul(qg, nullptr, 10) == 128 ? 128 : 64;
   if ((rc = dalloc(&x.blocks_tc, (size_t)nblocks * 256))) {
     free_index(x);
     return rc;

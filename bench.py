@@ -47,7 +47,8 @@ WORKLOADS = {
                stated="32:500:tiered200", serve="5000,20000,50000,100000,150000,200000"),
     # margin probing: 0.35 gives a median of ~46 probes (cap 128) on this mixture
     "c3": dict(n=113_500_000, centers=65536, k=16384, queries=100_000, search="128:2000:full:p0.35",
-               stated="128:500:tiered200:p0.35", serve="5000,20000,50000,100000,150000,200000",
+               stated="128:500:tiered200:p0.35",
+               serve="5000,10000,20000,30000,40000,50000,100000,150000,200000",
                secondary="c2"),
     # billion-scale L2 (bigann): 512 x 256 = 131,072 leaves, 2-bit refinement. The bench default
     # is a 100M-row cut of the 1B shape (--rows sets it): the 1B build does not fit the run's time.
@@ -439,6 +440,9 @@ def main():
                          "workload's); empty: skip")
     ap.add_argument("--serve-seconds", type=float, default=2.0)
     ap.add_argument("--no-tune", action="store_true", help="keep the default shapes (no autotuner)")
+    ap.add_argument("--tuning", default=None,
+                    help="pin the batched path's shapes instead of autotuning: "
+                         "tc_min_queries:chunk_blocks:scan_ctas_per_sm:seed_blocks:tc_split")
     ap.add_argument("--stated", default=None,
                     help="search config measured beside the headline (default: the workload's "
                          "stated search); empty: skip")
@@ -538,7 +542,12 @@ def main():
     # the autotuner picks the batched path's shapes on this batch size (untimed; results are
     # identical under every shape)
     tuning = None
-    if B >= 64 and not args.no_tune:
+    if args.tuning:
+        # shapes given on the command line (a profiling run that repeats a tuned bench's launches)
+        names = ("tc_min_queries", "chunk_blocks", "scan_ctas_per_sm", "seed_blocks", "tc_split")
+        tuning = dict(zip(names, (int(x) for x in args.tuning.split(":"))))
+        index.set_tuning(**tuning)
+    elif B >= 64 and not args.no_tune:
         index.set_timing(False)
         tuning = index.autotune(B, q768[nq_pool - B].data_ptr(), params, reps=2)
         index.set_timing(True)

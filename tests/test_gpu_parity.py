@@ -23,13 +23,11 @@ def cparams(p: Params) -> SgParams:
 def open_with(arrays, scan_mode: str):
     """Opens an index with the scan chosen by SIEVE_GPU_MMA (0 ALU, 1 automatic, 2 tensor-core);
     a suffix "h" selects the exact one-hot tcgen05 contraction instead of the bound pass
-    (SIEVE_GPU_TC=2), a suffix "g" the bound pass with work items of 128 queries
-    (SIEVE_GPU_TC_QG=128)."""
+    (SIEVE_GPU_TC=2)."""
     import os
 
     tc = "2" if scan_mode.endswith("h") else "1"
-    env = {"SIEVE_GPU_MMA": scan_mode.rstrip("hg"), "SIEVE_GPU_TC": tc,
-           "SIEVE_GPU_TC_QG": "128" if scan_mode.endswith("g") else "64"}
+    env = {"SIEVE_GPU_MMA": scan_mode.rstrip("h"), "SIEVE_GPU_TC": tc}
     old = {k: os.environ.get(k) for k in env}
     os.environ.update(env)
     try:
@@ -42,7 +40,7 @@ def open_with(arrays, scan_mode: str):
                 os.environ[k] = v
 
 
-@pytest.fixture(scope="module", params=["1", "2", "2g", "2h", "0"], ids=["auto", "tc", "tc128", "onehot", "alu"])
+@pytest.fixture(scope="module", params=["1", "2", "2h", "0"], ids=["auto", "tc", "onehot", "alu"])
 def gpu_a(request):
     arrays, q768, q256, _ = index_a()
     ix = open_with(arrays, request.param)
@@ -50,7 +48,7 @@ def gpu_a(request):
     ix.close()
 
 
-@pytest.fixture(scope="module", params=["1", "2", "2g", "2h"], ids=["auto", "tc", "tc128", "onehot"])
+@pytest.fixture(scope="module", params=["1", "2", "2h"], ids=["auto", "tc", "onehot"])
 def gpu_b(request):
     arrays, q768, q256, _ = index_b()
     ix = open_with(arrays, request.param)
