@@ -742,6 +742,21 @@ def recall10_ties(ids, cnt, gt_ids, gt_sc) -> tuple[float, float]:
     return float(np.mean(rt)), float(np.mean(rs))
 
 
+def bigann_launches(K: int, params, batch: int) -> int:
+    """Kernels one sg_search_bigann call launches (bg_run in csrc/bigann.cu): per pass of queries,
+    prep, the routing kernels (tensor-core: queries to bf16, the subset GEMM when the plan has one,
+    thresholds, the filtered GEMM, select; FP32: scores, select), the scan, rerank and top-k."""
+    P = max(min(params.nprobe, K), 1)
+    ksub = -(-K // 16)
+    subset, cap = False, K
+    if not params.route_fp32 and K > 8192 and ksub >= 2 * P and max(8192, 32 * P) < K:
+        subset, cap = True, max(8192, 32 * P)
+    per_query = (ksub * 4 if subset else 0) + cap * 8 if not params.route_fp32 else K * 4
+    per = max(1, min((1 << 30) // per_query, 65535))
+    route = (5 if subset else 4) if not params.route_fp32 else 2
+    return (1 + route + 1 + 2) * -(-batch // per)
+
+
 def main_bigann(args, rank: int, world: int, local: int, dev: str):
     from sieve_gpu import bigann_builder as BB
     from sieve_gpu.bigann import BigannIndex, BigannTiming, parse_config as bg_parse
@@ -897,7 +912,7 @@ def main_bigann(args, rank: int, world: int, local: int, dev: str):
         "cpu_baseline": cpu,
         "e2e": {"value": e2e_qps, "unit": "queries/s", "h2d_bytes_per_step": B * 100,
                 "d2h_bytes_per_step": B * k * 8 + B * 4},
-        "gpu_launches": 6 * args.steps * -(-B // min(65535, (1 << 28) // max(int(arrays["k"]), 1))),
+        "gpu_launches": args.steps * bigann_launches(int(arrays["k"]), params, B),
         "clocks": clocks.summary(),
         "build": build_info,
     }
