@@ -248,10 +248,6 @@ void form_batch(sg_server* srv, Slot& s) {
   const uint64_t budget = srv->cfg.scratch_bytes / std::max<uint32_t>(srv->cfg.contexts, 1);
   uint32_t limit = std::min<uint32_t>(srv->cfg.max_batch, s.cap);
   s.cfg = sg::index_config(srv->h);
-  // A batch's candidate buffers share half of this slot's scratch (a query whose share fills up
-  // is re-run with its exact bound, as in a batched search), so the batch size is not cut by the
-  // index-wide candidate budget sized for one large batch.
-  s.cfg.cbuf_budget = std::min<uint64_t>(s.cfg.cbuf_budget, budget / 2);
   // the largest batch whose scratch fits this slot's share (one query always goes)
   while (limit > 1 && sg::ctx_bytes(srv->h, s.cfg, p, limit) > budget) limit = (limit + 1) / 2;
   std::deque<std::shared_ptr<Req>> rest;

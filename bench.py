@@ -48,7 +48,7 @@ WORKLOADS = {
     # margin probing: 0.35 gives a median of ~46 probes (cap 128) on this mixture
     "c3": dict(n=113_500_000, centers=65536, k=16384, queries=100_000, search="128:2000:full:p0.35",
                stated="128:500:tiered200:p0.35",
-               serve="5000,10000,20000,30000,40000,50000,100000,150000,200000",
+               serve="5000,10000,20000,25000,30000,40000,50000,100000,150000,200000",
                secondary="c2"),
     # billion-scale L2 (bigann): 512 x 256 = 131,072 leaves, 2-bit refinement. The bench default
     # is a 100M-row cut of the 1B shape (--rows sets it): the 1B build does not fit the run's time.
