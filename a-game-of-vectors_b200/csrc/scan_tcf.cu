@@ -141,7 +141,7 @@ __global__ void __launch_bounds__(kFThreads, 1) k_scan_tcf(TcfArgs a) {
   __shared__ int s_abort;
   __shared__ uint32_t s_meta[2][8];  // b0, nb, cl, ng, -, end
   __shared__ float4 s_qc[2][kFQG];   // cent, a, b, threshold key (as bits)
-  __shared__ float4 s_qf[2][kFQG];   // gamma, R_hi, R_lo, -
+  __shared__ float4 s_qf[2][kFQG];   // gamma, R_hi, R_lo, threshold as an estimate
   __shared__ uint2 s_qk[2][kFQG];    // candidate order base, query
   __shared__ uint2 s_cb[kFEpiWarps][2][32];  // per column: reserved base, admitted lanes
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
@@ -217,7 +217,8 @@ __global__ void __launch_bounds__(kFThreads, 1) k_scan_tcf(TcfArgs a) {
         const float cent = a.global ? 0.0f : a.probe_sc[(size_t)q * a.P + r];
         const uint32_t thr = *(volatile const uint32_t*)(a.thr + q);
         s_qc[slot][qi] = make_float4(cent, p.z, p.w, __uint_as_float(thr));
-        s_qf[slot][qi] = a.fq[q];
+        const float4 f = a.fq[q];
+        s_qf[slot][qi] = make_float4(f.x, f.y, f.z, thr ? unord(thr) : -INFINITY);
         s_qk[slot][qi] = make_uint2(a.probe_off[(size_t)q * a.P + r], q);
       }
       if (lane == 0) {
@@ -361,13 +362,21 @@ __global__ void __launch_bounds__(kFThreads, 1) k_scan_tcf(TcfArgs a) {
             const uint32_t cbuf = p_on ? (p_buf ^ 1) : 0;
             const uint32_t ncol = min(32u, ng - 32 * cc);
             uint32_t adm = 0;
-#pragma unroll
-            for (int j = 0; j < 32; j++) {
+            // the threshold as an estimate (ord is monotone, so est >= it exactly when
+            // ord(est) >= the key; a finite mul gives a non-NaN est), -inf for the empty key
+            auto bound_col = [&](int j) {
               const float4 qc = s_qc[slot][32 * cc + j];
               const float4 qf = s_qf[slot][32 * cc + j];
               const float sb = __fadd_rn(__fmul_rn(qf.x, (float)(int)v[j]), neg ? qf.z : qf.y);
               const float est = __fadd_rn(qc.x, __fmul_rn(mv, __fadd_rn(__fmul_rn(qc.y, sb), qc.z)));
-              adm |= (always || ord(est) >= __float_as_uint(qc.w) ? 1u : 0u) << j;
+              adm |= (always || est >= qf.w ? 1u : 0u) << j;
+            };
+            // a group of at most 16 queries fills only the first 16 columns (MMA N = 16)
+#pragma unroll
+            for (int j = 0; j < 16; j++) bound_col(j);
+            if (ncol > 16) {
+#pragma unroll
+              for (int j = 16; j < 32; j++) bound_col(j);
             }
             adm &= lane_ok ? (ncol == 32 ? 0xFFFFFFFFu : (1u << ncol) - 1u) : 0u;
             if (adm && (a.allow || a.allow_q)) {  // allowlist filters (View::hidden)
