@@ -219,6 +219,65 @@ SG_DEV uint32_t block_select_nth_u32(Get get, uint32_t m, uint32_t n, uint32_t* 
   return prefix;
 }
 
+// The same select over the ordered keys of a float row in global memory, with each thread's
+// loads issued eight at a time before their histogram updates (a row of a routing score matrix
+// is re-read once per pass; one load in flight per thread left the passes latency-bound).
+SG_DEV uint32_t block_select_nth_row(const float* __restrict__ row, uint32_t m, uint32_t n, uint32_t* hist) {
+  constexpr uint32_t kBatch = 8;
+  uint32_t prefix = 0, mask = 0, remaining = n;
+  __shared__ uint32_t s_digitr, s_abover;
+  for (int shift = 24; shift >= 0; shift -= 8) {
+    for (int i = threadIdx.x; i < 256; i += blockDim.x) hist[i] = 0;
+    __syncthreads();
+    for (uint32_t i0 = threadIdx.x; i0 < m; i0 += kBatch * blockDim.x) {
+      uint32_t k[kBatch];
+#pragma unroll
+      for (uint32_t j = 0; j < kBatch; j++) {
+        const uint32_t i = i0 + j * blockDim.x;
+        k[j] = i < m ? ord(__ldg(row + i)) : 0u;
+      }
+#pragma unroll
+      for (uint32_t j = 0; j < kBatch; j++)
+        if (i0 + j * blockDim.x < m && (k[j] & mask) == prefix) atomicAdd(&hist[(k[j] >> shift) & 255], 1u);
+    }
+    __syncthreads();
+    if (threadIdx.x < 32) {
+      const int lane = threadIdx.x;
+      uint32_t c[8], sum = 0;
+#pragma unroll
+      for (int j = 0; j < 8; j++) {
+        c[j] = hist[255 - (lane * 8 + j)];
+        sum += c[j];
+      }
+      uint32_t incl = sum;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        uint32_t y = __shfl_up_sync(0xFFFFFFFFu, incl, o);
+        if (lane >= o) incl += y;
+      }
+      uint32_t excl = incl - sum;
+      if (excl < remaining && remaining <= incl) {
+        uint32_t run = excl;
+#pragma unroll
+        for (int j = 0; j < 8; j++) {
+          if (run < remaining && remaining <= run + c[j]) {
+            s_digitr = 255 - (lane * 8 + j);
+            s_abover = run;
+          }
+          run += c[j];
+        }
+      }
+    }
+    __syncthreads();
+    uint32_t d = s_digitr;
+    remaining -= s_abover;
+    prefix |= d << shift;
+    mask |= 255u << shift;
+    __syncthreads();
+  }
+  return prefix;
+}
+
 // Bitonic sort of (key, payload) pairs in shared memory by key, descending (n a power of two).
 SG_DEV void block_bitonic_sort_desc_kv(uint64_t* a, uint32_t* v, uint32_t n) {
   for (uint32_t size = 2; size <= n; size <<= 1) {

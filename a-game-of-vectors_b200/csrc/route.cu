@@ -366,15 +366,24 @@ __global__ void __launch_bounds__(256) k_route_select(SelectArgs a) {
   bool exact = !a.bf16;
   if (a.bf16) {
     // the P-th largest BF16 score and the window below it
-    const uint32_t kth = block_select_nth_u32([&](uint32_t i) { return ord(row[i]); }, K, P, hist);
+    const uint32_t kth = block_select_nth_row(row, K, P, hist);
     const float sP = unord(kth);
     float delta = 0.0085f * a.qnorm[q] * a.cent_norm_max;
     float lim = sP - 2.0f * delta;
-    for (uint32_t c = threadIdx.x; c < K; c += blockDim.x)
-      if (row[c] >= lim) {
-        uint32_t slot = atomicAdd(&s_nw, 1u);
-        if (slot < kWinCap) keys[slot] = c;
+    for (uint32_t c0 = threadIdx.x; c0 < K; c0 += 8 * blockDim.x) {
+      float v[8];
+#pragma unroll
+      for (uint32_t j = 0; j < 8; j++) {
+        const uint32_t c = c0 + j * blockDim.x;
+        v[j] = c < K ? __ldg(row + c) : -INFINITY;
       }
+#pragma unroll
+      for (uint32_t j = 0; j < 8; j++)
+        if (v[j] >= lim && c0 + j * blockDim.x < K) {
+          uint32_t slot = atomicAdd(&s_nw, 1u);
+          if (slot < kWinCap) keys[slot] = c0 + j * blockDim.x;
+        }
+    }
     __syncthreads();
     uint32_t nw = s_nw;
     // a window narrower than P means a non-finite score or norm: take the exact path
