@@ -31,7 +31,8 @@
 // loader warp fills two item slots (B weights and per-query constants); four producer warps
 // expand their slots' code bits into u8 A rows in tensor memory (one 64-column stage per tile,
 // four stages); one MMA warp issues each tile's 8 MMAs from an elected lane into one of four
-// accumulators; eight epilogue warps bound every (slot, query) pair and reserve buffer entries.
+// accumulators; sixteen epilogue warps (four per TMEM lane quarter, one per accumulator) bound
+// every (slot, query) pair and reserve buffer entries.
 // Every mbarrier wait is bounded: a wait that runs out raises kStatusTimeout, every role stops,
 // and the CTA frees its tensor memory and returns.
 #include <climits>
@@ -48,11 +49,11 @@ constexpr uint32_t kFCols = 512;    // TMEM columns: 4 x 64 (A) + 4 x 64 (D)
 constexpr uint32_t kFDCol = 256;    // first D column
 constexpr int kFDBufs = 4;          // accumulators
 constexpr int kFProducers = 4;      // warps 0-3 build A
-constexpr int kFEpi = 4;            // warps 4-11 bound the pairs
-constexpr int kFEpiWarps = 8;
-constexpr int kFMma = 12;           // warp 12 issues the MMAs
-constexpr int kFLoader = 13;        // warp 13 loads work items
-constexpr int kFThreads = 14 * 32;
+constexpr int kFEpi = 4;            // warps 4-19 bound the pairs
+constexpr int kFEpiWarps = 16;      // four per TMEM lane quarter, one per accumulator
+constexpr int kFMma = 20;           // warp 20 issues the MMAs
+constexpr int kFLoader = 21;        // warp 21 loads work items
+constexpr int kFThreads = 22 * 32;
 constexpr int kFBBytes = kFQG * SG_PDIM;  // B of one item slot: 64 queries x 256 s8 weights
 
 // ---- per-query weights and residual bounds --------------------------------------------------
@@ -133,7 +134,7 @@ struct TcfArgs {
 };
 
 
-__global__ void __launch_bounds__(kFThreads, 1) k_scan_tcf(TcfArgs a) {
+__global__ void __maxnreg__(88) k_scan_tcf(TcfArgs a) {
   extern __shared__ __align__(1024) uint8_t smem[];  // B of the two item slots
   __shared__ __align__(8) uint64_t bar_afull[kFStages], bar_aempty[kFStages], bar_dfull[kFDBufs],
       bar_dempty[kFDBufs], bar_ifull[2], bar_iempty[2];
@@ -158,7 +159,7 @@ __global__ void __launch_bounds__(kFThreads, 1) k_scan_tcf(TcfArgs a) {
     }
     for (int i = 0; i < kFDBufs; i++) {
       mbar_init(&bar_dfull[i], 1);
-      mbar_init(&bar_dempty[i], 4);  // the two epilogue warps of each lane quarter, per parity
+      mbar_init(&bar_dempty[i], 4);  // the epilogue warp of each lane quarter that reads buffer i
     }
     for (int i = 0; i < 2; i++) {
       mbar_init(&bar_ifull[i], 1);
@@ -265,14 +266,14 @@ __global__ void __launch_bounds__(kFThreads, 1) k_scan_tcf(TcfArgs a) {
             break;
           }
           // column c holds prefix dimensions 4c..4c+3: nibble c of the code (word c/8)
-          uint32_t r[32];
-          const uint32_t wl[4] = {lo.x, lo.y, lo.z, lo.w}, wh[4] = {hi.x, hi.y, hi.z, hi.w};
+          const uint32_t wd[8] = {lo.x, lo.y, lo.z, lo.w, hi.x, hi.y, hi.z, hi.w};
 #pragma unroll
-          for (int c = 0; c < 32; c++) r[c] = bits_to_bytes((wl[c >> 3] >> (4 * (c & 7))) & 15u);
-          tc_st32(tmem + lane_base + st * 64, r);
+          for (int q4 = 0; q4 < 4; q4++) {  // 16 columns (two code words) per store
+            uint32_t r[16];
 #pragma unroll
-          for (int c = 0; c < 32; c++) r[c] = bits_to_bytes((wh[c >> 3] >> (4 * (c & 7))) & 15u);
-          tc_st32(tmem + lane_base + st * 64 + 32, r);
+            for (int c = 0; c < 16; c++) r[c] = bits_to_bytes((wd[2 * q4 + (c >> 3)] >> (4 * (c & 7))) & 15u);
+            tc_st16(tmem + lane_base + st * 64 + 16 * q4, r);
+          }
           tc_wait_st();
           tc_fence_before();
           __syncwarp();
@@ -302,7 +303,7 @@ __global__ void __launch_bounds__(kFThreads, 1) k_scan_tcf(TcfArgs a) {
         if (lane == 0) mbar_arrive(&bar_iempty[slot]);
       } else {
         // ---- epilogue: slot (4t + qd)*32 + lane of the tiles of this warp's parity ----------
-        const uint32_t ew = warp - kFEpi, qd = ew & 3, par = ew >> 2;
+        const uint32_t ew = warp - kFEpi, qd = ew & 3, par = ew >> 2;  // par: the accumulator it reads
         const uint32_t lane_base = (32u * qd) << 16;
         const uint32_t ncc = (N + 31) >> 5;
         uint2* cb = &s_cb[ew][0][0];
@@ -339,44 +340,42 @@ __global__ void __launch_bounds__(kFThreads, 1) k_scan_tcf(TcfArgs a) {
           if (t >= ntiles || bl >= nb || bl * SG_BLOCK + lane >= cl) return 0.0f;
           return a.mul[(b0 + bl) * SG_BLOCK + lane];
         };
-        const uint32_t t0 = ((ts & 1) == par) ? 0 : 1;  // first tile of this warp's parity
+        const uint32_t t0 = (par + kFDBufs - (ts & (kFDBufs - 1))) & (kFDBufs - 1);  // first tile in its buffer
         float mv = tile_mul(t0);
-        for (uint32_t t = t0; t < ntiles; t += 2) {
+        for (uint32_t t = t0; t < ntiles; t += kFDBufs) {
           const uint32_t ds = ts + t, dbuf = ds & (kFDBufs - 1), duse = ds / kFDBufs;
           const uint32_t bl = 4 * t + qd;
           const uint32_t loc = bl * SG_BLOCK + lane;
           const bool lane_ok = bl < nb && loc < cl;
           const uint32_t gslot = (b0 + bl) * SG_BLOCK + lane;
-          const float nmv = tile_mul(t + 2);
+          const float nmv = tile_mul(t + kFDBufs);
           // the residual bound that gives an upper bound of the estimate for this slot's mul
           const bool neg = mv < 0.0f;
           const bool always = !isfinite(mv);  // no monotone bound: recheck every column
           if (!mbar_wait(&bar_dfull[dbuf], duse & 1, abort_flag)) break;
           tc_fence_after();
           for (uint32_t cc = 0; cc < ncc; cc++) {
-            uint32_t v[32];
-            tc_ld32(tmem + lane_base + kFDCol + dbuf * kFQG + 32 * cc, v);
-            tc_wait_ld();
             // 1. every column's bound of the estimate (the exact estimate's operations at the
-            //    bound of the score) against the query's admission key
+            //    bound of the score) against the query's admission key, 16 columns at a time (a
+            //    group of at most 16 queries fills only the first 16: MMA N = 16)
             const uint32_t cbuf = p_on ? (p_buf ^ 1) : 0;
             const uint32_t ncol = min(32u, ng - 32 * cc);
             uint32_t adm = 0;
-            // the threshold as an estimate (ord is monotone, so est >= it exactly when
-            // ord(est) >= the key; a finite mul gives a non-NaN est), -inf for the empty key
-            auto bound_col = [&](int j) {
-              const float4 qc = s_qc[slot][32 * cc + j];
-              const float4 qf = s_qf[slot][32 * cc + j];
-              const float sb = __fadd_rn(__fmul_rn(qf.x, (float)(int)v[j]), neg ? qf.z : qf.y);
-              const float est = __fadd_rn(qc.x, __fmul_rn(mv, __fadd_rn(__fmul_rn(qc.y, sb), qc.z)));
-              adm |= (always || est >= qf.w ? 1u : 0u) << j;
-            };
-            // a group of at most 16 queries fills only the first 16 columns (MMA N = 16)
+            for (uint32_t h = 0; h < (ncol > 16 ? 2u : 1u); h++) {
+              uint32_t v[16];
+              tc_ld16(tmem + lane_base + kFDCol + dbuf * kFQG + 32 * cc + 16 * h, v);
+              tc_wait_ld();
+              // the threshold as an estimate (ord is monotone, so est >= it exactly when
+              // ord(est) >= the key; a finite mul gives a non-NaN est), -inf for the empty key
 #pragma unroll
-            for (int j = 0; j < 16; j++) bound_col(j);
-            if (ncol > 16) {
-#pragma unroll
-              for (int j = 16; j < 32; j++) bound_col(j);
+              for (int j = 0; j < 16; j++) {
+                const uint32_t col = 32 * cc + 16 * h + j;
+                const float4 qc = s_qc[slot][col];
+                const float4 qf = s_qf[slot][col];
+                const float sb = __fadd_rn(__fmul_rn(qf.x, (float)(int)v[j]), neg ? qf.z : qf.y);
+                const float est = __fadd_rn(qc.x, __fmul_rn(mv, __fadd_rn(__fmul_rn(qc.y, sb), qc.z)));
+                adm |= (always || est >= qf.w ? 1u : 0u) << (16 * h + j);
+              }
             }
             adm &= lane_ok ? (ncol == 32 ? 0xFFFFFFFFu : (1u << ncol) - 1u) : 0u;
             if (adm && (a.allow || a.allow_q)) {  // allowlist filters (View::hidden)

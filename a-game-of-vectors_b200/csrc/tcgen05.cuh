@@ -106,6 +106,25 @@ SG_DEV void tc_ld32(uint32_t taddr, uint32_t* r) {
       : "r"(taddr));
 }
 
+// 32 lanes x 16 columns: thread i writes lane (taddr lane + i), register j to column + j.
+SG_DEV void tc_st16(uint32_t taddr, const uint32_t* r) {
+  asm volatile(
+      "tcgen05.st.sync.aligned.32x32b.x16.b32 [%0], {%1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, "
+      "%14, %15, %16};\n" ::"r"(taddr),
+      "r"(r[0]), "r"(r[1]), "r"(r[2]), "r"(r[3]), "r"(r[4]), "r"(r[5]), "r"(r[6]), "r"(r[7]), "r"(r[8]),
+      "r"(r[9]), "r"(r[10]), "r"(r[11]), "r"(r[12]), "r"(r[13]), "r"(r[14]), "r"(r[15]));
+}
+
+// 32 lanes x 16 columns: thread i reads lane (taddr lane + i), column + j into register j.
+SG_DEV void tc_ld16(uint32_t taddr, uint32_t* r) {
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, "
+      "%14, %15}, [%16];\n"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+        "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+      : "r"(taddr));
+}
+
 // Shared-memory matrix descriptor, K-major without swizzle: core matrices of 8 rows x 16 B,
 // `lbo` bytes between the two K halves of an instruction, `sbo` bytes between 8-row groups.
 SG_DEV uint64_t smem_desc(uint32_t saddr, uint32_t lbo, uint32_t sbo) {
