@@ -360,7 +360,7 @@ def domain_allowlist(dom: np.ndarray, selectivity: float) -> np.ndarray:
 
 
 def serve_load(index, arrays, queries_host: np.ndarray, params, rates, seconds: float, dom=None,
-               seed: int = 7, warmup_s: float = 0.3):
+               seed: int = 7, warmup_s: float = 0.3, contexts: int = 3):
     """Open-loop Poisson arrivals into the serving loop (continuous batching), replayed by the
     library's own submitter thread (sg_server_replay): for each rate, the achieved QPS and the
     p50/p99 latency from submit to results on the host. One request in ten carries a domain
@@ -378,7 +378,7 @@ def serve_load(index, arrays, queries_host: np.ndarray, params, rates, seconds: 
     out = []
     try:
         for rate in rates:
-            srv = Server(index, max_batch=4096, contexts=3)
+            srv = Server(index, max_batch=4096, contexts=contexts)
             try:
                 def trace(n):
                     t = np.cumsum(rng.exponential(1.0 / rate, n))
@@ -439,6 +439,7 @@ def main():
                     help="Poisson arrival rates (queries/s) for the serving loop (default: the "
                          "workload's); empty: skip")
     ap.add_argument("--serve-seconds", type=float, default=2.0)
+    ap.add_argument("--serve-contexts", type=int, default=3, help="execution contexts of the serving loop")
     ap.add_argument("--no-tune", action="store_true", help="keep the default shapes (no autotuner)")
     ap.add_argument("--tuning", default=None,
                     help="pin the batched path's shapes instead of autotuning: "
@@ -630,7 +631,7 @@ def main():
     if rates:
         rates = [float(x) for x in rates.split(",") if x]
         serving = serve_load(index, arrays, q_pool_host, params, rates, args.serve_seconds,
-                             dom=arrays.get("domain"))
+                             dom=arrays.get("domain"), contexts=args.serve_contexts)
 
     # the workload's search exactly as stated, beside the headline
     stated = None
@@ -666,7 +667,7 @@ def main():
                   "p99_ms": float(np.percentile(plain_ms, 99)), "queries": int(plain_ms.size)},
         "stage_ms": stage,
         "serving": serving,
-        "serving_note": "continuous batching (sg_server, 3 contexts, batches up to 4096): open-loop "
+        "serving_note": f"continuous batching (sg_server, {args.serve_contexts} contexts, batches up to 4096): open-loop "
                         "Poisson arrivals replayed by the library's submitter thread "
                         "(sg_server_replay), 10% of requests on domain allowlists (10,000 seeded "
                         "domains, whole domains at 0.1/1/10/50% of the rows, Post plan), after 0.3 s "
