@@ -134,7 +134,7 @@ struct TcfArgs {
 };
 
 
-__global__ void __maxnreg__(88) k_scan_tcf(TcfArgs a) {
+__global__ void __launch_bounds__(kFThreads, 1) k_scan_tcf(TcfArgs a) {
   extern __shared__ __align__(1024) uint8_t smem[];  // B of the two item slots
   __shared__ __align__(8) uint64_t bar_afull[kFStages], bar_aempty[kFStages], bar_dfull[kFDBufs],
       bar_dempty[kFDBufs], bar_ifull[2], bar_iempty[2];
