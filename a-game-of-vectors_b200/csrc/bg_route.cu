@@ -102,15 +102,6 @@ struct BrArgs {
   uint32_t* status;
 };
 
-// A bounded wait that ignores the abort flag: the exit path's wait for copies in flight.
-SG_DEV void mbar_drain(uint64_t* bar, uint32_t parity) {
-  const uint64_t t0 = globaltimer_ns();
-  for (uint32_t i = 0; i < kTcSpinLimit; i++) {
-    if (mbar_test(bar, parity)) return;
-    if ((i & 255u) == 255u && globaltimer_ns() - t0 > kTcWaitNs) return;
-  }
-}
-
 __global__ void __launch_bounds__(kBrThreads, 1) k_bg_route_tc(const __grid_constant__ CUtensorMap map_l,
                                                                const __grid_constant__ CUtensorMap map_q,
                                                                BrArgs a) {

@@ -30,7 +30,9 @@
 // Warp roles of the persistent CTA (one per SM), as in the one-hot kernel of scan_tc.cu: a
 // loader warp fills two item slots (B weights and per-query constants); four producer warps
 // expand their slots' code bits into u8 A rows in tensor memory (one 64-column stage per tile,
-// four stages); one MMA warp issues each tile's 8 MMAs from an elected lane into one of four
+// four stages), from the tile's codes that a copy warp streams into an eight-stage shared-memory
+// ring with bulk async copies (a tile's 128 slots are 4 KB of contiguous codes); one MMA warp
+// issues each tile's 8 MMAs from an elected lane into one of four
 // accumulators; sixteen epilogue warps (four per TMEM lane quarter, one per accumulator) bound
 // every (slot, query) pair and reserve buffer entries.
 // Every mbarrier wait is bounded: a wait that runs out raises kStatusTimeout, every role stops,
@@ -53,7 +55,10 @@ constexpr int kFEpi = 4;            // warps 4-19 bound the pairs
 constexpr int kFEpiWarps = 16;      // four per TMEM lane quarter, one per accumulator
 constexpr int kFMma = 20;           // warp 20 issues the MMAs
 constexpr int kFLoader = 21;        // warp 21 loads work items
-constexpr int kFThreads = 22 * 32;
+constexpr int kFCopy = 22;          // warp 22 streams each tile's codes into shared memory
+constexpr int kFThreads = 23 * 32;
+constexpr int kFCStages = 8;        // code stages: one tile's 128 slots x 32 B each
+constexpr int kFCBytes = 4 * SG_BLOCK * 32;  // 4 KB
 constexpr int kFBBytes = kFQG * SG_PDIM;  // B of one item slot: 64 queries x 256 s8 weights
 
 // ---- per-query weights and residual bounds --------------------------------------------------
@@ -137,7 +142,7 @@ struct TcfArgs {
 __global__ void __launch_bounds__(kFThreads, 1) k_scan_tcf(TcfArgs a) {
   extern __shared__ __align__(1024) uint8_t smem[];  // B of the two item slots
   __shared__ __align__(8) uint64_t bar_afull[kFStages], bar_aempty[kFStages], bar_dfull[kFDBufs],
-      bar_dempty[kFDBufs], bar_ifull[2], bar_iempty[2];
+      bar_dempty[kFDBufs], bar_ifull[2], bar_iempty[2], bar_cfull[kFCStages], bar_cempty[kFCStages];
   __shared__ uint32_t s_tmem;
   __shared__ int s_abort;
   __shared__ uint32_t s_meta[2][8];  // b0, nb, cl, ng, -, end
@@ -163,7 +168,11 @@ __global__ void __launch_bounds__(kFThreads, 1) k_scan_tcf(TcfArgs a) {
     }
     for (int i = 0; i < 2; i++) {
       mbar_init(&bar_ifull[i], 1);
-      mbar_init(&bar_iempty[i], kFProducers + kFEpiWarps + 1);
+      mbar_init(&bar_iempty[i], kFProducers + kFEpiWarps + 2);  // + the MMA and copy warps
+    }
+    for (int i = 0; i < kFCStages; i++) {
+      mbar_init(&bar_cfull[i], 1);
+      mbar_init(&bar_cempty[i], kFProducers);
     }
     s_abort = 0;
     fence_mbar_init();
@@ -173,6 +182,8 @@ __global__ void __launch_bounds__(kFThreads, 1) k_scan_tcf(TcfArgs a) {
   tc_fence_after();
   const uint32_t tmem = s_tmem;
   const uint32_t bs_base = smem_addr(smem);
+  const uint32_t cs_base = bs_base + 2 * kFBBytes;  // the code ring
+  uint32_t c_issued = 0;  // the copy warp's tiles issued (lane 0), for the exit path's drain
   uint32_t* status = a.counters + 2;
 
   if (warp == kFLoader) {
@@ -243,28 +254,48 @@ __global__ void __launch_bounds__(kFThreads, 1) k_scan_tcf(TcfArgs a) {
       const uint32_t b0 = s_meta[slot][0], nb = s_meta[slot][1], cl = s_meta[slot][2], ng = s_meta[slot][3];
       const uint32_t N = (ng + 15) & ~15u, ntiles = (nb + 3) >> 2;
       bool ok = true;
-      if (warp < kFProducers) {
-        // A: the code bits of block 4t + warp of the tile as u8 0/1, slot = lane, K = 256
-        const uint32_t qd = warp;
-        const uint32_t lane_base = (32u * qd) << 16;
-        auto codes_of = [&](uint32_t t, uint4& lo, uint4& hi) {
-          const uint32_t bl = 4 * t + qd;
-          lo = hi = make_uint4(0, 0, 0, 0);
-          if (t < ntiles && bl < nb) {
-            const uint64_t gs = (uint64_t)(b0 + bl) * SG_BLOCK + lane;
-            lo = a.codes[2 * gs];
-            hi = a.codes[2 * gs + 1];
-          }
-        };
-        uint4 lo, hi, nlo, nhi;
-        codes_of(0, lo, hi);
+      if (warp == kFCopy) {
+        // the codes of tile t (blocks 4t..4t+3, contiguous) into ring stage (ts + t) % kFCStages
         for (uint32_t t = 0; t < ntiles; t++) {
-          codes_of(t + 1, nlo, nhi);
-          const uint32_t ds = ts + t, st = ds & (kFStages - 1), su = ds / kFStages;
-          if (!mbar_wait(&bar_aempty[st], (su & 1) ^ 1, abort_flag)) {
+          const uint32_t ds = ts + t, cs = ds % kFCStages, cu = ds / kFCStages;
+          int r = 0;
+          if (lane == 0) r = mbar_wait(&bar_cempty[cs], (cu & 1) ^ 1, abort_flag) ? 1 : 0;
+          if (!__shfl_sync(0xFFFFFFFFu, r, 0)) {
             ok = false;
             break;
           }
+          if (lane == 0) {
+            const uint32_t bytes = min(4u, nb - 4 * t) * SG_BLOCK * 32;
+            mbar_expect_tx(&bar_cfull[cs], bytes);
+            bulk_load(cs_base + cs * kFCBytes,
+                      reinterpret_cast<const uint8_t*>(a.codes) + (size_t)(b0 + 4 * t) * SG_BLOCK * 32, bytes,
+                      &bar_cfull[cs]);
+            c_issued = ds + 1;
+          }
+        }
+        if (lane == 0) mbar_arrive(&bar_iempty[slot]);
+      } else if (warp < kFProducers) {
+        // A: the code bits of block 4t + warp of the tile as u8 0/1, slot = lane, K = 256
+        const uint32_t qd = warp;
+        const uint32_t lane_base = (32u * qd) << 16;
+        for (uint32_t t = 0; t < ntiles; t++) {
+          const uint32_t ds = ts + t, st = ds & (kFStages - 1), su = ds / kFStages;
+          const uint32_t cs = ds % kFCStages, cu = ds / kFCStages;
+          if (!mbar_wait(&bar_aempty[st], (su & 1) ^ 1, abort_flag) ||
+              !mbar_wait(&bar_cfull[cs], cu & 1, abort_flag)) {
+            ok = false;
+            break;
+          }
+          // this warp's block of the tile: slot `lane`'s 32 code bytes
+          uint4 lo = make_uint4(0, 0, 0, 0), hi = lo;
+          if (4 * t + qd < nb) {
+            const uint4* src = reinterpret_cast<const uint4*>(smem + 2 * kFBBytes + cs * kFCBytes +
+                                                              qd * (SG_BLOCK * 32) + lane * 32);
+            lo = src[0];
+            hi = src[1];
+          }
+          __syncwarp();
+          if (lane == 0) mbar_arrive(&bar_cempty[cs]);
           // column c holds prefix dimensions 4c..4c+3: nibble c of the code (word c/8)
           const uint32_t wd[8] = {lo.x, lo.y, lo.z, lo.w, hi.x, hi.y, hi.z, hi.w};
 #pragma unroll
@@ -278,8 +309,6 @@ __global__ void __launch_bounds__(kFThreads, 1) k_scan_tcf(TcfArgs a) {
           tc_fence_before();
           __syncwarp();
           if (lane == 0) mbar_arrive(&bar_afull[st]);
-          lo = nlo;
-          hi = nhi;
         }
         if (lane == 0) mbar_arrive(&bar_iempty[slot]);
       } else if (warp == kFMma) {
@@ -425,6 +454,12 @@ __global__ void __launch_bounds__(kFThreads, 1) k_scan_tcf(TcfArgs a) {
     }
   }
   if (tid == 0 && *abort_flag) atomicOr(status, kStatusTimeout);
+  // the copy warp's bulk copies in flight land before the CTA leaves (a no-op when every tile ran)
+  if (warp == kFCopy && lane == 0 && *abort_flag)
+    for (uint32_t back = 1; back <= (uint32_t)kFCStages && back <= c_issued; back++) {
+      const uint32_t ds = c_issued - back;
+      mbar_drain(&bar_cfull[ds % kFCStages], (ds / kFCStages) & 1);
+    }
   tc_fence_before();
   __syncthreads();
   if (warp == kFMma) {
@@ -493,7 +528,7 @@ __global__ void __launch_bounds__(256) k_tc_recheck(const uint8_t* __restrict__ 
   }
 }
 
-static int tcf_smem_bytes() { return 2 * kFBBytes; }
+static int tcf_smem_bytes() { return 2 * kFBBytes + kFCStages * kFCBytes; }
 
 // The tensor-core admission pass over the (cluster, query group) items launch_invert made:
 // weights and residual bounds per query, the bound pass, then the exact estimates of what it

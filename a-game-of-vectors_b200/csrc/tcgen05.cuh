@@ -52,6 +52,15 @@ SG_DEV bool mbar_wait(uint64_t* bar, uint32_t parity, volatile int* abort_flag) 
   return false;
 }
 
+// A bounded wait that ignores the abort flag: an exit path's wait for its copies in flight.
+SG_DEV void mbar_drain(uint64_t* bar, uint32_t parity) {
+  const uint64_t t0 = globaltimer_ns();
+  for (uint32_t i = 0; i < kTcSpinLimit; i++) {
+    if (mbar_test(bar, parity)) return;
+    if ((i & 255u) == 255u && globaltimer_ns() - t0 > kTcWaitNs) return;
+  }
+}
+
 SG_DEV void tc_alloc(uint32_t* dst, uint32_t ncols) {
   asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n" ::"r"(smem_addr(dst)),
                "r"(ncols));
@@ -156,6 +165,16 @@ SG_DEV void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
   asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(smem_addr(bar)), "r"(bytes)
                : "memory");
 }
+// Untiled bulk copy of `bytes` (a multiple of 16) from global memory at `src` (16-byte aligned)
+// into this CTA's shared memory at `dst` (16-byte aligned); completion is counted in bytes on
+// `bar`. No multicast.
+SG_DEV void bulk_load(uint32_t dst, const void* src, uint32_t bytes, uint64_t* bar) {
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n" ::"r"(dst),
+      "l"(reinterpret_cast<uint64_t>(src)), "r"(bytes), "r"(smem_addr(bar))
+      : "memory");
+}
+
 // Tiled TMA load of the box at (x, y) of a 2-D tensor map into this CTA's shared memory at `dst`
 // (128-byte aligned); completion is counted in bytes on `bar`. x * element size must be a
 // multiple of 16 bytes.
