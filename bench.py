@@ -439,7 +439,7 @@ def main():
                     help="Poisson arrival rates (queries/s) for the serving loop (default: the "
                          "workload's); empty: skip")
     ap.add_argument("--serve-seconds", type=float, default=2.0)
-    ap.add_argument("--serve-contexts", type=int, default=3, help="execution contexts of the serving loop")
+    ap.add_argument("--serve-contexts", type=int, default=6, help="execution contexts of the serving loop")
     ap.add_argument("--no-tune", action="store_true", help="keep the default shapes (no autotuner)")
     ap.add_argument("--tuning", default=None,
                     help="pin the batched path's shapes instead of autotuning: "
