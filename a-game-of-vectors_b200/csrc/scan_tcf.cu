@@ -14,7 +14,9 @@
 // all integers below 2^24, exact in f32. D is an exact s32 tensor-core product of the slot's 256
 // code bits (u8 0/1, A in tensor memory) and the query's weights (s8, B in shared memory):
 // tcgen05.mma.kind::i8 with K = 256, 8 instructions per 128-slot tile, where the exact one-hot
-// contraction needs K = 1024 (32 instructions).
+// contraction needs K = 1024 (32 instructions). The K order is free as long as A and B share it:
+// byte 32i + 4s + j of a row is bit 8j + s of code word i, so each 4-byte column of A is one
+// shift and one mask of a code word, and the weights are stored in that order.
 //
 // The estimate est = cent + mul * (a * s + b), rounded operation by operation (src/rabitq.rs:
 // 127-130), is non-decreasing in s for mul >= 0 (a > 0) and non-increasing for mul < 0, and IEEE
@@ -57,6 +59,8 @@ constexpr int kFMma = 20;           // warp 20 issues the MMAs
 constexpr int kFLoader = 21;        // warp 21 loads work items
 constexpr int kFCopy = 22;          // warp 22 streams each tile's codes into shared memory
 constexpr int kFThreads = 23 * 32;
+constexpr float kMagic = 12582912.0f;     // 1.5 * 2^23: floats in [2^23, 2^24) step by 1
+constexpr uint32_t kMagicBits = 0x4B400000u;
 constexpr int kFCStages = 8;        // code stages: one tile's 128 slots x 32 B each
 constexpr int kFCBytes = 4 * SG_BLOCK * 32;  // 4 KB
 constexpr int kFBBytes = kFQG * SG_PDIM;  // B of one item slot: 64 queries x 256 s8 weights
@@ -66,6 +70,7 @@ constexpr int kFBBytes = kFQG * SG_PDIM;  // B of one item slot: 64 queries x 25
 __global__ void __launch_bounds__(64) k_filter_prep(const uint8_t* __restrict__ tables,
                                                     uint32_t* __restrict__ w8, float4* __restrict__ fq) {
   __shared__ int s_hi[2], s_lo[2];
+  __shared__ uint32_t s_w[SG_GROUPS];
   const uint32_t q = blockIdx.x, g = threadIdx.x;
   const uint4 row = reinterpret_cast<const uint4*>(tables + (size_t)q * SG_GROUPS * 16)[g];
   int t[16];
@@ -90,8 +95,15 @@ __global__ void __launch_bounds__(64) k_filter_prep(const uint8_t* __restrict__ 
     rhi = max(rhi, v);
     rlo = min(rlo, v);
   }
-  w8[(size_t)q * SG_GROUPS + g] = (uint32_t)(uint8_t)(int8_t)w[0] | ((uint32_t)(uint8_t)(int8_t)w[1] << 8) |
-                                  ((uint32_t)(uint8_t)(int8_t)w[2] << 16) | ((uint32_t)(uint8_t)(int8_t)w[3] << 24);
+  // The weights in the K order of the A rows: K byte 32i + 4s + j holds the weight of prefix
+  // dimension 32i + 8j + s (A column 8i + s is bits s, s+8, s+16, s+24 of code word i). This
+  // thread's dimension 4g + m is bit b = 4(g%8) + m of word g/8: j = b/8, s = b%8.
+  uint8_t* sw = reinterpret_cast<uint8_t*>(s_w);
+#pragma unroll
+  for (int m = 0; m < 4; m++) {
+    const uint32_t b = 4 * (g & 7) + m;
+    sw[32 * (g >> 3) + 4 * (b & 7) + (b >> 3)] = (uint8_t)(int8_t)w[m];
+  }
   rhi = warp_sum_i(rhi);
   rlo = warp_sum_i(rlo);
   if ((g & 31) == 0) {
@@ -99,15 +111,12 @@ __global__ void __launch_bounds__(64) k_filter_prep(const uint8_t* __restrict__ 
     s_lo[g >> 5] = rlo;
   }
   __syncthreads();
+  w8[(size_t)q * SG_GROUPS + g] = s_w[g];
   if (g == 0) fq[q] = make_float4((float)gam, (float)(s_hi[0] + s_hi[1]), (float)(s_lo[0] + s_lo[1]), 0.0f);
 }
 
 // Instruction descriptor of kind::i8: u8 A, s8 B, both K-major, s32 accumulators, M = 128.
 SG_DEV uint32_t idesc_u8s8(uint32_t n) { return (2u << 4) | (1u << 10) | ((n >> 3) << 17) | ((128u >> 4) << 24); }
-
-// The four bits of a nibble as four bytes (bit j at byte j): the terms of the product are at
-// disjoint bit positions, so the multiply is four shifted ORs.
-SG_DEV uint32_t bits_to_bytes(uint32_t nib) { return (nib * 0x00204081u) & 0x01010101u; }
 
 struct TcfArgs {
   const uint4* codes;  // [nslots * 2] slot-major codes
@@ -230,7 +239,9 @@ __global__ void __launch_bounds__(kFThreads, 1) k_scan_tcf(TcfArgs a) {
         const uint32_t thr = *(volatile const uint32_t*)(a.thr + q);
         s_qc[slot][qi] = make_float4(cent, p.z, p.w, __uint_as_float(thr));
         const float4 f = a.fq[q];
-        s_qf[slot][qi] = make_float4(f.x, f.y, f.z, thr ? unord(thr) : -INFINITY);
+        // gamma as an integer; the residual bounds less 1.5 * 2^23 (exact: integers below 2^24)
+        s_qf[slot][qi] = make_float4(__uint_as_float((uint32_t)f.x), __fsub_rn(f.y, kMagic),
+                                     __fsub_rn(f.z, kMagic), thr ? unord(thr) : -INFINITY);
         s_qk[slot][qi] = make_uint2(a.probe_off[(size_t)q * a.P + r], q);
       }
       if (lane == 0) {
@@ -296,13 +307,14 @@ __global__ void __launch_bounds__(kFThreads, 1) k_scan_tcf(TcfArgs a) {
           }
           __syncwarp();
           if (lane == 0) mbar_arrive(&bar_cempty[cs]);
-          // column c holds prefix dimensions 4c..4c+3: nibble c of the code (word c/8)
+          // column 8i + s holds bits s, s+8, s+16, s+24 of code word i as bytes 0/1: prefix
+          // dimensions 32i + s, +8, +16, +24 (k_filter_prep orders the weights the same way)
           const uint32_t wd[8] = {lo.x, lo.y, lo.z, lo.w, hi.x, hi.y, hi.z, hi.w};
 #pragma unroll
           for (int q4 = 0; q4 < 4; q4++) {  // 16 columns (two code words) per store
             uint32_t r[16];
 #pragma unroll
-            for (int c = 0; c < 16; c++) r[c] = bits_to_bytes((wd[2 * q4 + (c >> 3)] >> (4 * (c & 7))) & 15u);
+            for (int c = 0; c < 16; c++) r[c] = (wd[2 * q4 + (c >> 3)] >> (c & 7)) & 0x01010101u;
             tc_st16(tmem + lane_base + st * 64 + 16 * q4, r);
           }
           tc_wait_st();
@@ -394,14 +406,18 @@ __global__ void __launch_bounds__(kFThreads, 1) k_scan_tcf(TcfArgs a) {
               uint32_t v[16];
               tc_ld16(tmem + lane_base + kFDCol + dbuf * kFQG + 32 * cc + 16 * h, v);
               tc_wait_ld();
-              // the threshold as an estimate (ord is monotone, so est >= it exactly when
-              // ord(est) >= the key; a finite mul gives a non-NaN est), -inf for the empty key
+              // The score bound sb = gamma * D + R exactly: gamma * D + 1.5 * 2^23, written into
+              // a float's bits, is that float for |gamma * D| < 2^22 (|D| <= 256 * 127), and
+              // adding R - 1.5 * 2^23 meets an integer below 2^24. The threshold as an estimate
+              // (ord is monotone, so est >= it exactly when ord(est) >= the key; a finite mul
+              // gives a non-NaN est), -inf for the empty key.
 #pragma unroll
               for (int j = 0; j < 16; j++) {
                 const uint32_t col = 32 * cc + 16 * h + j;
                 const float4 qc = s_qc[slot][col];
                 const float4 qf = s_qf[slot][col];
-                const float sb = __fadd_rn(__fmul_rn(qf.x, (float)(int)v[j]), neg ? qf.z : qf.y);
+                const float sb =
+                    __fadd_rn(__uint_as_float(v[j] * __float_as_uint(qf.x) + kMagicBits), neg ? qf.z : qf.y);
                 const float est = __fadd_rn(qc.x, __fmul_rn(mv, __fadd_rn(__fmul_rn(qc.y, sb), qc.z)));
                 adm |= (always || est >= qf.w ? 1u : 0u) << (16 * h + j);
               }

@@ -12,6 +12,9 @@ namespace sg {
 
 constexpr uint64_t kTcWaitNs = 2000000000ull;  // a pipeline wait gives up after 2 s
 constexpr uint32_t kTcSpinLimit = 1u << 30;    // backstop on the number of polls
+// A poll that finds the phase incomplete suspends the thread until the phase completes or this
+// many nanoseconds pass, so waiting warps leave their issue slots to the working ones.
+constexpr uint32_t kTcSuspendNs = 20000;
 
 SG_DEV uint32_t smem_addr(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
 
@@ -24,9 +27,9 @@ SG_DEV void mbar_arrive(uint64_t* bar) {
 SG_DEV bool mbar_test(uint64_t* bar, uint32_t parity) {
   uint32_t ok;
   asm volatile(
-      "{\n.reg .pred p;\nmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\nselp.u32 %0, 1, 0, p;\n}\n"
+      "{\n.reg .pred p;\nmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\nselp.u32 %0, 1, 0, p;\n}\n"
       : "=r"(ok)
-      : "r"(smem_addr(bar)), "r"(parity)
+      : "r"(smem_addr(bar)), "r"(parity), "r"(kTcSuspendNs)
       : "memory");
   return ok != 0;
 }
