@@ -1775,7 +1775,7 @@ int sg_autotune(sg_index* h, uint32_t nq, const float* d_q768, const float* d_q2
     const uint32_t chunks[] = {64, 128, 256, 512};
     const uint32_t seeds[] = {128, 256, 512};
     const uint32_t ctas[] = {1, 2};
-    const uint32_t splits[] = {0, 3, 6};
+    const uint32_t splits[] = {0, 2, 3, 6};
     auto sweep = [&](uint32_t* field, const uint32_t* vals, size_t nv) -> int {
       const uint32_t keep = *field;
       uint32_t best_v = keep;
