@@ -250,16 +250,19 @@ void form_batch(sg_server* srv, Slot& s) {
   s.cfg = sg::index_config(srv->h);
   // the largest batch whose scratch fits this slot's share (one query always goes)
   while (limit > 1 && sg::ctx_bytes(srv->h, s.cfg, p, limit) > budget) limit = (limit + 1) / 2;
-  std::deque<std::shared_ptr<Req>> rest;
-  while (!pend.empty()) {
+  // Requests of these params, oldest first, until the batch is full; the scan stops there (a
+  // backlog of many thousands would otherwise be walked once per batch), and requests of other
+  // params that it passed go back to the front in their order.
+  std::deque<std::shared_ptr<Req>> skipped;
+  while (!pend.empty() && s.batch.size() < limit) {
     auto r = pend.front();
     pend.pop_front();
-    if (s.batch.size() < limit && r->have_q256 == hq && memcmp(&r->p, &p, sizeof p) == 0)
+    if (r->have_q256 == hq && memcmp(&r->p, &p, sizeof p) == 0)
       s.batch.push_back(r);
     else
-      rest.push_back(r);
+      skipped.push_back(r);
   }
-  pend.swap(rest);
+  for (auto it = skipped.rbegin(); it != skipped.rend(); ++it) pend.push_front(*it);
   s.p = p;
   s.limit = limit;
   s.have_q256 = hq;
