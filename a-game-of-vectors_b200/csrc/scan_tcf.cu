@@ -23,7 +23,7 @@
 // rounding is monotone. So the same expression evaluated at s_ub = gamma * D + R_hi (mul >= 0) or
 // at gamma * D + R_lo (mul < 0) is an upper bound of the exact estimate, and a pair whose bound
 // misses the query's admission threshold cannot be admitted. Pairs that pass reserve their entry
-// in the query's candidate buffer (estimate field holding the probe's centroid score), and
+// in the query's candidate buffer (estimate field holding the slot's mul), and
 // k_tc_recheck replaces it with the exact estimate from the exact LUT score. An entry whose exact
 // estimate is below the threshold stays in the buffer with that estimate: the threshold is the
 // cand-th estimate of entries already buffered, so such an entry is never among the best cand
@@ -353,7 +353,9 @@ __global__ void __launch_bounds__(kFThreads, 1) k_scan_tcf(TcfArgs a) {
         // is in flight meanwhile: p_* is the pending chunk (its column ballots in buffer p_buf,
         // its reservation in p_base).
         bool p_on = false;
-        uint32_t p_adm = 0, p_base = 0, p_loc = 0, p_gslot = 0, p_c0 = 0, p_buf = 0;
+        // (p_gslot - b0 * SG_BLOCK is the pending slot's position within its cluster)
+        uint32_t p_adm = 0, p_base = 0, p_gslot = 0, p_c0 = 0, p_buf = 0;
+        float p_mv = 0.0f;
         auto flush = [&]() {
           if (!p_on) return;  // warp-uniform
           uint2* cbp = cb + p_buf * 32;
@@ -365,10 +367,10 @@ __global__ void __launch_bounds__(kFThreads, 1) k_scan_tcf(TcfArgs a) {
             const uint2 qk = s_qk[slot][p_c0 + j];
             const uint32_t pos = bc.x + (uint32_t)__popc(bc.y & lt);
             if (pos < a.cap) {
-              // the probe's centroid score; k_tc_recheck turns it into the exact estimate
-              a.cbuf_est[(size_t)qk.y * a.cap + pos] = __float_as_uint(s_qc[slot][p_c0 + j].x);
+              // the slot's mul; k_tc_recheck turns it into the exact estimate
+              a.cbuf_est[(size_t)qk.y * a.cap + pos] = __float_as_uint(p_mv);
               a.cbuf_info[(size_t)qk.y * a.cap + pos] =
-                  make_uint2(a.global ? a.ids[p_gslot] : qk.x + p_loc, p_gslot);
+                  make_uint2(a.global ? a.ids[p_gslot] : qk.x + (p_gslot - b0 * SG_BLOCK), p_gslot);
             } else {
               a.overflow[qk.y] = 1;
             }
@@ -452,8 +454,8 @@ __global__ void __launch_bounds__(kFThreads, 1) k_scan_tcf(TcfArgs a) {
             p_on = true;
             p_adm = adm;
             p_base = base;
-            p_loc = loc;
             p_gslot = gslot;
+            p_mv = mv;
             p_c0 = 32 * cc;
             p_buf = cbuf;
           }
@@ -488,22 +490,46 @@ __global__ void __launch_bounds__(kFThreads, 1) k_scan_tcf(TcfArgs a) {
 // entries of one query can number hundreds of thousands, so one CTA per query left a long tail),
 // each with the query's u8 tables in shared memory; per entry the 64 nibble lookups of its slot
 // (src/lut.rs:116-126) and the estimate in the reference's operation order (src/rabitq.rs:127-130).
-// A thread takes two entries at a time so their loads are in flight together.
+// The bound pass stored the slot's mul in the entry, and the probe's centroid score comes from
+// the entry's admission key: probe r's slots hold keys probe_off[r] .. probe_off[r+1]-1, so r is
+// the last probe whose offset is at most the key (the query's probe list sits in shared memory).
+// Only the slot's 32-byte code is gathered. A thread takes two entries at a time so their loads
+// are in flight together.
 constexpr uint32_t kRecheckSplit = 8;
 __global__ void __launch_bounds__(256) k_tc_recheck(const uint8_t* __restrict__ tables, const float4* __restrict__ qp,
-                                                    const uint4* __restrict__ codes, const float* __restrict__ mul,
-                                                    const uint32_t* __restrict__ tc_start,
+                                                    const uint4* __restrict__ codes,
+                                                    const uint32_t* __restrict__ probe_off,
+                                                    const float* __restrict__ probe_sc,
+                                                    const uint32_t* __restrict__ probe_n, uint32_t P,
+                                                    uint32_t global, const uint32_t* __restrict__ tc_start,
                                                     const uint32_t* __restrict__ ccount, uint32_t cap,
                                                     uint64_t nslots, uint32_t* __restrict__ cbuf_est,
                                                     const uint2* __restrict__ cbuf_info) {
   __shared__ __align__(16) uint8_t T[SG_GROUPS * 16];
+  extern __shared__ uint32_t s_po[];  // [np] probe offsets, then [np] centroid scores
   const uint32_t q = blockIdx.x;
   const uint32_t lo = tc_start[q], hi = min(ccount[q], cap);
   const uint32_t first = lo + blockIdx.y * blockDim.x + threadIdx.x, stride = gridDim.y * blockDim.x;
   if (lo + blockIdx.y * blockDim.x >= hi) return;  // uniform over the CTA
   reinterpret_cast<uint32_t*>(T)[threadIdx.x] =
       reinterpret_cast<const uint32_t*>(tables + (size_t)q * SG_GROUPS * 16)[threadIdx.x];
+  const uint32_t np = global ? 0u : min(probe_n[q], P);  // global codes: centroid score 0
+  float* s_ps = reinterpret_cast<float*>(s_po + np);
+  for (uint32_t r = threadIdx.x; r < np; r += blockDim.x) {
+    s_po[r] = probe_off[(size_t)q * P + r];
+    s_ps[r] = probe_sc[(size_t)q * P + r];
+  }
   __syncthreads();
+  auto cent_of = [&](uint32_t key) {
+    if (np == 0) return 0.0f;
+    uint32_t lo = 0, hi = np;  // first probe whose offset is above the key
+    while (lo < hi) {
+      const uint32_t mid = (lo + hi) >> 1;
+      if (s_po[mid] <= key) lo = mid + 1;
+      else hi = mid;
+    }
+    return s_ps[lo > 0 ? lo - 1 : 0];
+  };
   const float4 p = qp[q];
   uint32_t* E = cbuf_est + (size_t)q * cap;
   const uint2* I = cbuf_info + (size_t)q * cap;
@@ -523,21 +549,22 @@ __global__ void __launch_bounds__(256) k_tc_recheck(const uint8_t* __restrict__ 
     const uint32_t i2 = i + stride;
     const bool two = i2 < hi;
     // only an aborted bound pass leaves an entry unwritten (slot >= nslots)
-    const uint32_t gs = I[i].y, gs2 = two ? I[i2].y : 0xFFFFFFFFu;
+    const uint2 in = I[i], in2 = two ? I[i2] : make_uint2(0u, 0xFFFFFFFFu);
+    const uint32_t gs = in.y, gs2 = in2.y;
     const bool ok = gs < nslots, ok2 = gs2 < nslots;
     uint4 a0 = make_uint4(0, 0, 0, 0), a1 = a0, b0 = a0, b1 = a0;
     float m = 0.0f, m2 = 0.0f, ce = 0.0f, ce2 = 0.0f;
     if (ok) {
       a0 = codes[2 * (size_t)gs];
       a1 = codes[2 * (size_t)gs + 1];
-      m = mul[gs];
-      ce = __uint_as_float(E[i]);
+      m = __uint_as_float(E[i]);
+      ce = cent_of(in.x);
     }
     if (ok2) {
       b0 = codes[2 * (size_t)gs2];
       b1 = codes[2 * (size_t)gs2 + 1];
-      m2 = mul[gs2];
-      ce2 = __uint_as_float(E[i2]);
+      m2 = __uint_as_float(E[i2]);
+      ce2 = cent_of(in2.x);
     }
     if (ok) E[i] = __float_as_uint(estimate(ce, m, score(a0, a1)));
     if (ok2) E[i2] = __float_as_uint(estimate(ce2, m2, score(b0, b1)));
@@ -585,8 +612,9 @@ int launch_scan_tcf(const DevIndex& ix, Workspace& w, uint32_t nq, uint32_t P, c
   // entries from tc_start[q] on are the bound pass's (earlier ones are exact already)
   cudaMemcpyAsync(w.tc_start, w.ccount, (size_t)nq * 4, cudaMemcpyDeviceToDevice, st);
   k_scan_tcf<<<sms, kFThreads, tcf_smem_bytes(), st>>>(a);
-  k_tc_recheck<<<dim3(nq, kRecheckSplit), 256, 0, st>>>(w.tables, w.qp, reinterpret_cast<const uint4*>(ix.blocks_tc), ix.mul,
-                                   w.tc_start, w.ccount, w.cbuf_per_q, ix.nslots, w.cbuf_est, w.cbuf_info);
+  k_tc_recheck<<<dim3(nq, kRecheckSplit), 256, (size_t)(ix.global ? 0 : P) * 8, st>>>(
+      w.tables, w.qp, reinterpret_cast<const uint4*>(ix.blocks_tc), w.probe_off, w.probe_sc, w.probe_n, P,
+      ix.global, w.tc_start, w.ccount, w.cbuf_per_q, ix.nslots, w.cbuf_est, w.cbuf_info);
   return 2;
 }
 
