@@ -522,13 +522,13 @@ __global__ void __launch_bounds__(256) k_tc_recheck(const uint8_t* __restrict__ 
   __syncthreads();
   auto cent_of = [&](uint32_t key) {
     if (np == 0) return 0.0f;
-    uint32_t lo = 0, hi = np;  // first probe whose offset is above the key
-    while (lo < hi) {
-      const uint32_t mid = (lo + hi) >> 1;
-      if (s_po[mid] <= key) lo = mid + 1;
-      else hi = mid;
+    uint32_t rl = 0, rh = np;  // the first probe whose offset is above the key
+    while (rl < rh) {
+      const uint32_t mid = (rl + rh) >> 1;
+      if (s_po[mid] <= key) rl = mid + 1;
+      else rh = mid;
     }
-    return s_ps[lo > 0 ? lo - 1 : 0];
+    return s_ps[rl > 0 ? rl - 1 : 0];
   };
   const float4 p = qp[q];
   uint32_t* E = cbuf_est + (size_t)q * cap;
