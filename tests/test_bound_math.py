@@ -136,3 +136,23 @@ def test_estimate_at_the_score_bound_bounds_the_estimate(seed):
                 exact = est32(a, b, cent, mul, s)
                 assert exact == np.float32(O.estimate(a, b, cent, mul, s))
                 assert est32(a, b, cent, mul, sb) >= exact
+
+
+def test_admission_key_finds_its_probe():
+    """k_tc_recheck's lookup: probe r's slots hold admission keys probe_off[r] ..
+    probe_off[r] + slots(r) - 1 (offsets in probe order, src/ivf.rs:663-675), so the last probe
+    whose offset is at most a key owns it, with empty clusters (equal offsets) in between."""
+    rng = np.random.default_rng(21)
+    for _ in range(50):
+        sizes = rng.integers(0, 5, rng.integers(1, 40)) * 32  # padded slots; zero = empty cluster
+        off = np.concatenate([[0], np.cumsum(sizes)[:-1]]).astype(np.int64)
+        for r, n in enumerate(sizes):
+            for key in range(off[r], off[r] + n):
+                lo, hi = 0, len(off)  # the kernel's search: the first offset above the key
+                while lo < hi:
+                    mid = (lo + hi) >> 1
+                    if off[mid] <= key:
+                        lo = mid + 1
+                    else:
+                        hi = mid
+                assert lo - 1 == r
